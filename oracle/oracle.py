@@ -1,0 +1,209 @@
+"""ctypes wrapper of the FP64 oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
+the checker and by bench.py's CPU-baseline leg.  The product never imports it.
+PARITY UNPINNED: see pfem2_oracle.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "_build", "liboracle.so")
+
+ORDER_ID = 0
+ORDER_VECTOR = 1
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("q", C.c_int32 * 3),
+        ("max_per_part", C.c_int32),
+        ("substeps", C.c_int32),
+        ("dt", C.c_double),
+        ("removal_order", C.c_int32),
+        ("removal_seed", C.c_uint32),
+        ("n_threads", C.c_int32),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("n_particles", C.c_int64),
+        ("lost", C.c_int64),
+        ("removed", C.c_int64),
+        ("seeded", C.c_int64),
+        ("map_failures", C.c_int64),
+        ("near_face", C.c_int64),
+        ("searched", C.c_int64),
+        ("nan_dofs", C.c_int64),
+        ("next_id", C.c_uint32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_SO):
+            build()
+        L = C.CDLL(_SO)
+        P = C.c_void_p
+        dp = np.ctypeslib.ndpointer(np.float64, flags="C")
+        ip = np.ctypeslib.ndpointer(np.int32, flags="C")
+        up = np.ctypeslib.ndpointer(np.uint32, flags="C")
+        L.orc_create.restype = P
+        L.orc_create.argtypes = [C.c_int, C.POINTER(Params)]
+        L.orc_destroy.argtypes = [P]
+        L.orc_set_mesh.argtypes = [P, C.c_int64, C.c_int64, C.c_int64, dp, ip, ip]
+        L.orc_vertex_map_size.restype = C.c_int64
+        L.orc_vertex_map_size.argtypes = [P]
+        L.orc_get_vertex_maps.argtypes = [P, ip, ip, dp]
+        for f in (L.orc_seed, L.orc_move, L.orc_project):
+            f.argtypes = [P, dp]
+        L.orc_correct.argtypes = [P, dp, dp]
+        L.orc_n_particles.restype = C.c_int64
+        L.orc_n_particles.argtypes = [P]
+        L.orc_get_particles.argtypes = [P, up, ip, dp, dp, dp]
+        L.orc_set_particles.argtypes = [P, C.c_int64, up, ip, dp, dp, dp, C.c_uint32]
+        L.orc_get_stats.argtypes = [P, C.POINTER(Stats)]
+        L.orc_reset_stats.argtypes = [P]
+        L.orc_shape_values.argtypes = [C.c_int, dp, dp]
+        L.orc_forward_map.argtypes = [C.c_int, dp, dp, dp]
+        L.orc_inverse_map.argtypes = [C.c_int, dp, dp, dp]
+        L.orc_key.restype = C.c_uint32
+        L.orc_key.argtypes = [C.c_uint32, C.c_uint32]
+        _lib = L
+    return _lib
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class Oracle:
+    """FP64 restatement of pfem2ParticleHandler (src/pfem2particlehandler.h:17-71)."""
+
+    def __init__(self, mesh, q, max_per_part, substeps, dt, removal_order=ORDER_ID, removal_seed=0,
+                 n_threads=1):
+        self.L = lib()
+        self.dim = mesh.dim
+        p = Params()
+        for d in range(3):
+            p.q[d] = q[d] if d < len(q) else 1
+        p.max_per_part = max_per_part
+        p.substeps = substeps
+        p.dt = dt
+        p.removal_order = removal_order
+        p.removal_seed = removal_seed
+        p.n_threads = n_threads
+        self.h = self.L.orc_create(self.dim, C.byref(p))
+        if not self.h:
+            raise ValueError("orc_create failed")
+        self.mesh = mesh
+        rc = self.L.orc_set_mesh(self.h, mesh.n_cells, mesh.n_verts, mesh.n_dofs, _c(mesh.vertices, np.float64),
+                                 _c(mesh.cells, np.int32), _c(mesh.cell_dofs, np.int32))
+        if rc:
+            raise ValueError(f"orc_set_mesh failed: {rc}")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.orc_destroy(self.h)
+            self.h = None
+
+    def vertex_maps(self):
+        tot = self.L.orc_vertex_map_size(self.h)
+        off = np.zeros(self.mesh.n_verts + 1, np.int32)
+        cells = np.zeros(max(tot, 1), np.int32)
+        dirs = np.zeros((max(tot, 1), self.dim))
+        self.L.orc_get_vertex_maps(self.h, off, cells, dirs)
+        return off, cells[:tot], dirs[:tot]
+
+    def _V(self, V):
+        return _c(V, np.float64).reshape(-1)
+
+    def seed(self, V):
+        assert self.L.orc_seed(self.h, self._V(V)) == 0
+
+    def correct(self, V, Vold):
+        assert self.L.orc_correct(self.h, self._V(V), self._V(Vold)) == 0
+
+    def move(self, V):
+        assert self.L.orc_move(self.h, self._V(V)) == 0
+
+    def project(self):
+        out = np.zeros(self.dim * self.mesh.n_dofs)
+        assert self.L.orc_project(self.h, out) == 0
+        return out.reshape(self.dim, self.mesh.n_dofs)
+
+    def step(self, V, Vold):
+        self.correct(V, Vold)
+        self.move(V)
+        return self.project()
+
+    def particles(self):
+        n = self.L.orc_n_particles(self.h)
+        ids = np.zeros(n, np.uint32)
+        cell = np.zeros(n, np.int32)
+        x = np.zeros((n, self.dim))
+        xi = np.zeros((n, self.dim))
+        v = np.zeros((n, self.dim))
+        self.L.orc_get_particles(self.h, ids, cell, x, xi, v)
+        return {"id": ids, "cell": cell, "x": x, "xi": xi, "v": v}
+
+    def set_particles(self, P, next_id):
+        n = len(P["id"])
+        assert self.L.orc_set_particles(self.h, n, _c(P["id"], np.uint32), _c(P["cell"], np.int32),
+                                        _c(P["x"], np.float64), _c(P["xi"], np.float64),
+                                        _c(P["v"], np.float64), next_id) == 0
+
+    def stats(self):
+        s = Stats()
+        self.L.orc_get_stats(self.h, C.byref(s))
+        return s.as_dict()
+
+    def reset_stats(self):
+        self.L.orc_reset_stats(self.h)
+
+
+def shape_values(dim, xi):
+    N = np.zeros(1 << dim)
+    lib().orc_shape_values(dim, _c(xi, np.float64), N)
+    return N
+
+
+def _pad(X, dim):
+    Xp = np.zeros((1 << dim, 3))
+    Xp[:, :dim] = X
+    return Xp.reshape(-1)
+
+
+def forward_map(X, xi):
+    dim = X.shape[1]
+    out = np.zeros(dim)
+    lib().orc_forward_map(dim, _pad(X, dim), _c(xi, np.float64), out)
+    return out
+
+
+def inverse_map(X, p):
+    dim = X.shape[1]
+    out = np.zeros(dim)
+    rc = lib().orc_inverse_map(dim, _pad(X, dim), _c(p, np.float64), out)
+    return (out if rc == 0 else None)
+
+
+def key(i, seed):
+    return lib().orc_key(i, seed)

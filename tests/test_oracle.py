@@ -1,0 +1,225 @@
+"""Known-answer tests of the FP64 oracle (CPU).
+
+The reference ships no tests or golden data, so the oracle is pinned by
+mathematics: Q1 reproduction, exact Euler transport on affine cells,
+partition of unity in the projection, the seeding pattern, the count cap
+(max+1 survivors per part, src/pfem2particlehandler.cpp:372) and
+inverse/forward map round trips.
+"""
+import io
+
+import numpy as np
+import pytest
+
+from oracle.oracle import ORDER_ID, ORDER_VECTOR, Oracle, forward_map, inverse_map, key, shape_values
+from pfem2dealii_b200 import mesh as M
+
+
+def test_shape_partition_and_linear_reproduction():
+    rng = np.random.default_rng(1)
+    for dim in (2, 3):
+        corners = np.array([[(i >> d) & 1 for d in range(dim)] for i in range(1 << dim)], float)
+        a = rng.normal(size=dim)
+        for _ in range(50):
+            xi = rng.uniform(0, 1, dim)
+            N = shape_values(dim, xi)
+            assert abs(N.sum() - 1) < 1e-15
+            # multilinear field reproduced: f = a.xi + xi0*xi1
+            f = corners @ a + corners[:, 0] * corners[:, 1]
+            assert abs(N @ f - (a @ xi + xi[0] * xi[1])) < 1e-14
+
+
+def _random_cell(rng, dim, jitter):
+    X = np.array([[(i >> d) & 1 for d in range(dim)] for i in range(1 << dim)], float)
+    return X + rng.uniform(-jitter, jitter, X.shape)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_inverse_map_round_trip(dim):
+    rng = np.random.default_rng(dim)
+    for _ in range(200):
+        X = _random_cell(rng, dim, 0.2) * rng.uniform(0.01, 10) + rng.normal(size=dim)
+        xi = rng.uniform(0, 1, dim)
+        p = forward_map(X, xi)
+        back = inverse_map(X, p)
+        assert back is not None
+        assert np.max(np.abs(back - xi)) < 1e-10
+
+
+def test_inverse_map_outside_point():
+    X = np.array([[0, 0], [1, 0], [0, 1], [1, 1]], float)
+    back = inverse_map(X, np.array([1.5, 0.25]))
+    assert back is not None and abs(back[0] - 1.5) < 1e-14  # affine: exact, outside
+    X3 = _random_cell(np.random.default_rng(0), 3, 0.1)
+    p = forward_map(X3, np.array([1.2, 0.5, -0.1]))
+    b = inverse_map(X3, p)
+    assert b is not None and np.allclose(b, [1.2, 0.5, -0.1], atol=1e-9)
+
+
+def test_key_is_identity_without_seed_and_bijective_with_seed():
+    assert [key(i, 0) for i in range(5)] == [0, 1, 2, 3, 4]
+    ks = {key(i, 12345) for i in range(20000)}
+    assert len(ks) == 20000
+
+
+def _channel(nx=16, ny=4):
+    return M.hyper_rectangle((0.0, 0.0), (4.0, 1.0), (nx, ny))
+
+
+def test_seeding_pattern():
+    m = _channel()
+    V = M.field_at_dofs(m, M.channel_profile())
+    o = Oracle(m, (4, 3), 2, 4, 0.01)
+    o.seed(V)
+    P = o.particles()
+    assert len(P["id"]) == m.n_cells * 12
+    assert np.array_equal(P["id"], np.arange(1, m.n_cells * 12 + 1))
+    assert np.array_equal(np.bincount(P["cell"]), np.full(m.n_cells, 12))
+    xi = P["xi"][:12]
+    exp = np.array([[(i + 0.5) / 4, (j + 0.5) / 3] for i in range(4) for j in range(3)])  # x outermost
+    assert np.allclose(xi, exp, atol=1e-15)
+    # location = F(xi) and velocity = interpolated V
+    X = m.vertices[m.cells[P["cell"]]]
+    xq = np.einsum("pi,pid->pd", np.array([shape_values(2, z) for z in P["xi"]]), X)
+    assert np.allclose(P["x"], xq, atol=1e-14)
+    N = np.array([shape_values(2, z) for z in P["xi"]])
+    vq = np.einsum("pi,dpi->pd", N, V[:, m.cell_dofs[P["cell"]]])
+    assert np.allclose(P["v"], vq, atol=1e-15)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_uniform_flow_is_exact_on_affine_cells(dim):
+    if dim == 2:
+        m = M.hyper_rectangle((0.0, 0.0), (2.0, 1.0), (8, 4))
+        u = np.array([0.3, -0.1])
+    else:
+        m = M.hyper_rectangle((0.0, 0.0, 0.0), (2.0, 1.0, 1.0), (6, 3, 3))
+        u = np.array([0.3, -0.1, 0.05])
+    V = np.repeat(u[:, None], m.n_dofs, axis=1)
+    o = Oracle(m, (2,) * dim, 100, 3, 0.05)
+    o.seed(V)
+    P0 = o.particles()
+    o.move(V)
+    P1 = o.particles()
+    alive = np.isin(P0["id"], P1["id"])
+    x0 = P0["x"][alive][np.argsort(P0["id"][alive])]
+    x1 = P1["x"][np.isin(P1["id"], P0["id"])]
+    x1 = x1[np.argsort(P1["id"][np.isin(P1["id"], P0["id"])])]
+    assert np.allclose(x1, x0 + u * 0.05, atol=1e-13)
+    # relocated reference coordinates are consistent with the positions
+    X = m.vertices[m.cells[P1["cell"]]]
+    xq = np.einsum("pi,pid->pd", np.array([shape_values(dim, z) for z in P1["xi"]]), X)
+    assert np.allclose(xq, P1["x"], atol=1e-13)
+    assert np.all((P1["xi"] >= 0) & (P1["xi"] <= 1))
+
+
+def test_projection_partition_of_unity():
+    m = M.turek_channel(n_t=16, n_r=8, n_x=40)
+    c = np.array([0.7, -0.2])
+    V = np.repeat(c[:, None], m.n_dofs, axis=1)
+    o = Oracle(m, (2, 2), 2, 1, 1e-3)
+    o.seed(V)
+    Vp = o.project()
+    assert np.allclose(Vp, V, atol=1e-14)
+
+
+def test_count_cap_keeps_max_plus_one():
+    # all particles squeezed into one cell part: max/part = 2 keeps 3
+    m = _channel(4, 2)
+    V = np.zeros((2, m.n_dofs))
+    o = Oracle(m, (4, 4), 2, 1, 0.0)
+    n = 10
+    X = m.vertices[m.cells[5]]
+    xi = np.tile([[0.1, 0.1]], (n, 1))
+    x = np.array([forward_map(X, z) for z in xi])
+    P = {"id": np.arange(1, n + 1, dtype=np.uint32), "cell": np.full(n, 5, np.int32), "x": x, "xi": xi,
+         "v": np.zeros((n, 2))}
+    for order in (ORDER_ID, ORDER_VECTOR):
+        o = Oracle(m, (4, 4), 2, 1, 0.0, removal_order=order)
+        o.set_particles(P, n)
+        o.move(V)
+        Q = o.particles()
+        st = o.stats()
+        assert st["removed"] == 7 and st["seeded"] == 15
+        assert np.sum(Q["cell"] == 5) == 3 + 15
+        assert set(np.unique(Q["cell"])) == {5}  # empty cells are never reseeded
+        kept = sorted(Q["id"][Q["id"] <= n])
+        if order == ORDER_ID:
+            assert kept == [1, 2, 3]
+        else:
+            # swap-with-back: 1,2,3 counted, 4 replaced by 10 (removed), 9, 8, ...
+            assert kept == [1, 2, 3]
+        new = np.sort(Q["id"][Q["id"] > n])
+        assert np.array_equal(new, np.arange(n + 1, n + 16))
+
+
+def test_vector_and_id_order_agree_on_counts():
+    m = _channel(32, 8)
+    V = M.field_at_dofs(m, M.channel_profile())
+    res = []
+    for order in (ORDER_ID, ORDER_VECTOR):
+        o = Oracle(m, (3, 3), 1, 4, 0.02, removal_order=order)
+        o.seed(V)
+        o.step(V, 0.9 * V)
+        P = o.particles()
+        res.append((np.bincount(P["cell"], minlength=m.n_cells), o.stats()))
+    assert np.array_equal(res[0][0], res[1][0])
+    for k in ("lost", "removed", "seeded", "n_particles"):
+        assert res[0][1][k] == res[1][1][k]
+
+
+def test_closed_divergence_free_flow_loses_nothing():
+    m = M.perturbed_cube(6, amplitude=0.1, seed=0)
+    V = M.field_at_dofs(m, M.taylor_green_3d())
+    o = Oracle(m, (2, 2, 2), 2, 3, 0.05)
+    o.seed(V)
+    for _ in range(5):
+        o.step(V, V)
+    assert o.stats()["lost"] == 0
+
+
+def test_vertex_maps_match_host_builder():
+    for m in (_channel(8, 3), M.perturbed_cube(3), M.turek_channel(8, 4, 10)):
+        o = Oracle(m, (2,) * m.dim, 2, 1, 0.1)
+        off, cells, dirs = o.vertex_maps()
+        off2, cells2, dirs2 = M.vertex_maps(m)
+        assert np.array_equal(off, off2) and np.array_equal(cells, cells2)
+        assert np.array_equal(dirs, dirs2)  # bit-exact
+
+
+def test_threaded_oracle_matches_serial_state():
+    m = M.perturbed_cube(5, amplitude=0.1, seed=3)
+    V = M.field_at_dofs(m, M.taylor_green_3d())
+    outs = []
+    for nt in (1, 4):
+        o = Oracle(m, (2, 2, 2), 1, 3, 0.1, n_threads=nt)
+        o.seed(V)
+        for _ in range(3):
+            Vp = o.step(V, 0.5 * V)
+        outs.append((o.particles(), Vp))
+    a, b = outs
+    for k in ("id", "cell", "x", "xi", "v"):
+        assert np.array_equal(a[0][k], b[0][k])
+    assert np.allclose(a[1], b[1], rtol=1e-13, atol=1e-13)
+
+
+def test_unv_round_trip():
+    m = M.turek_channel(8, 4, 10)
+    buf = io.StringIO()
+    M.write_unv(m, buf)
+    buf.seek(0)
+    r = M.read_unv(buf)
+    assert r.n_cells == m.n_cells and r.n_verts == m.n_verts
+    assert np.allclose(r.vertices, m.vertices, rtol=0, atol=1e-15)
+    assert np.array_equal(r.cells, m.cells)
+
+
+def test_reference_turek_mesh_reads_if_present():
+    import os
+
+    p = "/root/reference/cases/TurekBenchmark/Mesh3.tgz"
+    if not os.path.exists(p):
+        pytest.skip("reference tree not mounted")
+    m = M.read_unv(p)
+    assert m.n_cells == 60450 and m.n_verts == 61075
+    assert np.allclose(m.vertices.min(0), [0, 0]) and np.allclose(m.vertices.max(0), [2.2, 0.41])
