@@ -1,0 +1,357 @@
+"""Benchmark of the PFEM-2 particle path on B200.
+
+Workload: 3D duct [0,8]x[0,1]^2, 128x32x32 Q1 hexes (131,072 cells), 27
+particles per cell on a 3x3x3 reference grid (3,538,944 particles), max 2
+per cell part, 3 sub-steps, dt = 2e-3, u = 16 y(1-y) z(1-z), Vold = 0.9 V
+(the velocity correction is exercised).  A step is one time step of the
+reference loop (src/pfem2solver.cpp:162-164): correct + move (3 sub-steps,
+relocation, count correction) + project, over every particle.
+
+value   : FP32 form, particle-steps/s, nodal velocities resident on the device
+e2e     : FP32 form through the host C ABI (pfem2gpu_correct/move/project
+          with pinned host vectors; H2D of V and Vold, D2H of the projected V
+          inside the timed region)
+fp64    : the plain FP64 form, same workload, device-resident
+roofline: the dominant kernel (advect) against measured HBM bandwidth
+
+`--impl reference` times the CPU restatement of the reference's particle
+path (the reference itself needs deal.II/Trilinos/MPI, absent here) on all
+host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s FP32 vs FP64 form at <=1e-4 rel L2; HBM GB/s; bwd/fwd time"
+UNIT = "particle-steps/s"
+WORKLOAD = "3D duct 128x32x32 Q1 hexes, 27 ppc (3,538,944 particles), max 2/part, 3 sub-steps, dt 2e-3"
+
+# Algorithmic bytes per particle of the advect kernel (3D): read cell u32 +
+# xi[3] + v[3], write xi[3] + v[3] + key u32 + slot u32.
+ADVECT_BYTES = {"fp32": 4 + 12 + 12 + 12 + 12 + 4 + 4, "fp64": 4 + 24 * 3 + 24 * 3 + 4 + 4}
+# Per particle-step, whole step (compulsory passes 5s + 8, s = 4 + 2*dim*w).
+STEP_BYTES = {"fp32": 5 * (4 + 24) + 8, "fp64": 5 * (4 + 48) + 8}
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.1)
+            self.proc.terminate()
+            out, _ = self.proc.communicate(timeout=10)
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self, busy_mhz=None):
+        rows = []
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        mx = max(r[1] for r in rows)
+        load = [r for r in rows if r[0] > 0.5 * mx] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in load for i, v in enumerate(r[2]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in load), "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def build_case():
+    from pfem2dealii_b200 import mesh as M
+    from pfem2dealii_b200.handler import ParticleParams
+
+    m = M.hyper_rectangle((0.0, 0.0, 0.0), (8.0, 1.0, 1.0), (128, 32, 32), "duct")
+    V = M.field_at_dofs(m, M.duct_profile(1.0))
+    prm = ParticleParams(particles_per_cell=(3, 3, 3), max_particles_per_cell_part=2,
+                         particle_integration_steps=3, time_step=2e-3)
+    return m, V, 0.9 * V, prm
+
+
+def timed_device_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, torch, profile=False):
+    """Seed, warm up, then time `steps` device-resident steps with CUDA events
+    on the handler's stream."""
+    g = handler_cls(3, prm, precision)
+    g.initialize_maps(m)
+    dev = torch.device("cuda:0")
+    dV = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
+    dVo = torch.from_numpy(np.ascontiguousarray(Vold)).to(dev)
+    dout = torch.empty_like(dV)
+    g.seed_particles_device(dV)
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+    for _ in range(warmup):
+        g.correct_particle_velocity_device(dV, dVo)
+        g.move_particles_device(None)
+        g.project_particle_fields_device(dout)
+    g.synchronize()
+    if profile:
+        g.profile(True)
+    s0 = g.stats()
+    l0 = g.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        g.correct_particle_velocity_device(dV, dVo)
+        g.move_particles_device(None)
+        g.project_particle_fields_device(dout)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    s1 = g.stats()
+    res = {"ms": ms, "particle_steps": s1["particle_steps"] - s0["particle_steps"],
+           "launches": g.launch_count() - l0, "n_particles": s1["n_particles"], "stats": s1,
+           "V": dout.cpu().numpy()}
+    if profile:
+        res["profile"] = g.profile_report()
+        g.profile(False)
+    g.close()
+    return res
+
+
+def timed_host_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, torch):
+    """The same steps through the host C ABI with pinned vectors: H2D of V
+    and Vold, D2H of the projected velocity, every step."""
+    g = handler_cls(3, prm, precision)
+    g.initialize_maps(m)
+    hV = torch.from_numpy(np.ascontiguousarray(V)).pin_memory()
+    hVo = torch.from_numpy(np.ascontiguousarray(Vold)).pin_memory()
+    hout = torch.empty_like(hV).pin_memory()
+    L, h = g.L, g.h
+    import ctypes as C
+
+    pV, pVo, pout = C.c_void_p(hV.data_ptr()), C.c_void_p(hVo.data_ptr()), C.c_void_p(hout.data_ptr())
+    g._ck(L.pfem2gpu_seed(h, pV))
+
+    def step():
+        g._ck(L.pfem2gpu_correct(h, pV, pVo))
+        g._ck(L.pfem2gpu_move(h, None))
+        g._ck(L.pfem2gpu_project(h, pout))
+
+    for _ in range(warmup):
+        step()
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+    s0 = g.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    s1 = g.stats()
+    g.close()
+    nbytes = V.size * 8
+    return {"ms": ms, "particle_steps": s1["particle_steps"] - s0["particle_steps"], "h2d": 2 * nbytes,
+            "d2h": nbytes}
+
+
+def cpu_baseline(m, V, Vold, prm, budget_s=20.0, max_steps=None):
+    """The FP64 CPU restatement (reference removal order) on all host cores,
+    on the full workload; steps until the time budget is spent."""
+    from oracle.oracle import ORDER_VECTOR, Oracle
+
+    cores = os.cpu_count() or 1
+    o = Oracle(m, prm.particles_per_cell, prm.max_particles_per_cell_part, prm.particle_integration_steps,
+               prm.time_step, removal_order=ORDER_VECTOR, n_threads=cores)
+    o.seed(V)
+    done, ps, t = 0, 0, 0.0
+    while t < budget_s and (max_steps is None or done < max_steps):
+        n = o.stats()["n_particles"]
+        t0 = time.perf_counter()
+        o.step(V, Vold)
+        t += time.perf_counter() - t0
+        ps += n
+        done += 1
+    return {"value": ps / t, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{done} time step(s) of the full {WORKLOAD} workload, FP64 restatement, "
+                      f"{cores} threads (not the reference binary: deal.II/Trilinos/MPI absent)",
+            "steps": done, "seconds": t}
+
+
+def rel_l2(a, b):
+    m = np.isfinite(a) & np.isfinite(b)
+    return float(np.linalg.norm((a - b)[m]) / np.linalg.norm(a[m]))
+
+
+def load_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    m, V, Vold, prm = build_case()
+    budget = 60.0
+    cb = cpu_baseline(m, V, Vold, prm, budget_s=budget, max_steps=max(1, args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": cb["steps"], "warmup": 0, "ms_per_step": 1000.0 * cb["seconds"] / cb["steps"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "form": "fp64 CPU restatement"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    rank, world, local = env_rank()
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    from pfem2dealii_b200.handler import ParticleHandler
+
+    m, V, Vold, prm = build_case()
+    gpu_index = torch.cuda.current_device()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # FP32 form, device-resident: the headline value
+    barrier()
+    with ClockSampler(gpu_index) as clk:
+        r32 = timed_device_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch)
+        barrier()
+    ms = r32["ms"]
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        ps = torch.tensor([float(r32["particle_steps"])], device="cuda")
+        torch.distributed.all_reduce(ps)
+        total_ps = float(ps.item())
+    else:
+        total_ps = float(r32["particle_steps"])
+    value = total_ps / (ms / 1000.0)
+    # FP64 form (plain) and the FP32 vs FP64 error after the same steps
+    r64 = timed_device_run(ParticleHandler, m, V, Vold, prm, "fp64", args.steps, args.warmup, torch)
+    v64 = r64["particle_steps"] / (r64["ms"] / 1000.0)
+    err = rel_l2(r64["V"], r32["V"])
+    # kernel-level timing pass (per-launch CUDA events)
+    rp = timed_device_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch, profile=True)
+    prof = rp["profile"]
+    adv_ms, adv_n = prof.get("advect", [0.0, 1])
+    per_launch_particles = rp["particle_steps"] / max(adv_n, 1)
+    peak, peak_kind = load_peak()
+    achieved = ADVECT_BYTES["fp32"] * per_launch_particles / (adv_ms / adv_n / 1000.0) / 1e9
+    step_ms_prof = sum(v[0] for v in prof.values()) / args.steps
+    # end to end through the host ABI
+    re2e = timed_host_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch)
+    e2e_value = re2e["particle_steps"] / (re2e["ms"] / 1000.0)
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+    cb = None
+    if not args.no_cpu_baseline:
+        cb = cpu_baseline(m, V, Vold, prm, budget_s=args.cpu_budget, max_steps=3)
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "form": "fp32", "particles": r32["n_particles"],
+                   "l2": "inputs larger than L2 (particle arrays ~300 MB per form)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "fp64": {"value": v64, "unit": UNIT, "ms_per_step": r64["ms"] / args.steps, "dtype": "f64",
+                 "fp32_over_fp64": value / v64},
+        "fp32_vs_fp64_rel_l2": {"projected_velocity": err, "tolerance": 1e-4},
+        "step_effective_gbs": STEP_BYTES["fp32"] * value / 1e9,
+        "roofline": {"bound": "hbm", "kernel": "k_advect32<3>", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "bytes_per_particle": ADVECT_BYTES["fp32"], "peak_source": peak_kind,
+                     "launch_ms": adv_ms / adv_n},
+        "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items())},
+        "profiled_ms_per_step": step_ms_prof,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": re2e["h2d"],
+                "d2h_bytes_per_step": re2e["d2h"], "ms_per_step": re2e["ms"] / args.steps},
+        "gpu_launches": r32["launches"],
+        "clocks": clk.summary(),
+        "stats": {k: r32["stats"][k] for k in ("n_particles", "lost", "removed", "seeded", "searched",
+                                               "fallback64", "error_flags")},
+    }
+    if cb:
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

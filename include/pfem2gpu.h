@@ -1,0 +1,135 @@
+/*
+ * pfem2gpu.h -- C ABI of the B200 PFEM-2 particle path.
+ *
+ * Drop-in for the particle cycle of pfem2ParticleHandler<dim>
+ * (src/pfem2particlehandler.h:17-71 of the reference): seeding, velocity
+ * correction, sub-stepped transport with relocation and count correction,
+ * and the particle-to-mesh velocity projection.  The FEM step stays with the
+ * caller; nodal velocities cross this boundary once per call as plain
+ * component-major double arrays, V[d * n_dofs + dof], the layout of the
+ * reference's std::array<TrilinosWrappers::MPI::Vector, dim>.
+ *
+ * Conventions: every function returns PFEM2GPU_OK (0) or an error code; no
+ * C++ exception crosses the ABI.  One handle is used from one host thread.
+ * All device work of a handle runs in order on the handle's CUDA stream, on
+ * the device that was current at pfem2gpu_create.  Host input arrays are
+ * read before the call returns unless they were registered with
+ * pfem2gpu_host_register, in which case they must stay unchanged until the
+ * next call that returns host data (project, get_particles, get_stats,
+ * synchronize).
+ */
+#ifndef PFEM2GPU_H
+#define PFEM2GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PFEM2GPU_OK 0
+#define PFEM2GPU_ERR_ARG 1        /* invalid argument or size */
+#define PFEM2GPU_ERR_CUDA 2       /* CUDA runtime error (details: pfem2gpu_last_error) */
+#define PFEM2GPU_ERR_STATE 3      /* call out of order (no mesh, no particles, ...) */
+#define PFEM2GPU_ERR_CAPACITY 4   /* particle arrays full; raise params.capacity */
+#define PFEM2GPU_ERR_NOMEM 5      /* device allocation failed */
+#define PFEM2GPU_ERR_NODEVICE 6   /* no CUDA device */
+#define PFEM2GPU_ERR_DEVICE 7     /* a kernel reported bad input (see stats.error_flags) */
+
+#define PFEM2GPU_FP64 0           /* plain form: the reference's arithmetic, FP64 state */
+#define PFEM2GPU_FP32 1           /* FP32 state and interpolation, FP64 for face crossings */
+
+/* Particle parameters; the names follow the reference's .prm keys
+ * (src/pfem2parameterhandler.cpp:64-74, 40). */
+typedef struct pfem2gpu_params {
+    int32_t particles_per_cell[3];        /* "Number of particles in the x/y/z direction" */
+    int32_t max_particles_per_cell_part;  /* "Maximum number of particles per cell part" */
+    int32_t particle_integration_steps;   /* "Particle integration steps" (0 -> 1) */
+    double time_step;                     /* "Time step" (sub-step = time_step / steps) */
+    uint32_t removal_seed;                /* over-full parts keep the smallest key(id); 0: key = id */
+    int32_t empty_dof_policy;             /* 0: reference (0/0 = NaN at DoFs no particle reaches); 1: keep input V */
+    int64_t capacity;                     /* particle capacity (0: 2 x cells x parts) */
+} pfem2gpu_params;
+
+typedef struct pfem2gpu_stats {
+    int64_t n_particles;
+    int64_t lost;          /* deleted by relocation (left the mesh) */
+    int64_t removed;       /* deleted by count correction */
+    int64_t seeded;        /* inserted by count correction */
+    int64_t map_failures;  /* inverse-map failures (ExcTransformationFailed) */
+    int64_t near_face;     /* relocations ending within 1e-12 of a face */
+    int64_t searched;      /* relocations that needed the vertex-patch search */
+    int64_t nan_dofs;      /* DoFs without particle weight in the last projection */
+    int64_t fallback64;    /* FP32 form: sub-steps relocated in FP64 */
+    int64_t particle_steps;/* particles advanced, summed over all moves */
+    uint32_t next_id;      /* last particle id handed out (particleCount) */
+    uint32_t error_flags;  /* 1 capacity, 2 vertex with > 64 cells, 4 bad cell index */
+} pfem2gpu_stats;
+
+typedef struct pfem2gpu_handle pfem2gpu_handle;
+
+/* Constructor + setPfem2Solver (src/pfem2particlehandler.cpp:10-15,30-40). */
+int pfem2gpu_create(int dim, int precision, const pfem2gpu_params* params, pfem2gpu_handle** out);
+int pfem2gpu_destroy(pfem2gpu_handle* h);
+
+/* Mesh and initialize_maps (src/pfem2particlehandler.cpp:320-324).
+ * vertices: n_verts x dim; cell_vertices, cell_dofs: n_cells x 2^dim in deal.II
+ * lexicographic vertex order (the DoF of vertex i is cell->vertex_dof_index(i,0),
+ * src/pfem2particle.cpp:83-87).  The vertex maps (GridTools::vertex_to_cell_map,
+ * vertex_to_cell_centers_directions) may be passed (offsets n_verts+1, cells
+ * ascending, unit directions dim per entry) or NULL to have them built. */
+int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int64_t n_dofs,
+                      const double* vertices, const int32_t* cell_vertices, const int32_t* cell_dofs,
+                      const int32_t* v2c_offsets, const int32_t* v2c_cells, const double* v2c_dirs);
+
+/* seed_particles (src/pfem2particlehandler.cpp:43-109). */
+int pfem2gpu_seed(pfem2gpu_handle* h, const double* V);
+/* correct_particle_velocity (:112-139): v += sum N_i (V - Vold)_i; applied
+ * fused with the next move, or before any call that reads particles. */
+int pfem2gpu_correct(pfem2gpu_handle* h, const double* V, const double* Vold);
+/* move_particles (:142-171): sub-steps + relocation + count correction.
+ * V == NULL reuses the velocity of the preceding seed/correct/move call. */
+int pfem2gpu_move(pfem2gpu_handle* h, const double* V);
+/* project_particle_fields (:174-215): V_out = sum N v / sum N per DoF. */
+int pfem2gpu_project(pfem2gpu_handle* h, double* V_out);
+
+/* Same with device-resident vectors (same layout); project does not synchronize. */
+int pfem2gpu_seed_device(pfem2gpu_handle* h, const double* dV);
+int pfem2gpu_correct_device(pfem2gpu_handle* h, const double* dV, const double* dVold);
+int pfem2gpu_move_device(pfem2gpu_handle* h, const double* dV);
+int pfem2gpu_project_device(pfem2gpu_handle* h, double* dV_out);
+
+/* Particle access for output_particle_solution (:218-317) and begin()/end():
+ * arrays sized >= capacity (n x dim for x, xi, v); any may be NULL.  *n gets
+ * the particle count; PFEM2GPU_ERR_ARG if capacity is too small. */
+int pfem2gpu_get_particles(pfem2gpu_handle* h, uint32_t* id, int32_t* cell, double* x, double* xi, double* v,
+                           int64_t capacity, int64_t* n);
+/* Replace the particle set (insert_particle/clear_particles, :327-344).
+ * x is used by the FP64 form, ignored by the FP32 form. */
+int pfem2gpu_set_particles(pfem2gpu_handle* h, int64_t n, const uint32_t* id, const int32_t* cell, const double* x,
+                           const double* xi, const double* v, uint32_t next_id);
+/* Particle VTU file as output_particle_solution writes it (rank 0 of 1). */
+int pfem2gpu_write_vtu(pfem2gpu_handle* h, const char* path);
+
+int pfem2gpu_get_stats(pfem2gpu_handle* h, pfem2gpu_stats* out);
+int pfem2gpu_reset_stats(pfem2gpu_handle* h);
+int pfem2gpu_synchronize(pfem2gpu_handle* h);
+int pfem2gpu_get_stream(pfem2gpu_handle* h, void** stream);
+int pfem2gpu_host_register(void* ptr, size_t bytes);
+int pfem2gpu_host_unregister(void* ptr);
+
+/* Timing hooks (the reference's TimerOutput sections, :114,144,176): with
+ * profiling on, every launch is bracketed by CUDA events on the handle's
+ * stream; the report is a JSON object {"kernel": [total_ms, launches], ...}. */
+int pfem2gpu_profile(pfem2gpu_handle* h, int enable);
+int pfem2gpu_profile_report(pfem2gpu_handle* h, char* buf, int64_t len);
+int pfem2gpu_launch_count(pfem2gpu_handle* h, uint64_t* count);
+
+const char* pfem2gpu_error_string(int code);
+int pfem2gpu_last_error(pfem2gpu_handle* h, char* buf, int64_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

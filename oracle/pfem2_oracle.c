@@ -660,9 +660,13 @@ static int relocate(const orc_handle* h, orc_particle* q, reloc_counts* rc)
         }
         perm[j] = pi;
     }
-    /* :458-478 first candidate whose inverse map lands inside */
+    /* :458-478 first candidate whose inverse map lands inside.  The list
+     * holds the particle's own cell too; its inverse map is deterministic and
+     * already failed above, so it is skipped (same outcome, one solve less). */
+    const int32_t own = q->cell;
     for (int k = 0; k < nn; ++k) {
         const int32_t c = h->v2c_cells[b + perm[k]];
+        if (c == own) continue;
         cell_coords(h, c, Xc);
         st = orc_inverse_map(dim, Xc, q->x, xi);
         if (st) {

@@ -1,0 +1,866 @@
+// C ABI of the particle path: handle, device memory, and the per-call kernel
+// sequences.  One time step of the reference loop (src/pfem2solver.cpp:162-164)
+// maps to
+//   correct(V, Vold)  -> stage V, V - Vold (the correction is fused into move)
+//   move(V)           -> advect | scan cells | bucket | count | scan | write | finalize
+//   project(V_out)    -> gather (per-cell partials were summed by write) | D2H
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/pfem2gpu.h"
+#include "launch.h"
+
+using namespace pfem2;
+
+struct pfem2gpu_handle {
+    int dim = 2, prec = 0, dev = 0;
+    pfem2gpu_params prm{};
+    PartParams pp{};
+    cudaStream_t stream = nullptr;
+    // mesh
+    int nC = 0, nV = 0, nD = 0;
+    bool has_mesh = false;
+    int32_t *cv = nullptr, *cd = nullptr, *v2c_off = nullptr, *v2c_cells = nullptr, *d2c_off = nullptr,
+            *d2c_ent = nullptr;
+    double *verts = nullptr, *cellX = nullptr, *aff = nullptr, *v2c_dirs = nullptr;
+    float* geo32 = nullptr;
+    // velocities
+    double *Vstage = nullptr, *Vstage2 = nullptr, *Vout = nullptr;
+    void *Vaos = nullptr, *dVaos = nullptr;
+    bool vaos_valid = false;
+    // particles
+    uint32_t cap = 0;
+    PartState S0{}, S1{}, T{};
+    uint32_t *key = nullptr, *slot = nullptr, *idx = nullptr;
+    double* xtmp = nullptr;
+    uint32_t *cell_count = nullptr, *cell_off = nullptr, *cell_start = nullptr, *tiles32 = nullptr;
+    unsigned long long *packed = nullptr, *packed_off = nullptr, *tiles64 = nullptr;
+    void* partials = nullptr;
+    DevStats* stats = nullptr;
+    DevStats* stats_h = nullptr;
+    bool has_particles = false, pending_correct = false, partials_valid = false;
+    // accounting
+    uint64_t launches = 0;
+    bool profiling = false;
+    struct Ev {
+        std::string name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Ev> open_ev;
+    std::vector<cudaEvent_t> ev_pool;
+    std::map<std::string, std::pair<double, long long>> prof;
+    std::string err;
+};
+
+namespace {
+
+size_t esize(const pfem2gpu_handle* h) { return h->prec == PFEM2GPU_FP64 ? 8 : 4; }
+
+int fail(pfem2gpu_handle* h, int code, const std::string& msg)
+{
+    if (h) h->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return fail(h, e_ == cudaErrorMemoryAllocation ? PFEM2GPU_ERR_NOMEM : PFEM2GPU_ERR_CUDA,  \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t n)
+{
+    *p = nullptr;
+    return cudaMalloc((void**)p, n ? n * sizeof(T) : sizeof(T));
+}
+
+void dfree(void* p)
+{
+    if (p) cudaFree(p);
+}
+
+cudaEvent_t take_event(pfem2gpu_handle* h)
+{
+    if (!h->ev_pool.empty()) {
+        cudaEvent_t e = h->ev_pool.back();
+        h->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Run one launcher, counting its kernels and, when profiling, timing it with
+// events on the handle's stream.
+template <typename F>
+void run(pfem2gpu_handle* h, const char* name, F&& f)
+{
+    if (h->profiling) {
+        cudaEvent_t a = take_event(h), b = take_event(h);
+        cudaEventRecord(a, h->stream);
+        h->launches += f();
+        cudaEventRecord(b, h->stream);
+        h->open_ev.push_back({name, a, b});
+    } else {
+        h->launches += f();
+    }
+}
+
+void collect_profile(pfem2gpu_handle* h)
+{
+    if (h->open_ev.empty()) return;
+    cudaStreamSynchronize(h->stream);
+    for (auto& e : h->open_ev) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e.a, e.b);
+        auto& slot = h->prof[e.name];
+        slot.first += ms;
+        slot.second += 1;
+        h->ev_pool.push_back(e.a);
+        h->ev_pool.push_back(e.b);
+    }
+    h->open_ev.clear();
+}
+
+StepArgs args(pfem2gpu_handle* h)
+{
+    StepArgs a{};
+    a.mesh.nC = h->nC;
+    a.mesh.nV = h->nV;
+    a.mesh.nD = h->nD;
+    a.mesh.cv = h->cv;
+    a.mesh.cd = h->cd;
+    a.mesh.cellX = h->cellX;
+    a.mesh.aff = h->aff;
+    a.mesh.geo32 = h->geo32;
+    a.mesh.v2c_off = h->v2c_off;
+    a.mesh.v2c_cells = h->v2c_cells;
+    a.mesh.v2c_dirs = h->v2c_dirs;
+    a.mesh.d2c_off = h->d2c_off;
+    a.mesh.d2c_ent = h->d2c_ent;
+    a.pp = h->pp;
+    a.S0 = h->S0;
+    a.S1 = h->S1;
+    a.T = h->T;
+    a.Vaos = h->Vaos;
+    a.dVaos = h->dVaos;
+    a.do_correct = 0;
+    a.apply_counts = 1;
+    a.key = h->key;
+    a.slot = h->slot;
+    a.idx = h->idx;
+    a.cell_count = h->cell_count;
+    a.cell_off = h->cell_off;
+    a.packed = h->packed;
+    a.packed_off = h->packed_off;
+    a.partials = h->partials;
+    a.Vout = h->Vout;
+    a.Vkeep = h->Vstage;
+    a.stats = h->stats;
+    a.capacity = h->cap;
+    return a;
+}
+
+void free_state(PartState& s)
+{
+    dfree(s.cell);
+    dfree(s.id);
+    for (int d = 0; d < 3; ++d) {
+        dfree(s.x[d]);
+        dfree(s.xi[d]);
+        dfree(s.v[d]);
+    }
+    s = PartState{};
+}
+
+cudaError_t alloc_state(pfem2gpu_handle* h, PartState& s, uint32_t cap, bool with_ids)
+{
+    cudaError_t e = cudaSuccess;
+    const size_t es = esize(h);
+    if (with_ids) {
+        if ((e = dalloc(&s.cell, cap)) != cudaSuccess) return e;
+        if ((e = dalloc(&s.id, cap)) != cudaSuccess) return e;
+    }
+    for (int d = 0; d < h->dim; ++d) {
+        if (h->prec == PFEM2GPU_FP64 && (e = cudaMalloc(&s.x[d], cap * 8ull)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&s.xi[d], cap * es)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&s.v[d], cap * es)) != cudaSuccess) return e;
+    }
+    return e;
+}
+
+// Particle arrays sized for `need` particles (grown by 1.5x, S0 kept).
+int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
+{
+    if (need <= h->cap && h->S0.cell) return PFEM2GPU_OK;
+    uint64_t cap = std::max<uint64_t>(need, (uint64_t)h->cap * 3 / 2);
+    cap = std::max<uint64_t>(cap, 1024);
+    if (cap > 0xFFFFFFF0ull) return fail(h, PFEM2GPU_ERR_CAPACITY, "particle capacity beyond 2^32");
+    PartState n0{}, n1{}, nt{};
+    CK(alloc_state(h, n0, (uint32_t)cap, true));
+    CK(alloc_state(h, n1, (uint32_t)cap, true));
+    CK(alloc_state(h, nt, (uint32_t)cap, false));
+    if (h->S0.cell && h->has_particles) {
+        const size_t n = h->cap, es = esize(h);
+        CK(cudaMemcpyAsync(n0.cell, h->S0.cell, n * 4, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(n0.id, h->S0.id, n * 4, cudaMemcpyDeviceToDevice, h->stream));
+        for (int d = 0; d < h->dim; ++d) {
+            if (h->S0.x[d]) CK(cudaMemcpyAsync(n0.x[d], h->S0.x[d], n * 8, cudaMemcpyDeviceToDevice, h->stream));
+            CK(cudaMemcpyAsync(n0.xi[d], h->S0.xi[d], n * es, cudaMemcpyDeviceToDevice, h->stream));
+            CK(cudaMemcpyAsync(n0.v[d], h->S0.v[d], n * es, cudaMemcpyDeviceToDevice, h->stream));
+        }
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    free_state(h->S0);
+    free_state(h->S1);
+    free_state(h->T);
+    dfree(h->key);
+    dfree(h->slot);
+    dfree(h->idx);
+    dfree(h->xtmp);
+    h->key = h->slot = h->idx = nullptr;
+    h->xtmp = nullptr;
+    h->S0 = n0;
+    h->S1 = n1;
+    h->T = nt;
+    CK(dalloc(&h->key, cap));
+    CK(dalloc(&h->slot, cap));
+    CK(dalloc(&h->idx, cap));
+    if (h->prec == PFEM2GPU_FP32) CK(dalloc(&h->xtmp, cap * h->dim));
+    h->cap = (uint32_t)cap;
+    return PFEM2GPU_OK;
+}
+
+// Nodal velocity staging: host or device component-major V (and Vold) ->
+// padded per-DoF V (and V - Vold) in the form's precision.
+int stage_v(pfem2gpu_handle* h, const double* V, const double* Vold, bool device)
+{
+    const size_t bytes = (size_t)h->dim * h->nD * sizeof(double);
+    const double* v = V;
+    const double* vo = Vold;
+    if (!device) {
+        CK(cudaMemcpyAsync(h->Vstage, V, bytes, cudaMemcpyHostToDevice, h->stream));
+        v = h->Vstage;
+        if (Vold) {
+            CK(cudaMemcpyAsync(h->Vstage2, Vold, bytes, cudaMemcpyHostToDevice, h->stream));
+            vo = h->Vstage2;
+        }
+    } else if (V != h->Vstage) {
+        CK(cudaMemcpyAsync(h->Vstage, V, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    run(h, "stage_velocity",
+        [&] { return launch_prep_v(h->dim, h->prec, v, vo, h->nD, h->Vaos, Vold ? h->dVaos : nullptr, h->stream); });
+    h->vaos_valid = true;
+    return PFEM2GPU_OK;
+}
+
+int check_async(pfem2gpu_handle* h)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, PFEM2GPU_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return PFEM2GPU_OK;
+}
+
+int apply_pending_correction(pfem2gpu_handle* h)
+{
+    if (!h->pending_correct) return PFEM2GPU_OK;
+    StepArgs a = args(h);
+    run(h, "correct", [&] { return launch_correct(h->dim, h->prec, a, h->stream); });
+    h->pending_correct = false;
+    h->partials_valid = false;
+    return check_async(h);
+}
+
+// Re-bucket and write the next sorted state from T (advected or uploaded
+// particles, keys and slots already set): the shared tail of move and
+// set_particles.
+int sort_and_write(pfem2gpu_handle* h, StepArgs& a, int count_step)
+{
+    run(h, "scan_cells", [&] { return launch_scan_u32(h->cell_count, h->nC, h->cell_off, h->tiles32, h->stream); });
+    run(h, "bucket", [&] { return launch_bucket(a, h->stream); });
+    run(h, "count", [&] { return launch_count(h->dim, h->prec, a, h->stream); });
+    run(h, "scan_counts", [&] { return launch_scan_u64(h->packed, h->nC, h->packed_off, h->tiles64, h->stream); });
+    run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->cell_start, h->stream); });
+    run(h, "finalize", [&] { return launch_finalize(a, h->cell_start, count_step, h->stream); });
+    std::swap(h->S0, h->S1);
+    h->partials_valid = true;
+    return check_async(h);
+}
+
+int do_move(pfem2gpu_handle* h)
+{
+    if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "move before seed");
+    if (!h->vaos_valid) return fail(h, PFEM2GPU_ERR_STATE, "move without a velocity");
+    StepArgs a = args(h);
+    a.do_correct = h->pending_correct ? 1 : 0;
+    h->pending_correct = false;
+    CK(cudaMemsetAsync(h->cell_count, 0, h->nC * sizeof(uint32_t), h->stream));
+    run(h, "advect", [&] { return launch_advect(h->dim, h->prec, a, h->stream); });
+    return sort_and_write(h, a, 1);
+}
+
+int sync_stats(pfem2gpu_handle* h)
+{
+    CK(cudaMemcpyAsync(h->stats_h, h->stats, sizeof(DevStats), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->profiling) collect_profile(h);
+    const uint32_t f = h->stats_h->error_flags;
+    if (f & ERR_CAPACITY) return fail(h, PFEM2GPU_ERR_CAPACITY, "particle capacity exceeded");
+    if (f) return fail(h, PFEM2GPU_ERR_DEVICE, "kernel error flags " + std::to_string(f));
+    return PFEM2GPU_OK;
+}
+
+// Grow the particle arrays ahead of need (the next step may add up to one
+// particle per empty part); only at points that already synchronize.
+int maybe_grow(pfem2gpu_handle* h)
+{
+    const uint64_t n = h->stats_h->n_particles;
+    if (n + (uint64_t)h->nC * h->pp.npart / 2 > h->cap) return ensure_capacity(h, n + (uint64_t)h->nC * h->pp.npart);
+    return PFEM2GPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pfem2gpu_error_string(int code)
+{
+    switch (code) {
+    case PFEM2GPU_OK: return "ok";
+    case PFEM2GPU_ERR_ARG: return "invalid argument";
+    case PFEM2GPU_ERR_CUDA: return "CUDA error";
+    case PFEM2GPU_ERR_STATE: return "call out of order";
+    case PFEM2GPU_ERR_CAPACITY: return "particle capacity exceeded";
+    case PFEM2GPU_ERR_NOMEM: return "device out of memory";
+    case PFEM2GPU_ERR_NODEVICE: return "no CUDA device";
+    case PFEM2GPU_ERR_DEVICE: return "kernel reported invalid data";
+    default: return "unknown error";
+    }
+}
+
+int pfem2gpu_last_error(pfem2gpu_handle* h, char* buf, int64_t len)
+{
+    if (!h || !buf || len <= 0) return PFEM2GPU_ERR_ARG;
+    std::snprintf(buf, (size_t)len, "%s", h->err.c_str());
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_create(int dim, int precision, const pfem2gpu_params* prm, pfem2gpu_handle** out)
+{
+    if (!out || !prm) return PFEM2GPU_ERR_ARG;
+    *out = nullptr;
+    if (dim != 2 && dim != 3) return PFEM2GPU_ERR_ARG;
+    if (precision != PFEM2GPU_FP64 && precision != PFEM2GPU_FP32) return PFEM2GPU_ERR_ARG;
+    int npart = 1, npe = 1;
+    for (int d = 0; d < dim; ++d) {
+        if (prm->particles_per_cell[d] < 1 || prm->particles_per_cell[d] > 64) return PFEM2GPU_ERR_ARG;
+        npart *= prm->particles_per_cell[d];
+        npe *= prm->particles_per_cell[d] + 1;
+    }
+    if (npe > NPE_MAX) return PFEM2GPU_ERR_ARG;
+    if (!(std::isfinite(prm->time_step)) || prm->particle_integration_steps < 0) return PFEM2GPU_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return PFEM2GPU_ERR_NODEVICE;
+    }
+    pfem2gpu_handle* h = new pfem2gpu_handle();
+    h->dim = dim;
+    h->prec = precision;
+    h->prm = *prm;
+    cudaGetDevice(&h->dev);
+    PartParams& pp = h->pp;
+    for (int d = 0; d < 3; ++d) {
+        pp.q[d] = d < dim ? prm->particles_per_cell[d] : 1;
+        pp.h[d] = 1.0 / pp.q[d];
+    }
+    pp.npart = npart;
+    pp.npe = npe;
+    pp.maxpp = prm->max_particles_per_cell_part;
+    pp.S = prm->particle_integration_steps == 0 ? 1 : prm->particle_integration_steps;  // :34-36
+    pp.dtp = prm->time_step / (double)pp.S;                                               // :38
+    pp.seed = prm->removal_seed;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&h->stats, sizeof(DevStats)) != cudaSuccess ||
+        cudaMallocHost(&h->stats_h, sizeof(DevStats)) != cudaSuccess ||
+        cudaMemsetAsync(h->stats, 0, sizeof(DevStats), h->stream) != cudaSuccess) {
+        pfem2gpu_destroy(h);
+        return PFEM2GPU_ERR_CUDA;
+    }
+    std::memset(h->stats_h, 0, sizeof(DevStats));
+    *out = h;
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_destroy(pfem2gpu_handle* h)
+{
+    if (!h) return PFEM2GPU_ERR_ARG;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : {(void*)h->cv, (void*)h->cd, (void*)h->v2c_off, (void*)h->v2c_cells, (void*)h->d2c_off,
+                    (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
+                    (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vaos, h->dVaos,
+                    (void*)h->key, (void*)h->slot, (void*)h->idx, (void*)h->xtmp, (void*)h->cell_count,
+                    (void*)h->cell_off, (void*)h->cell_start, (void*)h->tiles32, (void*)h->packed,
+                    (void*)h->packed_off, (void*)h->tiles64, h->partials, (void*)h->stats})
+        dfree(p);
+    free_state(h->S0);
+    free_state(h->S1);
+    free_state(h->T);
+    if (h->stats_h) cudaFreeHost(h->stats_h);
+    for (auto& e : h->open_ev) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    for (auto e : h->ev_pool) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int64_t n_dofs, const double* vertices,
+                      const int32_t* cell_vertices, const int32_t* cell_dofs, const int32_t* v2c_offsets,
+                      const int32_t* v2c_cells, const double* v2c_dirs)
+{
+    if (!h || !vertices || !cell_vertices || !cell_dofs) return PFEM2GPU_ERR_ARG;
+    if (n_cells < 1 || n_verts < 1 || n_dofs < 1 || n_cells > (1ll << 30) || n_verts > (1ll << 30) ||
+        n_dofs > (1ll << 30))
+        return fail(h, PFEM2GPU_ERR_ARG, "mesh sizes out of range");
+    if ((n_cells + SCAN_TILE - 1) / SCAN_TILE > SCAN_MAX_TILES) return fail(h, PFEM2GPU_ERR_ARG, "too many cells");
+    if (h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "mesh change with live particles");
+    const int dim = h->dim, NV = 1 << dim;
+    for (int64_t k = 0; k < n_cells * NV; ++k) {
+        if (cell_vertices[k] < 0 || cell_vertices[k] >= n_verts) return fail(h, PFEM2GPU_ERR_ARG, "bad cell vertex");
+        if (cell_dofs[k] < 0 || cell_dofs[k] >= n_dofs) return fail(h, PFEM2GPU_ERR_ARG, "bad cell dof");
+    }
+    // vertex -> cells (ascending) and unit vertex -> centre directions
+    std::vector<int32_t> off, cells;
+    std::vector<double> dirs;
+    if (v2c_offsets && v2c_cells && v2c_dirs) {
+        off.assign(v2c_offsets, v2c_offsets + n_verts + 1);
+        if (off[0] != 0) return fail(h, PFEM2GPU_ERR_ARG, "v2c offsets must start at 0");
+        for (int64_t v = 0; v < n_verts; ++v)
+            if (off[v + 1] < off[v]) return fail(h, PFEM2GPU_ERR_ARG, "v2c offsets not monotone");
+        cells.assign(v2c_cells, v2c_cells + off[n_verts]);
+        for (int32_t c : cells)
+            if (c < 0 || c >= n_cells) return fail(h, PFEM2GPU_ERR_ARG, "bad v2c cell");
+        dirs.assign(v2c_dirs, v2c_dirs + (size_t)off[n_verts] * dim);
+    } else {
+        off.assign(n_verts + 1, 0);
+        std::vector<int32_t> last(n_verts, -1);
+        for (int64_t c = 0; c < n_cells; ++c)
+            for (int i = 0; i < NV; ++i) {
+                const int32_t v = cell_vertices[c * NV + i];
+                if (last[v] != (int32_t)c) {
+                    last[v] = (int32_t)c;
+                    off[v + 1]++;
+                }
+            }
+        for (int64_t v = 0; v < n_verts; ++v) off[v + 1] += off[v];
+        cells.assign(off[n_verts], 0);
+        dirs.assign((size_t)off[n_verts] * dim, 0.0);
+        std::vector<int32_t> fill(off.begin(), off.end() - 1);
+        std::fill(last.begin(), last.end(), -1);
+        for (int64_t c = 0; c < n_cells; ++c)
+            for (int i = 0; i < NV; ++i) {
+                const int32_t v = cell_vertices[c * NV + i];
+                if (last[v] == (int32_t)c) continue;
+                last[v] = (int32_t)c;
+                cells[fill[v]++] = (int32_t)c;
+            }
+        for (int64_t v = 0; v < n_verts; ++v)
+            for (int32_t k = off[v]; k < off[v + 1]; ++k) {
+                const int64_t c = cells[k];
+                double dir[3], s = 0.0;
+                for (int d = 0; d < dim; ++d) {
+                    double ctr = 0.0;
+                    for (int i = 0; i < NV; ++i) ctr = ctr + vertices[(size_t)cell_vertices[c * NV + i] * dim + d];
+                    ctr = ctr / (double)NV;
+                    dir[d] = ctr - vertices[v * dim + d];
+                }
+                for (int d = 0; d < dim; ++d) s = s + dir[d] * dir[d];
+                s = std::sqrt(s);
+                for (int d = 0; d < dim; ++d) dirs[(size_t)k * dim + d] = dir[d] / s;
+            }
+    }
+    // dof -> (cell, local vertex), cells ascending
+    std::vector<int32_t> doff(n_dofs + 1, 0), dent((size_t)n_cells * NV);
+    for (int64_t k = 0; k < n_cells * NV; ++k) doff[cell_dofs[k] + 1]++;
+    for (int64_t d = 0; d < n_dofs; ++d) doff[d + 1] += doff[d];
+    {
+        std::vector<int32_t> fill(doff.begin(), doff.end() - 1);
+        for (int64_t k = 0; k < n_cells * NV; ++k) dent[fill[cell_dofs[k]]++] = (int32_t)k;
+    }
+    // release an older mesh
+    for (void* p : {(void*)h->cv, (void*)h->cd, (void*)h->v2c_off, (void*)h->v2c_cells, (void*)h->d2c_off,
+                    (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
+                    (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vaos, h->dVaos,
+                    (void*)h->cell_count, (void*)h->cell_off, (void*)h->cell_start, (void*)h->tiles32,
+                    (void*)h->packed, (void*)h->packed_off, (void*)h->tiles64, h->partials})
+        dfree(p);
+    h->has_mesh = false;
+    h->nC = (int)n_cells;
+    h->nV = (int)n_verts;
+    h->nD = (int)n_dofs;
+    const size_t nc = n_cells, nvx = n_verts, nd = n_dofs;
+    const int VS = dim == 3 ? 4 : 2, PW = dim == 3 ? 32 : 16, GS = dim == 3 ? 24 : 8, AFF = dim * dim + dim;
+    CK(dalloc(&h->cv, nc * NV));
+    CK(dalloc(&h->cd, nc * NV));
+    CK(dalloc(&h->verts, nvx * dim));
+    CK(dalloc(&h->v2c_off, nvx + 1));
+    CK(dalloc(&h->v2c_cells, cells.size()));
+    CK(dalloc(&h->v2c_dirs, dirs.size()));
+    CK(dalloc(&h->d2c_off, nd + 1));
+    CK(dalloc(&h->d2c_ent, dent.size()));
+    CK(dalloc(&h->cellX, nc * NV * dim));
+    CK(dalloc(&h->aff, nc * AFF));
+    CK(dalloc(&h->geo32, nc * GS));
+    CK(dalloc(&h->Vstage, nd * dim));
+    CK(dalloc(&h->Vstage2, nd * dim));
+    CK(dalloc(&h->Vout, nd * dim));
+    CK(cudaMalloc(&h->Vaos, nd * VS * esize(h)));
+    CK(cudaMalloc(&h->dVaos, nd * VS * esize(h)));
+    CK(dalloc(&h->cell_count, nc));
+    CK(dalloc(&h->cell_off, nc + 1));
+    CK(dalloc(&h->cell_start, nc + 1));
+    CK(dalloc(&h->packed, nc));
+    CK(dalloc(&h->packed_off, nc + 1));
+    CK(dalloc(&h->tiles32, SCAN_MAX_TILES));
+    CK(dalloc(&h->tiles64, SCAN_MAX_TILES));
+    CK(cudaMalloc(&h->partials, nc * PW * esize(h)));
+    CK(cudaMemcpyAsync(h->cv, cell_vertices, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->cd, cell_dofs, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->verts, vertices, nvx * dim * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->v2c_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->v2c_cells, cells.data(), cells.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->v2c_dirs, dirs.data(), dirs.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d2c_off, doff.data(), doff.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d2c_ent, dent.data(), dent.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->Vaos, 0, nd * VS * esize(h), h->stream));
+    CK(cudaMemsetAsync(h->dVaos, 0, nd * VS * esize(h), h->stream));
+    CK(cudaMemsetAsync(h->Vstage, 0, nd * dim * 8, h->stream));
+    run(h, "cell_setup",
+        [&] { return launch_cell_setup(dim, h->nC, h->verts, h->cv, h->cellX, h->aff, h->geo32, h->stream); });
+    CK(cudaStreamSynchronize(h->stream));  // host vectors above go out of scope
+    h->has_mesh = true;
+    h->vaos_valid = false;
+    return check_async(h);
+}
+
+static int seed_impl(pfem2gpu_handle* h, const double* V, bool device)
+{
+    if (!h || !V) return PFEM2GPU_ERR_ARG;
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "seed before set_mesh");
+    if (h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "seed called twice");
+    const uint64_t n = (uint64_t)h->nC * h->pp.npart;
+    const uint64_t want = h->prm.capacity > 0 ? (uint64_t)h->prm.capacity : 2 * n;
+    int rc = ensure_capacity(h, std::max(want, n));
+    if (rc) return rc;
+    if ((rc = stage_v(h, V, nullptr, device))) return rc;
+    StepArgs a = args(h);
+    run(h, "seed", [&] { return launch_seed(h->dim, h->prec, a, h->cell_start, h->stream); });
+    run(h, "finalize", [&] { return launch_set_state(h->stats, (long long)n, -1, (long long)n, h->stream); });
+    h->has_particles = true;
+    h->partials_valid = false;
+    h->pending_correct = false;
+    return check_async(h);
+}
+
+int pfem2gpu_seed(pfem2gpu_handle* h, const double* V) { return seed_impl(h, V, false); }
+int pfem2gpu_seed_device(pfem2gpu_handle* h, const double* dV) { return seed_impl(h, dV, true); }
+
+static int correct_impl(pfem2gpu_handle* h, const double* V, const double* Vold, bool device)
+{
+    if (!h || !V || !Vold) return PFEM2GPU_ERR_ARG;
+    if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "correct before seed");
+    int rc = apply_pending_correction(h);
+    if (rc) return rc;
+    if ((rc = stage_v(h, V, Vold, device))) return rc;
+    h->pending_correct = true;
+    h->partials_valid = false;
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_correct(pfem2gpu_handle* h, const double* V, const double* Vold) { return correct_impl(h, V, Vold, false); }
+int pfem2gpu_correct_device(pfem2gpu_handle* h, const double* dV, const double* dVold)
+{
+    return correct_impl(h, dV, dVold, true);
+}
+
+static int move_impl(pfem2gpu_handle* h, const double* V, bool device)
+{
+    if (!h) return PFEM2GPU_ERR_ARG;
+    if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "move before seed");
+    if (V) {
+        // keep a staged correction: only V is re-staged
+        int rc = stage_v(h, V, nullptr, device);
+        if (rc) return rc;
+    }
+    return do_move(h);
+}
+
+int pfem2gpu_move(pfem2gpu_handle* h, const double* V) { return move_impl(h, V, false); }
+int pfem2gpu_move_device(pfem2gpu_handle* h, const double* dV) { return move_impl(h, dV, true); }
+
+static int project_impl(pfem2gpu_handle* h, double* out, bool device)
+{
+    if (!h || !out) return PFEM2GPU_ERR_ARG;
+    if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "project before seed");
+    int rc = apply_pending_correction(h);
+    if (rc) return rc;
+    StepArgs a = args(h);
+    if (!h->partials_valid) {
+        run(h, "partials", [&] { return launch_partials(h->dim, h->prec, a, h->cell_start, h->stream); });
+        h->partials_valid = true;
+    }
+    CK(cudaMemsetAsync(&h->stats->nan_dofs, 0, sizeof(unsigned long long), h->stream));
+    run(h, "gather", [&] { return launch_gather(h->dim, h->prec, a, h->prm.empty_dof_policy == 1, h->stream); });
+    if ((rc = check_async(h))) return rc;
+    const size_t bytes = (size_t)h->dim * h->nD * sizeof(double);
+    if (device) {
+        if (out != h->Vout) CK(cudaMemcpyAsync(out, h->Vout, bytes, cudaMemcpyDeviceToDevice, h->stream));
+        return PFEM2GPU_OK;
+    }
+    CK(cudaMemcpyAsync(out, h->Vout, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if ((rc = sync_stats(h))) return rc;
+    return maybe_grow(h);
+}
+
+int pfem2gpu_project(pfem2gpu_handle* h, double* V_out) { return project_impl(h, V_out, false); }
+int pfem2gpu_project_device(pfem2gpu_handle* h, double* dV_out) { return project_impl(h, dV_out, true); }
+
+int pfem2gpu_get_particles(pfem2gpu_handle* h, uint32_t* id, int32_t* cell, double* x, double* xi, double* v,
+                           int64_t capacity, int64_t* n)
+{
+    if (!h || !n) return PFEM2GPU_ERR_ARG;
+    *n = 0;
+    if (!h->has_particles) return PFEM2GPU_OK;
+    int rc = apply_pending_correction(h);
+    if (rc) return rc;
+    if ((rc = sync_stats(h))) return rc;
+    const int64_t np = (int64_t)h->stats_h->n_particles;
+    *n = np;
+    if (capacity < np) return fail(h, PFEM2GPU_ERR_ARG, "output arrays too small");
+    const int dim = h->dim;
+    if (id) CK(cudaMemcpyAsync(id, h->S0.id, np * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (cell) CK(cudaMemcpyAsync(cell, h->S0.cell, np * 4, cudaMemcpyDeviceToHost, h->stream));
+    std::vector<double> tmp(np);
+    std::vector<float> tmpf(np);
+    auto fetch = [&](void* const* src, double* dst) -> int {
+        for (int d = 0; d < dim; ++d) {
+            if (h->prec == PFEM2GPU_FP64) {
+                CK(cudaMemcpyAsync(tmp.data(), src[d], np * 8, cudaMemcpyDeviceToHost, h->stream));
+                CK(cudaStreamSynchronize(h->stream));
+                for (int64_t i = 0; i < np; ++i) dst[i * dim + d] = tmp[i];
+            } else {
+                CK(cudaMemcpyAsync(tmpf.data(), src[d], np * 4, cudaMemcpyDeviceToHost, h->stream));
+                CK(cudaStreamSynchronize(h->stream));
+                for (int64_t i = 0; i < np; ++i) dst[i * dim + d] = (double)tmpf[i];
+            }
+        }
+        return PFEM2GPU_OK;
+    };
+    if (xi && (rc = fetch(h->S0.xi, xi))) return rc;
+    if (v && (rc = fetch(h->S0.v, v))) return rc;
+    if (x) {
+        if (h->prec == PFEM2GPU_FP64) {
+            if ((rc = fetch(h->S0.x, x))) return rc;
+        } else {
+            StepArgs a = args(h);
+            run(h, "positions", [&] { return launch_positions32(dim, a, h->xtmp, h->stream); });
+            CK(cudaMemcpyAsync(x, h->xtmp, np * dim * 8, cudaMemcpyDeviceToHost, h->stream));
+        }
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return check_async(h);
+}
+
+int pfem2gpu_set_particles(pfem2gpu_handle* h, int64_t n, const uint32_t* id, const int32_t* cell, const double* x,
+                           const double* xi, const double* v, uint32_t next_id)
+{
+    if (!h || n < 0 || (n > 0 && (!id || !cell || !xi || !v))) return PFEM2GPU_ERR_ARG;
+    if (h->prec == PFEM2GPU_FP64 && n > 0 && !x) return PFEM2GPU_ERR_ARG;
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "set_particles before set_mesh");
+    for (int64_t i = 0; i < n; ++i)
+        if (cell[i] < 0 || cell[i] >= h->nC) return fail(h, PFEM2GPU_ERR_ARG, "bad particle cell");
+    int rc = ensure_capacity(h, std::max<uint64_t>((uint64_t)n + (uint64_t)h->nC * h->pp.npart, h->cap));
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    const int dim = h->dim;
+    CK(cudaMemcpyAsync(h->S0.id, id, n * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->S0.cell, cell, n * 4, cudaMemcpyHostToDevice, h->stream));
+    std::vector<double> tmp(n);
+    std::vector<float> tmpf(n);
+    auto put = [&](const double* src, void* const* dst) -> int {
+        for (int d = 0; d < dim; ++d) {
+            if (h->prec == PFEM2GPU_FP64 || dst == h->T.x) {
+                for (int64_t i = 0; i < n; ++i) tmp[i] = src[i * dim + d];
+                CK(cudaMemcpyAsync(dst[d], tmp.data(), n * 8, cudaMemcpyHostToDevice, h->stream));
+            } else {
+                for (int64_t i = 0; i < n; ++i) tmpf[i] = (float)src[i * dim + d];
+                CK(cudaMemcpyAsync(dst[d], tmpf.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
+            }
+            CK(cudaStreamSynchronize(h->stream));
+        }
+        return PFEM2GPU_OK;
+    };
+    if ((rc = put(xi, h->T.xi))) return rc;
+    if ((rc = put(v, h->T.v))) return rc;
+    if (h->prec == PFEM2GPU_FP64 && (rc = put(x, h->T.x))) return rc;
+    CK(cudaMemsetAsync(h->stats, 0, sizeof(DevStats), h->stream));
+    run(h, "finalize", [&] { return launch_set_state(h->stats, n, next_id, 0, h->stream); });
+    CK(cudaMemsetAsync(h->cell_count, 0, h->nC * sizeof(uint32_t), h->stream));
+    StepArgs a = args(h);
+    a.apply_counts = 0;
+    run(h, "rekey", [&] { return launch_rekey(a, h->stream); });
+    h->has_particles = true;
+    h->pending_correct = false;
+    if ((rc = sort_and_write(h, a, 0))) return rc;
+    return sync_stats(h);
+}
+
+int pfem2gpu_get_stats(pfem2gpu_handle* h, pfem2gpu_stats* out)
+{
+    if (!h || !out) return PFEM2GPU_ERR_ARG;
+    int rc = sync_stats(h);
+    const DevStats& s = *h->stats_h;
+    out->n_particles = (int64_t)s.n_particles;
+    out->lost = (int64_t)s.lost;
+    out->removed = (int64_t)s.removed;
+    out->seeded = (int64_t)s.seeded;
+    out->map_failures = (int64_t)s.map_failures;
+    out->near_face = (int64_t)s.near_face;
+    out->searched = (int64_t)s.searched;
+    out->nan_dofs = (int64_t)s.nan_dofs;
+    out->fallback64 = (int64_t)s.fallback64;
+    out->particle_steps = (int64_t)s.particle_steps;
+    out->next_id = s.next_id;
+    out->error_flags = s.error_flags;
+    return rc == PFEM2GPU_ERR_CAPACITY || rc == PFEM2GPU_ERR_DEVICE ? PFEM2GPU_OK : rc;
+}
+
+int pfem2gpu_reset_stats(pfem2gpu_handle* h)
+{
+    if (!h) return PFEM2GPU_ERR_ARG;
+    CK(cudaMemcpyAsync(h->stats_h, h->stats, sizeof(DevStats), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    DevStats s{};
+    s.n_particles = h->stats_h->n_particles;
+    s.next_id = h->stats_h->next_id;
+    s.nan_dofs = h->stats_h->nan_dofs;
+    s.particle_steps = h->stats_h->particle_steps;
+    *h->stats_h = s;
+    CK(cudaMemcpyAsync(h->stats, h->stats_h, sizeof(DevStats), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_synchronize(pfem2gpu_handle* h)
+{
+    if (!h) return PFEM2GPU_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->profiling) collect_profile(h);
+    return check_async(h);
+}
+
+int pfem2gpu_get_stream(pfem2gpu_handle* h, void** stream)
+{
+    if (!h || !stream) return PFEM2GPU_ERR_ARG;
+    *stream = (void*)h->stream;
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_host_register(void* ptr, size_t bytes)
+{
+    if (!ptr || !bytes) return PFEM2GPU_ERR_ARG;
+    return cudaHostRegister(ptr, bytes, cudaHostRegisterDefault) == cudaSuccess ? PFEM2GPU_OK : PFEM2GPU_ERR_CUDA;
+}
+
+int pfem2gpu_host_unregister(void* ptr)
+{
+    if (!ptr) return PFEM2GPU_ERR_ARG;
+    return cudaHostUnregister(ptr) == cudaSuccess ? PFEM2GPU_OK : PFEM2GPU_ERR_CUDA;
+}
+
+int pfem2gpu_profile(pfem2gpu_handle* h, int enable)
+{
+    if (!h) return PFEM2GPU_ERR_ARG;
+    collect_profile(h);
+    if (enable) h->prof.clear();
+    h->profiling = enable != 0;
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_profile_report(pfem2gpu_handle* h, char* buf, int64_t len)
+{
+    if (!h || !buf || len <= 0) return PFEM2GPU_ERR_ARG;
+    collect_profile(h);
+    std::string s = "{";
+    bool first = true;
+    for (auto& kv : h->prof) {
+        char tmp[256];
+        std::snprintf(tmp, sizeof tmp, "%s\"%s\": [%.6f, %lld]", first ? "" : ", ", kv.first.c_str(),
+                      kv.second.first, kv.second.second);
+        s += tmp;
+        first = false;
+    }
+    s += "}";
+    if ((int64_t)s.size() + 1 > len) return PFEM2GPU_ERR_ARG;
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_launch_count(pfem2gpu_handle* h, uint64_t* count)
+{
+    if (!h || !count) return PFEM2GPU_ERR_ARG;
+    *count = h->launches;
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_write_vtu(pfem2gpu_handle* h, const char* path)
+{
+    if (!h || !path) return PFEM2GPU_ERR_ARG;
+    int64_t n = 0;
+    int rc = pfem2gpu_get_particles(h, nullptr, nullptr, nullptr, nullptr, nullptr, 0, &n);
+    if (rc && rc != PFEM2GPU_ERR_ARG) return rc;
+    std::vector<double> x((size_t)std::max<int64_t>(n, 1) * h->dim), v(x.size());
+    if ((rc = pfem2gpu_get_particles(h, nullptr, nullptr, x.data(), nullptr, v.data(), n, &n))) return rc;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return fail(h, PFEM2GPU_ERR_ARG, std::string("cannot open ") + path);
+    const int dim = h->dim;
+    // layout of output_particle_solution, src/pfem2particlehandler.cpp:223-291
+    std::fprintf(f, "<?xml version=\"1.0\" ?> \n<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" "
+                    "byte_order=\"LittleEndian\">\n  <UnstructuredGrid>\n");
+    std::fprintf(f, "    <Piece NumberOfPoints=\"%lld\" NumberOfCells=\"%lld\">\n", (long long)n, (long long)n);
+    std::fprintf(f, "      <Points>\n        <DataArray type=\"Float32\" NumberOfComponents=\"3\" Format=\"ascii\">\n");
+    for (int64_t i = 0; i < n; ++i)
+        std::fprintf(f, "          %g %.6f %.6f\n", x[i * dim], dim > 1 ? x[i * dim + 1] : 0.0,
+                     dim > 2 ? x[i * dim + 2] : 0.0);
+    std::fprintf(f, "        </DataArray>\n      </Points>\n      <Cells>\n");
+    std::fprintf(f, "        <DataArray type=\"Int32\" Name=\"connectivity\" Format=\"ascii\">\n");
+    for (int64_t i = 0; i < n; ++i) std::fprintf(f, "          %lld\n", (long long)i);
+    std::fprintf(f, "        </DataArray>\n        <DataArray type=\"Int32\" Name=\"offsets\" Format=\"ascii\">\n        ");
+    for (int64_t i = 0; i < n; ++i) std::fprintf(f, "  %lld", (long long)i + 1);
+    std::fprintf(f, "\n        </DataArray>\n        <DataArray type=\"Int32\" Name=\"types\" Format=\"ascii\">\n        ");
+    for (int64_t i = 0; i < n; ++i) std::fprintf(f, "  1");
+    std::fprintf(f, "\n        </DataArray>\n      </Cells>\n      <PointData Scalars=\"scalars\">\n");
+    std::fprintf(f, "        <DataArray type=\"Float32\" Name=\"velocity\" NumberOfComponents=\"3\" Format=\"ascii\">\n");
+    for (int64_t i = 0; i < n; ++i)
+        std::fprintf(f, "          %g %.6f %.6f\n", v[i * dim], dim > 1 ? v[i * dim + 1] : 0.0,
+                     dim > 2 ? v[i * dim + 2] : 0.0);
+    std::fprintf(f, "        </DataArray>\n        <DataArray type=\"Float32\" Name=\"subdomain\" Format=\"ascii\">\n        ");
+    for (int64_t i = 0; i < n; ++i) std::fprintf(f, "  0");
+    std::fprintf(f, "\n        </DataArray>\n      </PointData>\n    </Piece>\n  </UnstructuredGrid>\n</VTKFile>\n");
+    std::fclose(f);
+    return PFEM2GPU_OK;
+}
+
+}  // extern "C"

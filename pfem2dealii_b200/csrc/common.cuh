@@ -1,0 +1,166 @@
+// Shared device-side definitions of the PFEM-2 particle kernels.
+//
+// Particles live on the device as structure-of-arrays, sorted by (cell,
+// cell part, key(id)) after every step:
+//   cell u32 | id u32 | x[dim] f64 (FP64 form only) | xi[dim] | v[dim]
+// with xi and v in f64 (FP64 form) or f32 (FP32 form).  The reference keeps an
+// std::vector of 88/136-byte AoS records (src/pfem2particle.h:63-72); the
+// per-particle cell_dofs copy and velocity_ext are not stored: DoFs come from
+// the per-cell table and velocity_ext only lives inside one sub-step.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pfem2 {
+
+constexpr uint32_t LOST = 0xFFFFFFFFu;
+constexpr int MAX_CAND = 64;   // cells around one vertex tried by the relocation search
+constexpr int NPE_MAX = 512;   // extended cell parts (q0+1)(q1+1)(q2+1)
+constexpr int CELL_WARPS = 4;  // warps per block in the warp-per-cell kernels
+constexpr int KEY_CACHE = 128; // (part, key) pairs cached per warp in shared memory
+
+// error_flags bits
+constexpr uint32_t ERR_CAPACITY = 1u;        // more particles than the arrays hold
+constexpr uint32_t ERR_CAND_OVERFLOW = 2u;   // a vertex touches more than MAX_CAND cells
+constexpr uint32_t ERR_BAD_CELL = 4u;        // a particle carries an out-of-range cell
+
+struct DevStats {
+    unsigned long long n_particles;
+    unsigned long long lost;
+    unsigned long long removed;
+    unsigned long long seeded;
+    unsigned long long map_failures;
+    unsigned long long near_face;
+    unsigned long long searched;
+    unsigned long long nan_dofs;
+    unsigned long long fallback64;   // FP32 form: sub-steps relocated by the FP64 search
+    unsigned long long particle_steps; // particles advanced, summed over moves
+    unsigned int next_id;
+    unsigned int error_flags;
+};
+
+struct MeshDev {
+    int nC, nV, nD;
+    const int32_t* cv;        // nC x NV vertex ids
+    const int32_t* cd;        // nC x NV DoF ids
+    const double* cellX;      // nC x NV x DIM vertex coordinates, cell-major
+    const double* aff;        // nC x (DIM*DIM + DIM): inverse affine approximation A^-1 and b
+    const float* geo32;       // nC x GEO_STRIDE: FP32 multilinear coefficients relative to vertex 0
+    const int32_t* v2c_off;   // nV + 1
+    const int32_t* v2c_cells; // cells around each vertex, ascending
+    const double* v2c_dirs;   // DIM per entry: unit vertex -> cell-centre direction
+    const int32_t* d2c_off;   // nD + 1
+    const int32_t* d2c_ent;   // cell * NV + local vertex, cells ascending
+};
+
+struct PartParams {
+    int q[3];
+    int npart;     // q0*q1*q2 real cell parts
+    int npe;       // (q0+1)(q1+1)(q2+1) extended parts
+    int maxpp;     // maximum particles per cell part (max+1 survive)
+    int S;         // sub-steps
+    double dtp;    // dt / S
+    double h[3];   // 1.0 / q
+    uint32_t seed; // removal key seed
+};
+
+// SoA particle arrays; x is null in the FP32 form.
+struct PartState {
+    uint32_t* cell;
+    uint32_t* id;
+    void* x[3];
+    void* xi[3];
+    void* v[3];
+};
+
+struct StepArgs {
+    MeshDev mesh;
+    PartParams pp;
+    PartState S0;   // current, sorted
+    PartState S1;   // next, sorted
+    PartState T;    // advect output, in S0 order (cell/id unused)
+    const void* Vaos;   // nD x VS velocity, VS = 4 (3D) or 2 (2D)
+    const void* dVaos;  // nD x VS velocity increment V - Vold
+    int do_correct;
+    int apply_counts;   // write kernel: 1 = count correction, 0 = keep all (re-sort only)
+    uint32_t* key;      // advect output cell, or LOST
+    uint32_t* slot;     // rank of arrival in the cell counter
+    uint32_t* idx;      // bucketed particle indices, cell-major
+    uint32_t* cell_count;
+    uint32_t* cell_off;            // nC + 1
+    unsigned long long* packed;    // per cell: seeds << 32 | final count
+    unsigned long long* packed_off;// nC + 1 exclusive scan of packed
+    void* partials;                // nC x PW projection partial sums
+    double* Vout;                  // nD x DIM component-major projected velocity
+    const double* Vkeep;           // empty_dof_policy 1: value kept where no particle contributes
+    DevStats* stats;
+    uint32_t capacity;
+};
+
+template <int DIM> struct Dims {
+    static constexpr int NV = 1 << DIM;
+    static constexpr int VS = DIM == 3 ? 4 : 2;        // padded velocity stride
+    static constexpr int PW = DIM == 3 ? 32 : 16;      // projection partials per cell (NV x 4)
+    static constexpr int AFF = DIM * DIM + DIM;
+    static constexpr int GEO = DIM == 3 ? 24 : 8;      // FP32 geometry floats per cell
+};
+
+__host__ __device__ inline uint32_t key_of(uint32_t id, uint32_t seed)
+{
+    if (!seed) return id;
+    uint32_t x = id ^ seed;  // bijective 32-bit mixer (lowbias32, C. Wellons)
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+// Extended cell-part index of reference coordinates: (int)(xi_d / h_d) per
+// direction (src/pfem2particlehandler.cpp:369-370), which reaches q_d on the
+// upper face; digits combined x-major, base q_d + 1.
+template <int DIM, typename Real>
+__device__ __forceinline__ int ext_part(const Real* xi, const PartParams& pp)
+{
+    int e = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        int k = (int)((double)xi[d] / pp.h[d]);
+        k = k < 0 ? 0 : (k > pp.q[d] ? pp.q[d] : k);
+        e = e * (pp.q[d] + 1) + k;
+    }
+    return e;
+}
+
+// Is extended part e one of the q0*q1*q2 real parts?  Writes its digits.
+template <int DIM>
+__device__ __forceinline__ bool real_part(int e, const PartParams& pp, int* idx)
+{
+    bool real = true;
+#pragma unroll
+    for (int d = DIM - 1; d >= 0; --d) {
+        const int b = pp.q[d] + 1;
+        idx[d] = e % b;
+        e /= b;
+        real = real && idx[d] < pp.q[d];
+    }
+    return real;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One atomic per warp for a per-thread counter (all 32 lanes must call it).
+__device__ __forceinline__ void warp_count(unsigned long long* dst, unsigned long long v)
+{
+    v = warp_sum_u64(v);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
+}
+
+}  // namespace pfem2

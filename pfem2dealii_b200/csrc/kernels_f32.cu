@@ -1,0 +1,84 @@
+// FP32 form: FP32 reference coordinates and velocities, compensated FP32
+// projection sums; FP64 only for face-crossing relocation and the final DoF
+// division.  Also the precision-dispatching launchers.
+#include "advect.cuh"
+#include "cellwork.cuh"
+#include "launch.h"
+
+namespace pfem2 {
+
+int launch64_seed(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s);
+int launch64_advect(int dim, const StepArgs& a, cudaStream_t s);
+int launch64_count(int dim, const StepArgs& a, cudaStream_t s);
+int launch64_write(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s);
+int launch64_partials(int dim, const StepArgs& a, const uint32_t* cs, cudaStream_t s);
+int launch64_correct(int dim, const StepArgs& a, cudaStream_t s);
+int launch64_gather(int dim, const StepArgs& a, int keep, cudaStream_t s);
+
+#define PFEM2_GRID(kern, thr) occupancy_grid((const void*)(kern), (thr))
+#define CELL_THREADS (CELL_WARPS * 32)
+
+int launch_seed(int dim, int prec, const StepArgs& a, uint32_t* cs, cudaStream_t s)
+{
+    if (prec == 0) return launch64_seed(dim, a, cs, s);
+    if (dim == 2) k_seed<2, float><<<PFEM2_GRID((k_seed<2, float>), 256), 256, 0, s>>>(a, cs);
+    else k_seed<3, float><<<PFEM2_GRID((k_seed<3, float>), 256), 256, 0, s>>>(a, cs);
+    return 1;
+}
+
+int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s)
+{
+    if (prec == 0) return launch64_advect(dim, a, s);
+    if (dim == 2) k_advect32<2><<<PFEM2_GRID(k_advect32<2>, 256), 256, 0, s>>>(a);
+    else k_advect32<3><<<PFEM2_GRID(k_advect32<3>, 256), 256, 0, s>>>(a);
+    return 1;
+}
+
+int launch_count(int dim, int prec, const StepArgs& a, cudaStream_t s)
+{
+    if (prec == 0) return launch64_count(dim, a, s);
+    if (dim == 2) k_count<2, float><<<PFEM2_GRID((k_count<2, float>), CELL_THREADS), CELL_THREADS, 0, s>>>(a);
+    else k_count<3, float><<<PFEM2_GRID((k_count<3, float>), CELL_THREADS), CELL_THREADS, 0, s>>>(a);
+    return 1;
+}
+
+int launch_write(int dim, int prec, const StepArgs& a, uint32_t* cs, cudaStream_t s)
+{
+    if (prec == 0) return launch64_write(dim, a, cs, s);
+    if (dim == 2) k_write<2, float><<<PFEM2_GRID((k_write<2, float>), CELL_THREADS), CELL_THREADS, 0, s>>>(a, cs);
+    else k_write<3, float><<<PFEM2_GRID((k_write<3, float>), CELL_THREADS), CELL_THREADS, 0, s>>>(a, cs);
+    return 1;
+}
+
+int launch_partials(int dim, int prec, const StepArgs& a, const uint32_t* cs, cudaStream_t s)
+{
+    if (prec == 0) return launch64_partials(dim, a, cs, s);
+    if (dim == 2) k_partials<2, float><<<PFEM2_GRID((k_partials<2, float>), CELL_THREADS), CELL_THREADS, 0, s>>>(a, cs);
+    else k_partials<3, float><<<PFEM2_GRID((k_partials<3, float>), CELL_THREADS), CELL_THREADS, 0, s>>>(a, cs);
+    return 1;
+}
+
+int launch_correct(int dim, int prec, const StepArgs& a, cudaStream_t s)
+{
+    if (prec == 0) return launch64_correct(dim, a, s);
+    if (dim == 2) k_correct<2, float><<<PFEM2_GRID((k_correct<2, float>), 256), 256, 0, s>>>(a);
+    else k_correct<3, float><<<PFEM2_GRID((k_correct<3, float>), 256), 256, 0, s>>>(a);
+    return 1;
+}
+
+int launch_gather(int dim, int prec, const StepArgs& a, int keep, cudaStream_t s)
+{
+    if (prec == 0) return launch64_gather(dim, a, keep, s);
+    if (dim == 2) k_gather<2, float><<<PFEM2_GRID((k_gather<2, float>), 256), 256, 0, s>>>(a, keep);
+    else k_gather<3, float><<<PFEM2_GRID((k_gather<3, float>), 256), 256, 0, s>>>(a, keep);
+    return 1;
+}
+
+int launch_positions32(int dim, const StepArgs& a, double* xout, cudaStream_t s)
+{
+    if (dim == 2) k_positions32<2><<<PFEM2_GRID(k_positions32<2>, 256), 256, 0, s>>>(a, xout);
+    else k_positions32<3><<<PFEM2_GRID(k_positions32<3>, 256), 256, 0, s>>>(a, xout);
+    return 1;
+}
+
+}  // namespace pfem2

@@ -1,0 +1,127 @@
+// FP64 form (the plain form): compiled with --fmad=false so its arithmetic is
+// the reference's own, rounding for rounding.  Also hosts the per-cell
+// geometry set-up (vertex coordinates, inverse affine approximation, FP32
+// multilinear coefficients) shared by both forms.
+#include "advect.cuh"
+#include "cellwork.cuh"
+#include "launch.h"
+
+namespace pfem2 {
+
+namespace {
+
+template <int DIM>
+__global__ void k_cell_setup(int nC, const double* __restrict__ verts, const int32_t* __restrict__ cv,
+                             double* __restrict__ cellX, double* __restrict__ aff, float* __restrict__ geo32)
+{
+    constexpr int NV = 1 << DIM, GS = Dims<DIM>::GEO;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nC; c += gridDim.x * blockDim.x) {
+        double X[NV][DIM];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            const int32_t v = cv[(size_t)c * NV + i];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                X[i][d] = verts[(size_t)v * DIM + d];
+                cellX[((size_t)c * NV + i) * DIM + d] = X[i][d];
+            }
+        }
+        affine_setup64<DIM>(X, aff + (size_t)c * Dims<DIM>::AFF);
+        // nested forward differences: Y[k] = Delta^k X (Moebius coefficients)
+        double Y[NV][DIM];
+#pragma unroll
+        for (int i = 0; i < NV; ++i)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) Y[i][d] = X[i][d];
+#pragma unroll
+        for (int b = 0; b < DIM; ++b)
+#pragma unroll
+            for (int i = NV - 1; i >= 0; --i)
+                if ((i >> b) & 1)
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) Y[i][d] = Y[i][d] - Y[i ^ (1 << b)][d];
+        bool affine = true;
+        float* g = geo32 + (size_t)c * GS;
+#pragma unroll
+        for (int k = 1; k < NV; ++k)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                g[(k - 1) * DIM + d] = (float)Y[k][d];
+                if (__popc(k) >= 2 && Y[k][d] != 0.0) affine = false;
+            }
+        for (int k = (NV - 1) * DIM; k < GS - 1; ++k) g[k] = 0.0f;
+        g[GS - 1] = affine ? 1.0f : 0.0f;
+    }
+}
+
+int grid_of(const void* k, int threads) { return occupancy_grid(k, threads); }
+
+template <int DIM>
+int seed_t(const StepArgs& a, uint32_t* cs, cudaStream_t s)
+{
+    k_seed<DIM, double><<<grid_of((const void*)k_seed<DIM, double>, 256), 256, 0, s>>>(a, cs);
+    return 1;
+}
+
+}  // namespace
+
+int launch_cell_setup(int dim, int nC, const double* verts, const int32_t* cv, double* cellX, double* aff,
+                      float* geo32, cudaStream_t s)
+{
+    const int grid = (nC + 127) / 128;
+    if (dim == 2) k_cell_setup<2><<<grid, 128, 0, s>>>(nC, verts, cv, cellX, aff, geo32);
+    else k_cell_setup<3><<<grid, 128, 0, s>>>(nC, verts, cv, cellX, aff, geo32);
+    return 1;
+}
+
+// FP64 launchers (called through the precision-dispatching launchers below)
+int launch64_seed(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s)
+{
+    return dim == 2 ? seed_t<2>(a, cs, s) : seed_t<3>(a, cs, s);
+}
+
+#define PFEM2_GRID(kern, thr) occupancy_grid((const void*)(kern), (thr))
+
+int launch64_advect(int dim, const StepArgs& a, cudaStream_t s)
+{
+    if (dim == 2) k_advect64<2><<<PFEM2_GRID(k_advect64<2>, 256), 256, 0, s>>>(a);
+    else k_advect64<3><<<PFEM2_GRID(k_advect64<3>, 256), 256, 0, s>>>(a);
+    return 1;
+}
+
+int launch64_count(int dim, const StepArgs& a, cudaStream_t s)
+{
+    if (dim == 2) k_count<2, double><<<PFEM2_GRID((k_count<2, double>), CELL_WARPS * 32), CELL_WARPS * 32, 0, s>>>(a);
+    else k_count<3, double><<<PFEM2_GRID((k_count<3, double>), CELL_WARPS * 32), CELL_WARPS * 32, 0, s>>>(a);
+    return 1;
+}
+
+int launch64_write(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s)
+{
+    if (dim == 2) k_write<2, double><<<PFEM2_GRID((k_write<2, double>), CELL_WARPS * 32), CELL_WARPS * 32, 0, s>>>(a, cs);
+    else k_write<3, double><<<PFEM2_GRID((k_write<3, double>), CELL_WARPS * 32), CELL_WARPS * 32, 0, s>>>(a, cs);
+    return 1;
+}
+
+int launch64_partials(int dim, const StepArgs& a, const uint32_t* cs, cudaStream_t s)
+{
+    if (dim == 2) k_partials<2, double><<<PFEM2_GRID((k_partials<2, double>), CELL_WARPS * 32), CELL_WARPS * 32, 0, s>>>(a, cs);
+    else k_partials<3, double><<<PFEM2_GRID((k_partials<3, double>), CELL_WARPS * 32), CELL_WARPS * 32, 0, s>>>(a, cs);
+    return 1;
+}
+
+int launch64_correct(int dim, const StepArgs& a, cudaStream_t s)
+{
+    if (dim == 2) k_correct<2, double><<<PFEM2_GRID((k_correct<2, double>), 256), 256, 0, s>>>(a);
+    else k_correct<3, double><<<PFEM2_GRID((k_correct<3, double>), 256), 256, 0, s>>>(a);
+    return 1;
+}
+
+int launch64_gather(int dim, const StepArgs& a, int keep, cudaStream_t s)
+{
+    if (dim == 2) k_gather<2, double><<<PFEM2_GRID((k_gather<2, double>), 256), 256, 0, s>>>(a, keep);
+    else k_gather<3, double><<<PFEM2_GRID((k_gather<3, double>), 256), 256, 0, s>>>(a, keep);
+    return 1;
+}
+
+}  // namespace pfem2

@@ -1,0 +1,57 @@
+// Host-side launchers of the particle kernels (one translation unit per
+// precision form plus the integer kernels).  Each launcher returns the number
+// of kernels it enqueued on the stream.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <unordered_map>
+
+#include "common.cuh"
+
+namespace pfem2 {
+
+// Grid of a grid-stride kernel: every SM filled to its occupancy limit.
+inline int occupancy_grid(const void* kernel, int threads, size_t smem = 0)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(kernel);
+    if (it != cache.end()) return it->second;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
+    const int g = sms * (per > 0 ? per : 1);
+    cache[kernel] = g;
+    return g;
+}
+
+// kernels_f64.cu / kernels_f32.cu (prec: 0 = FP64 form, 1 = FP32 form)
+int launch_cell_setup(int dim, int nC, const double* verts, const int32_t* cv, double* cellX, double* aff,
+                      float* geo32, cudaStream_t s);
+int launch_seed(int dim, int prec, const StepArgs& a, uint32_t* cell_start, cudaStream_t s);
+int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s);
+int launch_count(int dim, int prec, const StepArgs& a, cudaStream_t s);
+int launch_write(int dim, int prec, const StepArgs& a, uint32_t* cell_start, cudaStream_t s);
+int launch_partials(int dim, int prec, const StepArgs& a, const uint32_t* cell_start, cudaStream_t s);
+int launch_correct(int dim, int prec, const StepArgs& a, cudaStream_t s);
+int launch_gather(int dim, int prec, const StepArgs& a, int keep_empty, cudaStream_t s);
+int launch_positions32(int dim, const StepArgs& a, double* xout, cudaStream_t s);
+
+// misc.cu
+constexpr int SCAN_TILE = 2048;        // elements per block
+constexpr int SCAN_MAX_TILES = 8192;   // top-level scan capacity
+int launch_scan_u32(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* tile_tmp, cudaStream_t s);
+int launch_scan_u64(const unsigned long long* in, uint32_t n, unsigned long long* out, unsigned long long* tile_tmp,
+                    cudaStream_t s);
+int launch_bucket(const StepArgs& a, cudaStream_t s);
+int launch_rekey(const StepArgs& a, cudaStream_t s);
+int launch_finalize(const StepArgs& a, uint32_t* cell_start, int count_step, cudaStream_t s);
+int launch_set_state(DevStats* st, long long n, long long next_id, long long add_id, cudaStream_t s);
+int launch_prep_v(int dim, int prec, const double* V, const double* Vold, int nD, void* Vaos, void* dVaos,
+                  cudaStream_t s);
+
+}  // namespace pfem2

@@ -1,0 +1,242 @@
+"""Python mirror of pfem2ParticleHandler<dim> over the C ABI.
+
+Method names and meaning follow src/pfem2particlehandler.h:17-71 of the
+reference; the solver-owned inputs (parameters, mesh, the FEM velocity
+vectors) are passed in explicitly instead of being fetched from a
+pfem2Solver.  Velocity vectors are component-major arrays of shape
+(dim, n_dofs), host numpy arrays or (for the *_device calls) CUDA tensors.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import json
+
+import numpy as np
+
+from . import _lib
+from .mesh import Mesh, vertex_maps
+
+
+@dataclasses.dataclass
+class ParticleParams:
+    """The particle keys of the reference's .prm file
+    (src/pfem2parameterhandler.cpp:64-74, 40)."""
+
+    particles_per_cell: tuple = (2, 2, 2)
+    max_particles_per_cell_part: int = 2
+    particle_integration_steps: int = 5
+    time_step: float = 0.1
+    removal_seed: int = 0
+    empty_dof_policy: int = 0
+    capacity: int = 0
+
+    def to_c(self, dim):
+        p = _lib.Params()
+        q = list(self.particles_per_cell) + [1, 1, 1]
+        for d in range(3):
+            p.particles_per_cell[d] = int(q[d]) if d < dim else 1
+        p.max_particles_per_cell_part = int(self.max_particles_per_cell_part)
+        p.particle_integration_steps = int(self.particle_integration_steps)
+        p.time_step = float(self.time_step)
+        p.removal_seed = int(self.removal_seed)
+        p.empty_dof_policy = int(self.empty_dof_policy)
+        p.capacity = int(self.capacity)
+        return p
+
+
+def read_prm(path_or_text) -> ParticleParams:
+    """Particle keys of a deal.II .prm file (subsections 'Particles' and
+    'Computation parameters'), as read by src/pfem2parameterhandler.cpp:25-156."""
+    text = path_or_text
+    if "\n" not in path_or_text:
+        with open(path_or_text) as f:
+            text = f.read()
+    sec = []
+    vals = {}
+    for raw in text.splitlines():
+        line = raw.split("#")[0].strip()
+        if not line:
+            continue
+        if line.startswith("subsection"):
+            sec.append(line[len("subsection"):].strip())
+        elif line == "end":
+            sec.pop()
+        elif line.startswith("set"):
+            k, _, v = line[3:].partition("=")
+            vals[(sec[-1] if sec else "", k.strip())] = v.strip()
+    P = "Particles"
+    q = [int(vals.get((P, f"Number of particles in the {a} direction"), 2)) for a in "xyz"]
+    return ParticleParams(
+        particles_per_cell=tuple(q),
+        max_particles_per_cell_part=int(vals.get((P, "Maximum number of particles per cell part"), 2)),
+        particle_integration_steps=int(vals.get((P, "Particle integration steps"), 5)),
+        time_step=float(vals.get(("Computation parameters", "Time step"), 0.1)),
+    )
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _host(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class ParticleHandler:
+    """pfem2ParticleHandler<dim> on one B200.  precision: "fp64" (the
+    reference's arithmetic) or "fp32"."""
+
+    def __init__(self, dim: int, params: ParticleParams, precision: str = "fp64"):
+        self.L = _lib.load()
+        self.dim = dim
+        self.params = params
+        self.precision = precision
+        h = C.c_void_p()
+        prec = _lib.FP64 if precision == "fp64" else _lib.FP32
+        _lib.check(self.L.pfem2gpu_create(dim, prec, C.byref(params.to_c(dim)), C.byref(h)))
+        self.h = h
+        self.mesh = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pfem2gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        _lib.check(rc, self.h)
+
+    # -- mesh -----------------------------------------------------------------
+    def initialize_maps(self, mesh: Mesh, with_maps: bool = True):
+        """Mesh upload plus initialize_maps (src/pfem2particlehandler.cpp:320-324)."""
+        assert mesh.dim == self.dim
+        self.mesh = mesh
+        self._keep = [
+            _host(mesh.vertices, np.float64),
+            _host(mesh.cells, np.int32),
+            _host(mesh.cell_dofs, np.int32),
+        ]
+        maps = [None, None, None]
+        if with_maps:
+            off, cells, dirs = vertex_maps(mesh)
+            maps = [_host(off, np.int32), _host(cells, np.int32), _host(dirs, np.float64)]
+            self._keep += maps
+        self._ck(self.L.pfem2gpu_set_mesh(self.h, mesh.n_cells, mesh.n_verts, mesh.n_dofs,
+                                          *[_ptr(a) for a in self._keep[:3]], *[_ptr(a) for a in maps]))
+
+    # -- the particle cycle ---------------------------------------------------
+    def seed_particles(self, V):
+        V = _host(V, np.float64)
+        self._ck(self.L.pfem2gpu_seed(self.h, _ptr(V)))
+
+    def correct_particle_velocity(self, V, Vold):
+        V = _host(V, np.float64)
+        Vold = _host(Vold, np.float64)
+        self._ck(self.L.pfem2gpu_correct(self.h, _ptr(V), _ptr(Vold)))
+
+    def move_particles(self, V=None):
+        V = None if V is None else _host(V, np.float64)
+        self._ck(self.L.pfem2gpu_move(self.h, _ptr(V)))
+
+    def project_particle_fields(self):
+        out = np.empty((self.dim, self.mesh.n_dofs))
+        self._ck(self.L.pfem2gpu_project(self.h, _ptr(out)))
+        return out
+
+    def step(self, V, Vold):
+        """One time step of the reference loop (src/pfem2solver.cpp:162-164)."""
+        self.correct_particle_velocity(V, Vold)
+        self.move_particles(None)
+        return self.project_particle_fields()
+
+    # device-resident variants (torch CUDA tensors, float64, shape (dim, n_dofs))
+    def seed_particles_device(self, dV):
+        self._ck(self.L.pfem2gpu_seed_device(self.h, _ptr(dV)))
+
+    def correct_particle_velocity_device(self, dV, dVold):
+        self._ck(self.L.pfem2gpu_correct_device(self.h, _ptr(dV), _ptr(dVold)))
+
+    def move_particles_device(self, dV=None):
+        self._ck(self.L.pfem2gpu_move_device(self.h, _ptr(dV)))
+
+    def project_particle_fields_device(self, dout):
+        self._ck(self.L.pfem2gpu_project_device(self.h, _ptr(dout)))
+
+    # -- particle access ------------------------------------------------------
+    def particles(self):
+        """Host copy of the particles (begin()/end() of the reference)."""
+        n = C.c_int64()
+        self.L.pfem2gpu_get_particles(self.h, None, None, None, None, None, 0, C.byref(n))
+        cap = max(n.value, 1)
+        ids = np.zeros(cap, np.uint32)
+        cell = np.zeros(cap, np.int32)
+        x = np.zeros((cap, self.dim))
+        xi = np.zeros((cap, self.dim))
+        v = np.zeros((cap, self.dim))
+        self._ck(self.L.pfem2gpu_get_particles(self.h, _ptr(ids), _ptr(cell), _ptr(x), _ptr(xi), _ptr(v), cap,
+                                               C.byref(n)))
+        k = n.value
+        return {"id": ids[:k], "cell": cell[:k], "x": x[:k], "xi": xi[:k], "v": v[:k]}
+
+    def set_particles(self, P, next_id):
+        n = len(P["id"])
+        arrs = [_host(P["id"], np.uint32), _host(P["cell"], np.int32), _host(P["x"], np.float64),
+                _host(P["xi"], np.float64), _host(P["v"], np.float64)]
+        self._ck(self.L.pfem2gpu_set_particles(self.h, n, *[_ptr(a) for a in arrs], next_id))
+
+    def output_particle_solution(self, timestep_number: int, directory: str = "."):
+        """particles-NN.000.vtu plus particles-NN.pvtu
+        (src/pfem2particlehandler.cpp:218-317, one rank)."""
+        import os
+
+        base = f"particles-{timestep_number:02d}"
+        self._ck(self.L.pfem2gpu_write_vtu(self.h, os.path.join(directory, base + ".000.vtu").encode()))
+        with open(os.path.join(directory, base + ".pvtu"), "w") as f:
+            f.write('<?xml version="1.0" ?> \n<VTKFile type="PUnstructuredGrid" version="0.1" '
+                    'byte_order="LittleEndian">\n  <PUnstructuredGrid GhostLevel="0">\n'
+                    '    <PPointData Scalars="scalars">\n'
+                    '      <PDataArray type="Float32" Name="velocity" NumberOfComponents="3" format="ascii"/>\n'
+                    '      <PDataArray type="Float32" Name="subdomain" format="ascii"/>\n'
+                    '    </PPointData>\n    <PPoints>\n'
+                    '      <PDataArray type="Float32" NumberOfComponents="3"/>\n    </PPoints>\n'
+                    f'    <Piece Source="{base}.000.vtu"/>  </PUnstructuredGrid>\n</VTKFile>\n')
+
+    # -- diagnostics ----------------------------------------------------------
+    def stats(self):
+        s = _lib.Stats()
+        self._ck(self.L.pfem2gpu_get_stats(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def reset_stats(self):
+        self._ck(self.L.pfem2gpu_reset_stats(self.h))
+
+    def synchronize(self):
+        self._ck(self.L.pfem2gpu_synchronize(self.h))
+
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        self._ck(self.L.pfem2gpu_get_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def profile(self, on: bool):
+        self._ck(self.L.pfem2gpu_profile(self.h, 1 if on else 0))
+
+    def profile_report(self):
+        buf = C.create_string_buffer(1 << 16)
+        self._ck(self.L.pfem2gpu_profile_report(self.h, buf, 1 << 16))
+        return json.loads(buf.value.decode())
+
+    def launch_count(self) -> int:
+        c = C.c_uint64()
+        self._ck(self.L.pfem2gpu_launch_count(self.h, C.byref(c)))
+        return c.value
