@@ -17,11 +17,6 @@
 
 namespace pfem2 {
 
-struct RelocCounters {
-    unsigned long long map_failures = 0, near_face = 0, searched = 0;
-    uint32_t err = 0;
-};
-
 template <int DIM>
 struct Vec {
     double v[DIM];
@@ -142,20 +137,6 @@ __device__ __noinline__ SearchOut search64(const MeshDev m, uint32_t c, Vec<DIM>
     return out;
 }
 
-template <int DIM>
-__device__ __forceinline__ bool take_search(const SearchOut& so, uint32_t& c, double* xi, RelocCounters& rc)
-{
-    rc.searched++;
-    rc.map_failures += so.map_failures;
-    if (so.flags & SRCH_OVERFLOW) rc.err |= ERR_CAND_OVERFLOW;
-    if (!(so.flags & SRCH_FOUND)) return false;
-    if (so.flags & SRCH_NEAR) rc.near_face++;
-    c = so.cell;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) xi[d] = so.xi[d];
-    return true;
-}
-
 // Full FP64 relocation of an FP32-form particle: rebuild x = F(xi) + u dt_p in
 // FP64, inverse map in the own cell, then the vertex-patch search.
 template <int DIM>
@@ -185,244 +166,457 @@ __device__ __noinline__ SearchOut fallback64(const MeshDev m, uint32_t c, Vec<DI
     return out;
 }
 
-template <int DIM>
-__device__ __forceinline__ void finish_counters(const StepArgs& a, unsigned long long lost, const RelocCounters& rc,
-                                                unsigned long long fb)
+struct AdvCounters {
+    uint32_t lost = 0, map_failures = 0, near_face = 0, searched = 0, fallback = 0, deferred = 0;
+    uint32_t err = 0;
+};
+
+__device__ __forceinline__ void flush_counters(const StepArgs& a, const AdvCounters& k)
 {
-    warp_count(&a.stats->lost, lost);
-    warp_count(&a.stats->map_failures, rc.map_failures);
-    warp_count(&a.stats->near_face, rc.near_face);
-    warp_count(&a.stats->searched, rc.searched);
-    warp_count(&a.stats->fallback64, fb);
-    const unsigned e = __reduce_or_sync(0xffffffffu, rc.err);
+    warp_count(&a.stats->lost, k.lost);
+    warp_count(&a.stats->map_failures, k.map_failures);
+    warp_count(&a.stats->near_face, k.near_face);
+    warp_count(&a.stats->searched, k.searched);
+    warp_count(&a.stats->fallback64, k.fallback);
+    const unsigned e = __reduce_or_sync(0xffffffffu, k.err);
     if ((threadIdx.x & 31) == 0 && e) atomicOr(&a.stats->error_flags, e);
 }
 
-// FP64 form: the reference's own state and arithmetic (global location x
-// advanced as x + u*dt_p, reference coordinates re-derived by the inverse map).
+// Queue a particle whose sub-step s needs the vertex-patch search (FP64
+// form) or the FP64 relocation (FP32 form); one atomic per warp.
+__device__ __forceinline__ void defer(const StepArgs& a, bool want, uint32_t i, int s)
+{
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(a.nxq, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (want) {
+        const uint32_t k = base + __popc(m & ((1u << lane) - 1u));
+        if (k < a.capacity) a.xq[k] = make_uint2(i, (uint32_t)s);
+    }
+}
+
+__device__ __forceinline__ void arrive(const StepArgs& a, uint32_t i, uint32_t c, bool alive)
+{
+    if (alive) {
+        a.key[i] = c;
+        a.slot[i] = atomicAdd(a.cell_count + c, 1u);
+    } else {
+        a.key[i] = LOST;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 form.  Per sub-step (src/pfem2particlehandler.cpp:150-167): u = sum N V,
+// x += u dt_p, inverse map in the own cell (:424-431).  A particle that leaves
+// its cell is queued with the sub-step index; k_search64 runs the
+// vertex-patch search for it and finishes its remaining sub-steps.  Values
+// are the same as running everything in one place: every operation is
+// repeated in the same order.
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+__device__ __forceinline__ void velocity64(const MeshDev& m, const double* __restrict__ V, const int32_t* dof,
+                                           const double* xi, double* u)
+{
+    constexpr int NV = 1 << DIM, VS = Dims<DIM>::VS;
+    double N[NV];
+    shape64<DIM>(xi, N);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) u[d] = 0.0;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv)
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) u[d] = u[d] + N[iv] * __ldg(V + (size_t)dof[iv] * VS + d);
+}
+
+template <int DIM>
+__device__ __forceinline__ void load_dofs(const MeshDev& m, uint32_t c, int32_t* dof)
+{
+#pragma unroll
+    for (int iv = 0; iv < (1 << DIM); ++iv) dof[iv] = __ldg(m.cd + (size_t)c * (1 << DIM) + iv);
+}
+
+// Sub-steps s0.. of one FP64 particle starting in cell c; returns the
+// sub-step at which it leaves its cell (S if it never does).
+template <int DIM>
+__device__ __forceinline__ int substeps64(const StepArgs& a, uint32_t c, int s0, double* x, double* xi, double* u,
+                                          AdvCounters& k)
+{
+    constexpr int NV = 1 << DIM;
+    const MeshDev& m = a.mesh;
+    const double* __restrict__ V = (const double*)a.Vaos;
+    double X[NV][DIM];
+    int32_t dof[NV];
+    load_cell64<DIM>(m.cellX, c, X);
+    load_dofs<DIM>(m, c, dof);
+    int s = s0;
+    for (; s < a.pp.S; ++s) {
+        velocity64<DIM>(m, V, dof, xi, u);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const double st = u[d] * a.pp.dtp;
+            x[d] = x[d] + st;
+        }
+        double xin[DIM];
+        const int st = inverse_map64<DIM>(X, m.aff + (size_t)c * Dims<DIM>::AFF, x, xin);
+        if (st) k.map_failures++;
+        if (st == 0 && inside_unit<DIM>(xin)) {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) xi[d] = xin[d];
+            if (near_face64<DIM>(xin)) k.near_face++;
+            continue;
+        }
+        break;
+    }
+    return s;
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
 {
     constexpr int NV = 1 << DIM, VS = Dims<DIM>::VS;
     const MeshDev& m = a.mesh;
     const uint32_t n = (uint32_t)a.stats->n_particles;
-    const double* __restrict__ V = (const double*)a.Vaos;
     const double* __restrict__ dV = (const double*)a.dVaos;
-    RelocCounters rc;
-    unsigned long long lost = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t c = a.S0.cell[i];
-        double x[DIM], xi[DIM], v[DIM];
+    AdvCounters k;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t nloop = (n + stride - 1) / stride * stride;  // whole warps iterate together
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nloop; i += stride) {
+        const bool act = i < n;
+        uint32_t c = act ? a.S0.cell[i] : 0u;
+        bool want = false;
+        int s = 0;
+        if (act) {
+            double x[DIM], xi[DIM], v[DIM], u[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                x[d] = ((const double*)a.S0.x[d])[i];
+                xi[d] = ((const double*)a.S0.xi[d])[i];
+                v[d] = ((const double*)a.S0.v[d])[i];
+            }
+            bool alive = c < (uint32_t)m.nC;
+            if (!alive) k.err |= ERR_BAD_CELL;
+            if (alive) {
+                if (a.do_correct) {  // :126-138
+                    int32_t dof[NV];
+                    load_dofs<DIM>(m, c, dof);
+                    double N[NV], corr[DIM];
+                    shape64<DIM>(xi, N);
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) corr[d] = 0.0;
+#pragma unroll
+                    for (int iv = 0; iv < NV; ++iv)
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d)
+                            corr[d] = corr[d] + N[iv] * __ldg(dV + (size_t)dof[iv] * VS + d);
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) v[d] = v[d] + corr[d];
+                }
+                s = substeps64<DIM>(a, c, 0, x, xi, u, k);
+                want = s < a.pp.S;
+            }
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                ((double*)a.T.x[d])[i] = x[d];
+                ((double*)a.T.xi[d])[i] = xi[d];
+                ((double*)a.T.v[d])[i] = v[d];
+            }
+            if (want) a.key[i] = c;
+            else {
+                arrive(a, i, c, alive);
+                if (!alive) k.lost++;
+            }
+        }
+        defer(a, want, i, s);
+    }
+    flush_counters(a, k);
+}
+
+// Deferred FP64 particles: the search of sub-step s (:438-491), then the
+// remaining sub-steps (searching again whenever needed).
+template <int DIM>
+__global__ void __launch_bounds__(128) k_search64(StepArgs a)
+{
+    const uint32_t nq = *a.nxq < a.capacity ? *a.nxq : a.capacity;
+    const MeshDev& m = a.mesh;
+    AdvCounters k;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const uint2 e = a.xq[q];
+        const uint32_t i = e.x;
+        int s = (int)e.y;
+        uint32_t c = a.key[i];
+        double x[DIM], xi[DIM], u[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
-            x[d] = ((const double*)a.S0.x[d])[i];
-            xi[d] = ((const double*)a.S0.xi[d])[i];
-            v[d] = ((const double*)a.S0.v[d])[i];
+            x[d] = ((const double*)a.T.x[d])[i];
+            xi[d] = ((const double*)a.T.xi[d])[i];
         }
-        bool alive = c < (uint32_t)m.nC;
-        if (!alive) rc.err |= ERR_BAD_CELL;
-        if (alive) {
-            double X[NV][DIM];
-            load_cell64<DIM>(m.cellX, c, X);
-            int32_t dof[NV];
+        bool alive = true;
+        while (true) {
+            // velocity_ext of sub-step s, recomputed from the start-of-sub-step state
+            int32_t dof[1 << DIM];
+            load_dofs<DIM>(m, c, dof);
+            velocity64<DIM>(m, (const double*)a.Vaos, dof, xi, u);
+            Vec<DIM> xo, ve, xp;
 #pragma unroll
-            for (int iv = 0; iv < NV; ++iv) dof[iv] = __ldg(m.cd + (size_t)c * NV + iv);
-            if (a.do_correct) {  // src/pfem2particlehandler.cpp:126-138
-                double N[NV], corr[DIM];
-                shape64<DIM>(xi, N);
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) corr[d] = 0.0;
-#pragma unroll
-                for (int iv = 0; iv < NV; ++iv)
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) corr[d] = corr[d] + N[iv] * __ldg(dV + (size_t)dof[iv] * VS + d);
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) v[d] = v[d] + corr[d];
+            for (int d = 0; d < DIM; ++d) {
+                xo.v[d] = xi[d];
+                ve.v[d] = u[d];
+                xp.v[d] = x[d];
             }
-            for (int s = 0; s < a.pp.S; ++s) {  // :150-167
-                double N[NV], u[DIM];
-                shape64<DIM>(xi, N);
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) u[d] = 0.0;
-#pragma unroll
-                for (int iv = 0; iv < NV; ++iv)
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) u[d] = u[d] + N[iv] * __ldg(V + (size_t)dof[iv] * VS + d);
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    const double st = u[d] * a.pp.dtp;
-                    x[d] = x[d] + st;
-                }
-                // relocation, :420-491
-                double xin[DIM];
-                const int st = inverse_map64<DIM>(X, m.aff + (size_t)c * Dims<DIM>::AFF, x, xin);
-                if (st) rc.map_failures++;
-                if (st == 0 && inside_unit<DIM>(xin)) {
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) xi[d] = xin[d];
-                    if (near_face64<DIM>(xin)) rc.near_face++;
-                    continue;
-                }
-                Vec<DIM> xo, ve, xp;
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    xo.v[d] = xi[d];
-                    ve.v[d] = u[d];
-                    xp.v[d] = x[d];
-                }
-                const SearchOut so = search64<DIM>(m, c, xo, ve, xp);
-                if (!take_search<DIM>(so, c, xi, rc)) {
-                    alive = false;
-                    break;
-                }
-                load_cell64<DIM>(m.cellX, c, X);
-#pragma unroll
-                for (int iv = 0; iv < NV; ++iv) dof[iv] = __ldg(m.cd + (size_t)c * NV + iv);
+            const SearchOut so = search64<DIM>(m, c, xo, ve, xp);
+            k.searched++;
+            k.map_failures += so.map_failures;
+            if (so.flags & SRCH_OVERFLOW) k.err |= ERR_CAND_OVERFLOW;
+            if (!(so.flags & SRCH_FOUND)) {
+                alive = false;
+                break;
             }
+            if (so.flags & SRCH_NEAR) k.near_face++;
+            c = so.cell;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) xi[d] = so.xi[d];
+            s = substeps64<DIM>(a, c, s + 1, x, xi, u, k);
+            if (s >= a.pp.S) break;
         }
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
             ((double*)a.T.x[d])[i] = x[d];
             ((double*)a.T.xi[d])[i] = xi[d];
-            ((double*)a.T.v[d])[i] = v[d];
         }
-        if (alive) {
-            a.key[i] = c;
-            a.slot[i] = atomicAdd(a.cell_count + c, 1u);
-        } else {
-            a.key[i] = LOST;
-            lost++;
-        }
+        arrive(a, i, c, alive);
+        if (!alive) k.lost++;
     }
-    finish_counters<DIM>(a, lost, rc, 0);
+    flush_counters(a, k);
 }
 
-// FP32 form: state = (cell, xi, v) in FP32.  A sub-step converts u*dt_p to a
-// reference-coordinate increment in FP32 (advance32); if the particle stays
-// in its cell the step is done, otherwise the global position is rebuilt in
-// FP64 (x = F(xi) + u dt_p) and relocated by the FP64 search above.
+// ---------------------------------------------------------------------------
+// FP32 form.  A sub-step converts u dt_p into a reference-coordinate
+// increment with the cell's FP32 inverse Jacobian (exact for affine cells;
+// Newton on the multilinear map otherwise) and stays in FP32 while the
+// particle stays in its cell.  Particles that leave their cell are queued
+// for k_cross32, which rebuilds the position in FP64 and relocates it there.
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+struct J32 {
+    float Ji[DIM][DIM];
+    bool affine;
+};
+
+template <int DIM>
+__device__ __forceinline__ void load_jinv32(const float* __restrict__ jinv, uint32_t c, J32<DIM>& j)
+{
+    const float4* p = reinterpret_cast<const float4*>(jinv + (size_t)c * Dims<DIM>::JS);
+    float b[Dims<DIM>::JS];
+#pragma unroll
+    for (int k = 0; k < Dims<DIM>::JS / 4; ++k) {
+        const float4 t = __ldg(p + k);
+        b[4 * k] = t.x;
+        b[4 * k + 1] = t.y;
+        b[4 * k + 2] = t.z;
+        b[4 * k + 3] = t.w;
+    }
+#pragma unroll
+    for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) j.Ji[r][q] = b[r * DIM + q];
+    j.affine = b[DIM * DIM] != 0.0f;
+}
+
+template <int DIM>
+struct F3 {
+    float v[DIM];
+    bool ok;
+};
+
+// Newton on a non-affine cell, out of line (by value).
+template <int DIM>
+__device__ __noinline__ F3<DIM> newton32(const float* __restrict__ geo, uint32_t c, F3<DIM> xi, F3<DIM> dx)
+{
+    Geo32<DIM> g;
+    load_geo32<DIM>(geo, c, g);
+    F3<DIM> out;
+    out.ok = advance32<DIM>(g, xi.v, dx.v, out.v);
+    return out;
+}
+
+template <int DIM>
+__device__ __forceinline__ void velocity32(const float* __restrict__ V, const int32_t* dof, const float* xi, float* u)
+{
+    float N[1 << DIM];
+    shape32<DIM>(xi, N);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) u[d] = 0.0f;
+#pragma unroll
+    for (int iv = 0; iv < (1 << DIM); ++iv) {
+        if constexpr (DIM == 3) {
+            const float4 t = __ldg(reinterpret_cast<const float4*>(V) + dof[iv]);
+            u[0] += N[iv] * t.x;
+            u[1] += N[iv] * t.y;
+            u[2] += N[iv] * t.z;
+        } else {
+            const float2 t = __ldg(reinterpret_cast<const float2*>(V) + dof[iv]);
+            u[0] += N[iv] * t.x;
+            u[1] += N[iv] * t.y;
+        }
+    }
+}
+
+// FP32 sub-steps s0.. in cell c; returns the sub-step that leaves the cell
+// (S if none).  xi is advanced in place.
+template <int DIM>
+__device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi, const int32_t* dof)
+{
+    J32<DIM> j;
+    load_jinv32<DIM>(a.mesh.jinv32, c, j);
+    const float dtp = (float)a.pp.dtp;
+    int s = s0;
+    for (; s < a.pp.S; ++s) {
+        float u[DIM], dl[DIM], y[DIM];
+        velocity32<DIM>((const float*)a.Vaos, dof, xi, u);
+        F3<DIM> dx;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) dx.v[d] = u[d] * dtp;
+        bool ok = true;
+        if (j.affine) {
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) {
+                float t = 0.0f;
+#pragma unroll
+                for (int q = 0; q < DIM; ++q) t += j.Ji[r][q] * dx.v[q];
+                dl[r] = t;
+            }
+        } else {
+            F3<DIM> x0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) x0.v[d] = xi[d];
+            const F3<DIM> r = newton32<DIM>(a.mesh.geo32, c, x0, dx);
+            ok = r.ok;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) dl[d] = r.v[d];
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) y[d] = xi[d] + dl[d];
+        if (!(ok && inside_unit<DIM>(y))) break;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xi[d] = y[d];
+    }
+    return s;
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(256) k_advect32(StepArgs a)
 {
-    constexpr int NV = 1 << DIM, VS = Dims<DIM>::VS;
+    constexpr int NV = 1 << DIM;
     const MeshDev& m = a.mesh;
     const uint32_t n = (uint32_t)a.stats->n_particles;
-    const float* __restrict__ V = (const float*)a.Vaos;
-    const float* __restrict__ dV = (const float*)a.dVaos;
-    RelocCounters rc;
-    unsigned long long lost = 0, fb = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t c = a.S0.cell[i];
-        float xi[DIM], v[DIM];
+    AdvCounters k;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t nloop = (n + stride - 1) / stride * stride;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nloop; i += stride) {
+        const bool act = i < n;
+        uint32_t c = act ? a.S0.cell[i] : 0u;
+        bool want = false;
+        int s = 0;
+        if (act) {
+            float xi[DIM], v[DIM];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            xi[d] = ((const float*)a.S0.xi[d])[i];
-            v[d] = ((const float*)a.S0.v[d])[i];
-        }
-        bool alive = c < (uint32_t)m.nC;
-        if (!alive) rc.err |= ERR_BAD_CELL;
-        if (alive) {
-            Geo32<DIM> g;
-            load_geo32<DIM>(m.geo32, c, g);
-            int32_t dof[NV];
-#pragma unroll
-            for (int iv = 0; iv < NV; ++iv) dof[iv] = __ldg(m.cd + (size_t)c * NV + iv);
-            if (a.do_correct) {
-                float N[NV];
-                shape32<DIM>(xi, N);
-#pragma unroll
-                for (int iv = 0; iv < NV; ++iv) {
-                    if constexpr (DIM == 3) {
-                        const float4 t = __ldg(reinterpret_cast<const float4*>(dV) + dof[iv]);
-                        v[0] += N[iv] * t.x;
-                        v[1] += N[iv] * t.y;
-                        v[2] += N[iv] * t.z;
-                    } else {
-                        const float2 t = __ldg(reinterpret_cast<const float2*>(dV) + dof[iv]);
-                        v[0] += N[iv] * t.x;
-                        v[1] += N[iv] * t.y;
-                    }
-                }
+            for (int d = 0; d < DIM; ++d) {
+                xi[d] = ((const float*)a.S0.xi[d])[i];
+                v[d] = ((const float*)a.S0.v[d])[i];
             }
-            for (int s = 0; s < a.pp.S; ++s) {
-                float N[NV], u[DIM];
-                shape32<DIM>(xi, N);
+            const bool alive = c < (uint32_t)m.nC;
+            if (!alive) k.err |= ERR_BAD_CELL;
+            if (alive) {
+                int32_t dof[NV];
+                load_dofs<DIM>(m, c, dof);
+                if (a.do_correct) {
+                    float dv[DIM];
+                    velocity32<DIM>((const float*)a.dVaos, dof, xi, dv);
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) u[d] = 0.0f;
-#pragma unroll
-                for (int iv = 0; iv < NV; ++iv) {
-                    if constexpr (DIM == 3) {
-                        const float4 t = __ldg(reinterpret_cast<const float4*>(V) + dof[iv]);
-                        u[0] += N[iv] * t.x;
-                        u[1] += N[iv] * t.y;
-                        u[2] += N[iv] * t.z;
-                    } else {
-                        const float2 t = __ldg(reinterpret_cast<const float2*>(V) + dof[iv]);
-                        u[0] += N[iv] * t.x;
-                        u[1] += N[iv] * t.y;
-                    }
+                    for (int d = 0; d < DIM; ++d) v[d] += dv[d];
                 }
-                const float dtp = (float)a.pp.dtp;
-                float dx[DIM], dl[DIM], y[DIM];
+                s = substeps32<DIM>(a, c, 0, xi, dof);
+                want = s < a.pp.S;
+            }
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) dx[d] = u[d] * dtp;
-                const bool ok = advance32<DIM>(g, xi, dx, dl);
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) y[d] = xi[d] + dl[d];
-                if (ok && inside_unit<DIM>(y)) {
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) xi[d] = y[d];
-                    continue;
-                }
-                // face crossing (or unsettled Newton): FP64 relocation
-                fb++;
-                Vec<DIM> xo, ue;
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    xo.v[d] = (double)xi[d];
-                    ue.v[d] = (double)u[d];
-                }
-                const uint32_t c0 = c;
-                const SearchOut so = fallback64<DIM>(m, c, xo, ue, a.pp.dtp);
-                double xin[DIM];
-                const bool searched = so.cell != c0 || !(so.flags & SRCH_FOUND);
-                if (searched) {
-                    if (!take_search<DIM>(so, c, xin, rc)) {
-                        alive = false;
-                        break;
-                    }
-                } else {
-                    rc.map_failures += so.map_failures;
-                    if (so.flags & SRCH_NEAR) rc.near_face++;
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) xin[d] = so.xi[d];
-                }
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    const float t = (float)xin[d];
-                    xi[d] = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
-                }
-                if (c != c0) {
-                    load_geo32<DIM>(m.geo32, c, g);
-#pragma unroll
-                    for (int iv = 0; iv < NV; ++iv) dof[iv] = __ldg(m.cd + (size_t)c * NV + iv);
-                }
+            for (int d = 0; d < DIM; ++d) {
+                ((float*)a.T.xi[d])[i] = xi[d];
+                ((float*)a.T.v[d])[i] = v[d];
+            }
+            if (want) a.key[i] = c;
+            else {
+                arrive(a, i, c, alive);
+                if (!alive) k.lost++;
             }
         }
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            ((float*)a.T.xi[d])[i] = xi[d];
-            ((float*)a.T.v[d])[i] = v[d];
-        }
-        if (alive) {
-            a.key[i] = c;
-            a.slot[i] = atomicAdd(a.cell_count + c, 1u);
-        } else {
-            a.key[i] = LOST;
-            lost++;
-        }
+        defer(a, want, i, s);
     }
-    finish_counters<DIM>(a, lost, rc, fb);
+    flush_counters(a, k);
+}
+
+// Queued FP32 particles: FP64 relocation of sub-step s (x = F(xi) + u dt_p,
+// own cell first, then the vertex-patch search), then the remaining
+// sub-steps in FP32 (relocating in FP64 again whenever needed).
+template <int DIM>
+__global__ void __launch_bounds__(128) k_cross32(StepArgs a)
+{
+    constexpr int NV = 1 << DIM;
+    const uint32_t nq = *a.nxq < a.capacity ? *a.nxq : a.capacity;
+    const MeshDev& m = a.mesh;
+    AdvCounters k;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const uint2 e = a.xq[q];
+        const uint32_t i = e.x;
+        int s = (int)e.y;
+        uint32_t c = a.key[i];
+        float xi[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xi[d] = ((const float*)a.T.xi[d])[i];
+        bool alive = true;
+        while (true) {
+            int32_t dof[NV];
+            load_dofs<DIM>(m, c, dof);
+            float u[DIM];
+            velocity32<DIM>((const float*)a.Vaos, dof, xi, u);
+            Vec<DIM> xo, ue;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                xo.v[d] = (double)xi[d];
+                ue.v[d] = (double)u[d];
+            }
+            k.fallback++;
+            const uint32_t c0 = c;
+            const SearchOut so = fallback64<DIM>(m, c, xo, ue, a.pp.dtp);
+            k.map_failures += so.map_failures;
+            if (so.flags & SRCH_OVERFLOW) k.err |= ERR_CAND_OVERFLOW;
+            if (so.cell != c0 || !(so.flags & SRCH_FOUND)) k.searched++;
+            if (!(so.flags & SRCH_FOUND)) {
+                alive = false;
+                break;
+            }
+            if (so.flags & SRCH_NEAR) k.near_face++;
+            c = so.cell;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                const float t = (float)so.xi[d];
+                xi[d] = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
+            }
+            load_dofs<DIM>(m, c, dof);
+            s = substeps32<DIM>(a, c, s + 1, xi, dof);
+            if (s >= a.pp.S) break;
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) ((float*)a.T.xi[d])[i] = xi[d];
+        arrive(a, i, c, alive);
+        if (!alive) k.lost++;
+    }
+    flush_counters(a, k);
 }
 
 }  // namespace pfem2

@@ -39,7 +39,12 @@ struct pfem2gpu_handle {
     uint32_t *key = nullptr, *slot = nullptr, *idx = nullptr;
     double* xtmp = nullptr;
     uint32_t *cell_count = nullptr, *cell_off = nullptr, *cell_start = nullptr, *tiles32 = nullptr;
-    unsigned long long *packed = nullptr, *packed_off = nullptr, *tiles64 = nullptr;
+    uint2* xq = nullptr;
+    uint32_t* nxq = nullptr;
+    unsigned long long *tile_status = nullptr, *totals = nullptr;
+    uint32_t* tile_counter = nullptr;
+    uint32_t ntiles = 0;
+    float* jinv32 = nullptr;
     void* partials = nullptr;
     DevStats* stats = nullptr;
     DevStats* stats_h = nullptr;
@@ -142,6 +147,7 @@ StepArgs args(pfem2gpu_handle* h)
     a.mesh.cellX = h->cellX;
     a.mesh.aff = h->aff;
     a.mesh.geo32 = h->geo32;
+    a.mesh.jinv32 = h->jinv32;
     a.mesh.v2c_off = h->v2c_off;
     a.mesh.v2c_cells = h->v2c_cells;
     a.mesh.v2c_dirs = h->v2c_dirs;
@@ -160,8 +166,12 @@ StepArgs args(pfem2gpu_handle* h)
     a.idx = h->idx;
     a.cell_count = h->cell_count;
     a.cell_off = h->cell_off;
-    a.packed = h->packed;
-    a.packed_off = h->packed_off;
+    a.xq = h->xq;
+    a.nxq = h->nxq;
+    a.tile_status = h->tile_status;
+    a.tile_counter = h->tile_counter;
+    a.ntiles = h->ntiles;
+    a.totals = h->totals;
     a.partials = h->partials;
     a.Vout = h->Vout;
     a.Vkeep = h->Vstage;
@@ -204,7 +214,7 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
     if (need <= h->cap && h->S0.cell) return PFEM2GPU_OK;
     uint64_t cap = std::max<uint64_t>(need, (uint64_t)h->cap * 3 / 2);
     cap = std::max<uint64_t>(cap, 1024);
-    if (cap > 0xFFFFFFF0ull) return fail(h, PFEM2GPU_ERR_CAPACITY, "particle capacity beyond 2^32");
+    if (cap > 0x7FFFFFF0ull) return fail(h, PFEM2GPU_ERR_CAPACITY, "particle capacity beyond 2^31");
     PartState n0{}, n1{}, nt{};
     CK(alloc_state(h, n0, (uint32_t)cap, true));
     CK(alloc_state(h, n1, (uint32_t)cap, true));
@@ -227,14 +237,18 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
     dfree(h->slot);
     dfree(h->idx);
     dfree(h->xtmp);
+    dfree(h->xq);
     h->key = h->slot = h->idx = nullptr;
     h->xtmp = nullptr;
+    h->xq = nullptr;
     h->S0 = n0;
     h->S1 = n1;
     h->T = nt;
     CK(dalloc(&h->key, cap));
     CK(dalloc(&h->slot, cap));
     CK(dalloc(&h->idx, cap));
+    CK(dalloc(&h->xq, cap));
+    if (!h->nxq) CK(dalloc(&h->nxq, 1));
     if (h->prec == PFEM2GPU_FP32) CK(dalloc(&h->xtmp, cap * h->dim));
     h->cap = (uint32_t)cap;
     return PFEM2GPU_OK;
@@ -287,8 +301,8 @@ int sort_and_write(pfem2gpu_handle* h, StepArgs& a, int count_step)
 {
     run(h, "scan_cells", [&] { return launch_scan_u32(h->cell_count, h->nC, h->cell_off, h->tiles32, h->stream); });
     run(h, "bucket", [&] { return launch_bucket(a, h->stream); });
-    run(h, "count", [&] { return launch_count(h->dim, h->prec, a, h->stream); });
-    run(h, "scan_counts", [&] { return launch_scan_u64(h->packed, h->nC, h->packed_off, h->tiles64, h->stream); });
+    CK(cudaMemsetAsync(h->tile_status, 0, h->ntiles * sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->tile_counter, 0, sizeof(uint32_t), h->stream));
     run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->cell_start, h->stream); });
     run(h, "finalize", [&] { return launch_finalize(a, h->cell_start, count_step, h->stream); });
     std::swap(h->S0, h->S1);
@@ -304,6 +318,7 @@ int do_move(pfem2gpu_handle* h)
     a.do_correct = h->pending_correct ? 1 : 0;
     h->pending_correct = false;
     CK(cudaMemsetAsync(h->cell_count, 0, h->nC * sizeof(uint32_t), h->stream));
+    CK(cudaMemsetAsync(h->nxq, 0, sizeof(uint32_t), h->stream));
     run(h, "advect", [&] { return launch_advect(h->dim, h->prec, a, h->stream); });
     return sort_and_write(h, a, 1);
 }
@@ -409,8 +424,9 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
                     (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
                     (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vaos, h->dVaos,
                     (void*)h->key, (void*)h->slot, (void*)h->idx, (void*)h->xtmp, (void*)h->cell_count,
-                    (void*)h->cell_off, (void*)h->cell_start, (void*)h->tiles32, (void*)h->packed,
-                    (void*)h->packed_off, (void*)h->tiles64, h->partials, (void*)h->stats})
+                    (void*)h->cell_off, (void*)h->cell_start, (void*)h->tiles32, (void*)h->tile_status,
+                    (void*)h->tile_counter, (void*)h->totals, (void*)h->jinv32, (void*)h->xq, (void*)h->nxq,
+                    h->partials, (void*)h->stats})
         dfree(p);
     free_state(h->S0);
     free_state(h->S1);
@@ -504,7 +520,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
                     (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
                     (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vaos, h->dVaos,
                     (void*)h->cell_count, (void*)h->cell_off, (void*)h->cell_start, (void*)h->tiles32,
-                    (void*)h->packed, (void*)h->packed_off, (void*)h->tiles64, h->partials})
+                    (void*)h->tile_status, (void*)h->tile_counter, (void*)h->totals, (void*)h->jinv32, h->partials})
         dfree(p);
     h->has_mesh = false;
     h->nC = (int)n_cells;
@@ -531,10 +547,12 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(dalloc(&h->cell_count, nc));
     CK(dalloc(&h->cell_off, nc + 1));
     CK(dalloc(&h->cell_start, nc + 1));
-    CK(dalloc(&h->packed, nc));
-    CK(dalloc(&h->packed_off, nc + 1));
+    h->ntiles = (uint32_t)((nc + WR_TILE - 1) / WR_TILE);
+    CK(dalloc(&h->tile_status, h->ntiles));
+    CK(dalloc(&h->tile_counter, 1));
+    CK(dalloc(&h->totals, 1));
+    CK(dalloc(&h->jinv32, nc * (dim == 3 ? 12 : 8)));
     CK(dalloc(&h->tiles32, SCAN_MAX_TILES));
-    CK(dalloc(&h->tiles64, SCAN_MAX_TILES));
     CK(cudaMalloc(&h->partials, nc * PW * esize(h)));
     CK(cudaMemcpyAsync(h->cv, cell_vertices, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->cd, cell_dofs, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
@@ -548,7 +566,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(cudaMemsetAsync(h->dVaos, 0, nd * VS * esize(h), h->stream));
     CK(cudaMemsetAsync(h->Vstage, 0, nd * dim * 8, h->stream));
     run(h, "cell_setup",
-        [&] { return launch_cell_setup(dim, h->nC, h->verts, h->cv, h->cellX, h->aff, h->geo32, h->stream); });
+        [&] { return launch_cell_setup(dim, h->nC, h->verts, h->cv, h->cellX, h->aff, h->geo32, h->jinv32, h->stream); });
     CK(cudaStreamSynchronize(h->stream));  // host vectors above go out of scope
     h->has_mesh = true;
     h->vaos_valid = false;

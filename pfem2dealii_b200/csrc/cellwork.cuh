@@ -1,16 +1,20 @@
-// Per-cell kernels: seeding, count correction (survivor/seed decisions and
-// the final sorted layout), projection partial sums and the DoF gather.
+// Per-cell kernels: seeding, count correction with the final sorted layout,
+// projection partial sums and the DoF gather.
 //
-// One warp owns one cell at a time.  Its particles arrive through the
-// bucketed index list (cell-major), their extended part index is counted in
-// shared memory, and the decisions of check_particle_distribution
-// (src/pfem2particlehandler.cpp:356-410) follow from the counts alone:
-// a part keeps min(count, max+1) particles, chosen by ascending key(id), and
-// every real part left empty in a cell that had particles gets one new
-// particle at its centre.  New ids continue the running count in
-// (cell ascending, part x-major) order, the order in which the reference
-// hands them out.  The output is sorted by (cell, part, key), so the layout
-// and every floating-point sum taken over it are deterministic.
+// Count correction (check_particle_distribution,
+// src/pfem2particlehandler.cpp:356-410) depends on per-(cell, part) counts
+// only: a part keeps min(count, max+1) particles, here the ones with the
+// smallest key(id), and every real part left without particles in a cell
+// that had any gets one new particle at its centre.  New ids continue the
+// running count in (cell ascending, part x-major) order, the order in which
+// the reference hands them out.  Output is sorted by (cell, part, key), so
+// the layout and every floating-point sum over it are deterministic.
+//
+// The write pass is a single pass with decoupled look-back: a block takes a
+// tile of 32 cells, a warp decides its cells (survivors, new particles, final
+// count), the tile's totals are published and the exclusive prefix of the
+// earlier tiles is collected, then the warps write their cells at their
+// final offsets and sum the projection partials.
 #pragma once
 
 #include <type_traits>
@@ -53,12 +57,11 @@ __device__ __forceinline__ void interp_v(const MeshDev& m, const void* Vaos, uin
 
 // A new particle at the centre of part idx of cell c (seed_particles
 // :87-104 and check_particle_distribution :390-407): xi = (idx + 1/2) h,
-// x = F(xi) (FP64 form), v = interpolated V.
+// x = F(xi) (FP64 form), v = interpolated V.  Returns xi and v.
 template <int DIM, typename Real>
-__device__ __forceinline__ void write_new_particle(const StepArgs& a, const PartState& S, uint32_t dst, uint32_t c,
-                                                   const int* idx, uint32_t id)
+__device__ __forceinline__ void new_particle(const StepArgs& a, const PartState& S, uint32_t dst, uint32_t c,
+                                             const int* idx, uint32_t id, Real* xi, Real* v)
 {
-    Real xi[DIM], v[DIM];
     double xid[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
@@ -82,6 +85,20 @@ __device__ __forceinline__ void write_new_particle(const StepArgs& a, const Part
     S.id[dst] = id;
 }
 
+template <int DIM>
+__device__ __forceinline__ void part_digits(int k, const PartParams& pp, int* idx)
+{
+    idx[2] = 0;
+    if (DIM == 2) {
+        idx[0] = k / pp.q[1];
+        idx[1] = k % pp.q[1];
+    } else {
+        idx[0] = k / (pp.q[1] * pp.q[2]);
+        idx[1] = (k / pp.q[2]) % pp.q[1];
+        idx[2] = k % pp.q[2];
+    }
+}
+
 // seed_particles (:43-109): nC x npart particles, cell-major, parts x-major.
 template <int DIM, typename Real>
 __global__ void k_seed(StepArgs a, uint32_t* cell_start)
@@ -91,21 +108,16 @@ __global__ void k_seed(StepArgs a, uint32_t* cell_start)
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         const uint32_t c = t / a.pp.npart;
         const int k = (int)(t % a.pp.npart);
-        int idx[3] = {0, 0, 0};
-        if (DIM == 2) {
-            idx[0] = k / a.pp.q[1];
-            idx[1] = k % a.pp.q[1];
-        } else {
-            idx[0] = k / (a.pp.q[1] * a.pp.q[2]);
-            idx[1] = (k / a.pp.q[2]) % a.pp.q[1];
-            idx[2] = k % a.pp.q[2];
-        }
-        write_new_particle<DIM, Real>(a, a.S0, t, c, idx, id0 + t + 1);
+        int idx[3];
+        part_digits<DIM>(k, a.pp, idx);
+        Real xi[DIM], v[DIM];
+        new_particle<DIM, Real>(a, a.S0, t, c, idx, id0 + t + 1, xi, v);
         if (k == 0) cell_start[c] = t;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) cell_start[a.mesh.nC] = total;
 }
 
+// Extended part of an advected particle (T arrays) and its removal key.
 template <int DIM, typename Real>
 __device__ __forceinline__ uint2 part_key(const StepArgs& a, uint32_t i)
 {
@@ -122,48 +134,27 @@ __device__ __forceinline__ int survivors(int cnt, int maxpp, int apply)
     return cnt < maxpp + 1 ? cnt : maxpp + 1;
 }
 
-// Count pass: per cell, seeds << 32 | (survivors + seeds).
-template <int DIM, typename Real>
-__global__ void __launch_bounds__(CELL_WARPS * 32) k_count(StepArgs a)
+// Ascending bitonic sort of one 64-bit key per lane across the warp.
+__device__ __forceinline__ unsigned long long warp_sort(unsigned long long x, int lane)
 {
-    __shared__ int cnt_s[CELL_WARPS][NPE_MAX];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int* cnt = cnt_s[warp];
-    const int npe = a.pp.npe;
-    for (int c = blockIdx.x * CELL_WARPS + warp; c < a.mesh.nC; c += gridDim.x * CELL_WARPS) {
-        const uint32_t b = a.cell_off[c], e = a.cell_off[c + 1];
-        if (b == e) {
-            if (lane == 0) a.packed[c] = 0ull;
-            continue;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, j);
+            const bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
+            x = take_min ? (x < y ? x : y) : (x > y ? x : y);
         }
-        for (int p = lane; p < npe; p += 32) cnt[p] = 0;
-        __syncwarp();
-        for (uint32_t j = b + lane; j < e; j += 32) {
-            const uint2 pk = part_key<DIM, Real>(a, a.idx[j]);
-            atomicAdd(cnt + pk.x, 1);
-        }
-        __syncwarp();
-        unsigned surv = 0, seeds = 0;
-        for (int p = lane; p < npe; p += 32) {
-            const int s = survivors(cnt[p], a.pp.maxpp, a.apply_counts);
-            int idx[3];
-            surv += s;
-            if (a.apply_counts && s == 0 && real_part<DIM>(p, a.pp, idx)) seeds++;
-        }
-        surv = __reduce_add_sync(0xffffffffu, surv);
-        seeds = __reduce_add_sync(0xffffffffu, seeds);
-        if (lane == 0) a.packed[c] = ((unsigned long long)seeds << 32) | (unsigned long long)(surv + seeds);
-        __syncwarp();
-    }
+    return x;
 }
 
 // ---------------------------------------------------------------------------
 // Projection partials: per cell and local vertex iv, sum_p N_iv v_p and
-// sum_p N_iv over the cell's final particles in their sorted order
-// (project_particle_fields :191-199 restricted to one cell).  Lane l sums
-// particles l, l+32, ...; the 32 lanes are combined by a butterfly
-// reduce-scatter after which lane k holds entry k = iv*4 + comp (comp = DIM
-// is the weight).  FP32 sums are compensated (TwoSum pairs).
+// sum_p N_iv (project_particle_fields :191-199 restricted to one cell), in
+// the cell's final particle order.  Each lane writes one particle's 4*NV
+// terms as a row of a per-warp shared array; lane e then adds column e row by
+// row (FP32: compensated TwoSum).  Entry e = iv*4 + comp, comp = DIM is the
+// weight.
 // ---------------------------------------------------------------------------
 
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e)
@@ -173,222 +164,435 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e)
     e = (a - (s - bb)) + (b - bb);
 }
 
-template <int W, typename T>
-__device__ __forceinline__ T reduce_scatter(T (&vals)[W], int lane)
-{
-    // after the loop lane l holds the total of entry (l & (W-1))
-#pragma unroll
-    for (int s = W / 2; s >= 1; s >>= 1) {
-        const bool upper = lane & s;
-#pragma unroll
-        for (int k = 0; k < s; ++k) {
-            const T send = upper ? vals[k] : vals[k + s];
-            const T keep = upper ? vals[k + s] : vals[k];
-            vals[k] = keep + __shfl_xor_sync(0xffffffffu, send, s);
-        }
-    }
-    T r = vals[0];
-#pragma unroll
-    for (int s = W; s < 32; s <<= 1) r += __shfl_xor_sync(0xffffffffu, r, s);
-    return r;
-}
-
-template <int W>
-__device__ __forceinline__ float reduce_scatter_comp(float (&hi)[W], float (&lo)[W], int lane)
-{
-#pragma unroll
-    for (int s = W / 2; s >= 1; s >>= 1) {
-        const bool upper = lane & s;
-#pragma unroll
-        for (int k = 0; k < s; ++k) {
-            const float sh = upper ? hi[k] : hi[k + s], sl = upper ? lo[k] : lo[k + s];
-            const float kh = upper ? hi[k + s] : hi[k], kl = upper ? lo[k + s] : lo[k];
-            const float rh = __shfl_xor_sync(0xffffffffu, sh, s);
-            const float rl = __shfl_xor_sync(0xffffffffu, sl, s);
-            float t, e;
-            two_sum(kh, rh, t, e);
-            hi[k] = t;
-            lo[k] = e + (kl + rl);
-        }
-    }
-    float h = hi[0], l = lo[0];
-#pragma unroll
-    for (int s = W; s < 32; s <<= 1) {
-        const float rh = __shfl_xor_sync(0xffffffffu, h, s);
-        const float rl = __shfl_xor_sync(0xffffffffu, l, s);
-        float t, e;
-        two_sum(h, rh, t, e);
-        h = t;
-        l = e + (l + rl);
-    }
-    return h + l;
-}
+template <typename Real>
+struct PartialAcc {
+    Real s = Real(0), c = Real(0);
+};
 
 template <int DIM, typename Real>
-__device__ __forceinline__ void cell_partials(const StepArgs& a, const PartState& S, uint32_t c, uint32_t fb,
-                                              uint32_t fcount, int lane)
+__device__ __forceinline__ void partial_rows(Real (*tr)[33], bool valid, const Real* xi, const Real* v, int rows,
+                                             int lane, PartialAcc<Real>& acc)
 {
     constexpr int NV = 1 << DIM, PW = Dims<DIM>::PW;
-    if constexpr (std::is_same<Real, double>::value) {
-        double vals[PW];
+    Real N[NV];
+    if constexpr (std::is_same<Real, double>::value) shape64<DIM>(xi, N);
+    else shape32<DIM>(xi, N);
+    if (lane < rows) {
 #pragma unroll
-        for (int k = 0; k < PW; ++k) vals[k] = 0.0;
-        for (uint32_t j = lane; j < fcount; j += 32) {
-            double xi[DIM], v[DIM], N[NV];
+        for (int iv = 0; iv < NV; ++iv) {
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                xi[d] = ldr<double>(S.xi[d], fb + j);
-                v[d] = ldr<double>(S.v[d], fb + j);
-            }
-            shape64<DIM>(xi, N);
-#pragma unroll
-            for (int iv = 0; iv < NV; ++iv) {
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) vals[iv * 4 + d] = vals[iv * 4 + d] + N[iv] * v[d];
-                vals[iv * 4 + DIM] = vals[iv * 4 + DIM] + N[iv];
+            for (int d = 0; d < DIM; ++d) tr[lane][iv * 4 + d] = valid ? N[iv] * v[d] : Real(0);
+            tr[lane][iv * 4 + DIM] = valid ? N[iv] : Real(0);
+            if (DIM == 2) tr[lane][iv * 4 + 3] = Real(0);
+        }
+    }
+    __syncwarp();
+    if (lane < PW) {
+        for (int r = 0; r < rows; ++r) {
+            const Real t = tr[r][lane];
+            if constexpr (std::is_same<Real, double>::value) {
+                acc.s = acc.s + t;
+            } else {
+                float s, e;
+                two_sum(acc.s, t, s, e);
+                acc.s = s;
+                acc.c += e;
             }
         }
-        const double r = reduce_scatter<PW, double>(vals, lane);
-        if (lane < PW) reinterpret_cast<double*>(a.partials)[(size_t)c * PW + lane] = r;
-    } else {
-        float hi[PW], lo[PW];
+    }
+    __syncwarp();
+}
+
+template <int DIM, typename Real>
+__device__ __forceinline__ void store_partial(const StepArgs& a, uint32_t c, const PartialAcc<Real>& acc, int lane)
+{
+    constexpr int PW = Dims<DIM>::PW;
+    if (lane < PW) reinterpret_cast<Real*>(a.partials)[(size_t)c * PW + lane] = acc.s + acc.c;
+}
+
+// Partials of particles [b, b+count) of a sorted state, in order.
+template <int DIM, typename Real>
+__device__ __forceinline__ void partials_of_range(const StepArgs& a, const PartState& S, uint32_t c, uint32_t b,
+                                                  uint32_t count, Real (*tr)[33], int lane)
+{
+    PartialAcc<Real> acc;
+    for (uint32_t base = 0; base < count; base += 32) {
+        const uint32_t j = base + lane;
+        const bool valid = j < count;
+        Real xi[DIM], v[DIM];
 #pragma unroll
-        for (int k = 0; k < PW; ++k) hi[k] = lo[k] = 0.0f;
-        for (uint32_t j = lane; j < fcount; j += 32) {
-            float xi[DIM], v[DIM], N[NV];
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                xi[d] = ldr<float>(S.xi[d], fb + j);
-                v[d] = ldr<float>(S.v[d], fb + j);
-            }
-            shape32<DIM>(xi, N);
-#pragma unroll
-            for (int iv = 0; iv < NV; ++iv) {
-#pragma unroll
-                for (int d = 0; d <= DIM; ++d) {
-                    const float term = d < DIM ? N[iv] * v[d] : N[iv];
-                    float t, e;
-                    two_sum(hi[iv * 4 + d], term, t, e);
-                    hi[iv * 4 + d] = t;
-                    lo[iv * 4 + d] += e;
-                }
-            }
+        for (int d = 0; d < DIM; ++d) {
+            xi[d] = valid ? ldr<Real>(S.xi[d], b + j) : Real(0);
+            v[d] = valid ? ldr<Real>(S.v[d], b + j) : Real(0);
         }
-        const float r = reduce_scatter_comp<PW>(hi, lo, lane);
-        if (lane < PW) reinterpret_cast<float*>(a.partials)[(size_t)c * PW + lane] = r;
+        const int rows = count - base < 32 ? (int)(count - base) : 32;
+        partial_rows<DIM, Real>(tr, valid, xi, v, rows, lane, acc);
+    }
+    store_partial<DIM, Real>(a, c, acc, lane);
+}
+
+template <typename Real>
+struct WriteSmem {
+    uint32_t outmap[WR_WARPS][WR_CPW][32];   // fast path: source index, or 0x80000000|part for a new particle
+    unsigned long long seedmask[WR_TILE];
+    uint32_t fin[WR_TILE];                   // final particles per cell
+    uint32_t nseed[WR_TILE];
+    uint32_t excl_fin[WR_TILE];              // exclusive prefix inside the tile
+    uint32_t excl_seed[WR_TILE];
+    uint32_t slow;                           // tile cells on the general path (bit per cell)
+    uint32_t tile;
+    unsigned long long prefix;               // seeds << 32 | particles before this tile
+    int cnt[WR_WARPS][NPE_MAX];
+    uint2 kc[WR_WARPS][KEY_CACHE];
+    Real tr[WR_WARPS][32][33];               // partial rows; general path: part prefixes first
+};
+
+__device__ __forceinline__ void store_release_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long load_acquire_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+constexpr unsigned long long LB_AGG = 1ull << 62, LB_INC = 2ull << 62;
+constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;
+
+__device__ __forceinline__ unsigned long long lb_pack(uint32_t f, uint32_t s)
+{
+    return ((unsigned long long)(f & 0x7fffffffu) << 31) | (unsigned long long)(s & 0x7fffffffu);
+}
+
+// Decoupled look-back (warp 0 of the block): publish this tile's aggregate,
+// add up the aggregates of earlier tiles until an inclusive prefix is found,
+// publish the inclusive prefix.  Every wait is bounded; on time-out the error
+// flag is raised and the partial sum is used (the output is then garbage but
+// every write stays in bounds).  Returns seeds << 32 | particles before.
+static __device__ __noinline__ unsigned long long lookback(const StepArgs& a, uint32_t tile, uint32_t agg_f, uint32_t agg_s, int lane)
+{
+    unsigned long long* st = a.tile_status;
+    if (tile == 0) {
+        if (lane == 0) store_release_u64(st, LB_INC | lb_pack(agg_f, agg_s));
+        return 0ull;
+    }
+    if (lane == 0) store_release_u64(st + tile, LB_AGG | lb_pack(agg_f, agg_s));
+    uint32_t ef = 0, es = 0;
+    long long pred = (long long)tile - 1;
+    uint32_t spins = 0;
+    bool timed_out = false;
+    while (true) {
+        const long long t = pred - lane;
+        unsigned long long w = t >= 0 ? load_acquire_u64(st + t) : LB_INC;
+        while (__any_sync(0xffffffffu, (w >> 62) == 0ull)) {
+            if (++spins > LB_SPIN_LIMIT) {
+                timed_out = true;
+                break;
+            }
+            __nanosleep(32);
+            if ((w >> 62) == 0ull) w = load_acquire_u64(st + t);
+        }
+        if (timed_out) break;
+        const unsigned pm = __ballot_sync(0xffffffffu, (w >> 62) == 2ull);
+        const int stop = pm ? __ffs(pm) - 1 : 31;
+        const uint32_t vf = lane <= stop ? (uint32_t)((w >> 31) & 0x7fffffffu) : 0u;
+        const uint32_t vs = lane <= stop ? (uint32_t)(w & 0x7fffffffu) : 0u;
+        ef += __reduce_add_sync(0xffffffffu, vf);
+        es += __reduce_add_sync(0xffffffffu, vs);
+        if (pm) break;
+        pred -= 32;
+    }
+    if (timed_out && lane == 0) atomicOr(&a.stats->error_flags, ERR_LOOKBACK);
+    if (lane == 0) store_release_u64(st + tile, LB_INC | lb_pack(ef + agg_f, es + agg_s));
+    return ((unsigned long long)es << 32) | ef;
+}
+
+// General-path phase 1: per-part counts of one cell (in cnt) and its
+// (final, seeds).  Also caches (part, key) pairs of the first KEY_CACHE.
+template <int DIM, typename Real>
+__device__ __forceinline__ uint2 count_cell(const StepArgs& a, int* cnt, uint2* kc, uint32_t b, uint32_t nseg, int lane)
+{
+    const int npe = a.pp.npe;
+    for (int p = lane; p < npe; p += 32) cnt[p] = 0;
+    __syncwarp();
+    for (uint32_t j = lane; j < nseg; j += 32) {
+        const uint2 pk = part_key<DIM, Real>(a, a.idx[b + j]);
+        atomicAdd(cnt + pk.x, 1);
+        if (j < KEY_CACHE) kc[j] = pk;
+    }
+    __syncwarp();
+    unsigned surv = 0, seeds = 0;
+    for (int p = lane; p < npe; p += 32) {
+        const int s = survivors(cnt[p], a.pp.maxpp, a.apply_counts);
+        int idx[3];
+        surv += s;
+        if (a.apply_counts && nseg > 0 && s == 0 && real_part<DIM>(p, a.pp, idx)) seeds++;
+    }
+    surv = __reduce_add_sync(0xffffffffu, surv);
+    seeds = __reduce_add_sync(0xffffffffu, seeds);
+    return make_uint2(surv + seeds, seeds);
+}
+
+template <int DIM, typename Real>
+__device__ __forceinline__ void copy_particle(const StepArgs& a, uint32_t i, uint32_t dst, uint32_t c, Real* xi, Real* v)
+{
+    a.S1.cell[dst] = c;
+    a.S1.id[dst] = a.S0.id[i];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        if constexpr (std::is_same<Real, double>::value) str<double>(a.S1.x[d], dst, ldr<double>(a.T.x[d], i));
+        xi[d] = ldr<Real>(a.T.xi[d], i);
+        v[d] = ldr<Real>(a.T.v[d], i);
+        str<Real>(a.S1.xi[d], dst, xi[d]);
+        str<Real>(a.S1.v[d], dst, v[d]);
     }
 }
 
-// Write pass: survivors in (part, key) order, then the new particles, into
-// the next sorted state; then the cell's projection partials.
+// General-path phase 2 of one cell (any particle count, any part count).
 template <int DIM, typename Real>
-__global__ void __launch_bounds__(CELL_WARPS * 32) k_write(StepArgs a, uint32_t* cell_start)
+__device__ void write_cell_general(const StepArgs& a, WriteSmem<Real>& sm, int warp, uint32_t c, uint32_t b,
+                                   uint32_t nseg, uint32_t fb, uint32_t sb, uint32_t id0, int lane,
+                                   unsigned long long& removed, uint32_t& err)
 {
-    __shared__ int cnt_s[CELL_WARPS][NPE_MAX];
-    __shared__ int pfx_s[CELL_WARPS][NPE_MAX];   // final position of each part's first particle
-    __shared__ int spfx_s[CELL_WARPS][NPE_MAX];  // number of new particles in earlier parts
-    __shared__ uint2 kc_s[CELL_WARPS][KEY_CACHE];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int* cnt = cnt_s[warp];
-    int* pfx = pfx_s[warp];
-    int* spfx = spfx_s[warp];
-    uint2* kc = kc_s[warp];
+    int* cnt = sm.cnt[warp];
+    uint2* kc = sm.kc[warp];
+    int* pfx = reinterpret_cast<int*>(&sm.tr[warp][0][0]);
+    int* spfx = pfx + NPE_MAX;
     const int npe = a.pp.npe;
+    const uint2 fs = count_cell<DIM, Real>(a, cnt, kc, b, nseg, lane);
+    int run = 0, srun = 0;
+    for (int base = 0; base < npe; base += 32) {
+        const int p = base + lane;
+        int fc = 0, sf = 0;
+        if (p < npe) {
+            const int s = survivors(cnt[p], a.pp.maxpp, a.apply_counts);
+            int idx[3];
+            sf = (a.apply_counts && nseg > 0 && s == 0 && real_part<DIM>(p, a.pp, idx)) ? 1 : 0;
+            fc = s + sf;
+        }
+        int ifc = fc, isf = sf;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t1 = __shfl_up_sync(0xffffffffu, ifc, o);
+            const int t2 = __shfl_up_sync(0xffffffffu, isf, o);
+            if (lane >= o) {
+                ifc += t1;
+                isf += t2;
+            }
+        }
+        if (p < npe) {
+            pfx[p] = run + ifc - fc;
+            spfx[p] = srun + isf - sf;
+        }
+        run += __shfl_sync(0xffffffffu, ifc, 31);
+        srun += __shfl_sync(0xffffffffu, isf, 31);
+    }
+    __syncwarp();
+    const uint32_t cap = a.capacity;
+    for (uint32_t j = lane; j < nseg; j += 32) {
+        const uint32_t i = a.idx[b + j];
+        const uint2 pk = j < KEY_CACHE ? kc[j] : part_key<DIM, Real>(a, i);
+        const int k = cnt[pk.x];
+        int rank = 0;
+        if (k > 1) {
+            for (uint32_t jj = 0; jj < nseg; ++jj) {
+                const uint2 q = jj < KEY_CACHE ? kc[jj] : part_key<DIM, Real>(a, a.idx[b + jj]);
+                rank += (q.x == pk.x && q.y < pk.y) ? 1 : 0;
+            }
+        }
+        if (rank < survivors(k, a.pp.maxpp, a.apply_counts)) {
+            const uint32_t dst = fb + (uint32_t)pfx[pk.x] + (uint32_t)rank;
+            Real xi[DIM], v[DIM];
+            if (dst < cap) copy_particle<DIM, Real>(a, i, dst, c, xi, v);
+            else err |= ERR_CAPACITY;
+        } else {
+            removed++;
+        }
+    }
+    if (a.apply_counts && nseg > 0) {
+        for (int p = lane; p < npe; p += 32) {
+            int idx[3] = {0, 0, 0};
+            if (!real_part<DIM>(p, a.pp, idx)) continue;
+            if (survivors(cnt[p], a.pp.maxpp, 1) != 0) continue;
+            const uint32_t dst = fb + (uint32_t)pfx[p];
+            Real xi[DIM], v[DIM];
+            if (dst < cap) new_particle<DIM, Real>(a, a.S1, dst, c, idx, id0 + sb + (uint32_t)spfx[p] + 1, xi, v);
+            else err |= ERR_CAPACITY;
+        }
+    }
+    __syncwarp();
+    __threadfence_block();
+    const uint32_t fcount = fs.x;
+    partials_of_range<DIM, Real>(a, a.S1, c, fb, (fb + fcount <= cap) ? fcount : 0, sm.tr[warp], lane);
+}
+
+// The write pass (one launch per step; see the file comment).
+template <int DIM, typename Real>
+__global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a, uint32_t* cell_start)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WriteSmem<Real>& sm = *reinterpret_cast<WriteSmem<Real>*>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int npe = a.pp.npe;
+    const bool fast_ok = npe <= 64;
+    unsigned long long realmask = 0;
+    if (fast_ok)
+        for (int p = 0; p < npe; ++p) {
+            int idx[3];
+            if (real_part<DIM>(p, a.pp, idx)) realmask |= 1ull << p;
+        }
     const uint32_t id0 = a.stats->next_id;
     const uint32_t cap = a.capacity;
     unsigned long long removed = 0;
     uint32_t err = 0;
-    for (int c = blockIdx.x * CELL_WARPS + warp; c < a.mesh.nC; c += gridDim.x * CELL_WARPS) {
-        const uint32_t b = a.cell_off[c], e = a.cell_off[c + 1];
-        const uint32_t nseg = e - b;
-        const unsigned long long po = a.packed_off[c];
-        const uint32_t fb = (uint32_t)po, sb = (uint32_t)(po >> 32);
-        if (lane == 0) cell_start[c] = fb;
-        if (nseg == 0) {
-            cell_partials<DIM, Real>(a, a.S1, (uint32_t)c, fb, 0, lane);
-            continue;
+    const int apply = a.apply_counts;
+    const int maxpp = a.pp.maxpp;
+    while (true) {
+        if (threadIdx.x == 0) {
+            sm.tile = atomicAdd(a.tile_counter, 1u);
+            sm.slow = 0;
         }
-        for (int p = lane; p < npe; p += 32) cnt[p] = 0;
-        __syncwarp();
-        for (uint32_t j = lane; j < nseg; j += 32) {
-            const uint2 pk = part_key<DIM, Real>(a, a.idx[b + j]);
-            atomicAdd(cnt + pk.x, 1);
-            if (j < KEY_CACHE) kc[j] = pk;
-        }
-        __syncwarp();
-        int run = 0, srun = 0;
-        for (int base = 0; base < npe; base += 32) {
-            const int p = base + lane;
-            int fc = 0, sf = 0;
-            if (p < npe) {
-                const int s = survivors(cnt[p], a.pp.maxpp, a.apply_counts);
-                int idx[3];
-                sf = (a.apply_counts && s == 0 && real_part<DIM>(p, a.pp, idx)) ? 1 : 0;
-                fc = s + sf;
+        __syncthreads();
+        const uint32_t tile = sm.tile;
+        if (tile >= a.ntiles) break;
+        // ---- phase 1: decide every cell of the tile ----
+        for (int j = 0; j < WR_CPW; ++j) {
+            const int slotc = warp * WR_CPW + j;
+            const uint32_t c = tile * WR_TILE + slotc;
+            uint32_t fin = 0, nsd = 0;
+            unsigned long long seedm = 0;
+            if (c < (uint32_t)a.mesh.nC) {
+                const uint32_t b = a.cell_off[c], nseg = a.cell_off[c + 1] - b;
+                bool fast = fast_ok && nseg <= 32;
+                if (fast) {
+                    const bool valid = (uint32_t)lane < nseg;
+                    uint32_t i = 0;
+                    unsigned long long k64 = ~0ull;
+                    if (valid) {
+                        i = a.idx[b + lane];
+                        const uint2 pk = part_key<DIM, Real>(a, i);
+                        k64 = ((unsigned long long)pk.x << 37) | ((unsigned long long)pk.y << 5) | (unsigned)lane;
+                    }
+                    k64 = warp_sort(k64, lane);
+                    const bool vs = k64 != ~0ull;
+                    const uint32_t ep = vs ? (uint32_t)(k64 >> 37) : 0xffffu;
+                    const uint32_t is = __shfl_sync(0xffffffffu, i, (int)(k64 & 31u));
+                    const uint32_t prev = __shfl_up_sync(0xffffffffu, ep, 1);
+                    const bool start = vs && (lane == 0 || ep != prev);
+                    const unsigned smask = __ballot_sync(0xffffffffu, start);
+                    const unsigned le = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+                    const int rank = lane - (31 - __clz(smask & le));
+                    const bool surv = vs && (!apply || (maxpp >= 0 && rank <= maxpp));
+                    const unsigned survm = __ballot_sync(0xffffffffu, surv);
+                    const unsigned long long occ_me = surv ? (1ull << ep) : 0ull;
+                    const unsigned long long occ =
+                        (unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)occ_me) |
+                        ((unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)(occ_me >> 32)) << 32);
+                    seedm = (apply && nseg > 0) ? (realmask & ~occ) : 0ull;
+                    nsd = __popcll(seedm);
+                    fin = __popc(survm) + nsd;
+                    if (fin <= 32) {
+                        uint32_t* om = sm.outmap[warp][j];
+                        if (surv) {
+                            const unsigned lt = (1u << lane) - 1u;
+                            const unsigned long long below = ep == 0 ? 0ull : (seedm & ((1ull << ep) - 1ull));
+                            om[__popc(survm & lt) + __popcll(below)] = is;
+                        }
+                        unsigned long long rest = seedm;
+                        int k = 0;
+                        while (rest) {
+                            const int p = __ffsll((long long)rest) - 1;
+                            rest &= rest - 1;
+                            const unsigned nb = __ballot_sync(0xffffffffu, surv && (int)ep < p);
+                            if (lane == 0) om[__popc(nb) + k] = 0x80000000u | (uint32_t)p;
+                            ++k;
+                        }
+                        if (lane == 0) removed += nseg - __popc(survm);
+                    } else {
+                        fast = false;
+                    }
+                }
+                if (!fast) {
+                    const uint2 fs = count_cell<DIM, Real>(a, sm.cnt[warp], sm.kc[warp], b, nseg, lane);
+                    fin = fs.x;
+                    nsd = fs.y;
+                    if (lane == 0) atomicOr(&sm.slow, 1u << slotc);
+                }
             }
-            int ifc = fc, isf = sf;
+            if (lane == 0) {
+                sm.fin[slotc] = fin;
+                sm.nseed[slotc] = nsd;
+                sm.seedmask[slotc] = seedm;
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        // ---- tile prefix: scan of the 32 cells, then look-back ----
+        if (warp == 0) {
+            uint32_t f = sm.fin[lane], s = sm.nseed[lane];
+            uint32_t fi = f, si = s;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const int t1 = __shfl_up_sync(0xffffffffu, ifc, o);
-                const int t2 = __shfl_up_sync(0xffffffffu, isf, o);
+                const uint32_t t1 = __shfl_up_sync(0xffffffffu, fi, o);
+                const uint32_t t2 = __shfl_up_sync(0xffffffffu, si, o);
                 if (lane >= o) {
-                    ifc += t1;
-                    isf += t2;
+                    fi += t1;
+                    si += t2;
                 }
             }
-            if (p < npe) {
-                pfx[p] = run + ifc - fc;
-                spfx[p] = srun + isf - sf;
+            sm.excl_fin[lane] = fi - f;
+            sm.excl_seed[lane] = si - s;
+            const uint32_t tf = __shfl_sync(0xffffffffu, fi, 31), ts = __shfl_sync(0xffffffffu, si, 31);
+            const unsigned long long pre = lookback(a, tile, tf, ts, lane);
+            if (lane == 0) {
+                sm.prefix = pre;
+                if (tile == a.ntiles - 1)
+                    *a.totals = (((pre >> 32) + ts) << 32) | (unsigned long long)((uint32_t)pre + tf);
             }
-            run += __shfl_sync(0xffffffffu, ifc, 31);
-            srun += __shfl_sync(0xffffffffu, isf, 31);
         }
-        __syncwarp();
-        // survivors
-        for (uint32_t j = lane; j < nseg; j += 32) {
-            const uint32_t i = a.idx[b + j];
-            const uint2 pk = j < KEY_CACHE ? kc[j] : part_key<DIM, Real>(a, i);
-            const int k = cnt[pk.x];
-            int rank = 0;
-            if (k > 1) {
-                for (uint32_t jj = 0; jj < nseg; ++jj) {
-                    const uint2 q = jj < KEY_CACHE ? kc[jj] : part_key<DIM, Real>(a, a.idx[b + jj]);
-                    rank += (q.x == pk.x && q.y < pk.y) ? 1 : 0;
-                }
+        __syncthreads();
+        // ---- phase 2: write the cells at their final offsets ----
+        const uint32_t pf = (uint32_t)sm.prefix, ps = (uint32_t)(sm.prefix >> 32);
+        for (int j = 0; j < WR_CPW; ++j) {
+            const int slotc = warp * WR_CPW + j;
+            const uint32_t c = tile * WR_TILE + slotc;
+            if (c >= (uint32_t)a.mesh.nC) continue;
+            const uint32_t fb = pf + sm.excl_fin[slotc], sb = ps + sm.excl_seed[slotc];
+            if (lane == 0) cell_start[c] = fb;
+            if (sm.slow & (1u << slotc)) {
+                const uint32_t b = a.cell_off[c], nseg = a.cell_off[c + 1] - b;
+                write_cell_general<DIM, Real>(a, sm, warp, c, b, nseg, fb, sb, id0, lane, removed, err);
+                continue;
             }
-            if (rank < survivors(k, a.pp.maxpp, a.apply_counts)) {
-                const uint32_t dst = fb + (uint32_t)pfx[pk.x] + (uint32_t)rank;
-                if (dst < cap) {
-                    a.S1.cell[dst] = (uint32_t)c;
-                    a.S1.id[dst] = a.S0.id[i];
+            const uint32_t fin = sm.fin[slotc];
+            const bool valid = (uint32_t)lane < fin;
+            Real xi[DIM], v[DIM];
 #pragma unroll
-                    for (int d = 0; d < DIM; ++d) {
-                        if constexpr (std::is_same<Real, double>::value)
-                            str<double>(a.S1.x[d], dst, ldr<double>(a.T.x[d], i));
-                        str<Real>(a.S1.xi[d], dst, ldr<Real>(a.T.xi[d], i));
-                        str<Real>(a.S1.v[d], dst, ldr<Real>(a.T.v[d], i));
-                    }
-                } else {
+            for (int d = 0; d < DIM; ++d) xi[d] = v[d] = Real(0);
+            if (valid) {
+                const uint32_t ent = sm.outmap[warp][j][lane];
+                const uint32_t dst = fb + lane;
+                if (dst >= cap) {
                     err |= ERR_CAPACITY;
+                } else if (ent & 0x80000000u) {
+                    const int p = (int)(ent & 0x7fffffffu);
+                    int idx[3] = {0, 0, 0};
+                    real_part<DIM>(p, a.pp, idx);
+                    const unsigned long long sdm = sm.seedmask[slotc];
+                    const uint32_t r = (uint32_t)__popcll(p == 0 ? 0ull : (sdm & ((1ull << p) - 1ull)));
+                    new_particle<DIM, Real>(a, a.S1, dst, c, idx, id0 + sb + r + 1, xi, v);
+                } else {
+                    copy_particle<DIM, Real>(a, ent, dst, c, xi, v);
                 }
-            } else {
-                removed++;
             }
+            PartialAcc<Real> acc;
+            partial_rows<DIM, Real>(sm.tr[warp], valid && fb + lane < cap, xi, v, (int)fin, lane, acc);
+            store_partial<DIM, Real>(a, c, acc, lane);
         }
-        // new particles in the empty parts
-        if (a.apply_counts) {
-            for (int p = lane; p < npe; p += 32) {
-                int idx[3] = {0, 0, 0};
-                if (!real_part<DIM>(p, a.pp, idx)) continue;
-                if (survivors(cnt[p], a.pp.maxpp, 1) != 0) continue;
-                const uint32_t dst = fb + (uint32_t)pfx[p];
-                if (dst < cap) write_new_particle<DIM, Real>(a, a.S1, dst, (uint32_t)c, idx, id0 + sb + (uint32_t)spfx[p] + 1);
-                else err |= ERR_CAPACITY;
-            }
-        }
-        __syncwarp();
-        const uint32_t fcount = (uint32_t)run;
-        cell_partials<DIM, Real>(a, a.S1, (uint32_t)c, fb, (fb + fcount <= cap) ? fcount : 0, lane);
+        __syncthreads();
     }
     warp_count(&a.stats->removed, removed);
     err = __reduce_or_sync(0xffffffffu, err);
@@ -399,10 +603,11 @@ __global__ void __launch_bounds__(CELL_WARPS * 32) k_write(StepArgs a, uint32_t*
 template <int DIM, typename Real>
 __global__ void __launch_bounds__(CELL_WARPS * 32) k_partials(StepArgs a, const uint32_t* cell_start)
 {
+    __shared__ Real tr_s[CELL_WARPS][32][33];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int c = blockIdx.x * CELL_WARPS + warp; c < a.mesh.nC; c += gridDim.x * CELL_WARPS) {
         const uint32_t b = cell_start[c], e = cell_start[c + 1];
-        cell_partials<DIM, Real>(a, a.S0, (uint32_t)c, b, e - b, lane);
+        partials_of_range<DIM, Real>(a, a.S0, (uint32_t)c, b, e - b, tr_s[warp], lane);
     }
 }
 
@@ -444,7 +649,10 @@ __global__ void k_gather(StepArgs a, int keep_empty)
     constexpr int NV = 1 << DIM, PW = Dims<DIM>::PW;
     const PReal* P = reinterpret_cast<const PReal*>(a.partials);
     unsigned long long nan_dofs = 0;
-    for (int dof = blockIdx.x * blockDim.x + threadIdx.x; dof < a.mesh.nD; dof += gridDim.x * blockDim.x) {
+    const int stride = gridDim.x * blockDim.x;
+    const int nloop = (a.mesh.nD + stride - 1) / stride * stride;
+    for (int dof = blockIdx.x * blockDim.x + threadIdx.x; dof < nloop; dof += stride) {
+        if (dof >= a.mesh.nD) continue;
         double num[DIM], den = 0.0;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) num[d] = 0.0;

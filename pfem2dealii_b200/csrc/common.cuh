@@ -18,12 +18,16 @@ constexpr uint32_t LOST = 0xFFFFFFFFu;
 constexpr int MAX_CAND = 64;   // cells around one vertex tried by the relocation search
 constexpr int NPE_MAX = 512;   // extended cell parts (q0+1)(q1+1)(q2+1)
 constexpr int CELL_WARPS = 4;  // warps per block in the warp-per-cell kernels
+constexpr int WR_WARPS = 8;    // write pass: warps per block
+constexpr int WR_CPW = 4;      // write pass: cells per warp
+constexpr int WR_TILE = WR_WARPS * WR_CPW;  // cells per look-back tile
 constexpr int KEY_CACHE = 128; // (part, key) pairs cached per warp in shared memory
 
 // error_flags bits
 constexpr uint32_t ERR_CAPACITY = 1u;        // more particles than the arrays hold
 constexpr uint32_t ERR_CAND_OVERFLOW = 2u;   // a vertex touches more than MAX_CAND cells
 constexpr uint32_t ERR_BAD_CELL = 4u;        // a particle carries an out-of-range cell
+constexpr uint32_t ERR_LOOKBACK = 8u;        // look-back wait gave up (bounded spin)
 
 struct DevStats {
     unsigned long long n_particles;
@@ -46,7 +50,8 @@ struct MeshDev {
     const int32_t* cd;        // nC x NV DoF ids
     const double* cellX;      // nC x NV x DIM vertex coordinates, cell-major
     const double* aff;        // nC x (DIM*DIM + DIM): inverse affine approximation A^-1 and b
-    const float* geo32;       // nC x GEO_STRIDE: FP32 multilinear coefficients relative to vertex 0
+    const float* geo32;       // nC x GEO: FP32 multilinear coefficients relative to vertex 0
+    const float* jinv32;      // nC x JS: FP32 inverse Jacobian at the centre, then the affine flag
     const int32_t* v2c_off;   // nV + 1
     const int32_t* v2c_cells; // cells around each vertex, ascending
     const double* v2c_dirs;   // DIM per entry: unit vertex -> cell-centre direction
@@ -89,8 +94,12 @@ struct StepArgs {
     uint32_t* idx;      // bucketed particle indices, cell-major
     uint32_t* cell_count;
     uint32_t* cell_off;            // nC + 1
-    unsigned long long* packed;    // per cell: seeds << 32 | final count
-    unsigned long long* packed_off;// nC + 1 exclusive scan of packed
+    uint2* xq;                     // particles (index, sub-step) queued for FP64 relocation
+    uint32_t* nxq;                 // queue length
+    unsigned long long* tile_status; // decoupled look-back words of the write pass
+    uint32_t* tile_counter;        // dynamic tile ticket of the write pass
+    uint32_t ntiles;
+    unsigned long long* totals;    // write pass: seeds << 32 | particles after the step
     void* partials;                // nC x PW projection partial sums
     double* Vout;                  // nD x DIM component-major projected velocity
     const double* Vkeep;           // empty_dof_policy 1: value kept where no particle contributes
@@ -104,6 +113,7 @@ template <int DIM> struct Dims {
     static constexpr int PW = DIM == 3 ? 32 : 16;      // projection partials per cell (NV x 4)
     static constexpr int AFF = DIM * DIM + DIM;
     static constexpr int GEO = DIM == 3 ? 24 : 8;      // FP32 geometry floats per cell
+    static constexpr int JS = DIM == 3 ? 12 : 8;       // FP32 inverse Jacobian + flag, padded
 };
 
 __host__ __device__ inline uint32_t key_of(uint32_t id, uint32_t seed)

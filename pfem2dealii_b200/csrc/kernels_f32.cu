@@ -9,7 +9,6 @@ namespace pfem2 {
 
 int launch64_seed(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s);
 int launch64_advect(int dim, const StepArgs& a, cudaStream_t s);
-int launch64_count(int dim, const StepArgs& a, cudaStream_t s);
 int launch64_write(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s);
 int launch64_partials(int dim, const StepArgs& a, const uint32_t* cs, cudaStream_t s);
 int launch64_correct(int dim, const StepArgs& a, cudaStream_t s);
@@ -29,25 +28,34 @@ int launch_seed(int dim, int prec, const StepArgs& a, uint32_t* cs, cudaStream_t
 int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s)
 {
     if (prec == 0) return launch64_advect(dim, a, s);
-    if (dim == 2) k_advect32<2><<<PFEM2_GRID(k_advect32<2>, 256), 256, 0, s>>>(a);
-    else k_advect32<3><<<PFEM2_GRID(k_advect32<3>, 256), 256, 0, s>>>(a);
-    return 1;
+    if (dim == 2) {
+        k_advect32<2><<<PFEM2_GRID(k_advect32<2>, 256), 256, 0, s>>>(a);
+        k_cross32<2><<<PFEM2_GRID(k_cross32<2>, 128), 128, 0, s>>>(a);
+    } else {
+        k_advect32<3><<<PFEM2_GRID(k_advect32<3>, 256), 256, 0, s>>>(a);
+        k_cross32<3><<<PFEM2_GRID(k_cross32<3>, 128), 128, 0, s>>>(a);
+    }
+    return 2;
 }
 
-int launch_count(int dim, int prec, const StepArgs& a, cudaStream_t s)
+template <int DIM>
+static int write32_t(const StepArgs& a, uint32_t* cs, cudaStream_t s)
 {
-    if (prec == 0) return launch64_count(dim, a, s);
-    if (dim == 2) k_count<2, float><<<PFEM2_GRID((k_count<2, float>), CELL_THREADS), CELL_THREADS, 0, s>>>(a);
-    else k_count<3, float><<<PFEM2_GRID((k_count<3, float>), CELL_THREADS), CELL_THREADS, 0, s>>>(a);
+    const int smem = (int)sizeof(WriteSmem<float>);
+    static bool init = false;
+    if (!init) {
+        cudaFuncSetAttribute(k_write<DIM, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        init = true;
+    }
+    const int grid = occupancy_grid((const void*)k_write<DIM, float>, WR_WARPS * 32, smem);
+    k_write<DIM, float><<<grid, WR_WARPS * 32, smem, s>>>(a, cs);
     return 1;
 }
 
 int launch_write(int dim, int prec, const StepArgs& a, uint32_t* cs, cudaStream_t s)
 {
     if (prec == 0) return launch64_write(dim, a, cs, s);
-    if (dim == 2) k_write<2, float><<<PFEM2_GRID((k_write<2, float>), CELL_THREADS), CELL_THREADS, 0, s>>>(a, cs);
-    else k_write<3, float><<<PFEM2_GRID((k_write<3, float>), CELL_THREADS), CELL_THREADS, 0, s>>>(a, cs);
-    return 1;
+    return dim == 2 ? write32_t<2>(a, cs, s) : write32_t<3>(a, cs, s);
 }
 
 int launch_partials(int dim, int prec, const StepArgs& a, const uint32_t* cs, cudaStream_t s)

@@ -12,9 +12,10 @@ namespace {
 
 template <int DIM>
 __global__ void k_cell_setup(int nC, const double* __restrict__ verts, const int32_t* __restrict__ cv,
-                             double* __restrict__ cellX, double* __restrict__ aff, float* __restrict__ geo32)
+                             double* __restrict__ cellX, double* __restrict__ aff, float* __restrict__ geo32,
+                             float* __restrict__ jinv32)
 {
-    constexpr int NV = 1 << DIM, GS = Dims<DIM>::GEO;
+    constexpr int NV = 1 << DIM, GS = Dims<DIM>::GEO, JS = Dims<DIM>::JS;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nC; c += gridDim.x * blockDim.x) {
         double X[NV][DIM];
 #pragma unroll
@@ -51,6 +52,27 @@ __global__ void k_cell_setup(int nC, const double* __restrict__ verts, const int
             }
         for (int k = (NV - 1) * DIM; k < GS - 1; ++k) g[k] = 0.0f;
         g[GS - 1] = affine ? 1.0f : 0.0f;
+        // inverse Jacobian at the cell centre (exact for affine cells)
+        double J[DIM][DIM], Ji[DIM][DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            if (DIM == 2) {
+                J[d][0] = Y[1][d] + 0.5 * Y[3][d];
+                J[d][1] = Y[2][d] + 0.5 * Y[3][d];
+            } else {
+                J[d][0] = Y[1][d] + 0.5 * Y[3][d] + 0.5 * Y[5 % NV][d] + 0.25 * Y[7 % NV][d];
+                J[d][1] = Y[2][d] + 0.5 * Y[3][d] + 0.5 * Y[6 % NV][d] + 0.25 * Y[7 % NV][d];
+                J[d][DIM - 1] = Y[4 % NV][d] + 0.5 * Y[5 % NV][d] + 0.5 * Y[6 % NV][d] + 0.25 * Y[7 % NV][d];
+            }
+        }
+        invert64<DIM>(J, Ji);
+        float* jj = jinv32 + (size_t)c * JS;
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int q = 0; q < DIM; ++q) jj[r * DIM + q] = (float)Ji[r][q];
+        for (int k = DIM * DIM; k < JS; ++k) jj[k] = 0.0f;
+        jj[DIM * DIM] = affine ? 1.0f : 0.0f;
     }
 }
 
@@ -66,11 +88,11 @@ int seed_t(const StepArgs& a, uint32_t* cs, cudaStream_t s)
 }  // namespace
 
 int launch_cell_setup(int dim, int nC, const double* verts, const int32_t* cv, double* cellX, double* aff,
-                      float* geo32, cudaStream_t s)
+                      float* geo32, float* jinv32, cudaStream_t s)
 {
     const int grid = (nC + 127) / 128;
-    if (dim == 2) k_cell_setup<2><<<grid, 128, 0, s>>>(nC, verts, cv, cellX, aff, geo32);
-    else k_cell_setup<3><<<grid, 128, 0, s>>>(nC, verts, cv, cellX, aff, geo32);
+    if (dim == 2) k_cell_setup<2><<<grid, 128, 0, s>>>(nC, verts, cv, cellX, aff, geo32, jinv32);
+    else k_cell_setup<3><<<grid, 128, 0, s>>>(nC, verts, cv, cellX, aff, geo32, jinv32);
     return 1;
 }
 
@@ -84,23 +106,33 @@ int launch64_seed(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s)
 
 int launch64_advect(int dim, const StepArgs& a, cudaStream_t s)
 {
-    if (dim == 2) k_advect64<2><<<PFEM2_GRID(k_advect64<2>, 256), 256, 0, s>>>(a);
-    else k_advect64<3><<<PFEM2_GRID(k_advect64<3>, 256), 256, 0, s>>>(a);
-    return 1;
+    if (dim == 2) {
+        k_advect64<2><<<PFEM2_GRID(k_advect64<2>, 256), 256, 0, s>>>(a);
+        k_search64<2><<<PFEM2_GRID(k_search64<2>, 128), 128, 0, s>>>(a);
+    } else {
+        k_advect64<3><<<PFEM2_GRID(k_advect64<3>, 256), 256, 0, s>>>(a);
+        k_search64<3><<<PFEM2_GRID(k_search64<3>, 128), 128, 0, s>>>(a);
+    }
+    return 2;
 }
 
-int launch64_count(int dim, const StepArgs& a, cudaStream_t s)
+template <int DIM>
+static int write_t(const StepArgs& a, uint32_t* cs, cudaStream_t s)
 {
-    if (dim == 2) k_count<2, double><<<PFEM2_GRID((k_count<2, double>), CELL_WARPS * 32), CELL_WARPS * 32, 0, s>>>(a);
-    else k_count<3, double><<<PFEM2_GRID((k_count<3, double>), CELL_WARPS * 32), CELL_WARPS * 32, 0, s>>>(a);
+    const int smem = (int)sizeof(WriteSmem<double>);
+    static bool init = false;
+    if (!init) {
+        cudaFuncSetAttribute(k_write<DIM, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        init = true;
+    }
+    const int grid = occupancy_grid((const void*)k_write<DIM, double>, WR_WARPS * 32, smem);
+    k_write<DIM, double><<<grid, WR_WARPS * 32, smem, s>>>(a, cs);
     return 1;
 }
 
 int launch64_write(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s)
 {
-    if (dim == 2) k_write<2, double><<<PFEM2_GRID((k_write<2, double>), CELL_WARPS * 32), CELL_WARPS * 32, 0, s>>>(a, cs);
-    else k_write<3, double><<<PFEM2_GRID((k_write<3, double>), CELL_WARPS * 32), CELL_WARPS * 32, 0, s>>>(a, cs);
-    return 1;
+    return dim == 2 ? write_t<2>(a, cs, s) : write_t<3>(a, cs, s);
 }
 
 int launch64_partials(int dim, const StepArgs& a, const uint32_t* cs, cudaStream_t s)

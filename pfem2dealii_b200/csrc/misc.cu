@@ -143,7 +143,7 @@ __global__ void k_rekey(StepArgs a)
 __global__ void k_finalize(StepArgs a, uint32_t* cell_start, int count_step)
 {
     if (count_step) a.stats->particle_steps += a.stats->n_particles;
-    const unsigned long long po = a.packed_off[a.mesh.nC];
+    const unsigned long long po = *a.totals;
     uint32_t total = (uint32_t)po;
     const uint32_t seeds = (uint32_t)(po >> 32);
     if (total > a.capacity) {
