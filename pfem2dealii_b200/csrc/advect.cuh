@@ -199,14 +199,13 @@ __device__ __forceinline__ void defer(const StepArgs& a, bool want, uint32_t i, 
     }
 }
 
-__device__ __forceinline__ void arrive(const StepArgs& a, uint32_t i, uint32_t c, bool alive)
+// Record where particle i ended: its cell, or LOST.  A particle that changed
+// cell is pushed on the arrival list of its new cell; the ones that stayed
+// are found by the write pass in their old cell range.
+__device__ __forceinline__ void arrive(const StepArgs& a, uint32_t i, uint32_t c, uint32_t c_old, bool alive)
 {
-    if (alive) {
-        a.key[i] = c;
-        a.slot[i] = atomicAdd(a.cell_count + c, 1u);
-    } else {
-        a.key[i] = LOST;
-    }
+    a.key[i] = alive ? c : LOST;
+    if (alive && c != c_old) a.next[i] = atomicExch(a.head + c, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -218,11 +217,13 @@ __device__ __forceinline__ void arrive(const StepArgs& a, uint32_t i, uint32_t c
 // repeated in the same order.
 // ---------------------------------------------------------------------------
 
+// u = sum_i N_i(xi) V_i with V_i the cell's vertex velocities (a per-step
+// copy of V[dof_i], so the values are V's own).
 template <int DIM>
-__device__ __forceinline__ void velocity64(const MeshDev& m, const double* __restrict__ V, const int32_t* dof,
-                                           const double* xi, double* u)
+__device__ __forceinline__ void velocity64(const double* __restrict__ Vc, uint32_t c, const double* xi, double* u)
 {
     constexpr int NV = 1 << DIM, VS = Dims<DIM>::VS;
+    const double* p = Vc + (size_t)c * NV * VS;
     double N[NV];
     shape64<DIM>(xi, N);
 #pragma unroll
@@ -230,14 +231,7 @@ __device__ __forceinline__ void velocity64(const MeshDev& m, const double* __res
 #pragma unroll
     for (int iv = 0; iv < NV; ++iv)
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) u[d] = u[d] + N[iv] * __ldg(V + (size_t)dof[iv] * VS + d);
-}
-
-template <int DIM>
-__device__ __forceinline__ void load_dofs(const MeshDev& m, uint32_t c, int32_t* dof)
-{
-#pragma unroll
-    for (int iv = 0; iv < (1 << DIM); ++iv) dof[iv] = __ldg(m.cd + (size_t)c * (1 << DIM) + iv);
+        for (int d = 0; d < DIM; ++d) u[d] = u[d] + N[iv] * __ldg(p + iv * VS + d);
 }
 
 // Sub-steps s0.. of one FP64 particle starting in cell c; returns the
@@ -248,14 +242,11 @@ __device__ __forceinline__ int substeps64(const StepArgs& a, uint32_t c, int s0,
 {
     constexpr int NV = 1 << DIM;
     const MeshDev& m = a.mesh;
-    const double* __restrict__ V = (const double*)a.Vaos;
     double X[NV][DIM];
-    int32_t dof[NV];
     load_cell64<DIM>(m.cellX, c, X);
-    load_dofs<DIM>(m, c, dof);
     int s = s0;
     for (; s < a.pp.S; ++s) {
-        velocity64<DIM>(m, V, dof, xi, u);
+        velocity64<DIM>((const double*)a.Vc, c, xi, u);
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
             const double st = u[d] * a.pp.dtp;
@@ -278,10 +269,8 @@ __device__ __forceinline__ int substeps64(const StepArgs& a, uint32_t c, int s0,
 template <int DIM>
 __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
 {
-    constexpr int NV = 1 << DIM, VS = Dims<DIM>::VS;
     const MeshDev& m = a.mesh;
     const uint32_t n = (uint32_t)a.stats->n_particles;
-    const double* __restrict__ dV = (const double*)a.dVaos;
     AdvCounters k;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t nloop = (n + stride - 1) / stride * stride;  // whole warps iterate together
@@ -301,18 +290,9 @@ __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
             bool alive = c < (uint32_t)m.nC;
             if (!alive) k.err |= ERR_BAD_CELL;
             if (alive) {
-                if (a.do_correct) {  // :126-138
-                    int32_t dof[NV];
-                    load_dofs<DIM>(m, c, dof);
-                    double N[NV], corr[DIM];
-                    shape64<DIM>(xi, N);
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) corr[d] = 0.0;
-#pragma unroll
-                    for (int iv = 0; iv < NV; ++iv)
-#pragma unroll
-                        for (int d = 0; d < DIM; ++d)
-                            corr[d] = corr[d] + N[iv] * __ldg(dV + (size_t)dof[iv] * VS + d);
+                if (a.do_correct) {  // :126-138, deltaV = V - Vold per vertex
+                    double corr[DIM];
+                    velocity64<DIM>((const double*)a.dVc, c, xi, corr);
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) v[d] = v[d] + corr[d];
                 }
@@ -327,7 +307,7 @@ __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
             }
             if (want) a.key[i] = c;
             else {
-                arrive(a, i, c, alive);
+                arrive(a, i, c, c, alive);
                 if (!alive) k.lost++;
             }
         }
@@ -349,6 +329,7 @@ __global__ void __launch_bounds__(128) k_search64(StepArgs a)
         const uint32_t i = e.x;
         int s = (int)e.y;
         uint32_t c = a.key[i];
+        const uint32_t c_old = a.S0.cell[i];
         double x[DIM], xi[DIM], u[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
@@ -358,9 +339,7 @@ __global__ void __launch_bounds__(128) k_search64(StepArgs a)
         bool alive = true;
         while (true) {
             // velocity_ext of sub-step s, recomputed from the start-of-sub-step state
-            int32_t dof[1 << DIM];
-            load_dofs<DIM>(m, c, dof);
-            velocity64<DIM>(m, (const double*)a.Vaos, dof, xi, u);
+            velocity64<DIM>((const double*)a.Vc, c, xi, u);
             Vec<DIM> xo, ve, xp;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
@@ -388,7 +367,7 @@ __global__ void __launch_bounds__(128) k_search64(StepArgs a)
             ((double*)a.T.x[d])[i] = x[d];
             ((double*)a.T.xi[d])[i] = xi[d];
         }
-        arrive(a, i, c, alive);
+        arrive(a, i, c, c_old, alive);
         if (!alive) k.lost++;
     }
     flush_counters(a, k);
@@ -446,21 +425,22 @@ __device__ __noinline__ F3<DIM> newton32(const float* __restrict__ geo, uint32_t
 }
 
 template <int DIM>
-__device__ __forceinline__ void velocity32(const float* __restrict__ V, const int32_t* dof, const float* xi, float* u)
+__device__ __forceinline__ void velocity32(const float* __restrict__ Vc, uint32_t c, const float* xi, float* u)
 {
-    float N[1 << DIM];
+    constexpr int NV = 1 << DIM;
+    float N[NV];
     shape32<DIM>(xi, N);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) u[d] = 0.0f;
 #pragma unroll
-    for (int iv = 0; iv < (1 << DIM); ++iv) {
+    for (int iv = 0; iv < NV; ++iv) {
         if constexpr (DIM == 3) {
-            const float4 t = __ldg(reinterpret_cast<const float4*>(V) + dof[iv]);
+            const float4 t = __ldg(reinterpret_cast<const float4*>(Vc) + (size_t)c * NV + iv);
             u[0] += N[iv] * t.x;
             u[1] += N[iv] * t.y;
             u[2] += N[iv] * t.z;
         } else {
-            const float2 t = __ldg(reinterpret_cast<const float2*>(V) + dof[iv]);
+            const float2 t = __ldg(reinterpret_cast<const float2*>(Vc) + (size_t)c * NV + iv);
             u[0] += N[iv] * t.x;
             u[1] += N[iv] * t.y;
         }
@@ -470,7 +450,7 @@ __device__ __forceinline__ void velocity32(const float* __restrict__ V, const in
 // FP32 sub-steps s0.. in cell c; returns the sub-step that leaves the cell
 // (S if none).  xi is advanced in place.
 template <int DIM>
-__device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi, const int32_t* dof)
+__device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi)
 {
     J32<DIM> j;
     load_jinv32<DIM>(a.mesh.jinv32, c, j);
@@ -478,7 +458,7 @@ __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0,
     int s = s0;
     for (; s < a.pp.S; ++s) {
         float u[DIM], dl[DIM], y[DIM];
-        velocity32<DIM>((const float*)a.Vaos, dof, xi, u);
+        velocity32<DIM>((const float*)a.Vc, c, xi, u);
         F3<DIM> dx;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) dx.v[d] = u[d] * dtp;
@@ -533,15 +513,13 @@ __global__ void __launch_bounds__(256) k_advect32(StepArgs a)
             const bool alive = c < (uint32_t)m.nC;
             if (!alive) k.err |= ERR_BAD_CELL;
             if (alive) {
-                int32_t dof[NV];
-                load_dofs<DIM>(m, c, dof);
                 if (a.do_correct) {
                     float dv[DIM];
-                    velocity32<DIM>((const float*)a.dVaos, dof, xi, dv);
+                    velocity32<DIM>((const float*)a.dVc, c, xi, dv);
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) v[d] += dv[d];
                 }
-                s = substeps32<DIM>(a, c, 0, xi, dof);
+                s = substeps32<DIM>(a, c, 0, xi);
                 want = s < a.pp.S;
             }
 #pragma unroll
@@ -551,7 +529,7 @@ __global__ void __launch_bounds__(256) k_advect32(StepArgs a)
             }
             if (want) a.key[i] = c;
             else {
-                arrive(a, i, c, alive);
+                arrive(a, i, c, c, alive);
                 if (!alive) k.lost++;
             }
         }
@@ -575,15 +553,14 @@ __global__ void __launch_bounds__(128) k_cross32(StepArgs a)
         const uint32_t i = e.x;
         int s = (int)e.y;
         uint32_t c = a.key[i];
+        const uint32_t c_old = a.S0.cell[i];
         float xi[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) xi[d] = ((const float*)a.T.xi[d])[i];
         bool alive = true;
         while (true) {
-            int32_t dof[NV];
-            load_dofs<DIM>(m, c, dof);
             float u[DIM];
-            velocity32<DIM>((const float*)a.Vaos, dof, xi, u);
+            velocity32<DIM>((const float*)a.Vc, c, xi, u);
             Vec<DIM> xo, ue;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
@@ -607,13 +584,12 @@ __global__ void __launch_bounds__(128) k_cross32(StepArgs a)
                 const float t = (float)so.xi[d];
                 xi[d] = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
             }
-            load_dofs<DIM>(m, c, dof);
-            s = substeps32<DIM>(a, c, s + 1, xi, dof);
+            s = substeps32<DIM>(a, c, s + 1, xi);
             if (s >= a.pp.S) break;
         }
 #pragma unroll
         for (int d = 0; d < DIM; ++d) ((float*)a.T.xi[d])[i] = xi[d];
-        arrive(a, i, c, alive);
+        arrive(a, i, c, c_old, alive);
         if (!alive) k.lost++;
     }
     flush_counters(a, k);

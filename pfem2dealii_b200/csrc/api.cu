@@ -1,8 +1,8 @@
 // C ABI of the particle path: handle, device memory, and the per-call kernel
 // sequences.  One time step of the reference loop (src/pfem2solver.cpp:162-164)
 // maps to
-//   correct(V, Vold)  -> stage V, V - Vold (the correction is fused into move)
-//   move(V)           -> advect | scan cells | bucket | count | scan | write | finalize
+//   correct(V, Vold)  -> stage V, V - Vold per cell vertex (the correction is fused into move)
+//   move(V)           -> advect | FP64 relocation queue | write (look-back) | finalize
 //   project(V_out)    -> gather (per-cell partials were summed by write) | D2H
 #include <algorithm>
 #include <cmath>
@@ -31,14 +31,14 @@ struct pfem2gpu_handle {
     float* geo32 = nullptr;
     // velocities
     double *Vstage = nullptr, *Vstage2 = nullptr, *Vout = nullptr;
-    void *Vaos = nullptr, *dVaos = nullptr;
+    void *Vc = nullptr, *dVc = nullptr;
     bool vaos_valid = false;
     // particles
     uint32_t cap = 0;
     PartState S0{}, S1{}, T{};
-    uint32_t *key = nullptr, *slot = nullptr, *idx = nullptr;
+    uint32_t *key = nullptr, *next = nullptr;
     double* xtmp = nullptr;
-    uint32_t *cell_count = nullptr, *cell_off = nullptr, *cell_start = nullptr, *tiles32 = nullptr;
+    uint32_t *head = nullptr, *cs0 = nullptr, *cs1 = nullptr;  // cs0: cell ranges of S0
     uint2* xq = nullptr;
     uint32_t* nxq = nullptr;
     unsigned long long *tile_status = nullptr, *totals = nullptr;
@@ -157,15 +157,15 @@ StepArgs args(pfem2gpu_handle* h)
     a.S0 = h->S0;
     a.S1 = h->S1;
     a.T = h->T;
-    a.Vaos = h->Vaos;
-    a.dVaos = h->dVaos;
+    a.Vc = h->Vc;
+    a.dVc = h->dVc;
     a.do_correct = 0;
     a.apply_counts = 1;
     a.key = h->key;
-    a.slot = h->slot;
-    a.idx = h->idx;
-    a.cell_count = h->cell_count;
-    a.cell_off = h->cell_off;
+    a.head = h->head;
+    a.next = h->next;
+    a.cs_old = h->cs0;
+    a.cs_new = h->cs1;
     a.xq = h->xq;
     a.nxq = h->nxq;
     a.tile_status = h->tile_status;
@@ -234,19 +234,17 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
     free_state(h->S1);
     free_state(h->T);
     dfree(h->key);
-    dfree(h->slot);
-    dfree(h->idx);
+    dfree(h->next);
     dfree(h->xtmp);
     dfree(h->xq);
-    h->key = h->slot = h->idx = nullptr;
+    h->key = h->next = nullptr;
     h->xtmp = nullptr;
     h->xq = nullptr;
     h->S0 = n0;
     h->S1 = n1;
     h->T = nt;
     CK(dalloc(&h->key, cap));
-    CK(dalloc(&h->slot, cap));
-    CK(dalloc(&h->idx, cap));
+    CK(dalloc(&h->next, cap));
     CK(dalloc(&h->xq, cap));
     if (!h->nxq) CK(dalloc(&h->nxq, 1));
     if (h->prec == PFEM2GPU_FP32) CK(dalloc(&h->xtmp, cap * h->dim));
@@ -271,8 +269,9 @@ int stage_v(pfem2gpu_handle* h, const double* V, const double* Vold, bool device
     } else if (V != h->Vstage) {
         CK(cudaMemcpyAsync(h->Vstage, V, bytes, cudaMemcpyDeviceToDevice, h->stream));
     }
-    run(h, "stage_velocity",
-        [&] { return launch_prep_v(h->dim, h->prec, v, vo, h->nD, h->Vaos, Vold ? h->dVaos : nullptr, h->stream); });
+    run(h, "stage_velocity", [&] {
+        return launch_cell_v(h->dim, h->prec, v, vo, h->cd, h->nC, h->nD, h->Vc, Vold ? h->dVc : nullptr, h->stream);
+    });
     h->vaos_valid = true;
     return PFEM2GPU_OK;
 }
@@ -294,18 +293,17 @@ int apply_pending_correction(pfem2gpu_handle* h)
     return check_async(h);
 }
 
-// Re-bucket and write the next sorted state from T (advected or uploaded
-// particles, keys and slots already set): the shared tail of move and
+// The write pass (count correction, sorted layout, projection partials) and
+// the counters of the step; S1 becomes the current state.  Shared by move and
 // set_particles.
-int sort_and_write(pfem2gpu_handle* h, StepArgs& a, int count_step)
+int write_and_swap(pfem2gpu_handle* h, StepArgs& a, int count_step)
 {
-    run(h, "scan_cells", [&] { return launch_scan_u32(h->cell_count, h->nC, h->cell_off, h->tiles32, h->stream); });
-    run(h, "bucket", [&] { return launch_bucket(a, h->stream); });
     CK(cudaMemsetAsync(h->tile_status, 0, h->ntiles * sizeof(unsigned long long), h->stream));
     CK(cudaMemsetAsync(h->tile_counter, 0, sizeof(uint32_t), h->stream));
-    run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->cell_start, h->stream); });
-    run(h, "finalize", [&] { return launch_finalize(a, h->cell_start, count_step, h->stream); });
+    run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->stream); });
+    run(h, "finalize", [&] { return launch_finalize(a, count_step, h->stream); });
     std::swap(h->S0, h->S1);
+    std::swap(h->cs0, h->cs1);
     h->partials_valid = true;
     return check_async(h);
 }
@@ -317,10 +315,9 @@ int do_move(pfem2gpu_handle* h)
     StepArgs a = args(h);
     a.do_correct = h->pending_correct ? 1 : 0;
     h->pending_correct = false;
-    CK(cudaMemsetAsync(h->cell_count, 0, h->nC * sizeof(uint32_t), h->stream));
     CK(cudaMemsetAsync(h->nxq, 0, sizeof(uint32_t), h->stream));
     run(h, "advect", [&] { return launch_advect(h->dim, h->prec, a, h->stream); });
-    return sort_and_write(h, a, 1);
+    return write_and_swap(h, a, 1);
 }
 
 int sync_stats(pfem2gpu_handle* h)
@@ -404,6 +401,16 @@ int pfem2gpu_create(int dim, int precision, const pfem2gpu_params* prm, pfem2gpu
     pp.S = prm->particle_integration_steps == 0 ? 1 : prm->particle_integration_steps;  // :34-36
     pp.dtp = prm->time_step / (double)pp.S;                                               // :38
     pp.seed = prm->removal_seed;
+    pp.realmask = 0;
+    for (int e = 0; e < npe && e < 64; ++e) {  // extended-part digits, x-major, base q_d + 1
+        int r = e;
+        bool real = true;
+        for (int d = dim - 1; d >= 0; --d) {
+            real = real && (r % (pp.q[d] + 1)) < pp.q[d];
+            r /= pp.q[d] + 1;
+        }
+        if (real) pp.realmask |= 1ull << e;
+    }
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&h->stats, sizeof(DevStats)) != cudaSuccess ||
         cudaMallocHost(&h->stats_h, sizeof(DevStats)) != cudaSuccess ||
@@ -422,9 +429,9 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (void* p : {(void*)h->cv, (void*)h->cd, (void*)h->v2c_off, (void*)h->v2c_cells, (void*)h->d2c_off,
                     (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
-                    (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vaos, h->dVaos,
-                    (void*)h->key, (void*)h->slot, (void*)h->idx, (void*)h->xtmp, (void*)h->cell_count,
-                    (void*)h->cell_off, (void*)h->cell_start, (void*)h->tiles32, (void*)h->tile_status,
+                    (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vc, h->dVc,
+                    (void*)h->key, (void*)h->next, (void*)h->xtmp, (void*)h->head, (void*)h->cs0, (void*)h->cs1,
+                    (void*)h->tile_status,
                     (void*)h->tile_counter, (void*)h->totals, (void*)h->jinv32, (void*)h->xq, (void*)h->nxq,
                     h->partials, (void*)h->stats})
         dfree(p);
@@ -450,7 +457,6 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     if (n_cells < 1 || n_verts < 1 || n_dofs < 1 || n_cells > (1ll << 30) || n_verts > (1ll << 30) ||
         n_dofs > (1ll << 30))
         return fail(h, PFEM2GPU_ERR_ARG, "mesh sizes out of range");
-    if ((n_cells + SCAN_TILE - 1) / SCAN_TILE > SCAN_MAX_TILES) return fail(h, PFEM2GPU_ERR_ARG, "too many cells");
     if (h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "mesh change with live particles");
     const int dim = h->dim, NV = 1 << dim;
     for (int64_t k = 0; k < n_cells * NV; ++k) {
@@ -518,9 +524,9 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     // release an older mesh
     for (void* p : {(void*)h->cv, (void*)h->cd, (void*)h->v2c_off, (void*)h->v2c_cells, (void*)h->d2c_off,
                     (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
-                    (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vaos, h->dVaos,
-                    (void*)h->cell_count, (void*)h->cell_off, (void*)h->cell_start, (void*)h->tiles32,
-                    (void*)h->tile_status, (void*)h->tile_counter, (void*)h->totals, (void*)h->jinv32, h->partials})
+                    (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vc, h->dVc,
+                    (void*)h->head, (void*)h->cs0, (void*)h->cs1, (void*)h->tile_status, (void*)h->tile_counter,
+                    (void*)h->totals, (void*)h->jinv32, h->partials})
         dfree(p);
     h->has_mesh = false;
     h->nC = (int)n_cells;
@@ -542,17 +548,16 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(dalloc(&h->Vstage, nd * dim));
     CK(dalloc(&h->Vstage2, nd * dim));
     CK(dalloc(&h->Vout, nd * dim));
-    CK(cudaMalloc(&h->Vaos, nd * VS * esize(h)));
-    CK(cudaMalloc(&h->dVaos, nd * VS * esize(h)));
-    CK(dalloc(&h->cell_count, nc));
-    CK(dalloc(&h->cell_off, nc + 1));
-    CK(dalloc(&h->cell_start, nc + 1));
+    CK(cudaMalloc(&h->Vc, nc * NV * VS * esize(h)));
+    CK(cudaMalloc(&h->dVc, nc * NV * VS * esize(h)));
+    CK(dalloc(&h->head, nc));
+    CK(dalloc(&h->cs0, nc + 1));
+    CK(dalloc(&h->cs1, nc + 1));
     h->ntiles = (uint32_t)((nc + WR_TILE - 1) / WR_TILE);
     CK(dalloc(&h->tile_status, h->ntiles));
     CK(dalloc(&h->tile_counter, 1));
     CK(dalloc(&h->totals, 1));
     CK(dalloc(&h->jinv32, nc * (dim == 3 ? 12 : 8)));
-    CK(dalloc(&h->tiles32, SCAN_MAX_TILES));
     CK(cudaMalloc(&h->partials, nc * PW * esize(h)));
     CK(cudaMemcpyAsync(h->cv, cell_vertices, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->cd, cell_dofs, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
@@ -562,8 +567,9 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(cudaMemcpyAsync(h->v2c_dirs, dirs.data(), dirs.size() * 8, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d2c_off, doff.data(), doff.size() * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d2c_ent, dent.data(), dent.size() * 4, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemsetAsync(h->Vaos, 0, nd * VS * esize(h), h->stream));
-    CK(cudaMemsetAsync(h->dVaos, 0, nd * VS * esize(h), h->stream));
+    CK(cudaMemsetAsync(h->Vc, 0, nc * NV * VS * esize(h), h->stream));
+    CK(cudaMemsetAsync(h->dVc, 0, nc * NV * VS * esize(h), h->stream));
+    run(h, "fill", [&] { return launch_fill_u32(h->head, (uint32_t)nc, LOST, h->stream); });
     CK(cudaMemsetAsync(h->Vstage, 0, nd * dim * 8, h->stream));
     run(h, "cell_setup",
         [&] { return launch_cell_setup(dim, h->nC, h->verts, h->cv, h->cellX, h->aff, h->geo32, h->jinv32, h->stream); });
@@ -584,7 +590,7 @@ static int seed_impl(pfem2gpu_handle* h, const double* V, bool device)
     if (rc) return rc;
     if ((rc = stage_v(h, V, nullptr, device))) return rc;
     StepArgs a = args(h);
-    run(h, "seed", [&] { return launch_seed(h->dim, h->prec, a, h->cell_start, h->stream); });
+    run(h, "seed", [&] { return launch_seed(h->dim, h->prec, a, h->cs0, h->stream); });
     run(h, "finalize", [&] { return launch_set_state(h->stats, (long long)n, -1, (long long)n, h->stream); });
     h->has_particles = true;
     h->partials_valid = false;
@@ -636,7 +642,7 @@ static int project_impl(pfem2gpu_handle* h, double* out, bool device)
     if (rc) return rc;
     StepArgs a = args(h);
     if (!h->partials_valid) {
-        run(h, "partials", [&] { return launch_partials(h->dim, h->prec, a, h->cell_start, h->stream); });
+        run(h, "partials", [&] { return launch_partials(h->dim, h->prec, a, h->cs0, h->stream); });
         h->partials_valid = true;
     }
     CK(cudaMemsetAsync(&h->stats->nan_dofs, 0, sizeof(unsigned long long), h->stream));
@@ -735,13 +741,13 @@ int pfem2gpu_set_particles(pfem2gpu_handle* h, int64_t n, const uint32_t* id, co
     if (h->prec == PFEM2GPU_FP64 && (rc = put(x, h->T.x))) return rc;
     CK(cudaMemsetAsync(h->stats, 0, sizeof(DevStats), h->stream));
     run(h, "finalize", [&] { return launch_set_state(h->stats, n, next_id, 0, h->stream); });
-    CK(cudaMemsetAsync(h->cell_count, 0, h->nC * sizeof(uint32_t), h->stream));
+    CK(cudaMemsetAsync(h->cs0, 0, (h->nC + 1) * sizeof(uint32_t), h->stream));
     StepArgs a = args(h);
     a.apply_counts = 0;
     run(h, "rekey", [&] { return launch_rekey(a, h->stream); });
     h->has_particles = true;
     h->pending_correct = false;
-    if ((rc = sort_and_write(h, a, 0))) return rc;
+    if ((rc = write_and_swap(h, a, 0))) return rc;
     return sync_stats(h);
 }
 

@@ -37,22 +37,22 @@ __device__ __forceinline__ void str(void* p, uint32_t i, Real v)
     reinterpret_cast<Real*>(p)[i] = v;
 }
 
-// Velocity interpolation at xi, FP64 (reference arithmetic) or FP32.
+// Velocity interpolation at xi from the cell's vertex velocities, FP64
+// (reference arithmetic) or FP32.
 template <int DIM, typename Real>
-__device__ __forceinline__ void interp_v(const MeshDev& m, const void* Vaos, uint32_t c, const Real* xi, Real* u)
+__device__ __forceinline__ void interp_v(const void* Vc, uint32_t c, const Real* xi, Real* u)
 {
     constexpr int NV = 1 << DIM, VS = Dims<DIM>::VS;
+    const Real* p = reinterpret_cast<const Real*>(Vc) + (size_t)c * NV * VS;
     Real N[NV];
     if constexpr (std::is_same<Real, double>::value) shape64<DIM>(xi, N);
     else shape32<DIM>(xi, N);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) u[d] = Real(0);
 #pragma unroll
-    for (int iv = 0; iv < NV; ++iv) {
-        const int32_t dof = __ldg(m.cd + (size_t)c * NV + iv);
+    for (int iv = 0; iv < NV; ++iv)
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) u[d] = u[d] + N[iv] * __ldg(reinterpret_cast<const Real*>(Vaos) + (size_t)dof * VS + d);
-    }
+        for (int d = 0; d < DIM; ++d) u[d] = u[d] + N[iv] * __ldg(p + iv * VS + d);
 }
 
 // A new particle at the centre of part idx of cell c (seed_particles
@@ -68,7 +68,7 @@ __device__ __forceinline__ void new_particle(const StepArgs& a, const PartState&
         xid[d] = (idx[d] + 0.5) * a.pp.h[d];
         xi[d] = (Real)xid[d];
     }
-    interp_v<DIM, Real>(a.mesh, a.Vaos, c, xi, v);
+    interp_v<DIM, Real>(a.Vc, c, xi, v);
     if constexpr (std::is_same<Real, double>::value) {
         double X[1 << DIM][DIM], x[DIM];
         load_cell64<DIM>(a.mesh.cellX, c, X);
@@ -310,19 +310,53 @@ static __device__ __noinline__ unsigned long long lookback(const StepArgs& a, ui
     return ((unsigned long long)es << 32) | ef;
 }
 
+// The particles of cell c after the move: those of its old range [s0, s0+L)
+// that stayed (key == c), then its arrival list.  Each particle is visited
+// by one lane: f(i, ord) with ord = j in the range or L + t on the list.
+// The list walk stops after `capacity` nodes (an unreset list can not loop).
+template <typename F>
+__device__ __forceinline__ void for_each_in_cell(const StepArgs& a, uint32_t c, uint32_t s0, uint32_t L, uint32_t h,
+                                                 int lane, F&& f)
+{
+    for (uint32_t j = lane; j < L; j += 32) {
+        const uint32_t i = s0 + j;
+        if (a.key[i] == c) f(i, j);
+    }
+    uint32_t t = 0;
+    for (uint32_t p = h; p != LOST && t < a.capacity; p = a.next[p], ++t)
+        if ((t & 31u) == (uint32_t)lane) f(p, L + t);
+}
+
+// Every particle of the cell in one lane (for the rank loops).
+template <typename F>
+__device__ __forceinline__ void for_all_in_cell(const StepArgs& a, uint32_t c, uint32_t s0, uint32_t L, uint32_t h,
+                                                F&& f)
+{
+    for (uint32_t j = 0; j < L; ++j) {
+        const uint32_t i = s0 + j;
+        if (a.key[i] == c) f(i, j);
+    }
+    uint32_t t = 0;
+    for (uint32_t p = h; p != LOST && t < a.capacity; p = a.next[p], ++t) f(p, L + t);
+}
+
 // General-path phase 1: per-part counts of one cell (in cnt) and its
-// (final, seeds).  Also caches (part, key) pairs of the first KEY_CACHE.
+// (final, seeds).  Also caches (part, key) pairs by ord below KEY_CACHE.
 template <int DIM, typename Real>
-__device__ __forceinline__ uint2 count_cell(const StepArgs& a, int* cnt, uint2* kc, uint32_t b, uint32_t nseg, int lane)
+__device__ __forceinline__ uint2 count_cell(const StepArgs& a, int* cnt, uint2* kc, uint32_t c, uint32_t s0, uint32_t L,
+                                            uint32_t h, int lane)
 {
     const int npe = a.pp.npe;
     for (int p = lane; p < npe; p += 32) cnt[p] = 0;
     __syncwarp();
-    for (uint32_t j = lane; j < nseg; j += 32) {
-        const uint2 pk = part_key<DIM, Real>(a, a.idx[b + j]);
+    unsigned nloc = 0;
+    for_each_in_cell(a, c, s0, L, h, lane, [&](uint32_t i, uint32_t ord) {
+        const uint2 pk = part_key<DIM, Real>(a, i);
         atomicAdd(cnt + pk.x, 1);
-        if (j < KEY_CACHE) kc[j] = pk;
-    }
+        if (ord < KEY_CACHE) kc[ord] = pk;
+        nloc++;
+    });
+    const uint32_t nseg = __reduce_add_sync(0xffffffffu, nloc);
     __syncwarp();
     unsigned surv = 0, seeds = 0;
     for (int p = lane; p < npe; p += 32) {
@@ -353,8 +387,8 @@ __device__ __forceinline__ void copy_particle(const StepArgs& a, uint32_t i, uin
 
 // General-path phase 2 of one cell (any particle count, any part count).
 template <int DIM, typename Real>
-__device__ void write_cell_general(const StepArgs& a, WriteSmem<Real>& sm, int warp, uint32_t c, uint32_t b,
-                                   uint32_t nseg, uint32_t fb, uint32_t sb, uint32_t id0, int lane,
+__device__ void write_cell_general(const StepArgs& a, WriteSmem<Real>& sm, int warp, uint32_t c, uint32_t s0,
+                                   uint32_t L, uint32_t h, uint32_t fb, uint32_t sb, uint32_t id0, int lane,
                                    unsigned long long& removed, uint32_t& err)
 {
     int* cnt = sm.cnt[warp];
@@ -362,7 +396,10 @@ __device__ void write_cell_general(const StepArgs& a, WriteSmem<Real>& sm, int w
     int* pfx = reinterpret_cast<int*>(&sm.tr[warp][0][0]);
     int* spfx = pfx + NPE_MAX;
     const int npe = a.pp.npe;
-    const uint2 fs = count_cell<DIM, Real>(a, cnt, kc, b, nseg, lane);
+    const uint2 fs = count_cell<DIM, Real>(a, cnt, kc, c, s0, L, h, lane);
+    bool has_any = false;
+    for (int p = lane; p < npe; p += 32) has_any = has_any || cnt[p] > 0;
+    has_any = __any_sync(0xffffffffu, has_any);
     int run = 0, srun = 0;
     for (int base = 0; base < npe; base += 32) {
         const int p = base + lane;
@@ -370,7 +407,7 @@ __device__ void write_cell_general(const StepArgs& a, WriteSmem<Real>& sm, int w
         if (p < npe) {
             const int s = survivors(cnt[p], a.pp.maxpp, a.apply_counts);
             int idx[3];
-            sf = (a.apply_counts && nseg > 0 && s == 0 && real_part<DIM>(p, a.pp, idx)) ? 1 : 0;
+            sf = (a.apply_counts && has_any && s == 0 && real_part<DIM>(p, a.pp, idx)) ? 1 : 0;
             fc = s + sf;
         }
         int ifc = fc, isf = sf;
@@ -392,16 +429,15 @@ __device__ void write_cell_general(const StepArgs& a, WriteSmem<Real>& sm, int w
     }
     __syncwarp();
     const uint32_t cap = a.capacity;
-    for (uint32_t j = lane; j < nseg; j += 32) {
-        const uint32_t i = a.idx[b + j];
-        const uint2 pk = j < KEY_CACHE ? kc[j] : part_key<DIM, Real>(a, i);
+    for_each_in_cell(a, c, s0, L, h, lane, [&](uint32_t i, uint32_t ord) {
+        const uint2 pk = ord < KEY_CACHE ? kc[ord] : part_key<DIM, Real>(a, i);
         const int k = cnt[pk.x];
         int rank = 0;
         if (k > 1) {
-            for (uint32_t jj = 0; jj < nseg; ++jj) {
-                const uint2 q = jj < KEY_CACHE ? kc[jj] : part_key<DIM, Real>(a, a.idx[b + jj]);
+            for_all_in_cell(a, c, s0, L, h, [&](uint32_t i2, uint32_t ord2) {
+                const uint2 q = ord2 < KEY_CACHE ? kc[ord2] : part_key<DIM, Real>(a, i2);
                 rank += (q.x == pk.x && q.y < pk.y) ? 1 : 0;
-            }
+            });
         }
         if (rank < survivors(k, a.pp.maxpp, a.apply_counts)) {
             const uint32_t dst = fb + (uint32_t)pfx[pk.x] + (uint32_t)rank;
@@ -411,8 +447,8 @@ __device__ void write_cell_general(const StepArgs& a, WriteSmem<Real>& sm, int w
         } else {
             removed++;
         }
-    }
-    if (a.apply_counts && nseg > 0) {
+    });
+    if (a.apply_counts && has_any) {
         for (int p = lane; p < npe; p += 32) {
             int idx[3] = {0, 0, 0};
             if (!real_part<DIM>(p, a.pp, idx)) continue;
@@ -431,19 +467,13 @@ __device__ void write_cell_general(const StepArgs& a, WriteSmem<Real>& sm, int w
 
 // The write pass (one launch per step; see the file comment).
 template <int DIM, typename Real>
-__global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a, uint32_t* cell_start)
+__global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WriteSmem<Real>& sm = *reinterpret_cast<WriteSmem<Real>*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int npe = a.pp.npe;
-    const bool fast_ok = npe <= 64;
-    unsigned long long realmask = 0;
-    if (fast_ok)
-        for (int p = 0; p < npe; ++p) {
-            int idx[3];
-            if (real_part<DIM>(p, a.pp, idx)) realmask |= 1ull << p;
-        }
+    const bool fast_ok = a.pp.npe <= 64;
+    const unsigned long long realmask = a.pp.realmask;
     const uint32_t id0 = a.stats->next_id;
     const uint32_t cap = a.capacity;
     unsigned long long removed = 0;
@@ -465,14 +495,31 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a, uint32_t* c
             uint32_t fin = 0, nsd = 0;
             unsigned long long seedm = 0;
             if (c < (uint32_t)a.mesh.nC) {
-                const uint32_t b = a.cell_off[c], nseg = a.cell_off[c + 1] - b;
-                bool fast = fast_ok && nseg <= 32;
+                const uint32_t s0 = a.cs_old[c], L = a.cs_old[c + 1] - s0;
+                const uint32_t h = a.head[c];
+                bool fast = fast_ok && L <= 32;
+                uint32_t i = 0, n = 0;
                 if (fast) {
-                    const bool valid = (uint32_t)lane < nseg;
-                    uint32_t i = 0;
+                    // stayers of the old range, compacted to lanes 0..ns-1
+                    const bool stay = (uint32_t)lane < L && a.key[s0 + lane] == c;
+                    const unsigned stm = __ballot_sync(0xffffffffu, stay);
+                    const uint32_t ns = __popc(stm);
+                    const uint32_t src = __fns(stm, 0, lane + 1);
+                    i = s0 + (src & 31u);
+                    // arrivals into lanes ns..
+                    uint32_t na = 0, p = h;
+                    while (p != LOST && ns + na < 32) {
+                        if ((uint32_t)lane == ns + na) i = p;
+                        ++na;
+                        p = a.next[p];
+                    }
+                    fast = p == LOST;
+                    n = ns + na;
+                }
+                if (fast) {
+                    const bool valid = (uint32_t)lane < n;
                     unsigned long long k64 = ~0ull;
                     if (valid) {
-                        i = a.idx[b + lane];
                         const uint2 pk = part_key<DIM, Real>(a, i);
                         k64 = ((unsigned long long)pk.x << 37) | ((unsigned long long)pk.y << 5) | (unsigned)lane;
                     }
@@ -491,7 +538,7 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a, uint32_t* c
                     const unsigned long long occ =
                         (unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)occ_me) |
                         ((unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)(occ_me >> 32)) << 32);
-                    seedm = (apply && nseg > 0) ? (realmask & ~occ) : 0ull;
+                    seedm = (apply && n > 0) ? (realmask & ~occ) : 0ull;
                     nsd = __popcll(seedm);
                     fin = __popc(survm) + nsd;
                     if (fin <= 32) {
@@ -510,13 +557,13 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a, uint32_t* c
                             if (lane == 0) om[__popc(nb) + k] = 0x80000000u | (uint32_t)p;
                             ++k;
                         }
-                        if (lane == 0) removed += nseg - __popc(survm);
+                        if (lane == 0) removed += n - __popc(survm);
                     } else {
                         fast = false;
                     }
                 }
                 if (!fast) {
-                    const uint2 fs = count_cell<DIM, Real>(a, sm.cnt[warp], sm.kc[warp], b, nseg, lane);
+                    const uint2 fs = count_cell<DIM, Real>(a, sm.cnt[warp], sm.kc[warp], c, s0, L, h, lane);
                     fin = fs.x;
                     nsd = fs.y;
                     if (lane == 0) atomicOr(&sm.slow, 1u << slotc);
@@ -561,36 +608,38 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a, uint32_t* c
             const uint32_t c = tile * WR_TILE + slotc;
             if (c >= (uint32_t)a.mesh.nC) continue;
             const uint32_t fb = pf + sm.excl_fin[slotc], sb = ps + sm.excl_seed[slotc];
-            if (lane == 0) cell_start[c] = fb;
+            if (lane == 0) a.cs_new[c] = fb;
             if (sm.slow & (1u << slotc)) {
-                const uint32_t b = a.cell_off[c], nseg = a.cell_off[c + 1] - b;
-                write_cell_general<DIM, Real>(a, sm, warp, c, b, nseg, fb, sb, id0, lane, removed, err);
-                continue;
-            }
-            const uint32_t fin = sm.fin[slotc];
-            const bool valid = (uint32_t)lane < fin;
-            Real xi[DIM], v[DIM];
+                const uint32_t s0 = a.cs_old[c], L = a.cs_old[c + 1] - s0;
+                write_cell_general<DIM, Real>(a, sm, warp, c, s0, L, a.head[c], fb, sb, id0, lane, removed, err);
+            } else {
+                const uint32_t fin = sm.fin[slotc];
+                const bool valid = (uint32_t)lane < fin;
+                Real xi[DIM], v[DIM];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) xi[d] = v[d] = Real(0);
-            if (valid) {
-                const uint32_t ent = sm.outmap[warp][j][lane];
-                const uint32_t dst = fb + lane;
-                if (dst >= cap) {
-                    err |= ERR_CAPACITY;
-                } else if (ent & 0x80000000u) {
-                    const int p = (int)(ent & 0x7fffffffu);
-                    int idx[3] = {0, 0, 0};
-                    real_part<DIM>(p, a.pp, idx);
-                    const unsigned long long sdm = sm.seedmask[slotc];
-                    const uint32_t r = (uint32_t)__popcll(p == 0 ? 0ull : (sdm & ((1ull << p) - 1ull)));
-                    new_particle<DIM, Real>(a, a.S1, dst, c, idx, id0 + sb + r + 1, xi, v);
-                } else {
-                    copy_particle<DIM, Real>(a, ent, dst, c, xi, v);
+                for (int d = 0; d < DIM; ++d) xi[d] = v[d] = Real(0);
+                if (valid) {
+                    const uint32_t ent = sm.outmap[warp][j][lane];
+                    const uint32_t dst = fb + lane;
+                    if (dst >= cap) {
+                        err |= ERR_CAPACITY;
+                    } else if (ent & 0x80000000u) {
+                        const int p = (int)(ent & 0x7fffffffu);
+                        int idx[3] = {0, 0, 0};
+                        real_part<DIM>(p, a.pp, idx);
+                        const unsigned long long sdm = sm.seedmask[slotc];
+                        const uint32_t r = (uint32_t)__popcll(p == 0 ? 0ull : (sdm & ((1ull << p) - 1ull)));
+                        new_particle<DIM, Real>(a, a.S1, dst, c, idx, id0 + sb + r + 1, xi, v);
+                    } else {
+                        copy_particle<DIM, Real>(a, ent, dst, c, xi, v);
+                    }
                 }
+                PartialAcc<Real> acc;
+                partial_rows<DIM, Real>(sm.tr[warp], valid && fb + lane < cap, xi, v, (int)fin, lane, acc);
+                store_partial<DIM, Real>(a, c, acc, lane);
             }
-            PartialAcc<Real> acc;
-            partial_rows<DIM, Real>(sm.tr[warp], valid && fb + lane < cap, xi, v, (int)fin, lane, acc);
-            store_partial<DIM, Real>(a, c, acc, lane);
+            __syncwarp();
+            if (lane == 0) a.head[c] = LOST;  // arrival list consumed
         }
         __syncthreads();
     }
@@ -615,26 +664,14 @@ __global__ void __launch_bounds__(CELL_WARPS * 32) k_partials(StepArgs a, const 
 template <int DIM, typename Real>
 __global__ void k_correct(StepArgs a)
 {
-    constexpr int NV = 1 << DIM, VS = Dims<DIM>::VS;
     const uint32_t n = (uint32_t)a.stats->n_particles;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t c = a.S0.cell[i];
         if (c >= (uint32_t)a.mesh.nC) continue;
-        Real xi[DIM], N[NV], corr[DIM];
+        Real xi[DIM], corr[DIM];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            xi[d] = ldr<Real>(a.S0.xi[d], i);
-            corr[d] = Real(0);
-        }
-        if constexpr (std::is_same<Real, double>::value) shape64<DIM>(xi, N);
-        else shape32<DIM>(xi, N);
-#pragma unroll
-        for (int iv = 0; iv < NV; ++iv) {
-            const int32_t dof = __ldg(a.mesh.cd + (size_t)c * NV + iv);
-#pragma unroll
-            for (int d = 0; d < DIM; ++d)
-                corr[d] = corr[d] + N[iv] * __ldg(reinterpret_cast<const Real*>(a.dVaos) + (size_t)dof * VS + d);
-        }
+        for (int d = 0; d < DIM; ++d) xi[d] = ldr<Real>(a.S0.xi[d], i);
+        interp_v<DIM, Real>(a.dVc, c, xi, corr);
 #pragma unroll
         for (int d = 0; d < DIM; ++d) str<Real>(a.S0.v[d], i, ldr<Real>(a.S0.v[d], i) + corr[d]);
     }

@@ -68,6 +68,7 @@ struct PartParams {
     double dtp;    // dt / S
     double h[3];   // 1.0 / q
     uint32_t seed; // removal key seed
+    unsigned long long realmask;  // real parts among the first 64 extended parts
 };
 
 // SoA particle arrays; x is null in the FP32 form.
@@ -85,15 +86,15 @@ struct StepArgs {
     PartState S0;   // current, sorted
     PartState S1;   // next, sorted
     PartState T;    // advect output, in S0 order (cell/id unused)
-    const void* Vaos;   // nD x VS velocity, VS = 4 (3D) or 2 (2D)
-    const void* dVaos;  // nD x VS velocity increment V - Vold
+    const void* Vc;     // nC x NV x VS nodal velocity per cell vertex, VS = 4 (3D) or 2 (2D)
+    const void* dVc;    // nC x NV x VS velocity increment V - Vold per cell vertex
     int do_correct;
     int apply_counts;   // write kernel: 1 = count correction, 0 = keep all (re-sort only)
-    uint32_t* key;      // advect output cell, or LOST
-    uint32_t* slot;     // rank of arrival in the cell counter
-    uint32_t* idx;      // bucketed particle indices, cell-major
-    uint32_t* cell_count;
-    uint32_t* cell_off;            // nC + 1
+    uint32_t* key;      // cell after the move, or LOST
+    uint32_t* head;     // nC: first particle that moved into the cell (LOST = none)
+    uint32_t* next;     // next particle that moved into the same cell
+    const uint32_t* cs_old;  // nC + 1: cell ranges of S0
+    uint32_t* cs_new;        // nC + 1: cell ranges of S1
     uint2* xq;                     // particles (index, sub-step) queued for FP64 relocation
     uint32_t* nxq;                 // queue length
     unsigned long long* tile_status; // decoupled look-back words of the write pass
@@ -131,13 +132,19 @@ __host__ __device__ inline uint32_t key_of(uint32_t id, uint32_t seed)
 // Extended cell-part index of reference coordinates: (int)(xi_d / h_d) per
 // direction (src/pfem2particlehandler.cpp:369-370), which reaches q_d on the
 // upper face; digits combined x-major, base q_d + 1.
+// xi_d * q_d and xi_d / h_d round to within 3 ulp of each other, so their
+// truncations can only differ within 1e-12 (xi_d * q_d <= 64) of an integer;
+// only there is the division evaluated.
 template <int DIM, typename Real>
 __device__ __forceinline__ int ext_part(const Real* xi, const PartParams& pp)
 {
     int e = 0;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
-        int k = (int)((double)xi[d] / pp.h[d]);
+        const double x = (double)xi[d];
+        const double t = x * (double)pp.q[d];
+        const double f = t - floor(t);
+        int k = (f > 1e-12 && f < 1.0 - 1e-12) ? (int)t : (int)(x / pp.h[d]);
         k = k < 0 ? 0 : (k > pp.q[d] ? pp.q[d] : k);
         e = e * (pp.q[d] + 1) + k;
     }

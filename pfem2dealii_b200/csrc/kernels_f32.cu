@@ -9,7 +9,7 @@ namespace pfem2 {
 
 int launch64_seed(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s);
 int launch64_advect(int dim, const StepArgs& a, cudaStream_t s);
-int launch64_write(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s);
+int launch64_write(int dim, const StepArgs& a, cudaStream_t s);
 int launch64_partials(int dim, const StepArgs& a, const uint32_t* cs, cudaStream_t s);
 int launch64_correct(int dim, const StepArgs& a, cudaStream_t s);
 int launch64_gather(int dim, const StepArgs& a, int keep, cudaStream_t s);
@@ -39,7 +39,7 @@ int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s)
 }
 
 template <int DIM>
-static int write32_t(const StepArgs& a, uint32_t* cs, cudaStream_t s)
+static int write32_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = (int)sizeof(WriteSmem<float>);
     static bool init = false;
@@ -48,14 +48,14 @@ static int write32_t(const StepArgs& a, uint32_t* cs, cudaStream_t s)
         init = true;
     }
     const int grid = occupancy_grid((const void*)k_write<DIM, float>, WR_WARPS * 32, smem);
-    k_write<DIM, float><<<grid, WR_WARPS * 32, smem, s>>>(a, cs);
+    k_write<DIM, float><<<grid, WR_WARPS * 32, smem, s>>>(a);
     return 1;
 }
 
-int launch_write(int dim, int prec, const StepArgs& a, uint32_t* cs, cudaStream_t s)
+int launch_write(int dim, int prec, const StepArgs& a, cudaStream_t s)
 {
-    if (prec == 0) return launch64_write(dim, a, cs, s);
-    return dim == 2 ? write32_t<2>(a, cs, s) : write32_t<3>(a, cs, s);
+    if (prec == 0) return launch64_write(dim, a, s);
+    return dim == 2 ? write32_t<2>(a, s) : write32_t<3>(a, s);
 }
 
 int launch_partials(int dim, int prec, const StepArgs& a, const uint32_t* cs, cudaStream_t s)

@@ -117,7 +117,7 @@ int launch64_advect(int dim, const StepArgs& a, cudaStream_t s)
 }
 
 template <int DIM>
-static int write_t(const StepArgs& a, uint32_t* cs, cudaStream_t s)
+static int write_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = (int)sizeof(WriteSmem<double>);
     static bool init = false;
@@ -126,13 +126,13 @@ static int write_t(const StepArgs& a, uint32_t* cs, cudaStream_t s)
         init = true;
     }
     const int grid = occupancy_grid((const void*)k_write<DIM, double>, WR_WARPS * 32, smem);
-    k_write<DIM, double><<<grid, WR_WARPS * 32, smem, s>>>(a, cs);
+    k_write<DIM, double><<<grid, WR_WARPS * 32, smem, s>>>(a);
     return 1;
 }
 
-int launch64_write(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s)
+int launch64_write(int dim, const StepArgs& a, cudaStream_t s)
 {
-    return dim == 2 ? write_t<2>(a, cs, s) : write_t<3>(a, cs, s);
+    return dim == 2 ? write_t<2>(a, s) : write_t<3>(a, s);
 }
 
 int launch64_partials(int dim, const StepArgs& a, const uint32_t* cs, cudaStream_t s)

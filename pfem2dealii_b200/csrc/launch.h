@@ -34,23 +34,18 @@ int launch_cell_setup(int dim, int nC, const double* verts, const int32_t* cv, d
                       float* geo32, float* jinv32, cudaStream_t s);
 int launch_seed(int dim, int prec, const StepArgs& a, uint32_t* cell_start, cudaStream_t s);
 int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s);
-int launch_write(int dim, int prec, const StepArgs& a, uint32_t* cell_start, cudaStream_t s);
+int launch_write(int dim, int prec, const StepArgs& a, cudaStream_t s);
 int launch_partials(int dim, int prec, const StepArgs& a, const uint32_t* cell_start, cudaStream_t s);
 int launch_correct(int dim, int prec, const StepArgs& a, cudaStream_t s);
 int launch_gather(int dim, int prec, const StepArgs& a, int keep_empty, cudaStream_t s);
 int launch_positions32(int dim, const StepArgs& a, double* xout, cudaStream_t s);
 
 // misc.cu
-constexpr int SCAN_TILE = 2048;        // elements per block
-constexpr int SCAN_MAX_TILES = 8192;   // top-level scan capacity
-int launch_scan_u32(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* tile_tmp, cudaStream_t s);
-int launch_scan_u64(const unsigned long long* in, uint32_t n, unsigned long long* out, unsigned long long* tile_tmp,
-                    cudaStream_t s);
-int launch_bucket(const StepArgs& a, cudaStream_t s);
 int launch_rekey(const StepArgs& a, cudaStream_t s);
-int launch_finalize(const StepArgs& a, uint32_t* cell_start, int count_step, cudaStream_t s);
+int launch_fill_u32(uint32_t* p, uint32_t n, uint32_t v, cudaStream_t s);
+int launch_finalize(const StepArgs& a, int count_step, cudaStream_t s);
 int launch_set_state(DevStats* st, long long n, long long next_id, long long add_id, cudaStream_t s);
-int launch_prep_v(int dim, int prec, const double* V, const double* Vold, int nD, void* Vaos, void* dVaos,
-                  cudaStream_t s);
+int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const int32_t* cd, int nC, int nD, void* Vc,
+                  void* dVc, cudaStream_t s);
 
 }  // namespace pfem2
