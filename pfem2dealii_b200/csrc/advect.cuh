@@ -374,37 +374,61 @@ __global__ void __launch_bounds__(128) k_search64(StepArgs a)
 }
 
 // ---------------------------------------------------------------------------
-// FP32 form.  A sub-step converts u dt_p into a reference-coordinate
-// increment with the cell's FP32 inverse Jacobian (exact for affine cells;
-// Newton on the multilinear map otherwise) and stays in FP32 while the
-// particle stays in its cell.  Particles that leave their cell are queued
-// for k_cross32, which rebuilds the position in FP64 and relocates it there.
+// FP32 form.  The per-step cell record holds the cell's trilinear velocity
+// field as monomial coefficients b_k (bit d of k selects xi_d):
+//   affine cells:     the reference-space velocity w = J^-1 u, so a sub-step
+//                     is  xi += dt_p w(xi)  (7 FMAs per component);
+//   non-affine cells: u itself; the increment solves x(xi + d) - x(xi) = u dt_p
+//                     by Newton (out of line).
+// A particle that leaves its cell is queued for k_cross32, which rebuilds its
+// position in FP64 and relocates it there.
 // ---------------------------------------------------------------------------
 
 template <int DIM>
-struct J32 {
-    float Ji[DIM][DIM];
+struct Rec32 {
+    float b[1 << DIM][DIM];
     bool affine;
 };
 
 template <int DIM>
-__device__ __forceinline__ void load_jinv32(const float* __restrict__ jinv, uint32_t c, J32<DIM>& j)
+__device__ __forceinline__ void load_rec32(const float* __restrict__ rec, uint32_t c, Rec32<DIM>& r)
 {
-    const float4* p = reinterpret_cast<const float4*>(jinv + (size_t)c * Dims<DIM>::JS);
-    float b[Dims<DIM>::JS];
+    constexpr int F4 = Dims<DIM>::REC4;
+    const float4* p = reinterpret_cast<const float4*>(rec) + (size_t)c * F4;
+    float buf[F4 * 4];
 #pragma unroll
-    for (int k = 0; k < Dims<DIM>::JS / 4; ++k) {
+    for (int k = 0; k < F4; ++k) {
         const float4 t = __ldg(p + k);
-        b[4 * k] = t.x;
-        b[4 * k + 1] = t.y;
-        b[4 * k + 2] = t.z;
-        b[4 * k + 3] = t.w;
+        buf[4 * k] = t.x;
+        buf[4 * k + 1] = t.y;
+        buf[4 * k + 2] = t.z;
+        buf[4 * k + 3] = t.w;
     }
 #pragma unroll
-    for (int r = 0; r < DIM; ++r)
+    for (int k = 0; k < (1 << DIM); ++k)
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) j.Ji[r][q] = b[r * DIM + q];
-    j.affine = b[DIM * DIM] != 0.0f;
+        for (int d = 0; d < DIM; ++d) r.b[k][d] = buf[k * DIM + d];
+    r.affine = buf[(1 << DIM) * DIM] != 0.0f;
+}
+
+// f(xi) = sum_k b_k prod_{d in k} xi_d, nested: 3 (2D) / 7 (3D) FMAs per component.
+template <int DIM>
+__device__ __forceinline__ void eval_poly(const float (*b)[DIM], const float* xi, float* f)
+{
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        if constexpr (DIM == 2) {
+            const float t0 = fmaf(b[1][d], xi[0], b[0][d]);
+            const float t1 = fmaf(b[3][d], xi[0], b[2][d]);
+            f[d] = fmaf(t1, xi[1], t0);
+        } else {
+            const float t0 = fmaf(b[1][d], xi[0], b[0][d]);
+            const float t1 = fmaf(b[3][d], xi[0], b[2][d]);
+            const float t2 = fmaf(b[5][d], xi[0], b[4][d]);
+            const float t3 = fmaf(b[7][d], xi[0], b[6][d]);
+            f[d] = fmaf(fmaf(t3, xi[1], t2), xi[2], fmaf(t1, xi[1], t0));
+        }
+    }
 }
 
 template <int DIM>
@@ -424,61 +448,33 @@ __device__ __noinline__ F3<DIM> newton32(const float* __restrict__ geo, uint32_t
     return out;
 }
 
-template <int DIM>
-__device__ __forceinline__ void velocity32(const float* __restrict__ Vc, uint32_t c, const float* xi, float* u)
-{
-    constexpr int NV = 1 << DIM;
-    float N[NV];
-    shape32<DIM>(xi, N);
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) u[d] = 0.0f;
-#pragma unroll
-    for (int iv = 0; iv < NV; ++iv) {
-        if constexpr (DIM == 3) {
-            const float4 t = __ldg(reinterpret_cast<const float4*>(Vc) + (size_t)c * NV + iv);
-            u[0] += N[iv] * t.x;
-            u[1] += N[iv] * t.y;
-            u[2] += N[iv] * t.z;
-        } else {
-            const float2 t = __ldg(reinterpret_cast<const float2*>(Vc) + (size_t)c * NV + iv);
-            u[0] += N[iv] * t.x;
-            u[1] += N[iv] * t.y;
-        }
-    }
-}
-
 // FP32 sub-steps s0.. in cell c; returns the sub-step that leaves the cell
 // (S if none).  xi is advanced in place.
 template <int DIM>
 __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi)
 {
-    J32<DIM> j;
-    load_jinv32<DIM>(a.mesh.jinv32, c, j);
+    Rec32<DIM> r;
+    load_rec32<DIM>(a.vrec32, c, r);
     const float dtp = (float)a.pp.dtp;
     int s = s0;
     for (; s < a.pp.S; ++s) {
-        float u[DIM], dl[DIM], y[DIM];
-        velocity32<DIM>((const float*)a.Vc, c, xi, u);
-        F3<DIM> dx;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) dx.v[d] = u[d] * dtp;
+        float w[DIM], dl[DIM], y[DIM];
+        eval_poly<DIM>(r.b, xi, w);
         bool ok = true;
-        if (j.affine) {
+        if (r.affine) {
 #pragma unroll
-            for (int r = 0; r < DIM; ++r) {
-                float t = 0.0f;
-#pragma unroll
-                for (int q = 0; q < DIM; ++q) t += j.Ji[r][q] * dx.v[q];
-                dl[r] = t;
-            }
+            for (int d = 0; d < DIM; ++d) dl[d] = dtp * w[d];
         } else {
-            F3<DIM> x0;
+            F3<DIM> x0, dx;
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) x0.v[d] = xi[d];
-            const F3<DIM> r = newton32<DIM>(a.mesh.geo32, c, x0, dx);
-            ok = r.ok;
+            for (int d = 0; d < DIM; ++d) {
+                x0.v[d] = xi[d];
+                dx.v[d] = w[d] * dtp;
+            }
+            const F3<DIM> res = newton32<DIM>(a.mesh.geo32, c, x0, dx);
+            ok = res.ok;
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) dl[d] = r.v[d];
+            for (int d = 0; d < DIM; ++d) dl[d] = res.v[d];
         }
 #pragma unroll
         for (int d = 0; d < DIM; ++d) y[d] = xi[d] + dl[d];
@@ -490,9 +486,8 @@ __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0,
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(256) k_advect32(StepArgs a)
+__global__ void __launch_bounds__(256, 3) k_advect32(StepArgs a)
 {
-    constexpr int NV = 1 << DIM;
     const MeshDev& m = a.mesh;
     const uint32_t n = (uint32_t)a.stats->n_particles;
     AdvCounters k;
@@ -513,9 +508,11 @@ __global__ void __launch_bounds__(256) k_advect32(StepArgs a)
             const bool alive = c < (uint32_t)m.nC;
             if (!alive) k.err |= ERR_BAD_CELL;
             if (alive) {
-                if (a.do_correct) {
+                if (a.do_correct) {  // v += sum N_i (V - Vold)_i, src/pfem2particlehandler.cpp:126-138
+                    Rec32<DIM> dr;
+                    load_rec32<DIM>(a.dvrec32, c, dr);
                     float dv[DIM];
-                    velocity32<DIM>((const float*)a.dVc, c, xi, dv);
+                    eval_poly<DIM>(dr.b, xi, dv);
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) v[d] += dv[d];
                 }
@@ -544,7 +541,6 @@ __global__ void __launch_bounds__(256) k_advect32(StepArgs a)
 template <int DIM>
 __global__ void __launch_bounds__(128) k_cross32(StepArgs a)
 {
-    constexpr int NV = 1 << DIM;
     const uint32_t nq = *a.nxq < a.capacity ? *a.nxq : a.capacity;
     const MeshDev& m = a.mesh;
     AdvCounters k;
@@ -559,14 +555,10 @@ __global__ void __launch_bounds__(128) k_cross32(StepArgs a)
         for (int d = 0; d < DIM; ++d) xi[d] = ((const float*)a.T.xi[d])[i];
         bool alive = true;
         while (true) {
-            float u[DIM];
-            velocity32<DIM>((const float*)a.Vc, c, xi, u);
             Vec<DIM> xo, ue;
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                xo.v[d] = (double)xi[d];
-                ue.v[d] = (double)u[d];
-            }
+            for (int d = 0; d < DIM; ++d) xo.v[d] = (double)xi[d];
+            velocity_from_dofs<DIM>(m.cd, a.Vd, m.nD, c, xo.v, ue.v);
             k.fallback++;
             const uint32_t c0 = c;
             const SearchOut so = fallback64<DIM>(m, c, xo, ue, a.pp.dtp);

@@ -41,10 +41,10 @@ struct pfem2gpu_handle {
     uint32_t *head = nullptr, *cs0 = nullptr, *cs1 = nullptr;  // cs0: cell ranges of S0
     uint2* xq = nullptr;
     uint32_t* nxq = nullptr;
-    unsigned long long *tile_status = nullptr, *totals = nullptr;
-    uint32_t* tile_counter = nullptr;
-    uint32_t ntiles = 0;
-    float* jinv32 = nullptr;
+    unsigned long long *blk_status = nullptr, *totals = nullptr, *cseedm = nullptr;
+    uint32_t *cfin = nullptr, *cseed = nullptr, *cseedoff = nullptr, *comap = nullptr;
+    float *jinv32 = nullptr, *vrec32 = nullptr, *dvrec32 = nullptr;
+    bool launch_failed = false;
     void* partials = nullptr;
     DevStats* stats = nullptr;
     DevStats* stats_h = nullptr;
@@ -109,15 +109,18 @@ cudaEvent_t take_event(pfem2gpu_handle* h)
 template <typename F>
 void run(pfem2gpu_handle* h, const char* name, F&& f)
 {
+    int n = 0;
     if (h->profiling) {
         cudaEvent_t a = take_event(h), b = take_event(h);
         cudaEventRecord(a, h->stream);
-        h->launches += f();
+        n = f();
         cudaEventRecord(b, h->stream);
         h->open_ev.push_back({name, a, b});
     } else {
-        h->launches += f();
+        n = f();
     }
+    if (n < 0) h->launch_failed = true;
+    else h->launches += n;
 }
 
 void collect_profile(pfem2gpu_handle* h)
@@ -159,6 +162,9 @@ StepArgs args(pfem2gpu_handle* h)
     a.T = h->T;
     a.Vc = h->Vc;
     a.dVc = h->dVc;
+    a.vrec32 = h->vrec32;
+    a.dvrec32 = h->dvrec32;
+    a.Vd = h->Vstage;
     a.do_correct = 0;
     a.apply_counts = 1;
     a.key = h->key;
@@ -168,10 +174,13 @@ StepArgs args(pfem2gpu_handle* h)
     a.cs_new = h->cs1;
     a.xq = h->xq;
     a.nxq = h->nxq;
-    a.tile_status = h->tile_status;
-    a.tile_counter = h->tile_counter;
-    a.ntiles = h->ntiles;
+    a.blk_status = h->blk_status;
     a.totals = h->totals;
+    a.cfin = h->cfin;
+    a.cseed = h->cseed;
+    a.cseedm = h->cseedm;
+    a.cseedoff = h->cseedoff;
+    a.comap = h->comap;
     a.partials = h->partials;
     a.Vout = h->Vout;
     a.Vkeep = h->Vstage;
@@ -269,15 +278,26 @@ int stage_v(pfem2gpu_handle* h, const double* V, const double* Vold, bool device
     } else if (V != h->Vstage) {
         CK(cudaMemcpyAsync(h->Vstage, V, bytes, cudaMemcpyDeviceToDevice, h->stream));
     }
-    run(h, "stage_velocity", [&] {
-        return launch_cell_v(h->dim, h->prec, v, vo, h->cd, h->nC, h->nD, h->Vc, Vold ? h->dVc : nullptr, h->stream);
-    });
+    if (h->prec == PFEM2GPU_FP64) {
+        run(h, "stage_velocity", [&] {
+            return launch_cell_v(h->dim, h->prec, v, vo, h->cd, h->nC, h->nD, h->Vc, Vold ? h->dVc : nullptr, h->stream);
+        });
+    } else {
+        run(h, "stage_velocity", [&] {
+            return launch_cell_rec32(h->dim, v, vo, h->cd, h->aff, h->jinv32, h->nC, h->nD, h->vrec32,
+                                     Vold ? h->dvrec32 : nullptr, h->stream);
+        });
+    }
     h->vaos_valid = true;
     return PFEM2GPU_OK;
 }
 
 int check_async(pfem2gpu_handle* h)
 {
+    if (h->launch_failed) {
+        h->launch_failed = false;
+        return fail(h, PFEM2GPU_ERR_CUDA, "kernel launch failed");
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(h, PFEM2GPU_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
     return PFEM2GPU_OK;
@@ -298,8 +318,7 @@ int apply_pending_correction(pfem2gpu_handle* h)
 // set_particles.
 int write_and_swap(pfem2gpu_handle* h, StepArgs& a, int count_step)
 {
-    CK(cudaMemsetAsync(h->tile_status, 0, h->ntiles * sizeof(unsigned long long), h->stream));
-    CK(cudaMemsetAsync(h->tile_counter, 0, sizeof(uint32_t), h->stream));
+    CK(cudaMemsetAsync(h->blk_status, 0, (size_t)write_grid(h->dim, h->prec) * sizeof(unsigned long long), h->stream));
     run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->stream); });
     run(h, "finalize", [&] { return launch_finalize(a, count_step, h->stream); });
     std::swap(h->S0, h->S1);
@@ -431,9 +450,9 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
                     (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
                     (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vc, h->dVc,
                     (void*)h->key, (void*)h->next, (void*)h->xtmp, (void*)h->head, (void*)h->cs0, (void*)h->cs1,
-                    (void*)h->tile_status,
-                    (void*)h->tile_counter, (void*)h->totals, (void*)h->jinv32, (void*)h->xq, (void*)h->nxq,
-                    h->partials, (void*)h->stats})
+                    (void*)h->blk_status, (void*)h->totals, (void*)h->jinv32, (void*)h->xq, (void*)h->nxq,
+                    (void*)h->cfin, (void*)h->cseed, (void*)h->cseedm, (void*)h->cseedoff, (void*)h->comap,
+                    (void*)h->vrec32, (void*)h->dvrec32, h->partials, (void*)h->stats})
         dfree(p);
     free_state(h->S0);
     free_state(h->S1);
@@ -525,8 +544,9 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     for (void* p : {(void*)h->cv, (void*)h->cd, (void*)h->v2c_off, (void*)h->v2c_cells, (void*)h->d2c_off,
                     (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
                     (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vc, h->dVc,
-                    (void*)h->head, (void*)h->cs0, (void*)h->cs1, (void*)h->tile_status, (void*)h->tile_counter,
-                    (void*)h->totals, (void*)h->jinv32, h->partials})
+                    (void*)h->head, (void*)h->cs0, (void*)h->cs1, (void*)h->blk_status, (void*)h->totals,
+                    (void*)h->jinv32, (void*)h->cfin, (void*)h->cseed, (void*)h->cseedm, (void*)h->cseedoff,
+                    (void*)h->comap, (void*)h->vrec32, (void*)h->dvrec32, h->partials})
         dfree(p);
     h->has_mesh = false;
     h->nC = (int)n_cells;
@@ -548,15 +568,26 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(dalloc(&h->Vstage, nd * dim));
     CK(dalloc(&h->Vstage2, nd * dim));
     CK(dalloc(&h->Vout, nd * dim));
-    CK(cudaMalloc(&h->Vc, nc * NV * VS * esize(h)));
-    CK(cudaMalloc(&h->dVc, nc * NV * VS * esize(h)));
+    const size_t vcn = h->prec == PFEM2GPU_FP64 ? nc * NV * VS : 1;
+    CK(cudaMalloc(&h->Vc, vcn * esize(h)));
+    CK(cudaMalloc(&h->dVc, vcn * esize(h)));
     CK(dalloc(&h->head, nc));
     CK(dalloc(&h->cs0, nc + 1));
     CK(dalloc(&h->cs1, nc + 1));
-    h->ntiles = (uint32_t)((nc + WR_TILE - 1) / WR_TILE);
-    CK(dalloc(&h->tile_status, h->ntiles));
-    CK(dalloc(&h->tile_counter, 1));
+    CK(dalloc(&h->blk_status, 4096));
     CK(dalloc(&h->totals, 1));
+    CK(dalloc(&h->cfin, nc));
+    CK(dalloc(&h->cseed, nc));
+    CK(dalloc(&h->cseedm, nc));
+    CK(dalloc(&h->cseedoff, nc));
+    CK(dalloc(&h->comap, nc * 32));
+    if (h->prec == PFEM2GPU_FP32) {
+        const size_t rec = (size_t)(dim == 3 ? 7 : 3) * 4;
+        CK(dalloc(&h->vrec32, nc * rec));
+        CK(dalloc(&h->dvrec32, nc * rec));
+        CK(cudaMemsetAsync(h->vrec32, 0, nc * rec * 4, h->stream));
+        CK(cudaMemsetAsync(h->dvrec32, 0, nc * rec * 4, h->stream));
+    }
     CK(dalloc(&h->jinv32, nc * (dim == 3 ? 12 : 8)));
     CK(cudaMalloc(&h->partials, nc * PW * esize(h)));
     CK(cudaMemcpyAsync(h->cv, cell_vertices, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
@@ -567,8 +598,8 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(cudaMemcpyAsync(h->v2c_dirs, dirs.data(), dirs.size() * 8, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d2c_off, doff.data(), doff.size() * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d2c_ent, dent.data(), dent.size() * 4, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemsetAsync(h->Vc, 0, nc * NV * VS * esize(h), h->stream));
-    CK(cudaMemsetAsync(h->dVc, 0, nc * NV * VS * esize(h), h->stream));
+    CK(cudaMemsetAsync(h->Vc, 0, vcn * esize(h), h->stream));
+    CK(cudaMemsetAsync(h->dVc, 0, vcn * esize(h), h->stream));
     run(h, "fill", [&] { return launch_fill_u32(h->head, (uint32_t)nc, LOST, h->stream); });
     CK(cudaMemsetAsync(h->Vstage, 0, nd * dim * 8, h->stream));
     run(h, "cell_setup",

@@ -10,11 +10,10 @@
 // the reference hands them out.  Output is sorted by (cell, part, key), so
 // the layout and every floating-point sum over it are deterministic.
 //
-// The write pass is a single pass with decoupled look-back: a block takes a
-// tile of 32 cells, a warp decides its cells (survivors, new particles, final
-// count), the tile's totals are published and the exclusive prefix of the
-// earlier tiles is collected, then the warps write their cells at their
-// final offsets and sum the projection partials.
+// The write pass is one cooperative launch: each block owns a contiguous
+// range of cells, decides them (survivors, new particles, final count), adds
+// the published totals of the earlier blocks to place its range, then writes
+// its cells at their final offsets and sums the projection partials.
 #pragma once
 
 #include <type_traits>
@@ -57,18 +56,21 @@ __device__ __forceinline__ void interp_v(const void* Vc, uint32_t c, const Real*
 
 // A new particle at the centre of part idx of cell c (seed_particles
 // :87-104 and check_particle_distribution :390-407): xi = (idx + 1/2) h,
-// x = F(xi) (FP64 form), v = interpolated V.  Returns xi and v.
+// x = F(xi) (FP64 form), v = V interpolated at xi in FP64 (rounded to the
+// form's precision).  Returns xi and v.
 template <int DIM, typename Real>
 __device__ __forceinline__ void new_particle(const StepArgs& a, const PartState& S, uint32_t dst, uint32_t c,
                                              const int* idx, uint32_t id, Real* xi, Real* v)
 {
-    double xid[DIM];
+    double xid[DIM], vd[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
         xid[d] = (idx[d] + 0.5) * a.pp.h[d];
         xi[d] = (Real)xid[d];
     }
-    interp_v<DIM, Real>(a.Vc, c, xi, v);
+    velocity_from_dofs<DIM>(a.mesh.cd, a.Vd, a.mesh.nD, c, xid, vd);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = (Real)vd[d];
     if constexpr (std::is_same<Real, double>::value) {
         double X[1 << DIM][DIM], x[DIM];
         load_cell64<DIM>(a.mesh.cellX, c, X);
@@ -233,18 +235,13 @@ __device__ __forceinline__ void partials_of_range(const StepArgs& a, const PartS
 
 template <typename Real>
 struct WriteSmem {
-    uint32_t outmap[WR_WARPS][WR_CPW][32];   // fast path: source index, or 0x80000000|part for a new particle
-    unsigned long long seedmask[WR_TILE];
-    uint32_t fin[WR_TILE];                   // final particles per cell
-    uint32_t nseed[WR_TILE];
-    uint32_t excl_fin[WR_TILE];              // exclusive prefix inside the tile
-    uint32_t excl_seed[WR_TILE];
-    uint32_t slow;                           // tile cells on the general path (bit per cell)
-    uint32_t tile;
-    unsigned long long prefix;               // seeds << 32 | particles before this tile
-    int cnt[WR_WARPS][NPE_MAX];
-    uint2 kc[WR_WARPS][KEY_CACHE];
+    int cnt[WR_WARPS][NPE_MAX];              // per-part counts (fast path: first 64)
+    uint2 kc[WR_WARPS][KEY_CACHE];           // general path: (part, key) cache
+    int fpfx[WR_WARPS][64];                  // fast path: first output slot of each part
     Real tr[WR_WARPS][32][33];               // partial rows; general path: part prefixes first
+    uint32_t blk_f, blk_s;                   // block totals (particles, new particles)
+    unsigned long long pre;                  // seeds << 32 | particles before this block
+    uint32_t ws_f[WR_WARPS], ws_s[WR_WARPS]; // block scan workspace
 };
 
 __device__ __forceinline__ void store_release_u64(unsigned long long* p, unsigned long long v)
@@ -259,54 +256,42 @@ __device__ __forceinline__ unsigned long long load_acquire_u64(const unsigned lo
     return v;
 }
 
-constexpr unsigned long long LB_AGG = 1ull << 62, LB_INC = 2ull << 62;
-constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;
+constexpr unsigned long long BLK_READY = 1ull << 62;
+constexpr uint32_t BLK_SPIN_LIMIT = 1u << 22;
 
-__device__ __forceinline__ unsigned long long lb_pack(uint32_t f, uint32_t s)
+__device__ __forceinline__ unsigned long long blk_pack(uint32_t f, uint32_t s)
 {
-    return ((unsigned long long)(f & 0x7fffffffu) << 31) | (unsigned long long)(s & 0x7fffffffu);
+    return BLK_READY | ((unsigned long long)(f & 0x7fffffffu) << 31) | (unsigned long long)(s & 0x7fffffffu);
 }
 
-// Decoupled look-back (warp 0 of the block): publish this tile's aggregate,
-// add up the aggregates of earlier tiles until an inclusive prefix is found,
-// publish the inclusive prefix.  Every wait is bounded; on time-out the error
-// flag is raised and the partial sum is used (the output is then garbage but
-// every write stays in bounds).  Returns seeds << 32 | particles before.
-static __device__ __noinline__ unsigned long long lookback(const StepArgs& a, uint32_t tile, uint32_t agg_f, uint32_t agg_s, int lane)
+// Warp 0: publish this block's totals, then add up the totals of all earlier
+// blocks (all blocks are co-resident: cooperative launch).  Every wait is
+// bounded; on time-out the error flag is raised and the partial sum is used
+// (the output is then wrong but every write stays in bounds).  Returns
+// seeds << 32 | particles before this block.
+static __device__ __noinline__ unsigned long long block_prefix(const StepArgs& a, uint32_t b, uint32_t f, uint32_t s,
+                                                               int lane)
 {
-    unsigned long long* st = a.tile_status;
-    if (tile == 0) {
-        if (lane == 0) store_release_u64(st, LB_INC | lb_pack(agg_f, agg_s));
-        return 0ull;
-    }
-    if (lane == 0) store_release_u64(st + tile, LB_AGG | lb_pack(agg_f, agg_s));
+    if (lane == 0) store_release_u64(a.blk_status + b, blk_pack(f, s));
     uint32_t ef = 0, es = 0;
-    long long pred = (long long)tile - 1;
     uint32_t spins = 0;
     bool timed_out = false;
-    while (true) {
-        const long long t = pred - lane;
-        unsigned long long w = t >= 0 ? load_acquire_u64(st + t) : LB_INC;
-        while (__any_sync(0xffffffffu, (w >> 62) == 0ull)) {
-            if (++spins > LB_SPIN_LIMIT) {
+    for (uint32_t base = 0; base < b && !timed_out; base += 32) {
+        const uint32_t t = base + lane;
+        unsigned long long w = t < b ? load_acquire_u64(a.blk_status + t) : BLK_READY;
+        while (__any_sync(0xffffffffu, !(w & BLK_READY))) {
+            if (++spins > BLK_SPIN_LIMIT) {
                 timed_out = true;
                 break;
             }
-            __nanosleep(32);
-            if ((w >> 62) == 0ull) w = load_acquire_u64(st + t);
+            __nanosleep(64);
+            if (!(w & BLK_READY)) w = load_acquire_u64(a.blk_status + t);
         }
-        if (timed_out) break;
-        const unsigned pm = __ballot_sync(0xffffffffu, (w >> 62) == 2ull);
-        const int stop = pm ? __ffs(pm) - 1 : 31;
-        const uint32_t vf = lane <= stop ? (uint32_t)((w >> 31) & 0x7fffffffu) : 0u;
-        const uint32_t vs = lane <= stop ? (uint32_t)(w & 0x7fffffffu) : 0u;
-        ef += __reduce_add_sync(0xffffffffu, vf);
-        es += __reduce_add_sync(0xffffffffu, vs);
-        if (pm) break;
-        pred -= 32;
+        const bool use = t < b && (w & BLK_READY);
+        ef += __reduce_add_sync(0xffffffffu, use ? (uint32_t)((w >> 31) & 0x7fffffffu) : 0u);
+        es += __reduce_add_sync(0xffffffffu, use ? (uint32_t)(w & 0x7fffffffu) : 0u);
     }
     if (timed_out && lane == 0) atomicOr(&a.stats->error_flags, ERR_LOOKBACK);
-    if (lane == 0) store_release_u64(st + tile, LB_INC | lb_pack(ef + agg_f, es + agg_s));
     return ((unsigned long long)es << 32) | ef;
 }
 
@@ -465,121 +450,145 @@ __device__ void write_cell_general(const StepArgs& a, WriteSmem<Real>& sm, int w
     partials_of_range<DIM, Real>(a, a.S1, c, fb, (fb + fcount <= cap) ? fcount : 0, sm.tr[warp], lane);
 }
 
-// The write pass (one launch per step; see the file comment).
+// The write pass, one cooperative launch per step.  Block b owns the cell
+// range [b R, (b+1) R).  Phase 1 decides every cell of the range (survivors,
+// new particles, final count, output map) into global scratch; the block then
+// publishes its totals, adds those of the earlier blocks and scans its own
+// cells into final offsets; phase 2 writes each cell at its offset and sums
+// its projection partials in final order.
 template <int DIM, typename Real>
 __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WriteSmem<Real>& sm = *reinterpret_cast<WriteSmem<Real>*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool fast_ok = a.pp.npe <= 64;
+    const int npe = a.pp.npe;
+    const bool fast_ok = npe <= 64;
     const unsigned long long realmask = a.pp.realmask;
     const uint32_t id0 = a.stats->next_id;
     const uint32_t cap = a.capacity;
-    unsigned long long removed = 0;
-    uint32_t err = 0;
     const int apply = a.apply_counts;
     const int maxpp = a.pp.maxpp;
-    while (true) {
-        if (threadIdx.x == 0) {
-            sm.tile = atomicAdd(a.tile_counter, 1u);
-            sm.slow = 0;
-        }
-        __syncthreads();
-        const uint32_t tile = sm.tile;
-        if (tile >= a.ntiles) break;
-        // ---- phase 1: decide every cell of the tile ----
-        for (int j = 0; j < WR_CPW; ++j) {
-            const int slotc = warp * WR_CPW + j;
-            const uint32_t c = tile * WR_TILE + slotc;
-            uint32_t fin = 0, nsd = 0;
-            unsigned long long seedm = 0;
-            if (c < (uint32_t)a.mesh.nC) {
-                const uint32_t s0 = a.cs_old[c], L = a.cs_old[c + 1] - s0;
-                const uint32_t h = a.head[c];
-                bool fast = fast_ok && L <= 32;
-                uint32_t i = 0, n = 0;
-                if (fast) {
-                    // stayers of the old range, compacted to lanes 0..ns-1
-                    const bool stay = (uint32_t)lane < L && a.key[s0 + lane] == c;
-                    const unsigned stm = __ballot_sync(0xffffffffu, stay);
-                    const uint32_t ns = __popc(stm);
-                    const uint32_t src = __fns(stm, 0, lane + 1);
-                    i = s0 + (src & 31u);
-                    // arrivals into lanes ns..
-                    uint32_t na = 0, p = h;
-                    while (p != LOST && ns + na < 32) {
-                        if ((uint32_t)lane == ns + na) i = p;
-                        ++na;
-                        p = a.next[p];
-                    }
-                    fast = p == LOST;
-                    n = ns + na;
-                }
-                if (fast) {
-                    const bool valid = (uint32_t)lane < n;
-                    unsigned long long k64 = ~0ull;
-                    if (valid) {
-                        const uint2 pk = part_key<DIM, Real>(a, i);
-                        k64 = ((unsigned long long)pk.x << 37) | ((unsigned long long)pk.y << 5) | (unsigned)lane;
-                    }
-                    k64 = warp_sort(k64, lane);
-                    const bool vs = k64 != ~0ull;
-                    const uint32_t ep = vs ? (uint32_t)(k64 >> 37) : 0xffffu;
-                    const uint32_t is = __shfl_sync(0xffffffffu, i, (int)(k64 & 31u));
-                    const uint32_t prev = __shfl_up_sync(0xffffffffu, ep, 1);
-                    const bool start = vs && (lane == 0 || ep != prev);
-                    const unsigned smask = __ballot_sync(0xffffffffu, start);
-                    const unsigned le = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
-                    const int rank = lane - (31 - __clz(smask & le));
-                    const bool surv = vs && (!apply || (maxpp >= 0 && rank <= maxpp));
-                    const unsigned survm = __ballot_sync(0xffffffffu, surv);
-                    const unsigned long long occ_me = surv ? (1ull << ep) : 0ull;
-                    const unsigned long long occ =
-                        (unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)occ_me) |
-                        ((unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)(occ_me >> 32)) << 32);
-                    seedm = (apply && n > 0) ? (realmask & ~occ) : 0ull;
-                    nsd = __popcll(seedm);
-                    fin = __popc(survm) + nsd;
-                    if (fin <= 32) {
-                        uint32_t* om = sm.outmap[warp][j];
-                        if (surv) {
-                            const unsigned lt = (1u << lane) - 1u;
-                            const unsigned long long below = ep == 0 ? 0ull : (seedm & ((1ull << ep) - 1ull));
-                            om[__popc(survm & lt) + __popcll(below)] = is;
-                        }
-                        unsigned long long rest = seedm;
-                        int k = 0;
-                        while (rest) {
-                            const int p = __ffsll((long long)rest) - 1;
-                            rest &= rest - 1;
-                            const unsigned nb = __ballot_sync(0xffffffffu, surv && (int)ep < p);
-                            if (lane == 0) om[__popc(nb) + k] = 0x80000000u | (uint32_t)p;
-                            ++k;
-                        }
-                        if (lane == 0) removed += n - __popc(survm);
-                    } else {
-                        fast = false;
-                    }
-                }
-                if (!fast) {
-                    const uint2 fs = count_cell<DIM, Real>(a, sm.cnt[warp], sm.kc[warp], c, s0, L, h, lane);
-                    fin = fs.x;
-                    nsd = fs.y;
-                    if (lane == 0) atomicOr(&sm.slow, 1u << slotc);
-                }
+    const uint32_t nC = (uint32_t)a.mesh.nC;
+    const uint32_t R = (nC + gridDim.x - 1) / gridDim.x;
+    const uint32_t c0 = blockIdx.x * R < nC ? blockIdx.x * R : nC;
+    const uint32_t c1 = c0 + R < nC ? c0 + R : nC;
+    unsigned long long removed = 0;
+    uint32_t err = 0;
+    if (threadIdx.x == 0) {
+        sm.blk_f = 0;
+        sm.blk_s = 0;
+    }
+    __syncthreads();
+    // ---- phase 1 ----
+    for (uint32_t c = c0 + warp; c < c1; c += WR_WARPS) {
+        const uint32_t s0 = a.cs_old[c], L = a.cs_old[c + 1] - s0;
+        const uint32_t h = a.head[c];
+        bool fast = fast_ok && L <= 32;
+        uint32_t i = 0, n = 0, fin = 0, nsd = 0;
+        unsigned long long seedm = 0;
+        if (fast) {
+            // stayers of the old range compacted to lanes 0..ns-1, then arrivals
+            const bool stay = (uint32_t)lane < L && a.key[s0 + lane] == c;
+            const unsigned stm = __ballot_sync(0xffffffffu, stay);
+            const uint32_t ns = __popc(stm);
+            i = s0 + (__fns(stm, 0, lane + 1) & 31u);
+            uint32_t na = 0, p = h;
+            while (p != LOST && ns + na < 32) {
+                if ((uint32_t)lane == ns + na) i = p;
+                ++na;
+                p = a.next[p];
             }
-            if (lane == 0) {
-                sm.fin[slotc] = fin;
-                sm.nseed[slotc] = nsd;
-                sm.seedmask[slotc] = seedm;
+            fast = p == LOST;
+            n = ns + na;
+        }
+        if (fast) {
+            const bool valid = (uint32_t)lane < n;
+            const uint2 pk = valid ? part_key<DIM, Real>(a, i) : make_uint2(0u, 0u);
+            int* cnt = sm.cnt[warp];
+            int* fpfx = sm.fpfx[warp];
+            cnt[lane] = 0;
+            cnt[lane + 32] = 0;
+            __syncwarp();
+            if (valid) atomicAdd(cnt + pk.x, 1);
+            __syncwarp();
+            int run = 0;
+#pragma unroll
+            for (int ch = 0; ch < 2; ++ch) {
+                const int p = ch * 32 + lane;
+                const int k = p < npe ? cnt[p] : 0;
+                const int sv = survivors(k, maxpp, apply);
+                const bool sf = apply && n > 0 && p < npe && ((realmask >> p) & 1ull) && sv == 0;
+                const int fc = sv + (sf ? 1 : 0);
+                int inc = fc;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += t;
+                }
+                fpfx[p] = run + inc - fc;
+                run += __shfl_sync(0xffffffffu, inc, 31);
+                seedm |= (unsigned long long)__ballot_sync(0xffffffffu, sf) << (32 * ch);
+            }
+            fin = (uint32_t)run;
+            nsd = __popcll(seedm);
+            if (fin <= 32) {
+                __syncwarp();
+                const int kme = valid ? cnt[pk.x] : 0;
+                int rank = 0;
+                if (__any_sync(0xffffffffu, kme > 1)) {
+                    for (int l = 0; l < 32; ++l) {
+                        const uint32_t ol = __shfl_sync(0xffffffffu, pk.x, l);
+                        const uint32_t kl = __shfl_sync(0xffffffffu, pk.y, l);
+                        rank += ((uint32_t)l < n && ol == pk.x && kl < pk.y) ? 1 : 0;
+                    }
+                }
+                const bool surv = valid && rank < survivors(kme, maxpp, apply);
+                uint32_t* om = a.comap + (size_t)c * 32;
+                if (surv) om[fpfx[pk.x] + rank] = i;
+#pragma unroll
+                for (int ch = 0; ch < 2; ++ch) {
+                    const int p = ch * 32 + lane;
+                    if ((seedm >> p) & 1ull) om[fpfx[p]] = 0x80000000u | (uint32_t)p;
+                }
+                removed += (valid && !surv) ? 1 : 0;
+            } else {
+                fast = false;
             }
             __syncwarp();
         }
-        __syncthreads();
-        // ---- tile prefix: scan of the 32 cells, then look-back ----
-        if (warp == 0) {
-            uint32_t f = sm.fin[lane], s = sm.nseed[lane];
+        if (!fast) {
+            const uint2 fs = count_cell<DIM, Real>(a, sm.cnt[warp], sm.kc[warp], c, s0, L, h, lane);
+            fin = fs.x;
+            nsd = fs.y;
+            seedm = 0;
+        }
+        if (lane == 0) {
+            a.cfin[c] = fin | (fast ? 0u : 0x80000000u);
+            a.cseed[c] = nsd;
+            a.cseedm[c] = seedm;
+            atomicAdd(&sm.blk_f, fin);
+            atomicAdd(&sm.blk_s, nsd);
+        }
+    }
+    __syncthreads();
+    // ---- block prefix over the earlier blocks ----
+    if (warp == 0) {
+        const unsigned long long pre = block_prefix(a, blockIdx.x, sm.blk_f, sm.blk_s, lane);
+        if (lane == 0) {
+            sm.pre = pre;
+            if (blockIdx.x == gridDim.x - 1)
+                *a.totals = (((pre >> 32) + sm.blk_s) << 32) | (unsigned long long)((uint32_t)pre + sm.blk_f);
+        }
+    }
+    __syncthreads();
+    // ---- final offsets of the range's cells (block scan) ----
+    {
+        uint32_t runf = (uint32_t)sm.pre, runs = (uint32_t)(sm.pre >> 32);
+        for (uint32_t base = c0; base < c1; base += WR_WARPS * 32) {
+            const uint32_t c = base + threadIdx.x;
+            const uint32_t f = c < c1 ? (a.cfin[c] & 0x7fffffffu) : 0u;
+            const uint32_t s = c < c1 ? a.cseed[c] : 0u;
             uint32_t fi = f, si = s;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -590,58 +599,64 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
                     si += t2;
                 }
             }
-            sm.excl_fin[lane] = fi - f;
-            sm.excl_seed[lane] = si - s;
-            const uint32_t tf = __shfl_sync(0xffffffffu, fi, 31), ts = __shfl_sync(0xffffffffu, si, 31);
-            const unsigned long long pre = lookback(a, tile, tf, ts, lane);
-            if (lane == 0) {
-                sm.prefix = pre;
-                if (tile == a.ntiles - 1)
-                    *a.totals = (((pre >> 32) + ts) << 32) | (unsigned long long)((uint32_t)pre + tf);
+            if (lane == 31) {
+                sm.ws_f[warp] = fi;
+                sm.ws_s[warp] = si;
             }
-        }
-        __syncthreads();
-        // ---- phase 2: write the cells at their final offsets ----
-        const uint32_t pf = (uint32_t)sm.prefix, ps = (uint32_t)(sm.prefix >> 32);
-        for (int j = 0; j < WR_CPW; ++j) {
-            const int slotc = warp * WR_CPW + j;
-            const uint32_t c = tile * WR_TILE + slotc;
-            if (c >= (uint32_t)a.mesh.nC) continue;
-            const uint32_t fb = pf + sm.excl_fin[slotc], sb = ps + sm.excl_seed[slotc];
-            if (lane == 0) a.cs_new[c] = fb;
-            if (sm.slow & (1u << slotc)) {
-                const uint32_t s0 = a.cs_old[c], L = a.cs_old[c + 1] - s0;
-                write_cell_general<DIM, Real>(a, sm, warp, c, s0, L, a.head[c], fb, sb, id0, lane, removed, err);
-            } else {
-                const uint32_t fin = sm.fin[slotc];
-                const bool valid = (uint32_t)lane < fin;
-                Real xi[DIM], v[DIM];
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) xi[d] = v[d] = Real(0);
-                if (valid) {
-                    const uint32_t ent = sm.outmap[warp][j][lane];
-                    const uint32_t dst = fb + lane;
-                    if (dst >= cap) {
-                        err |= ERR_CAPACITY;
-                    } else if (ent & 0x80000000u) {
-                        const int p = (int)(ent & 0x7fffffffu);
-                        int idx[3] = {0, 0, 0};
-                        real_part<DIM>(p, a.pp, idx);
-                        const unsigned long long sdm = sm.seedmask[slotc];
-                        const uint32_t r = (uint32_t)__popcll(p == 0 ? 0ull : (sdm & ((1ull << p) - 1ull)));
-                        new_particle<DIM, Real>(a, a.S1, dst, c, idx, id0 + sb + r + 1, xi, v);
-                    } else {
-                        copy_particle<DIM, Real>(a, ent, dst, c, xi, v);
-                    }
+            __syncthreads();
+            uint32_t wf = 0, wsum = 0, tf = 0, ts = 0;
+            for (int w = 0; w < WR_WARPS; ++w) {
+                if (w < warp) {
+                    wf += sm.ws_f[w];
+                    wsum += sm.ws_s[w];
                 }
-                PartialAcc<Real> acc;
-                partial_rows<DIM, Real>(sm.tr[warp], valid && fb + lane < cap, xi, v, (int)fin, lane, acc);
-                store_partial<DIM, Real>(a, c, acc, lane);
+                tf += sm.ws_f[w];
+                ts += sm.ws_s[w];
             }
-            __syncwarp();
-            if (lane == 0) a.head[c] = LOST;  // arrival list consumed
+            if (c < c1) {
+                a.cs_new[c] = runf + wf + fi - f;
+                a.cseedoff[c] = runs + wsum + si - s;
+            }
+            runf += tf;
+            runs += ts;
+            __syncthreads();
         }
-        __syncthreads();
+    }
+    // ---- phase 2 ----
+    for (uint32_t c = c0 + warp; c < c1; c += WR_WARPS) {
+        const uint32_t fb = a.cs_new[c], sb = a.cseedoff[c];
+        const uint32_t fw = a.cfin[c];
+        if (fw & 0x80000000u) {
+            const uint32_t s0 = a.cs_old[c], L = a.cs_old[c + 1] - s0;
+            write_cell_general<DIM, Real>(a, sm, warp, c, s0, L, a.head[c], fb, sb, id0, lane, removed, err);
+        } else {
+            const uint32_t fin = fw;
+            const bool valid = (uint32_t)lane < fin;
+            Real xi[DIM], v[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) xi[d] = v[d] = Real(0);
+            if (valid) {
+                const uint32_t ent = a.comap[(size_t)c * 32 + lane];
+                const uint32_t dst = fb + lane;
+                if (dst >= cap) {
+                    err |= ERR_CAPACITY;
+                } else if (ent & 0x80000000u) {
+                    const int p = (int)(ent & 0x7fffffffu);
+                    int idx[3] = {0, 0, 0};
+                    real_part<DIM>(p, a.pp, idx);
+                    const unsigned long long sdm = a.cseedm[c];
+                    const uint32_t r = (uint32_t)__popcll(p == 0 ? 0ull : (sdm & ((1ull << p) - 1ull)));
+                    new_particle<DIM, Real>(a, a.S1, dst, c, idx, id0 + sb + r + 1, xi, v);
+                } else {
+                    copy_particle<DIM, Real>(a, ent, dst, c, xi, v);
+                }
+            }
+            PartialAcc<Real> acc;
+            partial_rows<DIM, Real>(sm.tr[warp], valid && fb + lane < cap, xi, v, (int)fin, lane, acc);
+            store_partial<DIM, Real>(a, c, acc, lane);
+        }
+        __syncwarp();
+        if (lane == 0) a.head[c] = LOST;  // arrival list consumed
     }
     warp_count(&a.stats->removed, removed);
     err = __reduce_or_sync(0xffffffffu, err);
@@ -671,7 +686,13 @@ __global__ void k_correct(StepArgs a)
         Real xi[DIM], corr[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) xi[d] = ldr<Real>(a.S0.xi[d], i);
-        interp_v<DIM, Real>(a.dVc, c, xi, corr);
+        if constexpr (std::is_same<Real, double>::value) {
+            interp_v<DIM, Real>(a.dVc, c, xi, corr);
+        } else {
+            Rec32<DIM> r;
+            load_rec32<DIM>(a.dvrec32, c, r);
+            eval_poly<DIM>(r.b, xi, corr);
+        }
 #pragma unroll
         for (int d = 0; d < DIM; ++d) str<Real>(a.S0.v[d], i, ldr<Real>(a.S0.v[d], i) + corr[d]);
     }

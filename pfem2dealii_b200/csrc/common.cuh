@@ -19,8 +19,6 @@ constexpr int MAX_CAND = 64;   // cells around one vertex tried by the relocatio
 constexpr int NPE_MAX = 512;   // extended cell parts (q0+1)(q1+1)(q2+1)
 constexpr int CELL_WARPS = 4;  // warps per block in the warp-per-cell kernels
 constexpr int WR_WARPS = 8;    // write pass: warps per block
-constexpr int WR_CPW = 4;      // write pass: cells per warp
-constexpr int WR_TILE = WR_WARPS * WR_CPW;  // cells per look-back tile
 constexpr int KEY_CACHE = 128; // (part, key) pairs cached per warp in shared memory
 
 // error_flags bits
@@ -86,8 +84,11 @@ struct StepArgs {
     PartState S0;   // current, sorted
     PartState S1;   // next, sorted
     PartState T;    // advect output, in S0 order (cell/id unused)
-    const void* Vc;     // nC x NV x VS nodal velocity per cell vertex, VS = 4 (3D) or 2 (2D)
-    const void* dVc;    // nC x NV x VS velocity increment V - Vold per cell vertex
+    const void* Vc;     // FP64 form: nC x NV x VS nodal velocity per cell vertex, VS = 4 (3D) or 2 (2D)
+    const void* dVc;    // FP64 form: nC x NV x VS velocity increment V - Vold per cell vertex
+    const float* vrec32;  // FP32 form: nC x REC4 float4, velocity polynomial of each cell (+ affine flag)
+    const float* dvrec32; // FP32 form: nC x REC4 float4, polynomial of V - Vold
+    const double* Vd;     // staged nodal velocity, component-major (nD per component)
     int do_correct;
     int apply_counts;   // write kernel: 1 = count correction, 0 = keep all (re-sort only)
     uint32_t* key;      // cell after the move, or LOST
@@ -97,10 +98,13 @@ struct StepArgs {
     uint32_t* cs_new;        // nC + 1: cell ranges of S1
     uint2* xq;                     // particles (index, sub-step) queued for FP64 relocation
     uint32_t* nxq;                 // queue length
-    unsigned long long* tile_status; // decoupled look-back words of the write pass
-    uint32_t* tile_counter;        // dynamic tile ticket of the write pass
-    uint32_t ntiles;
+    unsigned long long* blk_status;  // write pass: per-block totals, published for later blocks
     unsigned long long* totals;    // write pass: seeds << 32 | particles after the step
+    uint32_t* cfin;                // write pass scratch per cell: final count (bit 31: general path)
+    uint32_t* cseed;               //   new particles
+    unsigned long long* cseedm;    //   parts that get a new particle (fast path)
+    uint32_t* cseedoff;            //   new particles in earlier cells
+    uint32_t* comap;               //   32 per cell: source particle, or 0x80000000|part
     void* partials;                // nC x PW projection partial sums
     double* Vout;                  // nD x DIM component-major projected velocity
     const double* Vkeep;           // empty_dof_policy 1: value kept where no particle contributes
@@ -115,6 +119,7 @@ template <int DIM> struct Dims {
     static constexpr int AFF = DIM * DIM + DIM;
     static constexpr int GEO = DIM == 3 ? 24 : 8;      // FP32 geometry floats per cell
     static constexpr int JS = DIM == 3 ? 12 : 8;       // FP32 inverse Jacobian + flag, padded
+    static constexpr int REC4 = DIM == 3 ? 7 : 3;      // float4 per FP32 velocity record (coefficients + flag)
 };
 
 __host__ __device__ inline uint32_t key_of(uint32_t id, uint32_t seed)

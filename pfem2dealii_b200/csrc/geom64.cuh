@@ -327,4 +327,24 @@ __device__ __forceinline__ void load_cell64(const double* __restrict__ cellX, ui
         for (int d = 0; d < DIM; ++d) X[i][d] = __ldg(p + i * DIM + d);
 }
 
+// u = sum_i N_i(xi) V[d][dof_i] from the staged component-major nodal
+// vectors (V_d[dof] at Vd + d*nD), accumulated from zero in vertex order:
+// the reference's interpolation (src/pfem2particlehandler.cpp:96-101).
+template <int DIM>
+__device__ __forceinline__ void velocity_from_dofs(const int32_t* __restrict__ cd, const double* __restrict__ Vd,
+                                                   int nD, uint32_t c, const double* xi, double* u)
+{
+    constexpr int NV = 1 << DIM;
+    double N[NV];
+    shape64<DIM>(xi, N);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) u[d] = 0.0;
+#pragma unroll
+    for (int iv = 0; iv < NV; ++iv) {
+        const int32_t dof = __ldg(cd + (size_t)c * NV + iv);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) u[d] = u[d] + N[iv] * __ldg(Vd + (size_t)d * nD + dof);
+    }
+}
+
 }  // namespace pfem2

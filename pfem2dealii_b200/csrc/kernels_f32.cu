@@ -39,23 +39,44 @@ int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s)
 }
 
 template <int DIM>
+static int write32_t_grid()
+{
+    const int smem = (int)sizeof(WriteSmem<float>);
+    static int grid = 0;
+    if (!grid) {
+        cudaFuncSetAttribute(k_write<DIM, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_write<DIM, float>, WR_WARPS * 32, smem);
+        grid = sms * (per > 0 ? per : 1);
+    }
+    return grid;
+}
+
+template <int DIM>
 static int write32_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = (int)sizeof(WriteSmem<float>);
-    static bool init = false;
-    if (!init) {
-        cudaFuncSetAttribute(k_write<DIM, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        init = true;
-    }
-    const int grid = occupancy_grid((const void*)k_write<DIM, float>, WR_WARPS * 32, smem);
-    k_write<DIM, float><<<grid, WR_WARPS * 32, smem, s>>>(a);
-    return 1;
+    StepArgs args = a;
+    void* params[] = {&args};
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_write<DIM, float>, dim3(write32_t_grid<DIM>()),
+                                                      dim3(WR_WARPS * 32), params, smem, s);
+    return e == cudaSuccess ? 1 : -1;
 }
 
 int launch_write(int dim, int prec, const StepArgs& a, cudaStream_t s)
 {
     if (prec == 0) return launch64_write(dim, a, s);
     return dim == 2 ? write32_t<2>(a, s) : write32_t<3>(a, s);
+}
+
+int launch64_write_grid(int dim);
+
+int write_grid(int dim, int prec)
+{
+    if (prec == 0) return launch64_write_grid(dim);
+    return dim == 2 ? write32_t_grid<2>() : write32_t_grid<3>();
 }
 
 int launch_partials(int dim, int prec, const StepArgs& a, const uint32_t* cs, cudaStream_t s)

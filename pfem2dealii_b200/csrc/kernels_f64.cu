@@ -117,18 +117,33 @@ int launch64_advect(int dim, const StepArgs& a, cudaStream_t s)
 }
 
 template <int DIM>
+static int write_t_grid()
+{
+    const int smem = (int)sizeof(WriteSmem<double>);
+    static int grid = 0;
+    if (!grid) {
+        cudaFuncSetAttribute(k_write<DIM, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_write<DIM, double>, WR_WARPS * 32, smem);
+        grid = sms * (per > 0 ? per : 1);
+    }
+    return grid;
+}
+
+template <int DIM>
 static int write_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = (int)sizeof(WriteSmem<double>);
-    static bool init = false;
-    if (!init) {
-        cudaFuncSetAttribute(k_write<DIM, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        init = true;
-    }
-    const int grid = occupancy_grid((const void*)k_write<DIM, double>, WR_WARPS * 32, smem);
-    k_write<DIM, double><<<grid, WR_WARPS * 32, smem, s>>>(a);
-    return 1;
+    StepArgs args = a;
+    void* params[] = {&args};
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_write<DIM, double>, dim3(write_t_grid<DIM>()),
+                                                      dim3(WR_WARPS * 32), params, smem, s);
+    return e == cudaSuccess ? 1 : -1;
 }
+
+int launch64_write_grid(int dim) { return dim == 2 ? write_t_grid<2>() : write_t_grid<3>(); }
 
 int launch64_write(int dim, const StepArgs& a, cudaStream_t s)
 {

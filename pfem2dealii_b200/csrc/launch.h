@@ -47,5 +47,9 @@ int launch_finalize(const StepArgs& a, int count_step, cudaStream_t s);
 int launch_set_state(DevStats* st, long long n, long long next_id, long long add_id, cudaStream_t s);
 int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const int32_t* cd, int nC, int nD, void* Vc,
                   void* dVc, cudaStream_t s);
+int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
+                      const float* jinv32, int nC, int nD, float* vrec, float* dvrec, cudaStream_t s);
+// co-resident blocks of the write pass (its cooperative launch grid)
+int write_grid(int dim, int prec);
 
 }  // namespace pfem2

@@ -83,9 +83,78 @@ __global__ void k_cell_v(const double* __restrict__ V, const double* __restrict_
     }
 }
 
+// FP32 form: per-cell polynomial of the velocity field, b_k = nested
+// differences of the vertex values (bit d of k selects xi_d).  On affine
+// cells the coefficients are mapped to reference space, w_k = J^-1 b_k, with
+// the cell's exact FP64 inverse Jacobian, so that d xi = dt w(xi).
+template <int DIM>
+__global__ void k_cell_rec32(const double* __restrict__ V, const double* __restrict__ Vold,
+                             const int32_t* __restrict__ cd, const double* __restrict__ aff,
+                             const float* __restrict__ jinv32, int nC, int nD, float* __restrict__ vrec,
+                             float* __restrict__ dvrec)
+{
+    constexpr int NV = 1 << DIM, F = Dims<DIM>::REC4 * 4, AFF = Dims<DIM>::AFF;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nC; c += gridDim.x * blockDim.x) {
+        double f[NV][DIM], g[NV][DIM];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            const int dof = __ldg(cd + (size_t)c * NV + i);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                f[i][d] = V[(size_t)d * nD + dof];
+                g[i][d] = Vold ? f[i][d] - Vold[(size_t)d * nD + dof] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < DIM; ++b)
+#pragma unroll
+            for (int i = NV - 1; i >= 0; --i)
+                if ((i >> b) & 1)
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        f[i][d] -= f[i ^ (1 << b)][d];
+                        g[i][d] -= g[i ^ (1 << b)][d];
+                    }
+        const bool affine = jinv32[(size_t)c * Dims<DIM>::JS + DIM * DIM] != 0.0f;
+        float* r = vrec + (size_t)c * F;
+#pragma unroll
+        for (int k = 0; k < NV; ++k)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                double w = f[k][d];
+                if (affine) {
+                    w = 0.0;
+#pragma unroll
+                    for (int e = 0; e < DIM; ++e) w += aff[(size_t)c * AFF + d * DIM + e] * f[k][e];
+                }
+                r[k * DIM + d] = (float)w;
+            }
+        for (int k = NV * DIM; k < F; ++k) r[k] = 0.0f;
+        r[NV * DIM] = affine ? 1.0f : 0.0f;
+        if (Vold) {
+            float* q = dvrec + (size_t)c * F;
+#pragma unroll
+            for (int k = 0; k < NV; ++k)
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) q[k * DIM + d] = (float)g[k][d];
+            for (int k = NV * DIM; k < F; ++k) q[k] = 0.0f;
+        }
+    }
+}
+
 int grid_for(const void* k, int threads) { return occupancy_grid(k, threads); }
 
 }  // namespace
+
+int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
+                      const float* jinv32, int nC, int nD, float* vrec, float* dvrec, cudaStream_t s)
+{
+    const int g = (nC + 127) / 128 < 8192 ? (nC + 127) / 128 : 8192;
+    const int grid = g > 0 ? g : 1;
+    if (dim == 2) k_cell_rec32<2><<<grid, 128, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    else k_cell_rec32<3><<<grid, 128, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    return 1;
+}
 
 int launch_rekey(const StepArgs& a, cudaStream_t s)
 {
