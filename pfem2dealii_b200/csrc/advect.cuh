@@ -11,9 +11,12 @@
 // DoF velocities a warp needs are mostly the same few cache lines.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "geom64.cuh"
 #include "geom32.cuh"
+#include "staging.cuh"
 
 namespace pfem2 {
 
@@ -167,7 +170,7 @@ __device__ __noinline__ SearchOut fallback64(const MeshDev m, uint32_t c, Vec<DI
 }
 
 struct AdvCounters {
-    uint32_t lost = 0, map_failures = 0, near_face = 0, searched = 0, fallback = 0, deferred = 0;
+    uint32_t lost = 0, map_failures = 0, near_face = 0, searched = 0, fallback = 0;
     uint32_t err = 0;
 };
 
@@ -200,12 +203,112 @@ __device__ __forceinline__ void defer(const StepArgs& a, bool want, uint32_t i, 
 }
 
 // Record where particle i ended: its cell, or LOST.  A particle that changed
-// cell is pushed on the arrival list of its new cell; the ones that stayed
-// are found by the write pass in their old cell range.
+// cell is entered among its new cell's arrivals (ARRCAP slots, then the
+// overflow list); the ones that stayed are found by the write pass in their
+// old cell range.
 __device__ __forceinline__ void arrive(const StepArgs& a, uint32_t i, uint32_t c, uint32_t c_old, bool alive)
 {
     a.key[i] = alive ? c : LOST;
-    if (alive && c != c_old) a.next[i] = atomicExch(a.head + c, i);
+    if (alive && c != c_old) {
+        const uint32_t k = atomicAdd(a.carr + c, 1u);
+        if (k < (uint32_t)ARRCAP) a.carrs[(size_t)c * ARRCAP + k] = i;
+        else a.next[i] = atomicExch(a.head + c, i);
+    }
+}
+
+// Cell count and part occupancy of the particles a warp finished (pe = the
+// particle's extended part): one atomic per distinct cell per word.
+__device__ __forceinline__ void count_cells(const StepArgs& a, bool counted, uint32_t c, int pe)
+{
+    const unsigned am = __ballot_sync(0xffffffffu, counted);
+    if (!counted) return;
+    const unsigned grp = __match_any_sync(am, c);
+    const int leader = __ffs(grp) - 1;
+    const bool lead = (int)(threadIdx.x & 31) == leader;
+    if (lead) atomicAdd(a.ccount + c, (uint32_t)__popc(grp));
+    for (int w = 0; w < a.pp.occw; ++w) {
+        const unsigned long long bit = (pe >> 6) == w ? (1ull << (pe & 63)) : 0ull;
+        const unsigned lo = __reduce_or_sync(grp, (unsigned)bit);
+        const unsigned hi = __reduce_or_sync(grp, (unsigned)(bit >> 32));
+        if (lead && (lo | hi)) atomicOr(a.cocc + (size_t)c * a.pp.occw + w, ((unsigned long long)hi << 32) | lo);
+    }
+}
+
+__device__ __forceinline__ void count_one(const StepArgs& a, uint32_t c, int pe)
+{
+    atomicAdd(a.ccount + c, 1u);
+    atomicOr(a.cocc + (size_t)c * a.pp.occw + (pe >> 6), 1ull << (pe & 63));
+}
+
+// One chunk of particle state staged in shared memory by bulk copies.
+template <int DIM, typename Real, int CH>
+struct AdvStage {
+    uint32_t cell[CH];
+    Real xi[DIM][CH];
+    Real v[DIM][CH];
+    Real x[std::is_same<Real, double>::value ? DIM : 1][std::is_same<Real, double>::value ? CH : 4];
+};
+
+__device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
+
+// Thread 0: bulk-copy particles [chunk*CH, chunk*CH + cnt) of S0 into stage st.
+template <int DIM, typename Real, int CH>
+__device__ __forceinline__ void stage_chunk(const StepArgs& a, AdvStage<DIM, Real, CH>& st, uint64_t* bar,
+                                            uint32_t chunk, uint32_t n)
+{
+    constexpr bool HX = std::is_same<Real, double>::value;
+    const uint32_t base = chunk * CH;
+    const uint32_t cnt = n - base < (uint32_t)CH ? n - base : (uint32_t)CH;
+    const uint32_t b4 = round16(cnt * 4u), br = round16(cnt * (uint32_t)sizeof(Real));
+    mbar_expect_tx(bar, b4 + (2 + (HX ? 1 : 0)) * DIM * br);
+    bulk_g2s(st.cell, a.S0.cell + base, b4, bar);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        bulk_g2s(st.xi[d], reinterpret_cast<const Real*>(a.S0.xi[d]) + base, br, bar);
+        bulk_g2s(st.v[d], reinterpret_cast<const Real*>(a.S0.v[d]) + base, br, bar);
+        if (HX) bulk_g2s(st.x[d], reinterpret_cast<const Real*>(a.S0.x[d]) + base, br, bar);
+    }
+}
+
+// The chunk loop shared by both forms: double-buffered staging, f(stage, t,
+// i, active) per particle slot (every lane of every warp calls it, so warp
+// collectives are allowed inside).
+template <int DIM, typename Real, int CH, typename F>
+__device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Real, CH>* st, uint64_t* bar, F&& f)
+{
+    const uint32_t n = (uint32_t)a.stats->n_slots;
+    const uint32_t nchunks = (n + CH - 1) / CH;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (blockIdx.x < nchunks) stage_chunk<DIM, Real, CH>(a, st[0], &bar[0], blockIdx.x, n);
+        if (blockIdx.x + gridDim.x < nchunks) stage_chunk<DIM, Real, CH>(a, st[1], &bar[1], blockIdx.x + gridDim.x, n);
+    }
+    uint32_t it = 0;
+    for (uint32_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x, ++it) {
+        const int sidx = it & 1;
+        const bool ok = mbar_wait(&bar[sidx], (it >> 1) & 1u);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(&a.stats->error_flags, ERR_TIMEOUT);
+            // let the copies still in flight land before the block leaves
+            mbar_wait(&bar[sidx ^ 1], ((it + 1) >> 1) & 1u);
+            return;
+        }
+        const uint32_t base = chunk * CH;
+        const uint32_t cnt = n - base < (uint32_t)CH ? n - base : (uint32_t)CH;
+#pragma unroll 1
+        for (uint32_t t = threadIdx.x; t < (uint32_t)CH; t += blockDim.x) f(st[sidx], t, base + t, t < cnt);
+        __syncthreads();
+        const uint32_t nxt = chunk + 2 * gridDim.x;
+        if (threadIdx.x == 0 && nxt < nchunks) {
+            fence_proxy_async();
+            stage_chunk<DIM, Real, CH>(a, st[sidx], &bar[sidx], nxt, n);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -266,28 +369,32 @@ __device__ __forceinline__ int substeps64(const StepArgs& a, uint32_t c, int s0,
     return s;
 }
 
+constexpr int ADV64_CH = 512;
+
 template <int DIM>
 __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
 {
+    extern __shared__ __align__(128) unsigned char adv_raw[];
+    __shared__ uint64_t bar[2];
+    auto* st = reinterpret_cast<AdvStage<DIM, double, ADV64_CH>*>(adv_raw);
     const MeshDev& m = a.mesh;
-    const uint32_t n = (uint32_t)a.stats->n_particles;
     AdvCounters k;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t nloop = (n + stride - 1) / stride * stride;  // whole warps iterate together
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nloop; i += stride) {
-        const bool act = i < n;
-        uint32_t c = act ? a.S0.cell[i] : 0u;
-        bool want = false;
-        int s = 0;
+    staged_loop<DIM, double, ADV64_CH>(a, st, bar, [&](AdvStage<DIM, double, ADV64_CH>& sg, uint32_t t, uint32_t i,
+                                                       bool in) {
+        const uint32_t c = in ? sg.cell[t] : HOLE;
+        const bool act = c != HOLE && in;
+        bool want = false, counted = false;
+        int s = 0, pe = 0;
+        if (in && c == HOLE) a.key[i] = LOST;
         if (act) {
             double x[DIM], xi[DIM], v[DIM], u[DIM];
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
-                x[d] = ((const double*)a.S0.x[d])[i];
-                xi[d] = ((const double*)a.S0.xi[d])[i];
-                v[d] = ((const double*)a.S0.v[d])[i];
+                x[d] = sg.x[d][t];
+                xi[d] = sg.xi[d][t];
+                v[d] = sg.v[d][t];
             }
-            bool alive = c < (uint32_t)m.nC;
+            const bool alive = c < (uint32_t)m.nC;
             if (!alive) k.err |= ERR_BAD_CELL;
             if (alive) {
                 if (a.do_correct) {  // :126-138, deltaV = V - Vold per vertex
@@ -309,10 +416,13 @@ __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
             else {
                 arrive(a, i, c, c, alive);
                 if (!alive) k.lost++;
+                counted = alive;
+                if (counted) pe = ext_part<DIM, double>(xi, a.pp);
             }
         }
         defer(a, want, i, s);
-    }
+        count_cells(a, counted, c, pe);
+    });
     flush_counters(a, k);
 }
 
@@ -368,7 +478,8 @@ __global__ void __launch_bounds__(128) k_search64(StepArgs a)
             ((double*)a.T.xi[d])[i] = xi[d];
         }
         arrive(a, i, c, c_old, alive);
-        if (!alive) k.lost++;
+        if (alive) count_one(a, c, ext_part<DIM, double>(xi, a.pp));
+        else k.lost++;
     }
     flush_counters(a, k);
 }
@@ -488,22 +599,23 @@ __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0,
 template <int DIM>
 __global__ void __launch_bounds__(256, 3) k_advect32(StepArgs a)
 {
+    extern __shared__ __align__(128) unsigned char adv_raw[];
+    __shared__ uint64_t bar[2];
+    auto* st = reinterpret_cast<AdvStage<DIM, float, ADV_CH>*>(adv_raw);
     const MeshDev& m = a.mesh;
-    const uint32_t n = (uint32_t)a.stats->n_particles;
     AdvCounters k;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t nloop = (n + stride - 1) / stride * stride;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nloop; i += stride) {
-        const bool act = i < n;
-        uint32_t c = act ? a.S0.cell[i] : 0u;
-        bool want = false;
-        int s = 0;
+    staged_loop<DIM, float, ADV_CH>(a, st, bar, [&](AdvStage<DIM, float, ADV_CH>& sg, uint32_t t, uint32_t i, bool in) {
+        const uint32_t c = in ? sg.cell[t] : HOLE;
+        const bool act = c != HOLE && in;
+        bool want = false, counted = false;
+        int s = 0, pe = 0;
+        if (in && c == HOLE) a.key[i] = LOST;
         if (act) {
             float xi[DIM], v[DIM];
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
-                xi[d] = ((const float*)a.S0.xi[d])[i];
-                v[d] = ((const float*)a.S0.v[d])[i];
+                xi[d] = sg.xi[d][t];
+                v[d] = sg.v[d][t];
             }
             const bool alive = c < (uint32_t)m.nC;
             if (!alive) k.err |= ERR_BAD_CELL;
@@ -528,10 +640,13 @@ __global__ void __launch_bounds__(256, 3) k_advect32(StepArgs a)
             else {
                 arrive(a, i, c, c, alive);
                 if (!alive) k.lost++;
+                counted = alive;
+                if (counted) pe = ext_part<DIM, float>(xi, a.pp);
             }
         }
         defer(a, want, i, s);
-    }
+        count_cells(a, counted, c, pe);
+    });
     flush_counters(a, k);
 }
 
@@ -582,7 +697,8 @@ __global__ void __launch_bounds__(128) k_cross32(StepArgs a)
 #pragma unroll
         for (int d = 0; d < DIM; ++d) ((float*)a.T.xi[d])[i] = xi[d];
         arrive(a, i, c, c_old, alive);
-        if (!alive) k.lost++;
+        if (alive) count_one(a, c, ext_part<DIM, float>(xi, a.pp));
+        else k.lost++;
     }
     flush_counters(a, k);
 }

@@ -2,7 +2,7 @@
 // sequences.  One time step of the reference loop (src/pfem2solver.cpp:162-164)
 // maps to
 //   correct(V, Vold)  -> stage V, V - Vold per cell vertex (the correction is fused into move)
-//   move(V)           -> advect | FP64 relocation queue | write (look-back) | finalize
+//   move(V)           -> advect (staged) | FP64 relocation queue | slots per cell | scan | write | finalize
 //   project(V_out)    -> gather (per-cell partials were summed by write) | D2H
 #include <algorithm>
 #include <cmath>
@@ -41,8 +41,9 @@ struct pfem2gpu_handle {
     uint32_t *head = nullptr, *cs0 = nullptr, *cs1 = nullptr;  // cs0: cell ranges of S0
     uint2* xq = nullptr;
     uint32_t* nxq = nullptr;
-    unsigned long long *blk_status = nullptr, *totals = nullptr, *cseedm = nullptr;
-    uint32_t *cfin = nullptr, *cseed = nullptr, *cseedoff = nullptr, *comap = nullptr;
+    uint32_t *carr = nullptr, *carrs = nullptr, *ccount = nullptr;
+    unsigned long long *cocc = nullptr, *cub = nullptr, *coff = nullptr, *tiles64 = nullptr;
+    uint4* gscr = nullptr;
     float *jinv32 = nullptr, *vrec32 = nullptr, *dvrec32 = nullptr;
     bool launch_failed = false;
     void* partials = nullptr;
@@ -174,13 +175,13 @@ StepArgs args(pfem2gpu_handle* h)
     a.cs_new = h->cs1;
     a.xq = h->xq;
     a.nxq = h->nxq;
-    a.blk_status = h->blk_status;
-    a.totals = h->totals;
-    a.cfin = h->cfin;
-    a.cseed = h->cseed;
-    a.cseedm = h->cseedm;
-    a.cseedoff = h->cseedoff;
-    a.comap = h->comap;
+    a.carr = h->carr;
+    a.carrs = h->carrs;
+    a.ccount = h->ccount;
+    a.cocc = h->cocc;
+    a.cub = h->cub;
+    a.coff = h->coff;
+    a.gscr = h->gscr;
     a.partials = h->partials;
     a.Vout = h->Vout;
     a.Vkeep = h->Vstage;
@@ -222,7 +223,7 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
 {
     if (need <= h->cap && h->S0.cell) return PFEM2GPU_OK;
     uint64_t cap = std::max<uint64_t>(need, (uint64_t)h->cap * 3 / 2);
-    cap = std::max<uint64_t>(cap, 1024);
+    cap = (std::max<uint64_t>(cap, 1024) + 3) & ~3ull;  // whole 16-byte chunks for the bulk copies
     if (cap > 0x7FFFFFF0ull) return fail(h, PFEM2GPU_ERR_CAPACITY, "particle capacity beyond 2^31");
     PartState n0{}, n1{}, nt{};
     CK(alloc_state(h, n0, (uint32_t)cap, true));
@@ -246,6 +247,8 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
     dfree(h->next);
     dfree(h->xtmp);
     dfree(h->xq);
+    dfree(h->gscr);
+    h->gscr = nullptr;
     h->key = h->next = nullptr;
     h->xtmp = nullptr;
     h->xq = nullptr;
@@ -255,6 +258,7 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
     CK(dalloc(&h->key, cap));
     CK(dalloc(&h->next, cap));
     CK(dalloc(&h->xq, cap));
+    CK(dalloc(&h->gscr, cap));
     if (!h->nxq) CK(dalloc(&h->nxq, 1));
     if (h->prec == PFEM2GPU_FP32) CK(dalloc(&h->xtmp, cap * h->dim));
     h->cap = (uint32_t)cap;
@@ -318,7 +322,8 @@ int apply_pending_correction(pfem2gpu_handle* h)
 // set_particles.
 int write_and_swap(pfem2gpu_handle* h, StepArgs& a, int count_step)
 {
-    CK(cudaMemsetAsync(h->blk_status, 0, (size_t)write_grid(h->dim, h->prec) * sizeof(unsigned long long), h->stream));
+    run(h, "cell_slots", [&] { return launch_cell_slots(a, h->stream); });
+    run(h, "scan_slots", [&] { return launch_scan_u64(h->cub, h->nC, h->coff, h->tiles64, h->stream); });
     run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->stream); });
     run(h, "finalize", [&] { return launch_finalize(a, count_step, h->stream); });
     std::swap(h->S0, h->S1);
@@ -354,7 +359,7 @@ int sync_stats(pfem2gpu_handle* h)
 // particle per empty part); only at points that already synchronize.
 int maybe_grow(pfem2gpu_handle* h)
 {
-    const uint64_t n = h->stats_h->n_particles;
+    const uint64_t n = h->stats_h->n_slots;
     if (n + (uint64_t)h->nC * h->pp.npart / 2 > h->cap) return ensure_capacity(h, n + (uint64_t)h->nC * h->pp.npart);
     return PFEM2GPU_OK;
 }
@@ -420,15 +425,16 @@ int pfem2gpu_create(int dim, int precision, const pfem2gpu_params* prm, pfem2gpu
     pp.S = prm->particle_integration_steps == 0 ? 1 : prm->particle_integration_steps;  // :34-36
     pp.dtp = prm->time_step / (double)pp.S;                                               // :38
     pp.seed = prm->removal_seed;
-    pp.realmask = 0;
-    for (int e = 0; e < npe && e < 64; ++e) {  // extended-part digits, x-major, base q_d + 1
+    pp.occw = (npe + 63) / 64;
+    for (int w = 0; w < OCCW_MAX; ++w) pp.realmask[w] = 0;
+    for (int e = 0; e < npe; ++e) {  // extended-part digits, x-major, base q_d + 1
         int r = e;
         bool real = true;
         for (int d = dim - 1; d >= 0; --d) {
             real = real && (r % (pp.q[d] + 1)) < pp.q[d];
             r /= pp.q[d] + 1;
         }
-        if (real) pp.realmask |= 1ull << e;
+        if (real) pp.realmask[e >> 6] |= 1ull << (e & 63);
     }
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&h->stats, sizeof(DevStats)) != cudaSuccess ||
@@ -450,8 +456,8 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
                     (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
                     (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vc, h->dVc,
                     (void*)h->key, (void*)h->next, (void*)h->xtmp, (void*)h->head, (void*)h->cs0, (void*)h->cs1,
-                    (void*)h->blk_status, (void*)h->totals, (void*)h->jinv32, (void*)h->xq, (void*)h->nxq,
-                    (void*)h->cfin, (void*)h->cseed, (void*)h->cseedm, (void*)h->cseedoff, (void*)h->comap,
+                    (void*)h->carr, (void*)h->carrs, (void*)h->ccount, (void*)h->cocc, (void*)h->cub, (void*)h->coff,
+                    (void*)h->tiles64, (void*)h->gscr, (void*)h->jinv32, (void*)h->xq, (void*)h->nxq,
                     (void*)h->vrec32, (void*)h->dvrec32, h->partials, (void*)h->stats})
         dfree(p);
     free_state(h->S0);
@@ -476,6 +482,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     if (n_cells < 1 || n_verts < 1 || n_dofs < 1 || n_cells > (1ll << 30) || n_verts > (1ll << 30) ||
         n_dofs > (1ll << 30))
         return fail(h, PFEM2GPU_ERR_ARG, "mesh sizes out of range");
+    if ((n_cells + 2047) / 2048 > SCAN_MAX_TILES) return fail(h, PFEM2GPU_ERR_ARG, "too many cells");
     if (h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "mesh change with live particles");
     const int dim = h->dim, NV = 1 << dim;
     for (int64_t k = 0; k < n_cells * NV; ++k) {
@@ -544,9 +551,9 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     for (void* p : {(void*)h->cv, (void*)h->cd, (void*)h->v2c_off, (void*)h->v2c_cells, (void*)h->d2c_off,
                     (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
                     (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vc, h->dVc,
-                    (void*)h->head, (void*)h->cs0, (void*)h->cs1, (void*)h->blk_status, (void*)h->totals,
-                    (void*)h->jinv32, (void*)h->cfin, (void*)h->cseed, (void*)h->cseedm, (void*)h->cseedoff,
-                    (void*)h->comap, (void*)h->vrec32, (void*)h->dvrec32, h->partials})
+                    (void*)h->head, (void*)h->cs0, (void*)h->cs1, (void*)h->carr, (void*)h->carrs,
+                    (void*)h->ccount, (void*)h->cocc, (void*)h->cub, (void*)h->coff, (void*)h->tiles64,
+                    (void*)h->jinv32, (void*)h->vrec32, (void*)h->dvrec32, h->partials})
         dfree(p);
     h->has_mesh = false;
     h->nC = (int)n_cells;
@@ -574,13 +581,17 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(dalloc(&h->head, nc));
     CK(dalloc(&h->cs0, nc + 1));
     CK(dalloc(&h->cs1, nc + 1));
-    CK(dalloc(&h->blk_status, 4096));
-    CK(dalloc(&h->totals, 1));
-    CK(dalloc(&h->cfin, nc));
-    CK(dalloc(&h->cseed, nc));
-    CK(dalloc(&h->cseedm, nc));
-    CK(dalloc(&h->cseedoff, nc));
-    CK(dalloc(&h->comap, nc * 32));
+    const int occw = h->pp.occw;
+    CK(dalloc(&h->carr, nc));
+    CK(dalloc(&h->carrs, nc * ARRCAP));
+    CK(dalloc(&h->ccount, nc));
+    CK(dalloc(&h->cocc, nc * occw));
+    CK(dalloc(&h->cub, nc));
+    CK(dalloc(&h->coff, nc + 1));
+    CK(dalloc(&h->tiles64, SCAN_MAX_TILES));
+    CK(cudaMemsetAsync(h->carr, 0, nc * 4, h->stream));
+    CK(cudaMemsetAsync(h->ccount, 0, nc * 4, h->stream));
+    CK(cudaMemsetAsync(h->cocc, 0, nc * occw * 8, h->stream));
     if (h->prec == PFEM2GPU_FP32) {
         const size_t rec = (size_t)(dim == 3 ? 7 : 3) * 4;
         CK(dalloc(&h->vrec32, nc * rec));
@@ -702,23 +713,39 @@ int pfem2gpu_get_particles(pfem2gpu_handle* h, uint32_t* id, int32_t* cell, doub
     if (rc) return rc;
     if ((rc = sync_stats(h))) return rc;
     const int64_t np = (int64_t)h->stats_h->n_particles;
+    const int64_t ns = (int64_t)h->stats_h->n_slots;
     *n = np;
     if (capacity < np) return fail(h, PFEM2GPU_ERR_ARG, "output arrays too small");
     const int dim = h->dim;
-    if (id) CK(cudaMemcpyAsync(id, h->S0.id, np * 4, cudaMemcpyDeviceToHost, h->stream));
-    if (cell) CK(cudaMemcpyAsync(cell, h->S0.cell, np * 4, cudaMemcpyDeviceToHost, h->stream));
-    std::vector<double> tmp(np);
-    std::vector<float> tmpf(np);
+    // slots of the current state; empty slots (cell HOLE) are skipped
+    std::vector<uint32_t> cells(ns), ids;
+    CK(cudaMemcpyAsync(cells.data(), h->S0.cell, ns * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (id) {
+        ids.resize(ns);
+        CK(cudaMemcpyAsync(ids.data(), h->S0.id, ns * 4, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<int64_t> live;
+    live.reserve(np);
+    for (int64_t i = 0; i < ns; ++i)
+        if (cells[i] != HOLE) live.push_back(i);
+    if ((int64_t)live.size() != np) return fail(h, PFEM2GPU_ERR_DEVICE, "slot count mismatch");
+    for (int64_t k = 0; k < np; ++k) {
+        if (id) id[k] = ids[live[k]];
+        if (cell) cell[k] = (int32_t)cells[live[k]];
+    }
+    std::vector<double> tmp(ns);
+    std::vector<float> tmpf(ns);
     auto fetch = [&](void* const* src, double* dst) -> int {
         for (int d = 0; d < dim; ++d) {
             if (h->prec == PFEM2GPU_FP64) {
-                CK(cudaMemcpyAsync(tmp.data(), src[d], np * 8, cudaMemcpyDeviceToHost, h->stream));
+                CK(cudaMemcpyAsync(tmp.data(), src[d], ns * 8, cudaMemcpyDeviceToHost, h->stream));
                 CK(cudaStreamSynchronize(h->stream));
-                for (int64_t i = 0; i < np; ++i) dst[i * dim + d] = tmp[i];
+                for (int64_t k = 0; k < np; ++k) dst[k * dim + d] = tmp[live[k]];
             } else {
-                CK(cudaMemcpyAsync(tmpf.data(), src[d], np * 4, cudaMemcpyDeviceToHost, h->stream));
+                CK(cudaMemcpyAsync(tmpf.data(), src[d], ns * 4, cudaMemcpyDeviceToHost, h->stream));
                 CK(cudaStreamSynchronize(h->stream));
-                for (int64_t i = 0; i < np; ++i) dst[i * dim + d] = (double)tmpf[i];
+                for (int64_t k = 0; k < np; ++k) dst[k * dim + d] = (double)tmpf[live[k]];
             }
         }
         return PFEM2GPU_OK;
@@ -731,7 +758,11 @@ int pfem2gpu_get_particles(pfem2gpu_handle* h, uint32_t* id, int32_t* cell, doub
         } else {
             StepArgs a = args(h);
             run(h, "positions", [&] { return launch_positions32(dim, a, h->xtmp, h->stream); });
-            CK(cudaMemcpyAsync(x, h->xtmp, np * dim * 8, cudaMemcpyDeviceToHost, h->stream));
+            std::vector<double> xs((size_t)ns * dim);
+            CK(cudaMemcpyAsync(xs.data(), h->xtmp, ns * dim * 8, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            for (int64_t k = 0; k < np; ++k)
+                for (int d = 0; d < dim; ++d) x[k * dim + d] = xs[(size_t)live[k] * dim + d];
         }
     }
     CK(cudaStreamSynchronize(h->stream));
@@ -775,7 +806,7 @@ int pfem2gpu_set_particles(pfem2gpu_handle* h, int64_t n, const uint32_t* id, co
     CK(cudaMemsetAsync(h->cs0, 0, (h->nC + 1) * sizeof(uint32_t), h->stream));
     StepArgs a = args(h);
     a.apply_counts = 0;
-    run(h, "rekey", [&] { return launch_rekey(a, h->stream); });
+    run(h, "rekey", [&] { return launch_rekey(h->dim, h->prec, a, h->stream); });
     h->has_particles = true;
     h->pending_correct = false;
     if ((rc = write_and_swap(h, a, 0))) return rc;
@@ -812,6 +843,7 @@ int pfem2gpu_reset_stats(pfem2gpu_handle* h)
     s.next_id = h->stats_h->next_id;
     s.nan_dofs = h->stats_h->nan_dofs;
     s.particle_steps = h->stats_h->particle_steps;
+    s.n_slots = h->stats_h->n_slots;
     *h->stats_h = s;
     CK(cudaMemcpyAsync(h->stats, h->stats_h, sizeof(DevStats), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));

@@ -14,18 +14,24 @@
 
 namespace pfem2 {
 
-constexpr uint32_t LOST = 0xFFFFFFFFu;
+constexpr uint32_t LOST = 0xFFFFFFFFu;  // no cell / end of a list
+constexpr uint32_t HOLE = 0xFFFFFFFEu;  // cell of an empty slot (where a removed particle would have gone)
 constexpr int MAX_CAND = 64;   // cells around one vertex tried by the relocation search
-constexpr int NPE_MAX = 512;   // extended cell parts (q0+1)(q1+1)(q2+1)
-constexpr int CELL_WARPS = 4;  // warps per block in the warp-per-cell kernels
-constexpr int WR_WARPS = 8;    // write pass: warps per block
-constexpr int KEY_CACHE = 128; // (part, key) pairs cached per warp in shared memory
+constexpr int NPE_MAX = 256;   // extended cell parts (q0+1)(q1+1)(q2+1)
+constexpr int OCCW_MAX = 4;    // 64-bit part-occupancy words per cell
+constexpr int ARRCAP = 4;      // arrival slots per cell before the overflow list
+constexpr int CELL_WARPS = 4;  // warps per block of the warp-per-cell helper kernels
+constexpr int KEY_CACHE = 128; // (part, key) pairs cached per warp on the general path
+constexpr int ADV_CH = 1024;   // particles per staged chunk of the advect pass
+constexpr int WR_WARPS = 4;    // write pass: warps per block
+constexpr int WR_CHC = 8;      // write pass: cells per warp chunk
 
 // error_flags bits
 constexpr uint32_t ERR_CAPACITY = 1u;        // more particles than the arrays hold
 constexpr uint32_t ERR_CAND_OVERFLOW = 2u;   // a vertex touches more than MAX_CAND cells
 constexpr uint32_t ERR_BAD_CELL = 4u;        // a particle carries an out-of-range cell
-constexpr uint32_t ERR_LOOKBACK = 8u;        // look-back wait gave up (bounded spin)
+constexpr uint32_t ERR_TIMEOUT = 8u;         // a bounded wait gave up
+constexpr uint32_t ERR_COUNT = 16u;          // write pass found other counts than the move recorded
 
 struct DevStats {
     unsigned long long n_particles;
@@ -38,6 +44,8 @@ struct DevStats {
     unsigned long long nan_dofs;
     unsigned long long fallback64;   // FP32 form: sub-steps relocated by the FP64 search
     unsigned long long particle_steps; // particles advanced, summed over moves
+    unsigned long long n_slots;      // length of the particle arrays (particles + empty slots)
+    unsigned long long step_holes;   // empty slots left by the last write pass
     unsigned int next_id;
     unsigned int error_flags;
 };
@@ -66,7 +74,8 @@ struct PartParams {
     double dtp;    // dt / S
     double h[3];   // 1.0 / q
     uint32_t seed; // removal key seed
-    unsigned long long realmask;  // real parts among the first 64 extended parts
+    unsigned long long realmask[OCCW_MAX];  // real parts among the extended parts, 64 per word
+    int occw;                               // occupancy words in use
 };
 
 // SoA particle arrays; x is null in the FP32 form.
@@ -92,19 +101,19 @@ struct StepArgs {
     int do_correct;
     int apply_counts;   // write kernel: 1 = count correction, 0 = keep all (re-sort only)
     uint32_t* key;      // cell after the move, or LOST
-    uint32_t* head;     // nC: first particle that moved into the cell (LOST = none)
-    uint32_t* next;     // next particle that moved into the same cell
-    const uint32_t* cs_old;  // nC + 1: cell ranges of S0
-    uint32_t* cs_new;        // nC + 1: cell ranges of S1
-    uint2* xq;                     // particles (index, sub-step) queued for FP64 relocation
-    uint32_t* nxq;                 // queue length
-    unsigned long long* blk_status;  // write pass: per-block totals, published for later blocks
-    unsigned long long* totals;    // write pass: seeds << 32 | particles after the step
-    uint32_t* cfin;                // write pass scratch per cell: final count (bit 31: general path)
-    uint32_t* cseed;               //   new particles
-    unsigned long long* cseedm;    //   parts that get a new particle (fast path)
-    uint32_t* cseedoff;            //   new particles in earlier cells
-    uint32_t* comap;               //   32 per cell: source particle, or 0x80000000|part
+    uint32_t* head;     // nC: overflow list of particles that moved into the cell (LOST = none)
+    uint32_t* next;     // next particle on the same overflow list
+    uint32_t* carr;     // nC: particles that moved into the cell
+    uint32_t* carrs;    // nC x ARRCAP: the first ARRCAP of them
+    uint32_t* ccount;   // nC: particles in the cell after the move
+    unsigned long long* cocc;  // nC x occw: parts occupied after the move
+    unsigned long long* cub;   // nC: new particles << 32 | slots needed
+    unsigned long long* coff;  // nC + 1: exclusive scan of cub
+    const uint32_t* cs_old;    // nC + 1: cell ranges of S0
+    uint32_t* cs_new;          // nC + 1: cell ranges of S1
+    uint2* xq;                 // particles (index, sub-step) queued for FP64 relocation
+    uint32_t* nxq;             // queue length
+    uint4* gscr;               // write pass, general path: per-particle scratch in the cell's output range
     void* partials;                // nC x PW projection partial sums
     double* Vout;                  // nD x DIM component-major projected velocity
     const double* Vkeep;           // empty_dof_policy 1: value kept where no particle contributes

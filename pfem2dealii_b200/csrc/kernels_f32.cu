@@ -25,58 +25,46 @@ int launch_seed(int dim, int prec, const StepArgs& a, uint32_t* cs, cudaStream_t
     return 1;
 }
 
-int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s)
+template <typename K>
+static int smem_grid32(K kernel, int threads, int smem)
 {
-    if (prec == 0) return launch64_advect(dim, a, s);
-    if (dim == 2) {
-        k_advect32<2><<<PFEM2_GRID(k_advect32<2>, 256), 256, 0, s>>>(a);
-        k_cross32<2><<<PFEM2_GRID(k_cross32<2>, 128), 128, 0, s>>>(a);
-    } else {
-        k_advect32<3><<<PFEM2_GRID(k_advect32<3>, 256), 256, 0, s>>>(a);
-        k_cross32<3><<<PFEM2_GRID(k_cross32<3>, 128), 128, 0, s>>>(a);
-    }
-    return 2;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
+    return sms * (per > 0 ? per : 1);
 }
 
 template <int DIM>
-static int write32_t_grid()
+static int advect32_t(const StepArgs& a, cudaStream_t s)
 {
-    const int smem = (int)sizeof(WriteSmem<float>);
-    static int grid = 0;
-    if (!grid) {
-        cudaFuncSetAttribute(k_write<DIM, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_write<DIM, float>, WR_WARPS * 32, smem);
-        grid = sms * (per > 0 ? per : 1);
-    }
-    return grid;
+    const int smem = 2 * (int)sizeof(AdvStage<DIM, float, ADV_CH>);
+    static const int grid = smem_grid32(k_advect32<DIM>, 256, smem);
+    k_advect32<DIM><<<grid, 256, smem, s>>>(a);
+    k_cross32<DIM><<<PFEM2_GRID(k_cross32<DIM>, 128), 128, 0, s>>>(a);
+    return 2;
+}
+
+int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s)
+{
+    if (prec == 0) return launch64_advect(dim, a, s);
+    return dim == 2 ? advect32_t<2>(a, s) : advect32_t<3>(a, s);
 }
 
 template <int DIM>
 static int write32_t(const StepArgs& a, cudaStream_t s)
 {
-    const int smem = (int)sizeof(WriteSmem<float>);
-    StepArgs args = a;
-    void* params[] = {&args};
-    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_write<DIM, float>, dim3(write32_t_grid<DIM>()),
-                                                      dim3(WR_WARPS * 32), params, smem, s);
-    return e == cudaSuccess ? 1 : -1;
+    const int smem = WR_WARPS * (int)sizeof(WrWarp<DIM, float>);
+    static const int grid = smem_grid32(k_write<DIM, float>, WR_WARPS * 32, smem);
+    k_write<DIM, float><<<grid, WR_WARPS * 32, smem, s>>>(a);
+    return 1;
 }
 
 int launch_write(int dim, int prec, const StepArgs& a, cudaStream_t s)
 {
     if (prec == 0) return launch64_write(dim, a, s);
     return dim == 2 ? write32_t<2>(a, s) : write32_t<3>(a, s);
-}
-
-int launch64_write_grid(int dim);
-
-int write_grid(int dim, int prec)
-{
-    if (prec == 0) return launch64_write_grid(dim);
-    return dim == 2 ? write32_t_grid<2>() : write32_t_grid<3>();
 }
 
 int launch_partials(int dim, int prec, const StepArgs& a, const uint32_t* cs, cudaStream_t s)

@@ -104,46 +104,40 @@ int launch64_seed(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s)
 
 #define PFEM2_GRID(kern, thr) occupancy_grid((const void*)(kern), (thr))
 
-int launch64_advect(int dim, const StepArgs& a, cudaStream_t s)
+template <typename K>
+static int smem_grid(K kernel, int threads, int smem)
 {
-    if (dim == 2) {
-        k_advect64<2><<<PFEM2_GRID(k_advect64<2>, 256), 256, 0, s>>>(a);
-        k_search64<2><<<PFEM2_GRID(k_search64<2>, 128), 128, 0, s>>>(a);
-    } else {
-        k_advect64<3><<<PFEM2_GRID(k_advect64<3>, 256), 256, 0, s>>>(a);
-        k_search64<3><<<PFEM2_GRID(k_search64<3>, 128), 128, 0, s>>>(a);
-    }
-    return 2;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
+    return sms * (per > 0 ? per : 1);
 }
 
 template <int DIM>
-static int write_t_grid()
+static int advect_t(const StepArgs& a, cudaStream_t s)
 {
-    const int smem = (int)sizeof(WriteSmem<double>);
-    static int grid = 0;
-    if (!grid) {
-        cudaFuncSetAttribute(k_write<DIM, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_write<DIM, double>, WR_WARPS * 32, smem);
-        grid = sms * (per > 0 ? per : 1);
-    }
-    return grid;
+    const int smem = 2 * (int)sizeof(AdvStage<DIM, double, ADV64_CH>);
+    static const int grid = smem_grid(k_advect64<DIM>, 256, smem);
+    k_advect64<DIM><<<grid, 256, smem, s>>>(a);
+    k_search64<DIM><<<PFEM2_GRID(k_search64<DIM>, 128), 128, 0, s>>>(a);
+    return 2;
+}
+
+int launch64_advect(int dim, const StepArgs& a, cudaStream_t s)
+{
+    return dim == 2 ? advect_t<2>(a, s) : advect_t<3>(a, s);
 }
 
 template <int DIM>
 static int write_t(const StepArgs& a, cudaStream_t s)
 {
-    const int smem = (int)sizeof(WriteSmem<double>);
-    StepArgs args = a;
-    void* params[] = {&args};
-    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_write<DIM, double>, dim3(write_t_grid<DIM>()),
-                                                      dim3(WR_WARPS * 32), params, smem, s);
-    return e == cudaSuccess ? 1 : -1;
+    const int smem = WR_WARPS * (int)sizeof(WrWarp<DIM, double>);
+    static const int grid = smem_grid(k_write<DIM, double>, WR_WARPS * 32, smem);
+    k_write<DIM, double><<<grid, WR_WARPS * 32, smem, s>>>(a);
+    return 1;
 }
-
-int launch64_write_grid(int dim) { return dim == 2 ? write_t_grid<2>() : write_t_grid<3>(); }
 
 int launch64_write(int dim, const StepArgs& a, cudaStream_t s)
 {

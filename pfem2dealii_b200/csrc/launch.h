@@ -41,7 +41,11 @@ int launch_gather(int dim, int prec, const StepArgs& a, int keep_empty, cudaStre
 int launch_positions32(int dim, const StepArgs& a, double* xout, cudaStream_t s);
 
 // misc.cu
-int launch_rekey(const StepArgs& a, cudaStream_t s);
+constexpr int SCAN_MAX_TILES = 8192;   // top-level scan capacity (x 2048 elements)
+int launch_scan_u64(const unsigned long long* in, uint32_t n, unsigned long long* out, unsigned long long* tiles,
+                    cudaStream_t s);
+int launch_cell_slots(const StepArgs& a, cudaStream_t s);
+int launch_rekey(int dim, int prec, const StepArgs& a, cudaStream_t s);
 int launch_fill_u32(uint32_t* p, uint32_t n, uint32_t v, cudaStream_t s);
 int launch_finalize(const StepArgs& a, int count_step, cudaStream_t s);
 int launch_set_state(DevStats* st, long long n, long long next_id, long long add_id, cudaStream_t s);
@@ -49,7 +53,5 @@ int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const 
                   void* dVc, cudaStream_t s);
 int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
                       const float* jinv32, int nC, int nD, float* vrec, float* dvrec, cudaStream_t s);
-// co-resident blocks of the write pass (its cooperative launch grid)
-int write_grid(int dim, int prec);
 
 }  // namespace pfem2

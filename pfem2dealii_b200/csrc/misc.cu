@@ -4,16 +4,129 @@
 // reference's std::array<TrilinosWrappers::MPI::Vector,dim>) into per-cell
 // vertex records the particle kernels read.
 #include "launch.h"
+#include "geom64.cuh"
 
 namespace pfem2 {
 
 namespace {
 
-// Links every particle of an uploaded set into the arrival list of its cell
-// (the old ranges are empty, so the write pass sorts them all).
+constexpr int SB = 256;              // scan block
+constexpr int SI = 8;                // items per thread
+constexpr int STILE = SB * SI;       // elements per tile
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T x)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// Exclusive block scan of one value per thread; returns the prefix and the
+// block total.
+template <typename T, int NT>
+__device__ __forceinline__ T block_excl_scan(T v, T& total)
+{
+    __shared__ T ws[NT / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const T inc = warp_incl_scan(v);
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < NT / 32 ? ws[lane] : T(0);
+        w = warp_incl_scan(w);
+        if (lane < NT / 32) ws[lane] = w;
+    }
+    __syncthreads();
+    const T wp = warp ? ws[warp - 1] : T(0);
+    total = ws[NT / 32 - 1];
+    __syncthreads();
+    return wp + inc - v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SB) k_scan_reduce(const T* __restrict__ in, uint32_t n, T* __restrict__ tiles)
+{
+    const uint32_t base = blockIdx.x * STILE + threadIdx.x;
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < SI; ++k) {
+        const uint32_t i = base + k * SB;
+        if (i < n) s += in[i];
+    }
+    T total;
+    block_excl_scan<T, SB>(s, total);
+    if (threadIdx.x == 0) tiles[blockIdx.x] = total;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_scan_top(T* __restrict__ tiles, uint32_t ntiles)
+{
+    constexpr int PER = SCAN_MAX_TILES / 1024;
+    T v[PER], s = 0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const uint32_t i = threadIdx.x * PER + k;
+        v[k] = i < ntiles ? tiles[i] : T(0);
+        s += v[k];
+    }
+    T total;
+    T p = block_excl_scan<T, 1024>(s, total);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const uint32_t i = threadIdx.x * PER + k;
+        if (i < ntiles) tiles[i] = p;
+        p += v[k];
+    }
+}
+
+// Rows of SB consecutive elements, one block scan per row.
+template <typename T>
+__global__ void __launch_bounds__(SB) k_scan_down(const T* __restrict__ in, uint32_t n, const T* __restrict__ tiles,
+                                                   T* __restrict__ out)
+{
+    T carry = tiles[blockIdx.x];
+#pragma unroll 1
+    for (int k = 0; k < SI; ++k) {
+        const uint32_t i = blockIdx.x * STILE + k * SB + threadIdx.x;
+        const T v = i < n ? in[i] : T(0);
+        T total;
+        const T p = block_excl_scan<T, SB>(v, total);
+        if (i < n) out[i] = carry + p;
+        if (i == n - 1) out[n] = carry + p + v;
+        carry += total;
+    }
+}
+
+// Slots needed per cell after the move (particles + new particles) and the
+// new particles alone, from the cell's count and part occupancy.
+__global__ void k_cell_slots(StepArgs a)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.mesh.nC; c += gridDim.x * blockDim.x) {
+        const uint32_t n = a.ccount[c];
+        uint32_t seeds = 0;
+        if (a.apply_counts && n > 0) {
+            if (a.pp.maxpp < 0) {
+                seeds = (uint32_t)a.pp.npart;
+            } else {
+                for (int w = 0; w < a.pp.occw; ++w)
+                    seeds += __popcll(a.pp.realmask[w] & ~a.cocc[(size_t)c * a.pp.occw + w]);
+            }
+        }
+        a.cub[c] = ((unsigned long long)seeds << 32) | (unsigned long long)(n + seeds);
+    }
+}
+
+// An uploaded particle set: every particle is an arrival of its cell (the old
+// ranges are empty), counted with its part.
+template <typename Real, int DIM>
 __global__ void k_rekey(StepArgs a)
 {
-    const uint32_t n = (uint32_t)a.stats->n_particles;
+    const uint32_t n = (uint32_t)a.stats->n_slots;
     uint32_t err = 0;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t nloop = (n + stride - 1) / stride * stride;
@@ -22,7 +135,15 @@ __global__ void k_rekey(StepArgs a)
         const uint32_t c = a.S0.cell[i];
         if (c < (uint32_t)a.mesh.nC) {
             a.key[i] = c;
-            a.next[i] = atomicExch(a.head + c, i);
+            const uint32_t k = atomicAdd(a.carr + c, 1u);
+            if (k < (uint32_t)ARRCAP) a.carrs[(size_t)c * ARRCAP + k] = i;
+            else a.next[i] = atomicExch(a.head + c, i);
+            Real xi[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) xi[d] = reinterpret_cast<const Real*>(a.T.xi[d])[i];
+            const int pe = ext_part<DIM, Real>(xi, a.pp);
+            atomicAdd(a.ccount + c, 1u);
+            atomicOr(a.cocc + (size_t)c * a.pp.occw + (pe >> 6), 1ull << (pe & 63));
         } else {
             a.key[i] = LOST;
             err = ERR_BAD_CELL;
@@ -32,37 +153,46 @@ __global__ void k_rekey(StepArgs a)
     if ((threadIdx.x & 31) == 0 && err) atomicOr(&a.stats->error_flags, err);
 }
 
-__global__ void k_fill_u32(uint32_t* p, uint32_t n, uint32_t v)
+template <typename T>
+__global__ void k_fill(T* p, uint32_t n, T v)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
 
+// End of a move: the new slot count and particle count, the ids handed out,
+// the cell ranges' end.
 __global__ void k_finalize(StepArgs a, int count_step)
 {
-    if (count_step) a.stats->particle_steps += a.stats->n_particles;
-    const unsigned long long po = *a.totals;
-    uint32_t total = (uint32_t)po;
+    DevStats* st = a.stats;
+    if (count_step) st->particle_steps += st->n_particles;
+    const unsigned long long po = a.coff[a.mesh.nC];
+    uint32_t slots = (uint32_t)po;
     const uint32_t seeds = (uint32_t)(po >> 32);
-    if (total > a.capacity) {
-        a.stats->error_flags |= ERR_CAPACITY;
-        total = a.capacity;
+    if (slots > a.capacity) {
+        st->error_flags |= ERR_CAPACITY;
+        slots = a.capacity;
     }
-    a.stats->n_particles = total;
-    a.stats->next_id += seeds;
-    a.stats->seeded += seeds;
-    a.cs_new[a.mesh.nC] = total;
+    st->n_slots = slots;
+    st->n_particles = slots - (st->step_holes < slots ? st->step_holes : slots);
+    st->step_holes = 0;
+    st->next_id += seeds;
+    st->seeded += seeds;
+    a.cs_new[a.mesh.nC] = slots;
 }
 
 __global__ void k_set_state(DevStats* st, long long n, long long next_id, long long add_id)
 {
-    if (n >= 0) st->n_particles = (unsigned long long)n;
+    if (n >= 0) {
+        st->n_particles = (unsigned long long)n;
+        st->n_slots = (unsigned long long)n;
+    }
     if (next_id >= 0) st->next_id = (unsigned)next_id;
     st->next_id += (unsigned)add_id;
 }
 
 // Per-cell copy of the nodal velocity (and V - Vold, deltaV of
 // src/pfem2particlehandler.cpp:120-124) for every cell vertex, padded to
-// VS components, in the form's precision.
+// VS components (FP64 form).
 template <int DIM, typename Real>
 __global__ void k_cell_v(const double* __restrict__ V, const double* __restrict__ Vold, const int32_t* __restrict__ cd,
                          int nC, int nD, Real* __restrict__ Vc, Real* __restrict__ dVc)
@@ -83,10 +213,10 @@ __global__ void k_cell_v(const double* __restrict__ V, const double* __restrict_
     }
 }
 
-// FP32 form: per-cell polynomial of the velocity field, b_k = nested
-// differences of the vertex values (bit d of k selects xi_d).  On affine
-// cells the coefficients are mapped to reference space, w_k = J^-1 b_k, with
-// the cell's exact FP64 inverse Jacobian, so that d xi = dt w(xi).
+// FP32 form: per-cell polynomial of the velocity field.  One lane per cell
+// vertex (8 or 4 lanes per cell): b_k = nested differences of the vertex
+// values (bit d of k selects xi_d), by xor-shuffles; on affine cells mapped
+// to reference space, w_k = J^-1 b_k, with the cell's exact FP64 inverse.
 template <int DIM>
 __global__ void k_cell_rec32(const double* __restrict__ V, const double* __restrict__ Vold,
                              const int32_t* __restrict__ cd, const double* __restrict__ aff,
@@ -94,77 +224,102 @@ __global__ void k_cell_rec32(const double* __restrict__ V, const double* __restr
                              float* __restrict__ dvrec)
 {
     constexpr int NV = 1 << DIM, F = Dims<DIM>::REC4 * 4, AFF = Dims<DIM>::AFF;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nC; c += gridDim.x * blockDim.x) {
-        double f[NV][DIM], g[NV][DIM];
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            const int dof = __ldg(cd + (size_t)c * NV + i);
+    const int lane = threadIdx.x & 31;
+    const int k = lane & (NV - 1);
+    const long long total = (long long)nC * NV;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long nloop = (total + stride - 1) / stride * stride;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nloop; t += stride) {
+        const bool act = t < total;
+        const int c = act ? (int)(t / NV) : 0;
+        double f[DIM], g[DIM];
+        if (act) {
+            const int dof = __ldg(cd + (size_t)c * NV + k);
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
-                f[i][d] = V[(size_t)d * nD + dof];
-                g[i][d] = Vold ? f[i][d] - Vold[(size_t)d * nD + dof] : 0.0;
+                f[d] = V[(size_t)d * nD + dof];
+                g[d] = Vold ? f[d] - Vold[(size_t)d * nD + dof] : 0.0;
             }
+        } else {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) f[d] = g[d] = 0.0;
         }
 #pragma unroll
         for (int b = 0; b < DIM; ++b)
 #pragma unroll
-            for (int i = NV - 1; i >= 0; --i)
-                if ((i >> b) & 1)
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) {
-                        f[i][d] -= f[i ^ (1 << b)][d];
-                        g[i][d] -= g[i ^ (1 << b)][d];
-                    }
+            for (int d = 0; d < DIM; ++d) {
+                const double fo = __shfl_xor_sync(0xffffffffu, f[d], 1 << b);
+                const double go = __shfl_xor_sync(0xffffffffu, g[d], 1 << b);
+                if ((k >> b) & 1) {
+                    f[d] -= fo;
+                    g[d] -= go;
+                }
+            }
+        if (!act) continue;
         const bool affine = jinv32[(size_t)c * Dims<DIM>::JS + DIM * DIM] != 0.0f;
         float* r = vrec + (size_t)c * F;
 #pragma unroll
-        for (int k = 0; k < NV; ++k)
+        for (int d = 0; d < DIM; ++d) {
+            double w = f[d];
+            if (affine) {
+                w = 0.0;
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                double w = f[k][d];
-                if (affine) {
-                    w = 0.0;
-#pragma unroll
-                    for (int e = 0; e < DIM; ++e) w += aff[(size_t)c * AFF + d * DIM + e] * f[k][e];
-                }
-                r[k * DIM + d] = (float)w;
+                for (int e = 0; e < DIM; ++e) w += aff[(size_t)c * AFF + d * DIM + e] * f[e];
             }
-        for (int k = NV * DIM; k < F; ++k) r[k] = 0.0f;
-        r[NV * DIM] = affine ? 1.0f : 0.0f;
+            r[k * DIM + d] = (float)w;
+        }
+        if (k == 0) {
+            for (int j = NV * DIM; j < F; ++j) r[j] = 0.0f;
+            r[NV * DIM] = affine ? 1.0f : 0.0f;
+        }
         if (Vold) {
             float* q = dvrec + (size_t)c * F;
 #pragma unroll
-            for (int k = 0; k < NV; ++k)
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) q[k * DIM + d] = (float)g[k][d];
-            for (int k = NV * DIM; k < F; ++k) q[k] = 0.0f;
+            for (int d = 0; d < DIM; ++d) q[k * DIM + d] = (float)g[d];
+            if (k == 0)
+                for (int j = NV * DIM; j < F; ++j) q[j] = 0.0f;
         }
     }
 }
 
 int grid_for(const void* k, int threads) { return occupancy_grid(k, threads); }
 
+template <typename T>
+int scan_impl(const T* in, uint32_t n, T* out, T* tiles, cudaStream_t s)
+{
+    const uint32_t ntiles = (n + STILE - 1) / STILE;
+    k_scan_reduce<T><<<ntiles, SB, 0, s>>>(in, n, tiles);
+    k_scan_top<T><<<1, 1024, 0, s>>>(tiles, ntiles);
+    k_scan_down<T><<<ntiles, SB, 0, s>>>(in, n, tiles, out);
+    return 3;
+}
+
 }  // namespace
 
-int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
-                      const float* jinv32, int nC, int nD, float* vrec, float* dvrec, cudaStream_t s)
+int launch_scan_u64(const unsigned long long* in, uint32_t n, unsigned long long* out, unsigned long long* tiles,
+                    cudaStream_t s)
 {
-    const int g = (nC + 127) / 128 < 8192 ? (nC + 127) / 128 : 8192;
-    const int grid = g > 0 ? g : 1;
-    if (dim == 2) k_cell_rec32<2><<<grid, 128, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
-    else k_cell_rec32<3><<<grid, 128, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    return scan_impl<unsigned long long>(in, n, out, tiles, s);
+}
+
+int launch_cell_slots(const StepArgs& a, cudaStream_t s)
+{
+    k_cell_slots<<<grid_for((const void*)k_cell_slots, 256), 256, 0, s>>>(a);
     return 1;
 }
 
-int launch_rekey(const StepArgs& a, cudaStream_t s)
+int launch_rekey(int dim, int prec, const StepArgs& a, cudaStream_t s)
 {
-    k_rekey<<<grid_for((const void*)k_rekey, 256), 256, 0, s>>>(a);
+    if (prec == 0 && dim == 2) k_rekey<double, 2><<<grid_for((const void*)k_rekey<double, 2>, 256), 256, 0, s>>>(a);
+    else if (prec == 0) k_rekey<double, 3><<<grid_for((const void*)k_rekey<double, 3>, 256), 256, 0, s>>>(a);
+    else if (dim == 2) k_rekey<float, 2><<<grid_for((const void*)k_rekey<float, 2>, 256), 256, 0, s>>>(a);
+    else k_rekey<float, 3><<<grid_for((const void*)k_rekey<float, 3>, 256), 256, 0, s>>>(a);
     return 1;
 }
 
 int launch_fill_u32(uint32_t* p, uint32_t n, uint32_t v, cudaStream_t s)
 {
-    k_fill_u32<<<grid_for((const void*)k_fill_u32, 256), 256, 0, s>>>(p, n, v);
+    k_fill<uint32_t><<<grid_for((const void*)k_fill<uint32_t>, 256), 256, 0, s>>>(p, n, v);
     return 1;
 }
 
@@ -190,6 +345,17 @@ int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const 
     else if (dim == 3 && prec == 0) k_cell_v<3, double><<<grid, 256, 0, s>>>(V, Vold, cd, nC, nD, (double*)Vc, (double*)dVc);
     else if (dim == 2) k_cell_v<2, float><<<grid, 256, 0, s>>>(V, Vold, cd, nC, nD, (float*)Vc, (float*)dVc);
     else k_cell_v<3, float><<<grid, 256, 0, s>>>(V, Vold, cd, nC, nD, (float*)Vc, (float*)dVc);
+    return 1;
+}
+
+int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
+                      const float* jinv32, int nC, int nD, float* vrec, float* dvrec, cudaStream_t s)
+{
+    const long long total = (long long)nC * (1 << dim);
+    const long long g = (total + 255) / 256 < 16384 ? (total + 255) / 256 : 16384;
+    const int grid = g > 0 ? (int)g : 1;
+    if (dim == 2) k_cell_rec32<2><<<grid, 256, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    else k_cell_rec32<3><<<grid, 256, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
     return 1;
 }
 
