@@ -249,6 +249,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
+                    help="run one device-resident pass of one form and print its timing (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -268,6 +270,11 @@ def main():
 
     m, V, Vold, prm = build_case()
     gpu_index = torch.cuda.current_device()
+    if args.only:
+        r = timed_device_run(ParticleHandler, m, V, Vold, prm, args.only, args.steps, args.warmup, torch)
+        print(json.dumps({"form": args.only, "ms_per_step": r["ms"] / args.steps,
+                          "value": r["particle_steps"] / (r["ms"] / 1000.0), "unit": UNIT}), flush=True)
+        return 0
 
     def barrier():
         if world > 1:

@@ -144,13 +144,17 @@ __device__ __forceinline__ bool gets_seed(const StepArgs& a, int p, int cnt, uin
 // (FP32: Kahan-compensated).  Entry e = iv*4 + comp, comp = DIM is the weight.
 // ---------------------------------------------------------------------------
 
+// Row stride of the partial-row array: 36 keeps rows 16-byte aligned (vector
+// stores) and the column reads (lane e reads entry e of row r) conflict-free.
+constexpr int TRW = 36;
+
 template <typename Real>
 struct PartialAcc {
     Real s = Real(0), c = Real(0);
 };
 
 template <int DIM, typename Real>
-__device__ __forceinline__ void partial_row(Real (*tr)[33], int row, bool valid, const Real* xi, const Real* v)
+__device__ __forceinline__ void partial_row(Real (*tr)[TRW], int row, const Real* xi, const Real* v)
 {
     constexpr int NV = 1 << DIM;
     Real N[NV];
@@ -158,15 +162,24 @@ __device__ __forceinline__ void partial_row(Real (*tr)[33], int row, bool valid,
     else shape32<DIM>(xi, N);
 #pragma unroll
     for (int iv = 0; iv < NV; ++iv) {
+        if constexpr (std::is_same<Real, float>::value) {
+            float4 t;
+            t.x = N[iv] * v[0];
+            t.y = N[iv] * v[1];
+            t.z = DIM == 3 ? N[iv] * v[DIM - 1] : N[iv];
+            t.w = DIM == 3 ? N[iv] : 0.0f;
+            *reinterpret_cast<float4*>(&tr[row][iv * 4]) = t;
+        } else {
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) tr[row][iv * 4 + d] = valid ? N[iv] * v[d] : Real(0);
-        tr[row][iv * 4 + DIM] = valid ? N[iv] : Real(0);
-        if (DIM == 2) tr[row][iv * 4 + 3] = Real(0);
+            for (int d = 0; d < DIM; ++d) tr[row][iv * 4 + d] = N[iv] * v[d];
+            tr[row][iv * 4 + DIM] = N[iv];
+            if (DIM == 2) tr[row][iv * 4 + 3] = 0.0;
+        }
     }
 }
 
 template <int DIM, typename Real>
-__device__ __forceinline__ void partial_sum_rows(Real (*tr)[33], int rows, int lane, PartialAcc<Real>& acc)
+__device__ __forceinline__ void partial_sum_rows(Real (*tr)[TRW], int rows, int lane, PartialAcc<Real>& acc)
 {
     constexpr int PW = Dims<DIM>::PW;
     if (lane < PW) {
@@ -195,7 +208,7 @@ __device__ __forceinline__ void store_partial(const StepArgs& a, uint32_t c, con
 // (empty slots contribute nothing).
 template <int DIM, typename Real>
 __device__ __forceinline__ void partials_of_range(const StepArgs& a, const PartState& S, uint32_t c, uint32_t b,
-                                                  uint32_t count, Real (*tr)[33], int lane)
+                                                  uint32_t count, Real (*tr)[TRW], int lane)
 {
     PartialAcc<Real> acc;
     for (uint32_t base = 0; base < count; base += 32) {
@@ -208,7 +221,7 @@ __device__ __forceinline__ void partials_of_range(const StepArgs& a, const PartS
             v[d] = valid ? ldr<Real>(S.v[d], b + j) : Real(0);
         }
         const int rows = count - base < 32 ? (int)(count - base) : 32;
-        if (lane < rows) partial_row<DIM, Real>(tr, lane, valid, xi, v);
+        if (lane < rows) partial_row<DIM, Real>(tr, lane, xi, v);
         __syncwarp();
         partial_sum_rows<DIM, Real>(tr, rows, lane, acc);
         __syncwarp();
@@ -231,7 +244,7 @@ struct WrCfg {
 };
 
 template <int DIM, typename Real>
-struct WrWarp {
+struct __align__(16) WrWarp {
     static constexpr int UCAP = WrCfg<DIM, Real>::UCAP;
     static constexpr bool HX = WrCfg<DIM, Real>::HX;
     uint32_t key[UCAP];
@@ -240,7 +253,7 @@ struct WrWarp {
     Real v[DIM][UCAP];
     Real x[HX ? DIM : 1][HX ? UCAP : 4];
     int cnt[NPE_MAX];
-    Real tr[32][33];
+    Real tr[32][TRW];
 };
 
 template <int DIM, typename Real>
@@ -320,11 +333,10 @@ __device__ __forceinline__ void write_holes(const StepArgs& a, uint32_t from, ui
 // slot base + k and gets id id0 + sb + k + 1.  With tr, its partial row is
 // written at row0 + k.  Returns the number of new particles.
 template <int DIM, typename Real>
-__device__ __forceinline__ uint32_t write_seeds(const StepArgs& a, uint32_t c, const int* cnt, uint32_t n, uint32_t base,
-                                                uint32_t id0, uint32_t sb, Real (*tr)[33], int row0, int lane,
-                                                uint32_t& err)
+__device__ __forceinline__ uint2 write_seeds(const StepArgs& a, uint32_t c, const int* cnt, uint32_t n, uint32_t base,
+                                          uint32_t id0, uint32_t sb, Real (*tr)[TRW], int row0, int lane)
 {
-    uint32_t done = 0;
+    uint32_t done = 0, err = 0;
     for (int p0 = 0; p0 < a.pp.npe; p0 += 32) {
         const int p = p0 + lane;
         const bool sf = p < a.pp.npe && gets_seed(a, p, cnt[p < a.pp.npe ? p : 0], n);
@@ -337,14 +349,14 @@ __device__ __forceinline__ uint32_t write_seeds(const StepArgs& a, uint32_t c, c
             Real xi[DIM], v[DIM];
             if (dst < a.capacity) {
                 new_particle<DIM, Real>(a, a.S1, dst, c, idx, id0 + sb + k + 1, xi, v);
-                if (tr && row0 + (int)k < 32) partial_row<DIM, Real>(tr, row0 + (int)k, true, xi, v);
+                if (tr && row0 + (int)k < 32) partial_row<DIM, Real>(tr, row0 + (int)k, xi, v);
             } else {
                 err |= ERR_CAPACITY;
             }
         }
         done += __popc(m);
     }
-    return done;
+    return make_uint2(done, err);
 }
 
 // General path of one cell (any particle count).  Per-element data goes to
@@ -352,19 +364,17 @@ __device__ __forceinline__ uint32_t write_seeds(const StepArgs& a, uint32_t c, c
 // are found by counting.  Order: stayers by slot, arrivals by key, new
 // particles by part -- the same as the fast path.
 template <int DIM, typename Real>
-__device__ void write_cell_general(const StepArgs& a, WrWarp<DIM, Real>& w, uint32_t c, uint32_t s0, uint32_t L,
-                                   uint32_t na, uint32_t h, uint32_t off, uint32_t ub, uint32_t nseed_expect,
-                                   uint32_t sb, uint32_t id0, int lane, unsigned long long& removed, uint32_t& err)
+__device__ uint2 write_cell_general(const StepArgs& a, WrWarp<DIM, Real>& w, uint32_t c, uint32_t s0,
+                                                 uint32_t L, uint32_t na, uint32_t h, uint32_t off, uint32_t ub,
+                                                 uint32_t nseed_expect, uint32_t sb, uint32_t id0, int lane)
 {
+    uint32_t removed = 0, err = 0;
     int* cnt = w.cnt;
     uint4* G = a.gscr + off;  // element -> (particle index, part, key, flags: 1 stayer, 2 survivor)
     const int npe = a.pp.npe;
     for (int p = lane; p < npe; p += 32) cnt[p] = 0;
     __syncwarp();
-    if (off + ub > a.capacity) {
-        err |= ERR_CAPACITY;
-        return;
-    }
+    if (off + ub > a.capacity) return make_uint2(0u, ERR_CAPACITY);
     // stayers: elements 0..ns-1 in slot order
     uint32_t ns = 0;
     for (uint32_t base = 0; base < L; base += 32) {
@@ -405,10 +415,7 @@ __device__ void write_cell_general(const StepArgs& a, WrWarp<DIM, Real>& w, uint
     const uint32_t n = ns + t;
     __syncwarp();
     __threadfence_block();
-    if (n > ub) {
-        err |= ERR_COUNT;
-        return;
-    }
+    if (n > ub) return make_uint2(0u, ERR_COUNT_UB);
     // survivors: rank by key inside the part
     uint32_t nsurv = 0;
     for (uint32_t e = lane; e < n; e += 32) {
@@ -446,13 +453,17 @@ __device__ void write_cell_general(const StepArgs& a, WrWarp<DIM, Real>& w, uint
         load_global<DIM, Real>(a, g.x, pd);
         store_particle<DIM, Real>(a, off + pos, c, pd);
     }
-    const uint32_t nseed = write_seeds<DIM, Real>(a, c, cnt, n, off + nsurv, id0, sb, nullptr, 0, lane, err);
+    const uint2 sd = write_seeds<DIM, Real>(a, c, cnt, n, off + nsurv, id0, sb, nullptr, 0, lane);
+    err |= sd.y;
+    const uint32_t nseed = sd.x;
     const uint32_t fin = nsurv + nseed;
-    if (nseed != nseed_expect || fin > ub) err |= ERR_COUNT;
+    if (nseed != nseed_expect) err |= ERR_COUNT;
+    if (fin > ub) err |= ERR_COUNT_UB;
     write_holes(a, off + fin, off + ub, lane);
     __syncwarp();
     __threadfence_block();
     partials_of_range<DIM, Real>(a, a.S1, c, off, fin, w.tr, lane);
+    return make_uint2(removed, err);
 }
 
 template <int DIM, typename Real>
@@ -518,27 +529,35 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
             const uint32_t n = ns + na;
             fast = fast && n <= 32;
             if (!fast) {
-                write_cell_general<DIM, Real>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0, lane, removed,
-                                              err);
+                const uint2 gr = write_cell_general<DIM, Real>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0,
+                                                               lane);
+                removed += gr.x;
+                err |= gr.y;
                 __syncwarp();
                 reset_cell(a, c, lane);
                 __syncwarp();
                 continue;
             }
-            const bool valid = (uint32_t)lane < n;
+            // lanes: the segment's stayers in place when segment + arrivals fit in
+            // 32 lanes (else compacted), arrivals after the segment
+            const bool spread = L + na <= 32;
+            const uint32_t abase = spread ? L : ns;
+            const bool is_stay = spread ? stay : (uint32_t)lane < ns;
+            const bool is_arr = (uint32_t)lane >= abase && (uint32_t)lane < abase + na;
+            const bool valid = is_stay || is_arr;
             PData<DIM, Real> pd;
             pd.i = 0;
             pd.id = 0;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) pd.xi[d] = pd.v[d] = Real(0);
-            if ((uint32_t)lane < ns) {
-                const uint32_t src = __fns(stm, 0, lane + 1);
+            if (is_stay) {
+                const uint32_t src = spread ? (uint32_t)lane : __fns(stm, 0, lane + 1);
                 if (staged) load_stage<DIM, Real>(w, s0 - S + src, s0 + src, pd);
                 else load_global<DIM, Real>(a, s0 + src, pd);
-            } else if (valid) {
-                const uint32_t ia = arrival(a, c, lane - ns, h);
+            } else if (is_arr) {
+                const uint32_t ia = arrival(a, c, lane - abase, h);
                 if (ia < cap) load_global<DIM, Real>(a, ia, pd);
-                else err |= ERR_COUNT;
+                else err |= ERR_ARRIVAL;
             }
             const int pe = valid ? ext_part<DIM, Real>(pd.xi, a.pp) : 0;
             const uint32_t key = valid ? key_of(pd.id, a.pp.seed) : 0xffffffffu;
@@ -549,29 +568,32 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
             __syncwarp();
             const int kme = valid ? cnt[pe] : 0;
             // rank inside an over-full part (by key)
+            const unsigned validm = __ballot_sync(0xffffffffu, valid);
             int rank = 0;
             if (__any_sync(0xffffffffu, apply && kme > maxpp + 1)) {
                 for (int l = 0; l < 32; ++l) {
                     const int pl = __shfl_sync(0xffffffffu, pe, l);
                     const uint32_t kl = __shfl_sync(0xffffffffu, key, l);
-                    rank += ((uint32_t)l < n && pl == pe && kl < key) ? 1 : 0;
+                    rank += (((validm >> l) & 1u) && pl == pe && kl < key) ? 1 : 0;
                 }
             }
             const bool surv = valid && rank < survivors(kme, maxpp, apply);
-            // order: stayers (lane order), then arrivals by key
-            uint32_t seq = (uint32_t)lane;
+            // order: stayers (slot order), then arrivals by key
+            const unsigned ltm = (1u << lane) - 1u;
+            uint32_t seq = is_stay ? (spread ? (uint32_t)__popc(stm & ltm) : (uint32_t)lane) : 0u;
+            if (is_arr) seq = ns + (uint32_t)lane - abase;
             if (na > 1) {
                 uint32_t ar = 0;
-                for (uint32_t l = ns; l < n; ++l) {
+                for (uint32_t l = abase; l < abase + na; ++l) {
                     const uint32_t kl = __shfl_sync(0xffffffffu, key, l);
                     ar += (kl < key) ? 1u : 0u;
                 }
-                if ((uint32_t)lane >= ns) seq = ns + ar;
+                if (is_arr) seq = ns + ar;
             }
             const unsigned survm = __ballot_sync(0xffffffffu, surv);
             const uint32_t nsurv = __popc(survm);
             uint32_t pos = seq;
-            if (nsurv != n) {
+            if (nsurv != n) {  // removals: survivors before in sequence order
                 pos = 0;
                 for (int l = 0; l < 32; ++l) {
                     const uint32_t sl = __shfl_sync(0xffffffffu, seq, l);
@@ -582,13 +604,18 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
                 const uint32_t dst = off + pos;
                 if (dst < cap) store_particle<DIM, Real>(a, dst, c, pd);
                 else err |= ERR_CAPACITY;
-                partial_row<DIM, Real>(w.tr, (int)pos, true, pd.xi, pd.v);
+                partial_row<DIM, Real>(w.tr, (int)pos, pd.xi, pd.v);
             }
             removed += (valid && !surv) ? 1 : 0;
-            const uint32_t nseed =
-                write_seeds<DIM, Real>(a, c, cnt, n, off + nsurv, id0, sb, w.tr, (int)nsurv, lane, err);
+            uint32_t nseed = 0;
+            if (nseed_expect) {
+                const uint2 sd = write_seeds<DIM, Real>(a, c, cnt, n, off + nsurv, id0, sb, w.tr, (int)nsurv, lane);
+                nseed = sd.x;
+                err |= sd.y;
+            }
             const uint32_t fin = nsurv + nseed;
-            if (nseed != nseed_expect || fin > ub) err |= ERR_COUNT;
+            if (nseed != nseed_expect) err |= ERR_COUNT;
+            if (fin > ub) err |= ERR_COUNT_UB;
             write_holes(a, off + fin, off + ub, lane);
             __syncwarp();
             PartialAcc<Real> acc;
@@ -608,7 +635,7 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
 template <int DIM, typename Real>
 __global__ void __launch_bounds__(CELL_WARPS * 32) k_partials(StepArgs a, const uint32_t* cell_start)
 {
-    __shared__ Real tr_s[CELL_WARPS][32][33];
+    __shared__ __align__(16) Real tr_s[CELL_WARPS][32][TRW];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int c = blockIdx.x * CELL_WARPS + warp; c < a.mesh.nC; c += gridDim.x * CELL_WARPS) {
         const uint32_t b = cell_start[c], e = cell_start[c + 1];

@@ -31,7 +31,9 @@ constexpr uint32_t ERR_CAPACITY = 1u;        // more particles than the arrays h
 constexpr uint32_t ERR_CAND_OVERFLOW = 2u;   // a vertex touches more than MAX_CAND cells
 constexpr uint32_t ERR_BAD_CELL = 4u;        // a particle carries an out-of-range cell
 constexpr uint32_t ERR_TIMEOUT = 8u;         // a bounded wait gave up
-constexpr uint32_t ERR_COUNT = 16u;          // write pass found other counts than the move recorded
+constexpr uint32_t ERR_COUNT = 16u;          // write pass: other new-particle count than the move's occupancy gave
+constexpr uint32_t ERR_COUNT_UB = 32u;       // write pass: more particles than the cell's slots
+constexpr uint32_t ERR_ARRIVAL = 64u;        // write pass: an arrival list shorter than its count
 
 struct DevStats {
     unsigned long long n_particles;
@@ -152,6 +154,17 @@ __host__ __device__ inline uint32_t key_of(uint32_t id, uint32_t seed)
 template <int DIM, typename Real>
 __device__ __forceinline__ int ext_part(const Real* xi, const PartParams& pp)
 {
+    if constexpr (sizeof(Real) == 4) {
+        // FP32 form: (int)(xi * q) in FP32
+        int e = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            int k = (int)(xi[d] * (float)pp.q[d]);
+            k = k < 0 ? 0 : (k > pp.q[d] ? pp.q[d] : k);
+            e = e * (pp.q[d] + 1) + k;
+        }
+        return e;
+    }
     int e = 0;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
