@@ -121,10 +121,16 @@ def timed_device_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, tor
     dout = torch.empty_like(dV)
     g.seed_particles_device(dV)
     stream = torch.cuda.ExternalStream(g.stream_handle())
+    def step():
+        if profile:  # per-kernel events: the separate calls, launched eagerly
+            g.correct_particle_velocity_device(dV, dVo)
+            g.move_particles_device(None)
+            g.project_particle_fields_device(dout)
+        else:  # one CUDA graph per step
+            g.step_device(dV, dVo, dout)
+
     for _ in range(warmup):
-        g.correct_particle_velocity_device(dV, dVo)
-        g.move_particles_device(None)
-        g.project_particle_fields_device(dout)
+        step()
     g.synchronize()
     if profile:
         g.profile(True)
@@ -134,9 +140,7 @@ def timed_device_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, tor
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(steps):
-        g.correct_particle_velocity_device(dV, dVo)
-        g.move_particles_device(None)
-        g.project_particle_fields_device(dout)
+        step()
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1)

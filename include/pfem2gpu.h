@@ -99,6 +99,9 @@ int pfem2gpu_seed_device(pfem2gpu_handle* h, const double* dV);
 int pfem2gpu_correct_device(pfem2gpu_handle* h, const double* dV, const double* dVold);
 int pfem2gpu_move_device(pfem2gpu_handle* h, const double* dV);
 int pfem2gpu_project_device(pfem2gpu_handle* h, double* dV_out);
+/* One whole time step (correct + move + project) on device vectors, replayed
+ * as one CUDA graph after the first calls with the same pointers. */
+int pfem2gpu_step_device(pfem2gpu_handle* h, const double* dV, const double* dVold, double* dV_out);
 
 /* Particle access for output_particle_solution (:218-317) and begin()/end():
  * arrays sized >= capacity (n x dim for x, xi, v); any may be NULL.  *n gets

@@ -46,6 +46,20 @@ struct pfem2gpu_handle {
     uint4* gscr = nullptr;
     float *jinv32 = nullptr, *vrec32 = nullptr, *dvrec32 = nullptr;
     bool launch_failed = false;
+    // CUDA graphs of the per-step sequences (one per buffer parity and
+    // variant), rebuilt whenever device buffers are reallocated
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t gen = 0;
+        uint64_t kernels = 0;
+        int seen = 0;
+        const void* key[3] = {nullptr, nullptr, nullptr};
+    };
+    Graph move_graph[2][2];  // [parity][do_correct]
+    Graph step_graph[2];     // [parity] fused correct+move+project (device vectors)
+    int parity = 0;
+    uint64_t gen = 1;
+    bool use_graphs = true;
     void* partials = nullptr;
     DevStats* stats = nullptr;
     DevStats* stats_h = nullptr;
@@ -262,6 +276,7 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
     if (!h->nxq) CK(dalloc(&h->nxq, 1));
     if (h->prec == PFEM2GPU_FP32) CK(dalloc(&h->xtmp, cap * h->dim));
     h->cap = (uint32_t)cap;
+    h->gen++;
     return PFEM2GPU_OK;
 }
 
@@ -320,28 +335,95 @@ int apply_pending_correction(pfem2gpu_handle* h)
 // The write pass (count correction, sorted layout, projection partials) and
 // the counters of the step; S1 becomes the current state.  Shared by move and
 // set_particles.
-int write_and_swap(pfem2gpu_handle* h, StepArgs& a, int count_step)
+void swap_state(pfem2gpu_handle* h)
+{
+    std::swap(h->S0, h->S1);
+    std::swap(h->cs0, h->cs1);
+    h->parity ^= 1;
+    h->partials_valid = true;
+}
+
+// The write pass (count correction, new layout, projection partials) and
+// the counters of the step.
+int enqueue_write(pfem2gpu_handle* h, StepArgs& a, int count_step)
 {
     run(h, "cell_slots", [&] { return launch_cell_slots(a, h->stream); });
     run(h, "scan_slots", [&] { return launch_scan_u64(h->cub, h->nC, h->coff, h->tiles64, h->stream); });
     run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->stream); });
     run(h, "finalize", [&] { return launch_finalize(a, count_step, h->stream); });
-    std::swap(h->S0, h->S1);
-    std::swap(h->cs0, h->cs1);
-    h->partials_valid = true;
+    return PFEM2GPU_OK;
+}
+
+int write_and_swap(pfem2gpu_handle* h, StepArgs& a, int count_step)
+{
+    enqueue_write(h, a, count_step);
+    swap_state(h);
     return check_async(h);
+}
+
+int enqueue_move(pfem2gpu_handle* h, int do_correct)
+{
+    StepArgs a = args(h);
+    a.do_correct = do_correct;
+    CK(cudaMemsetAsync(h->nxq, 0, sizeof(uint32_t), h->stream));
+    run(h, "advect", [&] { return launch_advect(h->dim, h->prec, a, h->stream); });
+    return enqueue_write(h, a, 1);
+}
+
+// Run `enqueue` through a cached CUDA graph: eager on the first use of a
+// variant (which also settles every one-time kernel attribute), captured on
+// the second, replayed afterwards.  Profiling runs stay eager so that every
+// launch is timed.
+template <typename F>
+int graphed(pfem2gpu_handle* h, pfem2gpu_handle::Graph& g, const void* k0, const void* k1, const void* k2, F&& enqueue)
+{
+    const bool same = g.key[0] == k0 && g.key[1] == k1 && g.key[2] == k2;
+    if (h->profiling || !h->use_graphs) return enqueue();
+    if (g.exec && g.gen == h->gen && same) {
+        CK(cudaGraphLaunch(g.exec, h->stream));
+        h->launches += g.kernels;
+        return PFEM2GPU_OK;
+    }
+    if (!same || g.gen != h->gen) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+        g.seen = 0;
+        g.key[0] = k0;
+        g.key[1] = k1;
+        g.key[2] = k2;
+    }
+    if (g.seen++ == 0) return enqueue();
+    const uint64_t l0 = h->launches;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ec != cudaSuccess) return fail(h, PFEM2GPU_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return fail(h, PFEM2GPU_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    g.gen = h->gen;
+    g.kernels = h->launches - l0;
+    h->launches = l0;
+    CK(cudaGraphLaunch(g.exec, h->stream));
+    h->launches += g.kernels;
+    return PFEM2GPU_OK;
 }
 
 int do_move(pfem2gpu_handle* h)
 {
     if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "move before seed");
     if (!h->vaos_valid) return fail(h, PFEM2GPU_ERR_STATE, "move without a velocity");
-    StepArgs a = args(h);
-    a.do_correct = h->pending_correct ? 1 : 0;
+    const int dc = h->pending_correct ? 1 : 0;
     h->pending_correct = false;
-    CK(cudaMemsetAsync(h->nxq, 0, sizeof(uint32_t), h->stream));
-    run(h, "advect", [&] { return launch_advect(h->dim, h->prec, a, h->stream); });
-    return write_and_swap(h, a, 1);
+    const int rc = graphed(h, h->move_graph[h->parity][dc], nullptr, nullptr, nullptr, [&] { return enqueue_move(h, dc); });
+    if (rc) return rc;
+    swap_state(h);
+    return check_async(h);
 }
 
 int sync_stats(pfem2gpu_handle* h)
@@ -464,6 +546,11 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
     free_state(h->S1);
     free_state(h->T);
     if (h->stats_h) cudaFreeHost(h->stats_h);
+    for (auto& row : h->move_graph)
+        for (auto& g : row)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto& g : h->step_graph)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     for (auto& e : h->open_ev) {
         cudaEventDestroy(e.a);
         cudaEventDestroy(e.b);
@@ -618,6 +705,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(cudaStreamSynchronize(h->stream));  // host vectors above go out of scope
     h->has_mesh = true;
     h->vaos_valid = false;
+    h->gen++;
     return check_async(h);
 }
 
@@ -702,6 +790,30 @@ static int project_impl(pfem2gpu_handle* h, double* out, bool device)
 
 int pfem2gpu_project(pfem2gpu_handle* h, double* V_out) { return project_impl(h, V_out, false); }
 int pfem2gpu_project_device(pfem2gpu_handle* h, double* dV_out) { return project_impl(h, dV_out, true); }
+
+int pfem2gpu_step_device(pfem2gpu_handle* h, const double* dV, const double* dVold, double* dV_out)
+{
+    if (!h || !dV || !dVold || !dV_out) return PFEM2GPU_ERR_ARG;
+    if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "step before seed");
+    int rc = apply_pending_correction(h);
+    if (rc) return rc;
+    rc = graphed(h, h->step_graph[h->parity], dV, dVold, dV_out, [&]() -> int {
+        int r = stage_v(h, dV, dVold, true);
+        if (r) return r;
+        if ((r = enqueue_move(h, 1))) return r;
+        StepArgs a = args(h);
+        CK(cudaMemsetAsync(&h->stats->nan_dofs, 0, sizeof(unsigned long long), h->stream));
+        run(h, "gather", [&] { return launch_gather(h->dim, h->prec, a, h->prm.empty_dof_policy == 1, h->stream); });
+        CK(cudaMemcpyAsync(dV_out, h->Vout, (size_t)h->dim * h->nD * sizeof(double), cudaMemcpyDeviceToDevice,
+                           h->stream));
+        return PFEM2GPU_OK;
+    });
+    if (rc) return rc;
+    h->vaos_valid = true;
+    h->pending_correct = false;
+    swap_state(h);
+    return check_async(h);
+}
 
 int pfem2gpu_get_particles(pfem2gpu_handle* h, uint32_t* id, int32_t* cell, double* x, double* xi, double* v,
                            int64_t capacity, int64_t* n)
@@ -830,6 +942,7 @@ int pfem2gpu_get_stats(pfem2gpu_handle* h, pfem2gpu_stats* out)
     out->particle_steps = (int64_t)s.particle_steps;
     out->next_id = s.next_id;
     out->error_flags = s.error_flags;
+    if (rc == PFEM2GPU_OK && h->has_particles) return maybe_grow(h);
     return rc == PFEM2GPU_ERR_CAPACITY || rc == PFEM2GPU_ERR_DEVICE ? PFEM2GPU_OK : rc;
 }
 

@@ -221,7 +221,12 @@ __device__ __forceinline__ void partials_of_range(const StepArgs& a, const PartS
             v[d] = valid ? ldr<Real>(S.v[d], b + j) : Real(0);
         }
         const int rows = count - base < 32 ? (int)(count - base) : 32;
-        if (lane < rows) partial_row<DIM, Real>(tr, lane, xi, v);
+        if (valid) {
+            partial_row<DIM, Real>(tr, lane, xi, v);
+        } else if (lane < rows) {  // an empty slot adds nothing
+#pragma unroll
+            for (int k = 0; k < Dims<DIM>::PW; ++k) tr[lane][k] = Real(0);
+        }
         __syncwarp();
         partial_sum_rows<DIM, Real>(tr, rows, lane, acc);
         __syncwarp();

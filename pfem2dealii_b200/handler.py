@@ -172,6 +172,10 @@ class ParticleHandler:
     def project_particle_fields_device(self, dout):
         self._ck(self.L.pfem2gpu_project_device(self.h, _ptr(dout)))
 
+    def step_device(self, dV, dVold, dout):
+        """correct + move + project on device vectors as one CUDA graph."""
+        self._ck(self.L.pfem2gpu_step_device(self.h, _ptr(dV), _ptr(dVold), _ptr(dout)))
+
     # -- particle access ------------------------------------------------------
     def particles(self):
         """Host copy of the particles (begin()/end() of the reference)."""

@@ -159,6 +159,23 @@ def test_fp64_correct_then_project_without_move():
     assert_same_particles(o.particles(), g.particles())
 
 
+def test_fp64_project_after_removals_ignores_empty_slots():
+    """A step that removes particles leaves empty slots in the cell's range;
+    a correct + project with no move in between must not count them."""
+    c = cases.channel(8, 4, q=(4, 4), maxpp=2, dt=0.0)
+    P = _crowd(c, 9, 300, np.random.default_rng(6))
+    o, g = make(c)
+    o.set_particles(P, 300)
+    g.set_particles(P, 300)
+    o.step(c.V, c.V)
+    g.step(c.V, c.V)
+    assert g.stats()["removed"] == 297
+    o.correct(c.V, 0.5 * c.V)
+    g.correct_particle_velocity(c.V, 0.5 * c.V)
+    assert_v_close(o.project(), g.project_particle_fields(), V_RTOL_FP64)
+    assert_same_particles(o.particles(), g.particles())
+
+
 def test_fp64_empty_dof_policy_keeps_input():
     c = cases.channel(8, 4, dt=0.0)
     P = _crowd(c, 0, 5, np.random.default_rng(1))
@@ -215,3 +232,40 @@ def test_vtu_output(tmp_path):
     text = (tmp_path / "particles-03.000.vtu").read_text()
     assert 'NumberOfPoints="128"' in text and "<VTKFile" in text
     assert (tmp_path / "particles-03.pvtu").exists()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_step_device_graph_replay(precision):
+    """pfem2gpu_step_device (eager first call, captured second, replayed
+    afterwards) gives the oracle's particles, bit-exact in FP64; a new output
+    pointer re-captures; the result matches the separate host calls."""
+    import torch
+
+    c = cases.duct(32, 8, 8, dt=0.05)
+    o, g = make(c, precision)
+    _, h = make(c, precision)
+    o.seed(c.V)
+    g.seed_particles(c.V)
+    h.seed_particles(c.V)
+    dV = torch.tensor(c.V, device="cuda")
+    dVo = torch.tensor(c.Vold, device="cuda")
+    outs = [torch.empty_like(dV), torch.empty_like(dV)]
+    for s in range(8):
+        Vo = o.step(c.V, c.Vold)
+        Vh = h.step(c.V, c.Vold)
+        out = outs[s // 5]
+        g.step_device(dV, dVo, out)
+        g.synchronize()  # the handler's stream is not torch's current stream
+        Vg = out.cpu().numpy()
+        if precision == "fp64":
+            assert_same_particles(o.particles(), g.particles())
+            so, sg = o.stats(), g.stats()
+            for k in STAT_KEYS:
+                assert so[k] == sg[k], (s, k, so[k], sg[k])
+            assert_v_close(Vo, Vg, V_RTOL_FP64)
+        else:
+            assert rel_l2(Vo, Vg) <= V_RTOL_FP32
+        assert np.array_equal(np.isnan(Vh), np.isnan(Vg))
+        m = np.isfinite(Vh)
+        assert np.array_equal(Vh[m], Vg[m])
+        assert_same_particles(h.particles(), g.particles())
