@@ -36,6 +36,7 @@ extern "C" {
 #define PFEM2GPU_ERR_NOMEM 5      /* device allocation failed */
 #define PFEM2GPU_ERR_NODEVICE 6   /* no CUDA device */
 #define PFEM2GPU_ERR_DEVICE 7     /* a kernel reported bad input (see stats.error_flags) */
+#define PFEM2GPU_ERR_SCRATCH 8    /* pfem2gpu_project_noalloc: mesh larger than its static scratch */
 
 #define PFEM2GPU_FP64 0           /* plain form: the reference's arithmetic, FP64 state */
 #define PFEM2GPU_FP32 1           /* FP32 state and interpolation, FP64 for face crossings */
@@ -128,6 +129,52 @@ int pfem2gpu_host_unregister(void* ptr);
 int pfem2gpu_profile(pfem2gpu_handle* h, int enable);
 int pfem2gpu_profile_report(pfem2gpu_handle* h, char* buf, int64_t len);
 int pfem2gpu_launch_count(pfem2gpu_handle* h, uint64_t* count);
+
+/* ---------------------------------------------------------------------------
+ * pfem2gpu_project_noalloc -- projection that allocates no device memory.
+ *
+ * No counterpart in the reference: it has no GPU path.  This is
+ * project_particle_fields (src/pfem2particlehandler.cpp:174-215) as one
+ * stateless call, for callers that may not allocate device memory at the
+ * point where they need the projection: a solver whose device memory is all
+ * reserved by its own pool or caching allocator, a time loop that must not
+ * hit cudaMalloc/cudaFree (cudaFree synchronises the whole device), or code
+ * that cannot keep a pfem2gpu handle.  It needs no handle and takes mesh
+ * and particles from caller-owned device arrays.
+ *
+ * The work memory is one static device array of
+ * PFEM2GPU_NOALLOC_SCRATCH_BYTES (64 MiB) per device, part of this library's
+ * image: it exists on each device where the call has run.  The call needs
+ *   256 + 4*n_dofs + 4*(n_dofs+1) + 4*ceil(n_dofs/2048)
+ *       + 4*n_cells*2^dim + 32*n_cells*2^dim          bytes
+ * (each term rounded up to 256), about 290 B per cell in 3D and 115 B per
+ * cell in 2D: up to roughly 230,000 hexes or 580,000 quads.  A larger mesh
+ * is refused with PFEM2GPU_ERR_SCRATCH before any device work.
+ *
+ * Inputs, all on the current device: cell_dofs n_cells x 2^dim (deal.II
+ * lexicographic vertex order); the particles' cells (ascending: each cell's
+ * particles contiguous, as the particle handler stores them), reference
+ * coordinates xi and velocities v, both component-major (xi[d*n + p]).
+ * Output V_out: dim x n_dofs component-major; DoFs that no particle reaches
+ * get NaN (empty_dof_policy 0, the reference's 0/0) or keep their value on
+ * entry (policy 1).  Nothing else needs any value on entry: the call zeroes
+ * the counters it uses itself.  *n_empty_dofs (if not NULL) gets the count of
+ * such DoFs.  Unsorted or out-of-range cells or DoFs: PFEM2GPU_ERR_ARG.
+ *
+ * The call runs on `stream` (a cudaStream_t; NULL = the default stream) and
+ * returns after its work there has finished.  Calls on one device share the
+ * one scratch array: the library serialises them with a lock, so they never
+ * overlap; a caller that runs its own kernels on the scratch's results does
+ * not exist (the results are only V_out).  A stream that is being captured
+ * into a CUDA graph is refused (PFEM2GPU_ERR_STATE).  The first call on a
+ * device looks up the scratch array's address (cudaGetSymbolAddress) there.
+ * The sums are those of the FP64 form: V_out equals pfem2gpu_project of an
+ * FP64 handle that holds the same particles in the same order, bit for bit.
+ */
+#define PFEM2GPU_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int pfem2gpu_project_noalloc(int dim, int32_t n_cells, int32_t n_dofs, const int32_t* d_cell_dofs,
+                             int64_t n_particles, const int32_t* d_cell, const double* d_xi, const double* d_v,
+                             int empty_dof_policy, double* d_V_out, int64_t* n_empty_dofs, void* stream);
 
 const char* pfem2gpu_error_string(int code);
 int pfem2gpu_last_error(pfem2gpu_handle* h, char* buf, int64_t len);

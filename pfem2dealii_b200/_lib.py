@@ -24,7 +24,11 @@ ERRORS = {
     5: "device out of memory",
     6: "no CUDA device",
     7: "kernel reported invalid data",
+    8: "mesh larger than the static scratch of pfem2gpu_project_noalloc",
 }
+ERR_ARG = 1
+ERR_STATE = 3
+ERR_SCRATCH = 8
 
 
 class Pfem2GpuError(RuntimeError):
@@ -109,6 +113,8 @@ def load():
         "pfem2gpu_profile_report": [P, C.c_char_p, i64],
         "pfem2gpu_launch_count": [P, C.POINTER(C.c_uint64)],
         "pfem2gpu_last_error": [P, C.c_char_p, i64],
+        "pfem2gpu_project_noalloc": [C.c_int, C.c_int32, C.c_int32, dptr, i64, dptr, dptr, dptr, C.c_int, dptr,
+                                     C.POINTER(i64), P],
     }
     for name, argt in sig.items():
         f = getattr(L, name)

@@ -1,7 +1,8 @@
 """Builds libpfem2gpu.so in-tree (pfem2dealii_b200/_build/) for sm_100a.
 
-kernels_f64.cu is compiled with --fmad=false: the FP64 form rounds every
-product and sum separately, as the CPU build of the reference arithmetic does.
+kernels_f64.cu and noalloc.cu are compiled with --fmad=false: the FP64 form
+rounds every product and sum separately, as the CPU build of the reference
+arithmetic does.
 The other sources use the default contraction.  Run ``python -m
 pfem2dealii_b200.build`` or call ``build()``.
 """
@@ -25,6 +26,7 @@ SOURCES = {
     "kernels_f32.cu": [],
     "misc.cu": [],
     "api.cu": [],
+    "noalloc.cu": ["--fmad=false"],
 }
 
 

@@ -461,6 +461,7 @@ const char* pfem2gpu_error_string(int code)
     case PFEM2GPU_ERR_NOMEM: return "device out of memory";
     case PFEM2GPU_ERR_NODEVICE: return "no CUDA device";
     case PFEM2GPU_ERR_DEVICE: return "kernel reported invalid data";
+    case PFEM2GPU_ERR_SCRATCH: return "mesh larger than the static scratch of pfem2gpu_project_noalloc";
     default: return "unknown error";
     }
 }

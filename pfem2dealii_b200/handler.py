@@ -87,6 +87,19 @@ def _host(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
+def project_noalloc(cell_dofs, cell, xi, v, out, empty_dof_policy=0, stream=None):
+    """pfem2gpu_project_noalloc on CUDA tensors: cell_dofs (n_cells, 2^dim)
+    int32, cell (n,) int32 ascending, xi and v (dim, n) float64, out
+    (dim, n_dofs) float64.  Allocates no device memory; returns the number of
+    DoFs no particle reaches."""
+    dim, n_dofs = out.shape
+    n_empty = C.c_int64(0)
+    _lib.check(_lib.load().pfem2gpu_project_noalloc(
+        dim, cell_dofs.shape[0], n_dofs, _ptr(cell_dofs), cell.shape[0], _ptr(cell), _ptr(xi), _ptr(v),
+        int(empty_dof_policy), _ptr(out), C.byref(n_empty), stream))
+    return n_empty.value
+
+
 class ParticleHandler:
     """pfem2ParticleHandler<dim> on one B200.  precision: "fp64" (the
     reference's arithmetic) or "fp32"."""
