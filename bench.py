@@ -192,15 +192,18 @@ def timed_host_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, torch
             "d2h": nbytes}
 
 
-def cpu_baseline(m, V, Vold, prm, budget_s=20.0, max_steps=None):
+def cpu_baseline(m, V, Vold, prm, budget_s=20.0, max_steps=None, warmup=0):
     """The FP64 CPU restatement (reference removal order) on all host cores,
-    on the full workload; steps until the time budget is spent."""
+    on the full workload; `warmup` untimed steps, then steps until the time
+    budget is spent."""
     from oracle.oracle import ORDER_VECTOR, Oracle
 
     cores = os.cpu_count() or 1
     o = Oracle(m, prm.particles_per_cell, prm.max_particles_per_cell_part, prm.particle_integration_steps,
                prm.time_step, removal_order=ORDER_VECTOR, n_threads=cores)
     o.seed(V)
+    for _ in range(warmup):
+        o.step(V, Vold)
     done, ps, t = 0, 0, 0.0
     while t < budget_s and (max_steps is None or done < max_steps):
         n = o.stats()["n_particles"]
@@ -234,9 +237,10 @@ def run_reference(args):
         return 0
     m, V, Vold, prm = build_case()
     budget = 60.0
-    cb = cpu_baseline(m, V, Vold, prm, budget_s=budget, max_steps=max(1, args.steps))
+    warm = min(args.warmup, 3)  # CPU steps: a few suffice to settle caches and threads
+    cb = cpu_baseline(m, V, Vold, prm, budget_s=budget, max_steps=max(1, args.steps), warmup=warm)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-            "steps": cb["steps"], "warmup": 0, "ms_per_step": 1000.0 * cb["seconds"] / cb["steps"],
+            "steps": cb["steps"], "warmup": warm, "ms_per_step": 1000.0 * cb["seconds"] / cb["steps"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": WORKLOAD, "form": "fp64 CPU restatement"},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
