@@ -163,11 +163,12 @@ int pfem2gpu_launch_count(pfem2gpu_handle* h, uint64_t* count);
  *
  * The call runs on `stream` (a cudaStream_t; NULL = the default stream) and
  * returns after its work there has finished.  Calls on one device share the
- * one scratch array: the library serialises them with a lock, so they never
- * overlap; a caller that runs its own kernels on the scratch's results does
- * not exist (the results are only V_out).  A stream that is being captured
- * into a CUDA graph is refused (PFEM2GPU_ERR_STATE).  The first call on a
- * device looks up the scratch array's address (cudaGetSymbolAddress) there.
+ * one scratch array, so two calls in flight at once would race on it; the
+ * library prevents that with a per-device lock held until the call's work
+ * has finished, so concurrent callers wait for each other.  A stream that is
+ * being captured into a CUDA graph is refused (PFEM2GPU_ERR_STATE).  The
+ * first call on a device looks up the scratch array's address
+ * (cudaGetSymbolAddress) with that device current.
  * The sums are those of the FP64 form: V_out equals pfem2gpu_project of an
  * FP64 handle that holds the same particles in the same order, bit for bit.
  */

@@ -1,0 +1,236 @@
+// pfem2gpu_handler.hpp -- C++ mirror of pfem2ParticleHandler<dim> over the C ABI.
+//
+// Same public method names and call sequence as the reference class
+// (src/pfem2particlehandler.h:17-71): the solver-side inputs that the
+// reference fetches through its pfem2Solver pointer (mesh, parameters, the
+// FEM velocity vectors getSolutionV/getOldSolutionV/setSolutionV,
+// src/pfem2fem.cpp:622-644) are bound once instead, so that
+//
+//     handler.seed_particles();
+//     handler.initialize_maps();
+//     for (...) {
+//         handler.correct_particle_velocity();
+//         handler.move_particles();
+//         handler.project_particle_fields();
+//         ...
+//     }
+//
+// reads as src/pfem2solver.cpp:155-164 does.  Errors throw pfem2gpu::Error
+// (the reference throws deal.II exceptions); no CUDA type appears here.
+// Header-only; link with libpfem2gpu.so.
+#ifndef PFEM2GPU_HANDLER_HPP
+#define PFEM2GPU_HANDLER_HPP
+
+#include <array>
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "pfem2gpu.h"
+
+namespace pfem2gpu {
+
+class Error : public std::runtime_error {
+public:
+    Error(int code, const std::string& what) : std::runtime_error(what), code(code) {}
+    int code;
+};
+
+inline void check(int rc, pfem2gpu_handle* h = nullptr)
+{
+    if (rc == PFEM2GPU_OK) return;
+    std::string msg = std::string("pfem2gpu: ") + pfem2gpu_error_string(rc);
+    if (h) {
+        char buf[512] = {0};
+        if (pfem2gpu_last_error(h, buf, sizeof buf) == PFEM2GPU_OK && buf[0]) msg += std::string(": ") + buf;
+    }
+    throw Error(rc, msg);
+}
+
+// Q1 mesh in deal.II numbering: vertices (n_verts x dim), and per cell the
+// 2^dim vertex indices (cell->vertex_index(i)) and vertex DoFs
+// (cell->vertex_dof_index(i, 0)) in lexicographic vertex order.
+struct Mesh {
+    int64_t n_cells = 0, n_verts = 0, n_dofs = 0;
+    std::vector<double> vertices;
+    std::vector<int32_t> cell_vertices, cell_dofs;
+};
+
+// The particle record of the reference (src/pfem2particle.h:63-72), without
+// the per-particle DoF copy (the cell's DoFs are a per-cell table here).
+template <int dim>
+struct Particle {
+    uint32_t id = 0;
+    int32_t cell = 0;
+    std::array<double, dim> location{}, reference_location{}, velocity{};
+};
+
+template <int dim>
+class ParticleHandler {
+public:
+    static_assert(dim == 2 || dim == 3, "dim must be 2 or 3");
+
+    // pfem2ParticleHandler(fe) + setPfem2Solver (src/pfem2particlehandler.cpp:10-15,30-40):
+    // the particle keys of the .prm file and the form (PFEM2GPU_FP64 / PFEM2GPU_FP32).
+    explicit ParticleHandler(const pfem2gpu_params& params, int precision = PFEM2GPU_FP64)
+    {
+        check(pfem2gpu_create(dim, precision, &params, &h_));
+    }
+    ~ParticleHandler()
+    {
+        if (h_) pfem2gpu_destroy(h_);
+    }
+    ParticleHandler(const ParticleHandler&) = delete;
+    ParticleHandler& operator=(const ParticleHandler&) = delete;
+
+    // The mesh the reference borrows from its solver.
+    void set_mesh(const Mesh& m)
+    {
+        mesh_ = m;
+        maps_ = false;
+    }
+    // The FEM vectors, component-major V[d * n_dofs + dof] (the reference's
+    // std::array<TrilinosWrappers::MPI::Vector, dim> copied component by
+    // component); out receives the projection.  They must outlive the calls.
+    void set_solution_vectors(const double* V, const double* Vold, double* V_out)
+    {
+        V_ = V;
+        Vold_ = Vold;
+        Vout_ = V_out;
+    }
+
+    // initialize_maps (src/pfem2particlehandler.cpp:320-324): uploads the mesh;
+    // the library builds vertex_to_cells and the centre directions.
+    void initialize_maps()
+    {
+        if (maps_) return;
+        check(pfem2gpu_set_mesh(h_, mesh_.n_cells, mesh_.n_verts, mesh_.n_dofs, mesh_.vertices.data(),
+                                mesh_.cell_vertices.data(), mesh_.cell_dofs.data(), nullptr, nullptr, nullptr),
+              h_);
+        maps_ = true;
+    }
+
+    // seed_particles (:43-109).  The reference seeds before initialize_maps;
+    // the mesh is uploaded here when that has not happened yet.
+    void seed_particles()
+    {
+        initialize_maps();
+        check(pfem2gpu_seed(h_, need(V_)), h_);
+    }
+    // correct_particle_velocity (:112-139).
+    void correct_particle_velocity() { check(pfem2gpu_correct(h_, need(V_), need(Vold_)), h_); }
+    // move_particles (:142-171), with the velocity of the last seed/correct.
+    void move_particles() { check(pfem2gpu_move(h_, nullptr), h_); }
+    // project_particle_fields (:174-215) into the bound output vector.
+    void project_particle_fields() { check(pfem2gpu_project(h_, need(Vout_)), h_); }
+
+    // Explicit-vector forms of the same calls.
+    void seed_particles(const double* V)
+    {
+        initialize_maps();
+        check(pfem2gpu_seed(h_, V), h_);
+    }
+    void correct_particle_velocity(const double* V, const double* Vold) { check(pfem2gpu_correct(h_, V, Vold), h_); }
+    void move_particles(const double* V) { check(pfem2gpu_move(h_, V), h_); }
+    void project_particle_fields(double* V_out) { check(pfem2gpu_project(h_, V_out), h_); }
+
+    // output_particle_solution (:218-317) for one rank: particles-NN.000.vtu + particles-NN.pvtu.
+    void output_particle_solution(int timestep_number, const std::string& directory = ".")
+    {
+        char base[64];
+        std::snprintf(base, sizeof base, "particles-%02d", timestep_number);
+        const std::string dir = directory.empty() ? std::string(".") : directory;
+        check(pfem2gpu_write_vtu(h_, (dir + "/" + base + ".000.vtu").c_str()), h_);
+        std::ofstream f(dir + "/" + base + ".pvtu");
+        f << "<?xml version=\"1.0\" ?> \n<VTKFile type=\"PUnstructuredGrid\" version=\"0.1\" "
+             "byte_order=\"LittleEndian\">\n  <PUnstructuredGrid GhostLevel=\"0\">\n"
+             "    <PPointData Scalars=\"scalars\">\n"
+             "      <PDataArray type=\"Float32\" Name=\"velocity\" NumberOfComponents=\"3\" format=\"ascii\"/>\n"
+             "      <PDataArray type=\"Float32\" Name=\"subdomain\" format=\"ascii\"/>\n"
+             "    </PPointData>\n    <PPoints>\n"
+             "      <PDataArray type=\"Float32\" NumberOfComponents=\"3\"/>\n    </PPoints>\n"
+          << "    <Piece Source=\"" << base << ".000.vtu\"/>  </PUnstructuredGrid>\n</VTKFile>\n";
+        if (!f) throw Error(PFEM2GPU_ERR_ARG, "pfem2gpu: cannot write " + dir + "/" + base + ".pvtu");
+    }
+
+    // begin()/end(): a host copy of the particles, in the device order
+    // (cells ascending).
+    std::vector<Particle<dim>> particles()
+    {
+        int64_t n = 0;  // count query: ERR_ARG (arrays too small) still sets n
+        const int rc = pfem2gpu_get_particles(h_, nullptr, nullptr, nullptr, nullptr, nullptr, 0, &n);
+        if (rc != PFEM2GPU_ERR_ARG) check(rc, h_);
+        std::vector<uint32_t> id(n);
+        std::vector<int32_t> cell(n);
+        std::vector<double> x(n * dim), xi(n * dim), v(n * dim);
+        check(pfem2gpu_get_particles(h_, id.data(), cell.data(), x.data(), xi.data(), v.data(), n, &n), h_);
+        std::vector<Particle<dim>> out(n);
+        for (int64_t p = 0; p < n; ++p) {
+            out[p].id = id[p];
+            out[p].cell = cell[p];
+            for (int d = 0; d < dim; ++d) {
+                out[p].location[d] = x[p * dim + d];
+                out[p].reference_location[d] = xi[p * dim + d];
+                out[p].velocity[d] = v[p * dim + d];
+            }
+        }
+        return out;
+    }
+
+    // clear_particles / insert_particle (:327-344): collected on the host and
+    // uploaded by the next call of commit_particles().
+    void clear_particles() { pending_.clear(); }
+    void insert_particle(const Particle<dim>& p) { pending_.push_back(p); }
+    void commit_particles(uint32_t next_id)
+    {
+        initialize_maps();
+        const size_t n = pending_.size();
+        std::vector<uint32_t> id(n);
+        std::vector<int32_t> cell(n);
+        std::vector<double> x(n * dim), xi(n * dim), v(n * dim);
+        for (size_t p = 0; p < n; ++p) {
+            id[p] = pending_[p].id;
+            cell[p] = pending_[p].cell;
+            for (int d = 0; d < dim; ++d) {
+                x[p * dim + d] = pending_[p].location[d];
+                xi[p * dim + d] = pending_[p].reference_location[d];
+                v[p * dim + d] = pending_[p].velocity[d];
+            }
+        }
+        check(pfem2gpu_set_particles(h_, (int64_t)n, id.data(), cell.data(), x.data(), xi.data(), v.data(), next_id),
+              h_);
+        pending_.clear();
+    }
+
+    pfem2gpu_stats stats()
+    {
+        pfem2gpu_stats s{};
+        check(pfem2gpu_get_stats(h_, &s), h_);
+        return s;
+    }
+    void synchronize() { check(pfem2gpu_synchronize(h_), h_); }
+    pfem2gpu_handle* handle() const { return h_; }
+
+private:
+    template <typename T>
+    static T* need(T* p)
+    {
+        if (!p) throw Error(PFEM2GPU_ERR_STATE, "pfem2gpu: solution vectors not bound (set_solution_vectors)");
+        return p;
+    }
+
+    pfem2gpu_handle* h_ = nullptr;
+    Mesh mesh_;
+    bool maps_ = false;
+    const double* V_ = nullptr;
+    const double* Vold_ = nullptr;
+    double* Vout_ = nullptr;
+    std::vector<Particle<dim>> pending_;
+};
+
+}  // namespace pfem2gpu
+
+#endif

@@ -1,0 +1,92 @@
+"""The C++ mirror of pfem2ParticleHandler (include/pfem2gpu_handler.hpp),
+driven through the reference's call sequence by tests/cpp/handler_driver.cpp:
+it compiles and links against libpfem2gpu.so, reports a missing device as an
+exception, and on a GPU gives the oracle's particles bit for bit (FP64 form).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from pfem2dealii_b200 import _lib
+
+from . import cases
+from .cases import by_id
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.dirname(_lib.LIB_PATH)
+
+
+def _compile(tmp_path):
+    exe = str(tmp_path / "handler_driver")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "handler_driver.cpp"), "-L", LIBDIR, "-lpfem2gpu",
+           f"-Wl,-rpath,{LIBDIR}", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def _write_input(path, case, steps, precision=0):
+    m = case.mesh
+    q = list(case.q) + [1] * (3 - len(case.q))
+    hd = np.array([m.dim, precision, m.n_cells, m.n_verts, m.n_dofs, steps, *q, case.max_per_part, case.substeps],
+                  np.int64)
+    with open(path, "wb") as f:
+        f.write(hd.tobytes())
+        f.write(np.float64(case.dt).tobytes())
+        for a, t in ((m.vertices, np.float64), (m.cells, np.int32), (m.cell_dofs, np.int32), (case.V, np.float64),
+                     (case.Vold, np.float64)):
+            f.write(np.ascontiguousarray(a, t).tobytes())
+
+
+def _read_output(path, case, steps):
+    dim, nD = case.mesh.dim, case.mesh.n_dofs
+    raw = open(path, "rb").read()
+    off = steps * dim * nD * 8
+    V = np.frombuffer(raw[:off], np.float64).reshape(steps, dim, nD)
+    n = int(np.frombuffer(raw[off:off + 8], np.int64)[0])
+    off += 8
+    P = {}
+    for k, t, w in (("id", np.uint32, 1), ("cell", np.int32, 1), ("x", np.float64, dim), ("xi", np.float64, dim),
+                    ("v", np.float64, dim)):
+        a = np.frombuffer(raw[off:off + n * w * np.dtype(t).itemsize], t)
+        off += a.nbytes
+        P[k] = a.reshape(n, w) if w > 1 else a
+    return V, P
+
+
+def test_cpp_mirror_builds_and_reports_no_device(tmp_path):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    exe = _compile(tmp_path)
+    c = cases.channel(8, 4)
+    _write_input(tmp_path / "in.bin", c, 1)
+    r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], capture_output=True, text=True)
+    assert r.returncode == 10 + 6, (r.returncode, r.stderr)  # PFEM2GPU_ERR_NODEVICE, thrown as pfem2gpu::Error
+    assert "no CUDA device" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["channel", "duct"])
+def test_cpp_mirror_matches_oracle(tmp_path, which):
+    c = cases.channel(32, 8, dt=0.02) if which == "channel" else cases.duct(16, 6, 6, dt=0.05)
+    steps = 6
+    exe = _compile(tmp_path)
+    _write_input(tmp_path / "in.bin", c, steps)
+    r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    V, P = _read_output(tmp_path / "out.bin", c, steps)
+    o = cases.oracle_for(c)
+    o.seed(c.V)
+    for s in range(steps):
+        Vo = o.step(c.V, c.Vold)
+        assert np.array_equal(np.isnan(Vo), np.isnan(V[s]))
+        m = np.isfinite(Vo)
+        assert np.max(np.abs(Vo[m] - V[s][m])) <= 1e-12 * np.max(np.abs(Vo[m]))
+    a, b = by_id(o.particles()), by_id(P)
+    for k in ("id", "cell", "x", "xi", "v"):
+        assert np.array_equal(a[k], b[k].reshape(a[k].shape)), k
