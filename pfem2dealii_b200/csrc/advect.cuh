@@ -560,8 +560,10 @@ __device__ __noinline__ F3<DIM> newton32(const float* __restrict__ geo, uint32_t
 }
 
 // FP32 sub-steps s0.. in cell c; returns the sub-step that leaves the cell
-// (S if none).  xi is advanced in place.
-template <int DIM>
+// (S if none).  xi is advanced in place.  AFF: every cell of the mesh is
+// affine, so the Newton branch (an out-of-line call whose saved registers
+// would spill in the hot loop) is left out.
+template <int DIM, bool AFF = false>
 __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi)
 {
     Rec32<DIM> r;
@@ -572,7 +574,7 @@ __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0,
         float w[DIM], dl[DIM], y[DIM];
         eval_poly<DIM>(r.b, xi, w);
         bool ok = true;
-        if (r.affine) {
+        if (AFF || r.affine) {
 #pragma unroll
             for (int d = 0; d < DIM; ++d) dl[d] = dtp * w[d];
         } else {
@@ -596,8 +598,8 @@ __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0,
     return s;
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(256, 3) k_advect32(StepArgs a)
+template <int DIM, bool AFF>
+__global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
 {
     extern __shared__ __align__(128) unsigned char adv_raw[];
     __shared__ uint64_t bar[2];
@@ -628,7 +630,7 @@ __global__ void __launch_bounds__(256, 3) k_advect32(StepArgs a)
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) v[d] += dv[d];
                 }
-                s = substeps32<DIM>(a, c, 0, xi);
+                s = substeps32<DIM, AFF>(a, c, 0, xi);
                 want = s < a.pp.S;
             }
 #pragma unroll

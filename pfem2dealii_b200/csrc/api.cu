@@ -29,6 +29,8 @@ struct pfem2gpu_handle {
             *d2c_ent = nullptr;
     double *verts = nullptr, *cellX = nullptr, *aff = nullptr, *v2c_dirs = nullptr;
     float* geo32 = nullptr;
+    uint32_t* twisted = nullptr;  // cells whose map is not affine (set by cell_setup)
+    bool all_affine = false;
     // velocities
     double *Vstage = nullptr, *Vstage2 = nullptr, *Vout = nullptr;
     void *Vc = nullptr, *dVc = nullptr;
@@ -158,6 +160,7 @@ StepArgs args(pfem2gpu_handle* h)
 {
     StepArgs a{};
     a.mesh.nC = h->nC;
+    a.mesh.all_affine = h->all_affine ? 1 : 0;
     a.mesh.nV = h->nV;
     a.mesh.nD = h->nD;
     a.mesh.cv = h->cv;
@@ -541,7 +544,7 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
                     (void*)h->key, (void*)h->next, (void*)h->xtmp, (void*)h->head, (void*)h->cs0, (void*)h->cs1,
                     (void*)h->carr, (void*)h->carrs, (void*)h->ccount, (void*)h->cocc, (void*)h->cub, (void*)h->coff,
                     (void*)h->tiles64, (void*)h->gscr, (void*)h->jinv32, (void*)h->xq, (void*)h->nxq,
-                    (void*)h->vrec32, (void*)h->dvrec32, h->partials, (void*)h->stats})
+                    (void*)h->vrec32, (void*)h->dvrec32, h->partials, (void*)h->stats, (void*)h->twisted})
         dfree(p);
     free_state(h->S0);
     free_state(h->S1);
@@ -641,7 +644,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
                     (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vc, h->dVc,
                     (void*)h->head, (void*)h->cs0, (void*)h->cs1, (void*)h->carr, (void*)h->carrs,
                     (void*)h->ccount, (void*)h->cocc, (void*)h->cub, (void*)h->coff, (void*)h->tiles64,
-                    (void*)h->jinv32, (void*)h->vrec32, (void*)h->dvrec32, h->partials})
+                    (void*)h->jinv32, (void*)h->vrec32, (void*)h->dvrec32, h->partials, (void*)h->twisted})
         dfree(p);
     h->has_mesh = false;
     h->nC = (int)n_cells;
@@ -688,6 +691,8 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
         CK(cudaMemsetAsync(h->dvrec32, 0, nc * rec * 4, h->stream));
     }
     CK(dalloc(&h->jinv32, nc * (dim == 3 ? 12 : 8)));
+    CK(dalloc(&h->twisted, 1));
+    CK(cudaMemsetAsync(h->twisted, 0, 4, h->stream));
     CK(cudaMalloc(&h->partials, nc * PW * esize(h)));
     CK(cudaMemcpyAsync(h->cv, cell_vertices, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->cd, cell_dofs, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
@@ -702,8 +707,14 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     run(h, "fill", [&] { return launch_fill_u32(h->head, (uint32_t)nc, LOST, h->stream); });
     CK(cudaMemsetAsync(h->Vstage, 0, nd * dim * 8, h->stream));
     run(h, "cell_setup",
-        [&] { return launch_cell_setup(dim, h->nC, h->verts, h->cv, h->cellX, h->aff, h->geo32, h->jinv32, h->stream); });
+        [&] {
+            return launch_cell_setup(dim, h->nC, h->verts, h->cv, h->cellX, h->aff, h->geo32, h->jinv32, h->twisted,
+                                     h->stream);
+        });
+    uint32_t twisted = 0;
+    CK(cudaMemcpyAsync(&twisted, h->twisted, 4, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));  // host vectors above go out of scope
+    h->all_affine = twisted == 0;
     h->has_mesh = true;
     h->vaos_valid = false;
     h->gen++;

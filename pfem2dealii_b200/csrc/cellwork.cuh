@@ -178,21 +178,28 @@ __device__ __forceinline__ void partial_row(Real (*tr)[TRW], int row, const Real
     }
 }
 
+// Column sums of up to 32 partial rows into acc (lane = column).  FP64:
+// the rows in order, as the oracle adds them.  FP32: a pairwise tree over the
+// 32 rows (empty rows read as 0), then one compensated add into acc.
 template <int DIM, typename Real>
 __device__ __forceinline__ void partial_sum_rows(Real (*tr)[TRW], int rows, int lane, PartialAcc<Real>& acc)
 {
     constexpr int PW = Dims<DIM>::PW;
     if (lane < PW) {
-        for (int r = 0; r < rows; ++r) {
-            const Real t = tr[r][lane];
-            if constexpr (std::is_same<Real, double>::value) {
-                acc.s = acc.s + t;
-            } else {  // Kahan
-                const float y = t - acc.c;
-                const float s = acc.s + y;
-                acc.c = (s - acc.s) - y;
-                acc.s = s;
-            }
+        if constexpr (std::is_same<Real, double>::value) {
+            for (int r = 0; r < rows; ++r) acc.s = acc.s + tr[r][lane];
+        } else {
+            float t[32];
+#pragma unroll
+            for (int r = 0; r < 32; ++r) t[r] = r < rows ? tr[r][lane] : 0.0f;
+#pragma unroll
+            for (int w = 16; w >= 1; w >>= 1)
+#pragma unroll
+                for (int r = 0; r < w; ++r) t[r] = t[r] + t[r + w];
+            const float y = t[0] - acc.c;
+            const float s = acc.s + y;
+            acc.c = (s - acc.s) - y;
+            acc.s = s;
         }
     }
 }
@@ -244,8 +251,8 @@ __device__ __forceinline__ void partials_of_range(const StepArgs& a, const PartS
 template <int DIM, typename Real>
 struct WrCfg {
     static constexpr bool HX = std::is_same<Real, double>::value;
-    static constexpr int CHC = HX ? 4 : WR_CHC;   // cells per chunk
-    static constexpr int UCAP = HX ? 128 : 256;   // staged particles per chunk
+    static constexpr int CHC = WR_CHC;   // cells per chunk
+    static constexpr int UCAP = 128;     // staged particles per chunk
 };
 
 template <int DIM, typename Real>

@@ -22,9 +22,9 @@ constexpr int OCCW_MAX = 4;    // 64-bit part-occupancy words per cell
 constexpr int ARRCAP = 4;      // arrival slots per cell before the overflow list
 constexpr int CELL_WARPS = 4;  // warps per block of the warp-per-cell helper kernels
 constexpr int KEY_CACHE = 128; // (part, key) pairs cached per warp on the general path
-constexpr int ADV_CH = 1024;   // particles per staged chunk of the advect pass
+constexpr int ADV_CH = 768;    // particles per staged chunk of the FP32 advect pass
 constexpr int WR_WARPS = 4;    // write pass: warps per block
-constexpr int WR_CHC = 8;      // write pass: cells per warp chunk
+constexpr int WR_CHC = 4;      // write pass: cells per warp chunk
 
 // error_flags bits
 constexpr uint32_t ERR_CAPACITY = 1u;        // more particles than the arrays hold
@@ -54,6 +54,7 @@ struct DevStats {
 
 struct MeshDev {
     int nC, nV, nD;
+    int all_affine;           // 1 if every cell's multilinear map is affine (no twist terms)
     const int32_t* cv;        // nC x NV vertex ids
     const int32_t* cd;        // nC x NV DoF ids
     const double* cellX;      // nC x NV x DIM vertex coordinates, cell-major

@@ -40,8 +40,13 @@ template <int DIM>
 static int advect32_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = 2 * (int)sizeof(AdvStage<DIM, float, ADV_CH>);
-    static const int grid = smem_grid32(k_advect32<DIM>, 256, smem);
-    k_advect32<DIM><<<grid, 256, smem, s>>>(a);
+    if (a.mesh.all_affine) {
+        static const int grid = smem_grid32(k_advect32<DIM, true>, 256, smem);
+        k_advect32<DIM, true><<<grid, 256, smem, s>>>(a);
+    } else {
+        static const int grid = smem_grid32(k_advect32<DIM, false>, 256, smem);
+        k_advect32<DIM, false><<<grid, 256, smem, s>>>(a);
+    }
     k_cross32<DIM><<<PFEM2_GRID(k_cross32<DIM>, 128), 128, 0, s>>>(a);
     return 2;
 }

@@ -13,7 +13,7 @@ namespace {
 template <int DIM>
 __global__ void k_cell_setup(int nC, const double* __restrict__ verts, const int32_t* __restrict__ cv,
                              double* __restrict__ cellX, double* __restrict__ aff, float* __restrict__ geo32,
-                             float* __restrict__ jinv32)
+                             float* __restrict__ jinv32, uint32_t* __restrict__ twisted)
 {
     constexpr int NV = 1 << DIM, GS = Dims<DIM>::GEO, JS = Dims<DIM>::JS;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nC; c += gridDim.x * blockDim.x) {
@@ -73,6 +73,7 @@ __global__ void k_cell_setup(int nC, const double* __restrict__ verts, const int
             for (int q = 0; q < DIM; ++q) jj[r * DIM + q] = (float)Ji[r][q];
         for (int k = DIM * DIM; k < JS; ++k) jj[k] = 0.0f;
         jj[DIM * DIM] = affine ? 1.0f : 0.0f;
+        if (!affine) atomicAdd(twisted, 1u);
     }
 }
 
@@ -88,11 +89,11 @@ int seed_t(const StepArgs& a, uint32_t* cs, cudaStream_t s)
 }  // namespace
 
 int launch_cell_setup(int dim, int nC, const double* verts, const int32_t* cv, double* cellX, double* aff,
-                      float* geo32, float* jinv32, cudaStream_t s)
+                      float* geo32, float* jinv32, uint32_t* twisted, cudaStream_t s)
 {
     const int grid = (nC + 127) / 128;
-    if (dim == 2) k_cell_setup<2><<<grid, 128, 0, s>>>(nC, verts, cv, cellX, aff, geo32, jinv32);
-    else k_cell_setup<3><<<grid, 128, 0, s>>>(nC, verts, cv, cellX, aff, geo32, jinv32);
+    if (dim == 2) k_cell_setup<2><<<grid, 128, 0, s>>>(nC, verts, cv, cellX, aff, geo32, jinv32, twisted);
+    else k_cell_setup<3><<<grid, 128, 0, s>>>(nC, verts, cv, cellX, aff, geo32, jinv32, twisted);
     return 1;
 }
 

@@ -31,7 +31,7 @@ inline int occupancy_grid(const void* kernel, int threads, size_t smem = 0)
 
 // kernels_f64.cu / kernels_f32.cu (prec: 0 = FP64 form, 1 = FP32 form)
 int launch_cell_setup(int dim, int nC, const double* verts, const int32_t* cv, double* cellX, double* aff,
-                      float* geo32, float* jinv32, cudaStream_t s);
+                      float* geo32, float* jinv32, uint32_t* twisted, cudaStream_t s);
 int launch_seed(int dim, int prec, const StepArgs& a, uint32_t* cell_start, cudaStream_t s);
 int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s);
 int launch_write(int dim, int prec, const StepArgs& a, cudaStream_t s);
