@@ -350,8 +350,7 @@ void swap_state(pfem2gpu_handle* h)
 // the counters of the step.
 int enqueue_write(pfem2gpu_handle* h, StepArgs& a, int count_step)
 {
-    run(h, "cell_slots", [&] { return launch_cell_slots(a, h->stream); });
-    run(h, "scan_slots", [&] { return launch_scan_u64(h->cub, h->nC, h->coff, h->tiles64, h->stream); });
+    run(h, "slots_scan", [&] { return launch_slots_scan(a, h->tiles64, h->stream); });
     run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->stream); });
     run(h, "finalize", [&] { return launch_finalize(a, count_step, h->stream); });
     return PFEM2GPU_OK;
@@ -573,7 +572,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     if (n_cells < 1 || n_verts < 1 || n_dofs < 1 || n_cells > (1ll << 30) || n_verts > (1ll << 30) ||
         n_dofs > (1ll << 30))
         return fail(h, PFEM2GPU_ERR_ARG, "mesh sizes out of range");
-    if ((n_cells + 2047) / 2048 > SCAN_MAX_TILES) return fail(h, PFEM2GPU_ERR_ARG, "too many cells");
+    if ((n_cells + SCAN_TILE - 1) / SCAN_TILE > SCAN_MAX_TILES) return fail(h, PFEM2GPU_ERR_ARG, "too many cells");
     if (h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "mesh change with live particles");
     const int dim = h->dim, NV = 1 << dim;
     for (int64_t k = 0; k < n_cells * NV; ++k) {

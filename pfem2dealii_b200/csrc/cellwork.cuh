@@ -532,14 +532,20 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
             const uint32_t ub = (uint32_t)ubw, nseed_expect = (uint32_t)(ubw >> 32);
             const uint32_t off = (uint32_t)ofw, sb = (uint32_t)(ofw >> 32);
             if (lane == 0) a.cs_new[c] = off;
-            bool fast = L <= 32 && ub <= 32;
-            // stayers compacted to lanes 0..ns-1, arrivals after them
-            const bool stay =
-                fast && (uint32_t)lane < L && (staged ? w.key[s0 - S + lane] : a.key[s0 + lane]) == c;
-            const unsigned stm = __ballot_sync(0xffffffffu, stay);
-            const uint32_t ns = __popc(stm);
-            const uint32_t n = ns + na;
-            fast = fast && n <= 32;
+            // Virtual slots u = 32 r + lane (two rounds of the warp): u < L
+            // the cell's old slots (a stayer where its key is c), L <= u < L +
+            // na the arrivals.  Cells beyond 64 take the general path.
+            const bool fast = L + na <= 64 && ub <= 64;
+            const bool two = L + na > 32;  // warp-uniform: a second round is needed
+            bool is_stay[2];
+            unsigned stm[2];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const uint32_t u = 32u * r + (uint32_t)lane;
+                is_stay[r] = fast && (r == 0 || two) && u < L &&
+                             (staged ? w.key[s0 - S + u] : a.key[s0 + u]) == c;
+                stm[r] = __ballot_sync(0xffffffffu, is_stay[r]);
+            }
             if (!fast) {
                 const uint2 gr = write_cell_general<DIM, Real>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0,
                                                                lane);
@@ -550,78 +556,118 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
                 __syncwarp();
                 continue;
             }
-            // lanes: the segment's stayers in place when segment + arrivals fit in
-            // 32 lanes (else compacted), arrivals after the segment
-            const bool spread = L + na <= 32;
-            const uint32_t abase = spread ? L : ns;
-            const bool is_stay = spread ? stay : (uint32_t)lane < ns;
-            const bool is_arr = (uint32_t)lane >= abase && (uint32_t)lane < abase + na;
-            const bool valid = is_stay || is_arr;
-            PData<DIM, Real> pd;
-            pd.i = 0;
-            pd.id = 0;
+            const uint32_t ns = __popc(stm[0]) + __popc(stm[1]);
+            const uint32_t n = ns + na;
+            PData<DIM, Real> pd[2];
+            bool is_arr[2], valid[2];
+            int pe[2];
+            uint32_t key[2];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) pd.xi[d] = pd.v[d] = Real(0);
-            if (is_stay) {
-                const uint32_t src = spread ? (uint32_t)lane : __fns(stm, 0, lane + 1);
-                if (staged) load_stage<DIM, Real>(w, s0 - S + src, s0 + src, pd);
-                else load_global<DIM, Real>(a, s0 + src, pd);
-            } else if (is_arr) {
-                const uint32_t ia = arrival(a, c, lane - abase, h);
-                if (ia < cap) load_global<DIM, Real>(a, ia, pd);
-                else err |= ERR_ARRIVAL;
+            for (int r = 0; r < 2; ++r) {
+                const uint32_t u = 32u * r + (uint32_t)lane;
+                is_arr[r] = (r == 0 || two) && u >= L && u < L + na;
+                valid[r] = is_stay[r] || is_arr[r];
+                pd[r].i = 0;
+                pd[r].id = 0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) pd[r].xi[d] = pd[r].v[d] = Real(0);
+                if (is_stay[r]) {
+                    if (staged) load_stage<DIM, Real>(w, s0 - S + u, s0 + u, pd[r]);
+                    else load_global<DIM, Real>(a, s0 + u, pd[r]);
+                } else if (is_arr[r]) {
+                    const uint32_t ia = arrival(a, c, u - L, h);
+                    if (ia < cap) load_global<DIM, Real>(a, ia, pd[r]);
+                    else err |= ERR_ARRIVAL;
+                }
+                pe[r] = valid[r] ? ext_part<DIM, Real>(pd[r].xi, a.pp) : 0;
+                key[r] = valid[r] ? key_of(pd[r].id, a.pp.seed) : 0xffffffffu;
             }
-            const int pe = valid ? ext_part<DIM, Real>(pd.xi, a.pp) : 0;
-            const uint32_t key = valid ? key_of(pd.id, a.pp.seed) : 0xffffffffu;
             int* cnt = w.cnt;
             for (int p = lane; p < a.pp.npe; p += 32) cnt[p] = 0;
             __syncwarp();
-            if (valid) atomicAdd(cnt + pe, 1);
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+                if (valid[r]) atomicAdd(cnt + pe[r], 1);
             __syncwarp();
-            const int kme = valid ? cnt[pe] : 0;
+            int kme[2], rank[2] = {0, 0};
+            unsigned validm[2];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                kme[r] = valid[r] ? cnt[pe[r]] : 0;
+                validm[r] = __ballot_sync(0xffffffffu, valid[r]);
+            }
             // rank inside an over-full part (by key)
-            const unsigned validm = __ballot_sync(0xffffffffu, valid);
-            int rank = 0;
-            if (__any_sync(0xffffffffu, apply && kme > maxpp + 1)) {
-                for (int l = 0; l < 32; ++l) {
-                    const int pl = __shfl_sync(0xffffffffu, pe, l);
-                    const uint32_t kl = __shfl_sync(0xffffffffu, key, l);
-                    rank += (((validm >> l) & 1u) && pl == pe && kl < key) ? 1 : 0;
+            if (__any_sync(0xffffffffu, apply && (kme[0] > maxpp + 1 || kme[1] > maxpp + 1))) {
+#pragma unroll
+                for (int r2 = 0; r2 < 2; ++r2) {
+                    if (r2 == 1 && !two) break;
+                    for (int l = 0; l < 32; ++l) {
+                        const int pl = __shfl_sync(0xffffffffu, pe[r2], l);
+                        const uint32_t kl = __shfl_sync(0xffffffffu, key[r2], l);
+                        const bool vl = (validm[r2] >> l) & 1u;
+#pragma unroll
+                        for (int r = 0; r < 2; ++r) rank[r] += (vl && pl == pe[r] && kl < key[r]) ? 1 : 0;
+                    }
                 }
             }
-            const bool surv = valid && rank < survivors(kme, maxpp, apply);
             // order: stayers (slot order), then arrivals by key
             const unsigned ltm = (1u << lane) - 1u;
-            uint32_t seq = is_stay ? (spread ? (uint32_t)__popc(stm & ltm) : (uint32_t)lane) : 0u;
-            if (is_arr) seq = ns + (uint32_t)lane - abase;
+            uint32_t seq[2];
+            seq[0] = is_stay[0] ? (uint32_t)__popc(stm[0] & ltm) : ns + (uint32_t)lane - L;
+            seq[1] = is_stay[1] ? (uint32_t)(__popc(stm[0]) + __popc(stm[1] & ltm)) : ns + 32u + (uint32_t)lane - L;
             if (na > 1) {
-                uint32_t ar = 0;
-                for (uint32_t l = abase; l < abase + na; ++l) {
-                    const uint32_t kl = __shfl_sync(0xffffffffu, key, l);
-                    ar += (kl < key) ? 1u : 0u;
+                uint32_t ar[2] = {0u, 0u};
+                for (uint32_t t = 0; t < na; ++t) {
+                    const uint32_t u2 = L + t;
+                    const uint32_t k0 = __shfl_sync(0xffffffffu, key[0], (int)(u2 & 31u));
+                    const uint32_t k1 = __shfl_sync(0xffffffffu, key[1], (int)(u2 & 31u));
+                    const uint32_t kl = (u2 >> 5) ? k1 : k0;
+#pragma unroll
+                    for (int r = 0; r < 2; ++r) ar[r] += (kl < key[r]) ? 1u : 0u;
                 }
-                if (is_arr) seq = ns + ar;
+#pragma unroll
+                for (int r = 0; r < 2; ++r)
+                    if (is_arr[r]) seq[r] = ns + ar[r];
             }
-            const unsigned survm = __ballot_sync(0xffffffffu, surv);
-            const uint32_t nsurv = __popc(survm);
-            uint32_t pos = seq;
+            bool surv[2];
+            unsigned survm[2];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                surv[r] = valid[r] && rank[r] < survivors(kme[r], maxpp, apply);
+                survm[r] = __ballot_sync(0xffffffffu, surv[r]);
+            }
+            const uint32_t nsurv = __popc(survm[0]) + __popc(survm[1]);
+            uint32_t pos[2] = {seq[0], seq[1]};
             if (nsurv != n) {  // removals: survivors before in sequence order
-                pos = 0;
-                for (int l = 0; l < 32; ++l) {
-                    const uint32_t sl = __shfl_sync(0xffffffffu, seq, l);
-                    pos += (((survm >> l) & 1u) && sl < seq) ? 1u : 0u;
+                pos[0] = pos[1] = 0;
+#pragma unroll
+                for (int r2 = 0; r2 < 2; ++r2) {
+                    if (r2 == 1 && !two) break;
+                    for (int l = 0; l < 32; ++l) {
+                        const uint32_t sl = __shfl_sync(0xffffffffu, seq[r2], l);
+                        const bool bl = (survm[r2] >> l) & 1u;
+#pragma unroll
+                        for (int r = 0; r < 2; ++r) pos[r] += (bl && sl < seq[r]) ? 1u : 0u;
+                    }
                 }
             }
-            if (surv) {
-                const uint32_t dst = off + pos;
-                if (dst < cap) store_particle<DIM, Real>(a, dst, c, pd);
-                else err |= ERR_CAPACITY;
-                partial_row<DIM, Real>(w.tr, (int)pos, pd.xi, pd.v);
+            // partial rows in registers -> shared rows when the cell's final
+            // particles fit one row block, else re-read from the new layout
+            const bool rows = nsurv + nseed_expect <= 32u;
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                if (surv[r]) {
+                    const uint32_t dst = off + pos[r];
+                    if (dst < cap) store_particle<DIM, Real>(a, dst, c, pd[r]);
+                    else err |= ERR_CAPACITY;
+                    if (rows) partial_row<DIM, Real>(w.tr, (int)pos[r], pd[r].xi, pd[r].v);
+                }
+                removed += (valid[r] && !surv[r]) ? 1 : 0;
             }
-            removed += (valid && !surv) ? 1 : 0;
             uint32_t nseed = 0;
             if (nseed_expect) {
-                const uint2 sd = write_seeds<DIM, Real>(a, c, cnt, n, off + nsurv, id0, sb, w.tr, (int)nsurv, lane);
+                const uint2 sd = write_seeds<DIM, Real>(a, c, cnt, n, off + nsurv, id0, sb, rows ? w.tr : nullptr,
+                                                        (int)nsurv, lane);
                 nseed = sd.x;
                 err |= sd.y;
             }
@@ -630,9 +676,14 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
             if (fin > ub) err |= ERR_COUNT_UB;
             write_holes(a, off + fin, off + ub, lane);
             __syncwarp();
-            PartialAcc<Real> acc;
-            partial_sum_rows<DIM, Real>(w.tr, fin < 32u ? (int)fin : 32, lane, acc);
-            store_partial<DIM, Real>(a, c, acc, lane);
+            if (rows) {
+                PartialAcc<Real> acc;
+                partial_sum_rows<DIM, Real>(w.tr, fin < 32u ? (int)fin : 32, lane, acc);
+                store_partial<DIM, Real>(a, c, acc, lane);
+            } else {
+                __threadfence_block();
+                partials_of_range<DIM, Real>(a, a.S1, c, off, fin < ub ? fin : ub, w.tr, lane);
+            }
             reset_cell(a, c, lane);
             __syncwarp();
         }
@@ -678,6 +729,25 @@ __global__ void k_correct(StepArgs a)
     }
 }
 
+// The 4 values of one (cell, vertex) partial entry (16-byte aligned).
+__device__ __forceinline__ void load4(const float* p, float* q)
+{
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    q[0] = t.x;
+    q[1] = t.y;
+    q[2] = t.z;
+    q[3] = t.w;
+}
+__device__ __forceinline__ void load4(const double* p, double* q)
+{
+    const double2 t0 = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 t1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    q[0] = t0.x;
+    q[1] = t0.y;
+    q[2] = t1.x;
+    q[3] = t1.y;
+}
+
 // DoF gather: V_d = sum num_d / sum den over the cells sharing the DoF, in
 // ascending cell order, FP64 sums and division (0/0 -> NaN as the reference,
 // or the kept input value under empty_dof_policy 1).  Up to 8 cell entries
@@ -704,9 +774,8 @@ __global__ void k_gather(StepArgs a, int keep_empty)
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 const int32_t en = ent[j] < 0 ? 0 : ent[j];
-                const PReal* src = P + (size_t)(en / NV) * PW + (en % NV) * 4;
-#pragma unroll
-                for (int d = 0; d < 4; ++d) q[j][d] = ent[j] < 0 ? PReal(0) : src[d];
+                load4(P + (size_t)(en / NV) * PW + (en % NV) * 4, q[j]);  // one vector load per entry
+                if (ent[j] < 0) q[j][0] = q[j][1] = q[j][2] = q[j][3] = PReal(0);
             }
 #pragma unroll
             for (int j = 0; j < 8; ++j) {

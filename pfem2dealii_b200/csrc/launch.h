@@ -41,10 +41,11 @@ int launch_gather(int dim, int prec, const StepArgs& a, int keep_empty, cudaStre
 int launch_positions32(int dim, const StepArgs& a, double* xout, cudaStream_t s);
 
 // misc.cu
-constexpr int SCAN_MAX_TILES = 8192;   // top-level scan capacity (x 2048 elements)
-int launch_scan_u64(const unsigned long long* in, uint32_t n, unsigned long long* out, unsigned long long* tiles,
-                    cudaStream_t s);
-int launch_cell_slots(const StepArgs& a, cudaStream_t s);
+constexpr int SCAN_TILE = 1024;       // cells per tile of the slot-offset scan
+constexpr int SCAN_MAX_TILES = 8192;  // tile sums the scan buffer holds
+// Slots per cell (count + new particles) into cub, their exclusive scan into
+// coff (coff[nC] = totals); two kernels.
+int launch_slots_scan(const StepArgs& a, unsigned long long* tiles, cudaStream_t s);
 int launch_rekey(int dim, int prec, const StepArgs& a, cudaStream_t s);
 int launch_fill_u32(uint32_t* p, uint32_t n, uint32_t v, cudaStream_t s);
 int launch_finalize(const StepArgs& a, int count_step, cudaStream_t s);

@@ -11,8 +11,8 @@ namespace pfem2 {
 namespace {
 
 constexpr int SB = 256;              // scan block
-constexpr int SI = 8;                // items per thread
-constexpr int STILE = SB * SI;       // elements per tile
+constexpr int SI = SCAN_TILE / SB;   // rows of SB cells per tile
+constexpr int STILE = SCAN_TILE;     // cells per tile
 
 template <typename T>
 __device__ __forceinline__ T warp_incl_scan(T x)
@@ -48,76 +48,67 @@ __device__ __forceinline__ T block_excl_scan(T v, T& total)
     return wp + inc - v;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(SB) k_scan_reduce(const T* __restrict__ in, uint32_t n, T* __restrict__ tiles)
+// Slots needed per cell after the move (particles + new particles) and the
+// new particles alone, from the cell's count and part occupancy, packed as
+// new << 32 | slots so that one u64 scan gives both offsets.
+__device__ __forceinline__ unsigned long long cell_slot_word(const StepArgs& a, uint32_t c)
 {
-    const uint32_t base = blockIdx.x * STILE + threadIdx.x;
-    T s = 0;
+    const uint32_t n = a.ccount[c];
+    uint32_t seeds = 0;
+    if (a.apply_counts && n > 0) {
+        if (a.pp.maxpp < 0) {
+            seeds = (uint32_t)a.pp.npart;
+        } else {
+            for (int w = 0; w < a.pp.occw; ++w)
+                seeds += __popcll(a.pp.realmask[w] & ~a.cocc[(size_t)c * a.pp.occw + w]);
+        }
+    }
+    return ((unsigned long long)seeds << 32) | (unsigned long long)(n + seeds);
+}
+
+// Pass 1: every cell's slot word (stored to cub) and each tile's sum.
+__global__ void __launch_bounds__(SB) k_slots_reduce(StepArgs a, unsigned long long* __restrict__ tiles)
+{
+    const uint32_t n = (uint32_t)a.mesh.nC;
+    unsigned long long s = 0;
 #pragma unroll
     for (int k = 0; k < SI; ++k) {
-        const uint32_t i = base + k * SB;
-        if (i < n) s += in[i];
+        const uint32_t c = blockIdx.x * STILE + k * SB + threadIdx.x;
+        if (c < n) {
+            const unsigned long long w = cell_slot_word(a, c);
+            a.cub[c] = w;
+            s += w;
+        }
     }
-    T total;
-    block_excl_scan<T, SB>(s, total);
+    unsigned long long total;
+    block_excl_scan<unsigned long long, SB>(s, total);
     if (threadIdx.x == 0) tiles[blockIdx.x] = total;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(1024) k_scan_top(T* __restrict__ tiles, uint32_t ntiles)
+// Pass 2: each tile adds the sums of the tiles before it (read by one warp)
+// and scans its rows of SB cells; coff[nC] = the grand total.
+__global__ void __launch_bounds__(SB) k_slots_down(StepArgs a, const unsigned long long* __restrict__ tiles)
 {
-    constexpr int PER = SCAN_MAX_TILES / 1024;
-    T v[PER], s = 0;
+    __shared__ unsigned long long carry_s;
+    const uint32_t n = (uint32_t)a.mesh.nC;
+    if (threadIdx.x < 32) {
+        unsigned long long p = 0;
+        for (uint32_t t = threadIdx.x; t < blockIdx.x; t += 32) p += tiles[t];
 #pragma unroll
-    for (int k = 0; k < PER; ++k) {
-        const uint32_t i = threadIdx.x * PER + k;
-        v[k] = i < ntiles ? tiles[i] : T(0);
-        s += v[k];
+        for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+        if (threadIdx.x == 0) carry_s = p;
     }
-    T total;
-    T p = block_excl_scan<T, 1024>(s, total);
-#pragma unroll
-    for (int k = 0; k < PER; ++k) {
-        const uint32_t i = threadIdx.x * PER + k;
-        if (i < ntiles) tiles[i] = p;
-        p += v[k];
-    }
-}
-
-// Rows of SB consecutive elements, one block scan per row.
-template <typename T>
-__global__ void __launch_bounds__(SB) k_scan_down(const T* __restrict__ in, uint32_t n, const T* __restrict__ tiles,
-                                                   T* __restrict__ out)
-{
-    T carry = tiles[blockIdx.x];
+    __syncthreads();
+    unsigned long long carry = carry_s;
 #pragma unroll 1
     for (int k = 0; k < SI; ++k) {
         const uint32_t i = blockIdx.x * STILE + k * SB + threadIdx.x;
-        const T v = i < n ? in[i] : T(0);
-        T total;
-        const T p = block_excl_scan<T, SB>(v, total);
-        if (i < n) out[i] = carry + p;
-        if (i == n - 1) out[n] = carry + p + v;
+        const unsigned long long v = i < n ? a.cub[i] : 0ull;
+        unsigned long long total;
+        const unsigned long long p = block_excl_scan<unsigned long long, SB>(v, total);
+        if (i < n) a.coff[i] = carry + p;
+        if (i == n - 1) a.coff[n] = carry + p + v;
         carry += total;
-    }
-}
-
-// Slots needed per cell after the move (particles + new particles) and the
-// new particles alone, from the cell's count and part occupancy.
-__global__ void k_cell_slots(StepArgs a)
-{
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.mesh.nC; c += gridDim.x * blockDim.x) {
-        const uint32_t n = a.ccount[c];
-        uint32_t seeds = 0;
-        if (a.apply_counts && n > 0) {
-            if (a.pp.maxpp < 0) {
-                seeds = (uint32_t)a.pp.npart;
-            } else {
-                for (int w = 0; w < a.pp.occw; ++w)
-                    seeds += __popcll(a.pp.realmask[w] & ~a.cocc[(size_t)c * a.pp.occw + w]);
-            }
-        }
-        a.cub[c] = ((unsigned long long)seeds << 32) | (unsigned long long)(n + seeds);
     }
 }
 
@@ -213,99 +204,107 @@ __global__ void k_cell_v(const double* __restrict__ V, const double* __restrict_
     }
 }
 
-// FP32 form: per-cell polynomial of the velocity field.  One lane per cell
-// vertex (8 or 4 lanes per cell): b_k = nested differences of the vertex
-// values (bit d of k selects xi_d), by xor-shuffles; on affine cells mapped
-// to reference space, w_k = J^-1 b_k, with the cell's exact FP64 inverse.
+// FP32 form: per-cell polynomial of the velocity field, one thread per cell
+// (a warp reads 32 consecutive cells' vertex values: coalesced on structured
+// numberings).  b_k = nested differences of the vertex values (bit d of k
+// selects xi_d); on affine cells mapped to reference space, w_k = J^-1 b_k,
+// with the cell's exact FP64 inverse.  The increment record (V - Vold) stays
+// in physical space.
 template <int DIM>
-__global__ void k_cell_rec32(const double* __restrict__ V, const double* __restrict__ Vold,
-                             const int32_t* __restrict__ cd, const double* __restrict__ aff,
-                             const float* __restrict__ jinv32, int nC, int nD, float* __restrict__ vrec,
-                             float* __restrict__ dvrec)
+__device__ __forceinline__ void moebius(double (*f)[DIM])
+{
+    constexpr int NV = 1 << DIM;
+#pragma unroll
+    for (int b = 0; b < DIM; ++b)
+#pragma unroll
+        for (int k = NV - 1; k >= 0; --k)
+            if ((k >> b) & 1)
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) f[k][d] = f[k][d] - f[k ^ (1 << b)][d];
+}
+
+template <int DIM>
+__device__ __forceinline__ void store_rec(float* r, const float* w, float flag)
+{
+    constexpr int F4 = Dims<DIM>::REC4, NW = (1 << DIM) * DIM;
+    float4* q = reinterpret_cast<float4*>(r);
+#pragma unroll
+    for (int k = 0; k < F4; ++k) {
+        float t[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int i = 4 * k + j;
+            t[j] = i < NW ? w[i < NW ? i : 0] : (i == NW ? flag : 0.0f);
+        }
+        q[k] = make_float4(t[0], t[1], t[2], t[3]);
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128) k_cell_rec32(const double* __restrict__ V, const double* __restrict__ Vold,
+                                                    const int32_t* __restrict__ cd, const double* __restrict__ aff,
+                                                    const float* __restrict__ jinv32, int nC, int nD,
+                                                    float* __restrict__ vrec, float* __restrict__ dvrec)
 {
     constexpr int NV = 1 << DIM, F = Dims<DIM>::REC4 * 4, AFF = Dims<DIM>::AFF;
-    const int lane = threadIdx.x & 31;
-    const int k = lane & (NV - 1);
-    const long long total = (long long)nC * NV;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long nloop = (total + stride - 1) / stride * stride;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nloop; t += stride) {
-        const bool act = t < total;
-        const int c = act ? (int)(t / NV) : 0;
-        double f[DIM], g[DIM];
-        if (act) {
-            const int dof = __ldg(cd + (size_t)c * NV + k);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nC; c += gridDim.x * blockDim.x) {
+        int dof[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) dof[k] = __ldg(cd + (size_t)c * NV + k);
+        double f[NV][DIM], g[NV][DIM];
+#pragma unroll
+        for (int k = 0; k < NV; ++k)
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
-                f[d] = V[(size_t)d * nD + dof];
-                g[d] = Vold ? f[d] - Vold[(size_t)d * nD + dof] : 0.0;
+                f[k][d] = __ldg(V + (size_t)d * nD + dof[k]);
+                g[k][d] = Vold ? f[k][d] - __ldg(Vold + (size_t)d * nD + dof[k]) : 0.0;
             }
+        moebius<DIM>(f);
+        const bool affine = __ldg(jinv32 + (size_t)c * Dims<DIM>::JS + DIM * DIM) != 0.0f;
+        float w[NV * DIM];
+        if (affine) {
+            double A[DIM][DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+#pragma unroll
+                for (int e = 0; e < DIM; ++e) A[d][e] = __ldg(aff + (size_t)c * AFF + d * DIM + e);
+#pragma unroll
+            for (int k = 0; k < NV; ++k)
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int e = 0; e < DIM; ++e) t += A[d][e] * f[k][e];
+                    w[k * DIM + d] = (float)t;
+                }
         } else {
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) f[d] = g[d] = 0.0;
+            for (int k = 0; k < NV; ++k)
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) w[k * DIM + d] = (float)f[k][d];
         }
-#pragma unroll
-        for (int b = 0; b < DIM; ++b)
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                const double fo = __shfl_xor_sync(0xffffffffu, f[d], 1 << b);
-                const double go = __shfl_xor_sync(0xffffffffu, g[d], 1 << b);
-                if ((k >> b) & 1) {
-                    f[d] -= fo;
-                    g[d] -= go;
-                }
-            }
-        if (!act) continue;
-        const bool affine = jinv32[(size_t)c * Dims<DIM>::JS + DIM * DIM] != 0.0f;
-        float* r = vrec + (size_t)c * F;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            double w = f[d];
-            if (affine) {
-                w = 0.0;
-#pragma unroll
-                for (int e = 0; e < DIM; ++e) w += aff[(size_t)c * AFF + d * DIM + e] * f[e];
-            }
-            r[k * DIM + d] = (float)w;
-        }
-        if (k == 0) {
-            for (int j = NV * DIM; j < F; ++j) r[j] = 0.0f;
-            r[NV * DIM] = affine ? 1.0f : 0.0f;
-        }
+        store_rec<DIM>(vrec + (size_t)c * F, w, affine ? 1.0f : 0.0f);
         if (Vold) {
-            float* q = dvrec + (size_t)c * F;
+            moebius<DIM>(g);
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) q[k * DIM + d] = (float)g[d];
-            if (k == 0)
-                for (int j = NV * DIM; j < F; ++j) q[j] = 0.0f;
+            for (int k = 0; k < NV; ++k)
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) w[k * DIM + d] = (float)g[k][d];
+            store_rec<DIM>(dvrec + (size_t)c * F, w, 0.0f);
         }
     }
 }
 
 int grid_for(const void* k, int threads) { return occupancy_grid(k, threads); }
 
-template <typename T>
-int scan_impl(const T* in, uint32_t n, T* out, T* tiles, cudaStream_t s)
-{
-    const uint32_t ntiles = (n + STILE - 1) / STILE;
-    k_scan_reduce<T><<<ntiles, SB, 0, s>>>(in, n, tiles);
-    k_scan_top<T><<<1, 1024, 0, s>>>(tiles, ntiles);
-    k_scan_down<T><<<ntiles, SB, 0, s>>>(in, n, tiles, out);
-    return 3;
-}
-
 }  // namespace
 
-int launch_scan_u64(const unsigned long long* in, uint32_t n, unsigned long long* out, unsigned long long* tiles,
-                    cudaStream_t s)
+int launch_slots_scan(const StepArgs& a, unsigned long long* tiles, cudaStream_t s)
 {
-    return scan_impl<unsigned long long>(in, n, out, tiles, s);
-}
-
-int launch_cell_slots(const StepArgs& a, cudaStream_t s)
-{
-    k_cell_slots<<<grid_for((const void*)k_cell_slots, 256), 256, 0, s>>>(a);
-    return 1;
+    const uint32_t ntiles = ((uint32_t)a.mesh.nC + STILE - 1) / STILE;
+    k_slots_reduce<<<ntiles, SB, 0, s>>>(a, tiles);
+    k_slots_down<<<ntiles, SB, 0, s>>>(a, tiles);
+    return 2;
 }
 
 int launch_rekey(int dim, int prec, const StepArgs& a, cudaStream_t s)
@@ -351,11 +350,10 @@ int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const 
 int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
                       const float* jinv32, int nC, int nD, float* vrec, float* dvrec, cudaStream_t s)
 {
-    const long long total = (long long)nC * (1 << dim);
-    const long long g = (total + 255) / 256 < 16384 ? (total + 255) / 256 : 16384;
-    const int grid = g > 0 ? (int)g : 1;
-    if (dim == 2) k_cell_rec32<2><<<grid, 256, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
-    else k_cell_rec32<3><<<grid, 256, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    const int g = (nC + 127) / 128;
+    const int grid = g < 1 ? 1 : g;
+    if (dim == 2) k_cell_rec32<2><<<grid, 128, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    else k_cell_rec32<3><<<grid, 128, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
     return 1;
 }
 

@@ -100,6 +100,16 @@ def test_fp64_perturbed_cube_many_particles_per_cell():
     run_fp64(c, 6)
 
 
+@pytest.mark.parametrize("q,maxpp", [((6, 6), 1), ((7, 7), 0)])
+def test_fp64_cells_of_33_to_64_particles(q, maxpp):
+    """36 or 49 particles per cell: the write pass's two-round path (more
+    than one warp's worth of particles), with arrivals and removals."""
+    c = cases.channel(32, 8, q=q, maxpp=maxpp, dt=0.03)
+    o, g = run_fp64(c, 10)
+    st = g.stats()
+    assert st["searched"] > 0
+
+
 def test_fp64_first_touch_dofs_and_removal_seed():
     c = cases.channel(16, 8, q=(3, 2), dt=0.05)
     c.mesh = c.mesh.renumber_dofs_first_touch()
