@@ -2,8 +2,11 @@
 
 Workload: 3D duct [0,8]x[0,1]^2, 128x32x32 Q1 hexes (131,072 cells), 27
 particles per cell on a 3x3x3 reference grid (3,538,944 particles), max 2
-per cell part, 3 sub-steps, dt = 2e-3, u = 16 y(1-y) z(1-z), Vold = 0.9 V
-(the velocity correction is exercised).  A step is one time step of the
+per cell part, 3 sub-steps, dt = 2e-3, u = 16 y(1-y) z(1-z).  The nodal
+velocity sequence stands in for the FEM step: V_k alternates between V and
+0.9 V, and step k runs correct(V_k, V_{k-1}), so every step applies a +-10 %
+velocity correction and particle velocities stay of the order of V, as in a
+solver run.  A step is one time step of the
 reference loop (src/pfem2solver.cpp:162-164): correct + move (3 sub-steps,
 relocation, count correction) + project, over every particle.
 
@@ -110,9 +113,11 @@ def build_case():
     return m, V, 0.9 * V, prm
 
 
-def timed_device_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, torch, profile=False):
+def timed_device_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, torch, profile=False,
+                     alternate=True):
     """Seed, warm up, then time `steps` device-resident steps with CUDA events
-    on the handler's stream."""
+    on the handler's stream.  alternate: step k runs with (V_k, V_{k-1}) where
+    V_k alternates between V and Vold; otherwise (V, Vold) every step."""
     g = handler_cls(3, prm, precision)
     g.initialize_maps(m)
     dev = torch.device("cuda:0")
@@ -121,13 +126,18 @@ def timed_device_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, tor
     dout = torch.empty_like(dV)
     g.seed_particles_device(dV)
     stream = torch.cuda.ExternalStream(g.stream_handle())
+    pairs = [(dVo, dV), (dV, dVo)] if alternate else [(dV, dVo)] * 2
+    k = [0]
+
     def step():
+        a, b = pairs[k[0] & 1]
+        k[0] += 1
         if profile:  # per-kernel events: the separate calls, launched eagerly
-            g.correct_particle_velocity_device(dV, dVo)
+            g.correct_particle_velocity_device(a, b)
             g.move_particles_device(None)
             g.project_particle_fields_device(dout)
         else:  # one CUDA graph per step
-            g.step_device(dV, dVo, dout)
+            g.step_device(a, b, dout)
 
     for _ in range(warmup):
         step()
@@ -168,9 +178,13 @@ def timed_host_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, torch
 
     pV, pVo, pout = C.c_void_p(hV.data_ptr()), C.c_void_p(hVo.data_ptr()), C.c_void_p(hout.data_ptr())
     g._ck(L.pfem2gpu_seed(h, pV))
+    pairs = [(pVo, pV), (pV, pVo)]
+    k = [0]
 
     def step():
-        g._ck(L.pfem2gpu_correct(h, pV, pVo))
+        a, b = pairs[k[0] & 1]
+        k[0] += 1
+        g._ck(L.pfem2gpu_correct(h, a, b))
         g._ck(L.pfem2gpu_move(h, None))
         g._ck(L.pfem2gpu_project(h, pout))
 
@@ -192,6 +206,96 @@ def timed_host_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, torch
             "d2h": nbytes}
 
 
+def timed_window(handler_cls, m, V, Vold, prm, precision, K, C, torch, pre_steps=5, reps=3, n_probe=64):
+    """The differentiated window on the workload: K steps of correct + move
+    (count correction left out) + projection, then its adjoint for
+    J = sum over n_probe DoFs of (U - T)^2, T = U + 0.01.  Forward and
+    backward are timed with CUDA events on the handler's stream (best of
+    reps).  Also the directional derivative along the inflow amplitude
+    (V -> a V at the DoFs where V != 0) against central differences of the
+    FP64 form's window (h = 1e-6)."""
+    g = handler_cls(3, prm, precision)
+    g.initialize_maps(m)
+    dev = torch.device("cuda:0")
+    dV = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
+    dVo = torch.from_numpy(np.ascontiguousarray(Vold)).to(dev)
+    out = torch.empty_like(dV)
+    g.seed_particles_device(dV)
+    for k in range(pre_steps):
+        a, b = ((dVo, dV), (dV, dVo))[k & 1]
+        g.step_device(a, b, out)
+    g.synchronize()
+    n = g.stats()["n_particles"]
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+    U = torch.empty_like(dV)
+    gv0 = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    gV, gVo = torch.empty_like(dV), torch.empty_like(dV)
+    rng = np.random.default_rng(7)
+    g.window_forward_device(K, C, dV, dVo, None, U)
+    g.synchronize()
+    Un = U.cpu().numpy()
+    probe = rng.choice(np.where(np.all(np.isfinite(Un), 0))[0], n_probe, replace=False)
+    T = Un[:, probe] + 0.01
+    gUn = np.zeros_like(Un)
+    gUn[:, probe] = 2.0 * (Un[:, probe] - T)
+    gU = torch.from_numpy(gUn).to(dev)
+    fwd, bwd = [], []
+    for _ in range(reps):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        g.window_forward_device(K, C, dV, dVo, None, U)
+        e1.record(stream)
+        g.window_backward_device(gU, gv0, gV, gVo)
+        e2.record(stream)
+        e2.synchronize()
+        fwd.append(e0.elapsed_time(e1))
+        bwd.append(e1.elapsed_time(e2))
+    gVn = gV.cpu().numpy()
+    g.close()
+    return {"fwd_ms": min(fwd), "bwd_ms": min(bwd), "bwd_over_fwd": min(bwd) / min(fwd), "particles": n,
+            "dJ_da": float(np.sum(gVn * V)), "probe": probe, "T": T}
+
+
+def fd_inflow(handler_cls, m, V, Vold, prm, K, C, probe, T, torch, pre_steps=5, h=1e-6):
+    """Central difference of J along V -> (1 + t) V with the FP64 form."""
+    g = handler_cls(3, prm, "fp64")
+    g.initialize_maps(m)
+    dev = torch.device("cuda:0")
+    dV = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
+    dVo = torch.from_numpy(np.ascontiguousarray(Vold)).to(dev)
+    out = torch.empty_like(dV)
+    g.seed_particles_device(dV)
+    for k in range(pre_steps):
+        a, b = ((dVo, dV), (dV, dVo))[k & 1]
+        g.step_device(a, b, out)
+    js = []
+    for t in (h, -h):
+        U = g.window_forward_device(K, C, (1.0 + t) * dV, dVo)
+        g.synchronize()
+        Un = U.cpu().numpy()
+        js.append(float(np.sum((Un[:, probe] - T) ** 2)))
+    g.close()
+    return (js[0] - js[1]) / (2 * h)
+
+
+def adjoint_report(handler_cls, m, V, Vold, prm, torch, K=20, C=5):
+    """K-step window + adjoint on the workload, both forms, with the
+    directional derivative along the inflow amplitude against FP64 central
+    differences."""
+    rep = {"steps": K, "checkpoint_every": C, "objective": "sum over 64 DoFs of (U - T)^2"}
+    for form in ("fp32", "fp64"):
+        r = timed_window(handler_cls, m, V, Vold, prm, form, K, C, torch)
+        rep[form] = {k: r[k] for k in ("fwd_ms", "bwd_ms", "bwd_over_fwd", "particles", "dJ_da")}
+        if form == "fp32":
+            probe, T = r["probe"], r["T"]
+    fd = fd_inflow(handler_cls, m, V, Vold, prm, K, C, probe, T, torch)
+    for form in ("fp32", "fp64"):
+        rep[form]["fd_rel_err"] = abs(rep[form]["dJ_da"] - fd) / abs(fd)
+    rep["fd_dJ_da"] = fd
+    return rep
+
+
 def cpu_baseline(m, V, Vold, prm, budget_s=20.0, max_steps=None, warmup=0):
     """The FP64 CPU restatement (reference removal order) on all host cores,
     on the full workload; `warmup` untimed steps, then steps until the time
@@ -202,13 +306,14 @@ def cpu_baseline(m, V, Vold, prm, budget_s=20.0, max_steps=None, warmup=0):
     o = Oracle(m, prm.particles_per_cell, prm.max_particles_per_cell_part, prm.particle_integration_steps,
                prm.time_step, removal_order=ORDER_VECTOR, n_threads=cores)
     o.seed(V)
-    for _ in range(warmup):
-        o.step(V, Vold)
+    pairs = [(Vold, V), (V, Vold)]
+    for k in range(warmup):
+        o.step(*pairs[k & 1])
     done, ps, t = 0, 0, 0.0
     while t < budget_s and (max_steps is None or done < max_steps):
         n = o.stats()["n_particles"]
         t0 = time.perf_counter()
-        o.step(V, Vold)
+        o.step(*pairs[(warmup + done) & 1])
         t += time.perf_counter() - t0
         ps += n
         done += 1
@@ -257,6 +362,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="time the differentiated window and its adjoint only (prints one JSON object)")
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
                     help="run one device-resident pass of one form and print its timing (profiling runs)")
     args = ap.parse_args()
@@ -278,6 +385,9 @@ def main():
 
     m, V, Vold, prm = build_case()
     gpu_index = torch.cuda.current_device()
+    if args.adjoint_only:
+        print(json.dumps(adjoint_report(ParticleHandler, m, V, Vold, prm, torch)), flush=True)
+        return 0
     if args.only:
         r = timed_device_run(ParticleHandler, m, V, Vold, prm, args.only, args.steps, args.warmup, torch)
         print(json.dumps({"form": args.only, "ms_per_step": r["ms"] / args.steps,
@@ -309,6 +419,10 @@ def main():
     r64 = timed_device_run(ParticleHandler, m, V, Vold, prm, "fp64", args.steps, args.warmup, torch)
     v64 = r64["particle_steps"] / (r64["ms"] / 1000.0)
     err = rel_l2(r64["V"], r32["V"])
+    # the same comparison with Vold = 0.9 V held fixed (velocities grow by 0.1 V per step)
+    f32 = timed_device_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch, alternate=False)
+    f64 = timed_device_run(ParticleHandler, m, V, Vold, prm, "fp64", args.steps, args.warmup, torch, alternate=False)
+    err_fixed = rel_l2(f64["V"], f32["V"])
     # kernel-level timing pass (per-launch CUDA events)
     rp = timed_device_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch, profile=True)
     prof = rp["profile"]
@@ -345,7 +459,9 @@ def main():
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "fp64": {"value": v64, "unit": UNIT, "ms_per_step": r64["ms"] / args.steps, "dtype": "f64",
                  "fp32_over_fp64": value / v64},
-        "fp32_vs_fp64_rel_l2": {"projected_velocity": err, "tolerance": 1e-4},
+        "fp32_vs_fp64_rel_l2": {"projected_velocity": err, "tolerance": 1e-4,
+                                "steps": args.warmup + args.steps,
+                                "fixed_vold_0.9v": err_fixed},
         "step_effective_gbs": STEP_BYTES["fp32"] * value / 1e9,
         "roofline": {"bound": "hbm", "kernel": "k_advect32<3>", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": None,

@@ -131,6 +131,53 @@ int pfem2gpu_profile_report(pfem2gpu_handle* h, char* buf, int64_t len);
 int pfem2gpu_launch_count(pfem2gpu_handle* h, uint64_t* count);
 
 /* ---------------------------------------------------------------------------
+ * Differentiated window and its adjoint.
+ *
+ * No counterpart in the reference (it has no adjoint).  The window is
+ * `steps` time steps of correct_particle_velocity (when Vold is given, with
+ * the same V - Vold every step) and move_particles' sub-steps with relocation
+ * (src/pfem2particlehandler.cpp:112-167, 413-503) from the handle's current
+ * particles, with check_particle_distribution (:356-410) left out, followed by
+ * project_particle_fields (:174-215): U = P(v0, V, Vold), dim x n_dofs
+ * component-major (empty_dof_policy applies to DoFs no particle reaches).
+ * The per-particle arithmetic is the form's own (FP64 or FP32); the
+ * projection sums of the window are FP64 and deterministic.  The handle's
+ * particles are not changed; the handle's staged velocity becomes V.
+ *
+ * The adjoint returns, for a given gU = dJ/dU of a scalar objective J, the
+ * gradients dJ/dv0 (n x dim, one row per particle in the order of
+ * pfem2gpu_get_particles at the window start, n = stats.n_particles),
+ * dJ/dV and dJ/dVold (dim x n_dofs).  Every particle's cell sequence is held
+ * fixed (cell assignment is discrete and not differentiated); particles
+ * deleted inside the window get zero gradient.  The forward keeps the
+ * particle state at the start of every `checkpoint_every` steps; the
+ * backward recomputes one such segment at a time from its checkpoint, so
+ * memory grows with steps / checkpoint_every, not with steps.
+ * checkpoint_every x particle_integration_steps is limited by the backward
+ * kernel's shared memory (about 200 states in 3D FP64): PFEM2GPU_ERR_ARG
+ * beyond.  dJ/dV and dJ/dVold are summed with FP64 atomics per cell vertex:
+ * their last bits can differ between runs; U and dJ/dv0 are deterministic.
+ *
+ * window_forward_device: device arrays (v0 may be NULL: the particles' own
+ * velocities; Vold may be NULL: no correction).  window_backward_device
+ * differentiates the most recent forward (it may be called again with another
+ * gU); outputs may be NULL.  pfem2gpu_adjoint: forward + backward on host
+ * arrays.  PFEM2GPU_ERR_DEVICE if a recomputed segment does not end where the
+ * forward pass ended it (never expected).
+ */
+int pfem2gpu_window_forward_device(pfem2gpu_handle* h, int32_t steps, int32_t checkpoint_every, const double* dV,
+                                   const double* dVold, const double* dv0, double* dU_out);
+int pfem2gpu_window_backward_device(pfem2gpu_handle* h, const double* dgU, double* dg_v0, double* dg_V,
+                                    double* dg_Vold);
+int pfem2gpu_adjoint(pfem2gpu_handle* h, int32_t steps, int32_t checkpoint_every, const double* V, const double* Vold,
+                     const double* v0, const double* gU, double* U, double* g_v0, double* g_V, double* g_Vold);
+/* Particles of the most recent window forward (-1: none). */
+int pfem2gpu_window_size(pfem2gpu_handle* h, int64_t* n);
+/* Their states at the end of that window (cell -1: deleted inside it), host
+ * arrays of >= capacity rows in the window's particle order. */
+int pfem2gpu_window_particles(pfem2gpu_handle* h, int32_t* cell, double* xi, double* v, int64_t capacity, int64_t* n);
+
+/* ---------------------------------------------------------------------------
  * pfem2gpu_project_noalloc -- projection that allocates no device memory.
  *
  * No counterpart in the reference: it has no GPU path.  This is

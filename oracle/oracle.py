@@ -84,6 +84,9 @@ def lib():
         L.orc_shape_values.argtypes = [C.c_int, dp, dp]
         L.orc_forward_map.argtypes = [C.c_int, dp, dp, dp]
         L.orc_inverse_map.argtypes = [C.c_int, dp, dp, dp]
+        L.orc_window_forward.argtypes = [P, C.c_int, dp, P, P, C.c_int, dp]
+        L.orc_window_particles.argtypes = [P, C.c_int, dp, P, P, ip, dp, dp, dp]
+        L.orc_window_adjoint.argtypes = [P, C.c_int, dp, P, P, C.c_int, dp, P, P, P, P]
         L.orc_key.restype = C.c_uint32
         L.orc_key.argtypes = [C.c_uint32, C.c_uint32]
         _lib = L
@@ -92,6 +95,10 @@ def lib():
 
 def _c(a, dt):
     return np.ascontiguousarray(a, dtype=dt)
+
+
+def _vp(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
 class Oracle:
@@ -169,6 +176,40 @@ class Oracle:
         assert self.L.orc_set_particles(self.h, n, _c(P["id"], np.uint32), _c(P["cell"], np.int32),
                                         _c(P["x"], np.float64), _c(P["xi"], np.float64),
                                         _c(P["v"], np.float64), next_id) == 0
+
+    def window_forward(self, K, V, Vold=None, v0=None, empty_policy=0):
+        """K steps of correct (Vold given) + move without count correction
+        from the current particles, then the projection; particles unchanged."""
+        U = np.zeros(self.dim * self.mesh.n_dofs)
+        vo = _c(Vold, np.float64) if Vold is not None else None
+        v0c = _c(v0, np.float64) if v0 is not None else None
+        rc = self.L.orc_window_forward(self.h, K, self._V(V), _vp(vo), _vp(v0c), empty_policy, U)
+        assert rc == 0
+        return U.reshape(self.dim, self.mesh.n_dofs)
+
+    def window_particles(self, K, V, Vold=None, v0=None):
+        """Final particle states of the window (cell -1: deleted), oracle order."""
+        n = self.L.orc_n_particles(self.h)
+        cell = np.zeros(max(n, 1), np.int32)
+        x, xi, v = (np.zeros((max(n, 1), self.dim)) for _ in range(3))
+        vo = _c(Vold, np.float64) if Vold is not None else None
+        v0c = _c(v0, np.float64) if v0 is not None else None
+        assert self.L.orc_window_particles(self.h, K, self._V(V), _vp(vo), _vp(v0c), cell, x, xi, v) == 0
+        return {"cell": cell[:n], "x": x[:n], "xi": xi[:n], "v": v[:n]}
+
+    def window_adjoint(self, K, V, gU, Vold=None, v0=None, empty_policy=0):
+        """Forward + adjoint of the window: (U, g_v0 (n x dim), g_V, g_Vold)."""
+        n = self.L.orc_n_particles(self.h)
+        nd = self.dim * self.mesh.n_dofs
+        U, gv0, gV, gVo = np.zeros(nd), np.zeros(max(n, 1) * self.dim), np.zeros(nd), np.zeros(nd)
+        vo = _c(Vold, np.float64) if Vold is not None else None
+        v0c = _c(v0, np.float64) if v0 is not None else None
+        g = _c(gU, np.float64).reshape(-1)
+        rc = self.L.orc_window_adjoint(self.h, K, self._V(V), _vp(vo), _vp(v0c), empty_policy, g,
+                                       _vp(U), _vp(gv0), _vp(gV), _vp(gVo))
+        assert rc == 0
+        sh = (self.dim, self.mesh.n_dofs)
+        return U.reshape(sh), gv0[: n * self.dim].reshape(n, self.dim), gV.reshape(sh), gVo.reshape(sh)
 
     def stats(self):
         s = Stats()

@@ -1035,3 +1035,271 @@ void orc_reset_stats(orc_handle* h)
     h->st.nan_dofs = nan;
     h->st.n_particles = h->n;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Differentiated window (no reference counterpart: the reference has no     */
+/* adjoint).  K time steps of correct_particle_velocity (:112-139, when Vold  */
+/* is given) and move_particles' sub-steps with relocation (:142-167,        */
+/* :413-503) from the current particles, check_particle_distribution left    */
+/* out, then project_particle_fields (:174-215).  The particle set is not    */
+/* changed.  The backward pass holds every particle's cell sequence fixed     */
+/* (cell assignment is the discrete, non-differentiated part) and applies    */
+/* the chain rule to                                                         */
+/*   correction   v  += sum_i N_i(xi) dV_i                                   */
+/*   sub-step     x'  = F_c(xi) + h u_c(xi),  xi' = F_c'^-1(x'),  h = dt/S    */
+/*   projection   U_j = sum N_j v / sum N_j                                  */
+/* with dxi'/dx' = J_c'(xi')^-1.  Particles lost inside the window do not    */
+/* reach the projection and get zero gradient.                              */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    int32_t cell;
+    double xi[3];
+} orc_wstate;
+
+/* One particle through the window; states[t] = (cell, xi) before sub-step t,
+ * states[K*S] = the final one (states may be NULL).  Returns 1 if the particle
+ * is alive at the end. */
+static int window_particle(const orc_handle* h, orc_particle* q, int K, const double* V, const double* Vold,
+                           orc_wstate* states)
+{
+    const int dim = h->dim, nv = h->nv, S = h->S;
+    reloc_counts rc = {0, 0, 0};
+    for (int k = 0; k < K; ++k) {
+        if (Vold) { /* orc_correct's arithmetic */
+            double N[MAXV], corr[3] = {0.0, 0.0, 0.0};
+            orc_shape_values(dim, q->xi, N);
+            for (int i = 0; i < nv; ++i) {
+                const int64_t dof = h->cd[(int64_t)q->cell * nv + i];
+                for (int d = 0; d < dim; ++d) {
+                    const double dv = V[d * h->nD + dof] - Vold[d * h->nD + dof];
+                    corr[d] = corr[d] + N[i] * dv;
+                }
+            }
+            for (int d = 0; d < dim; ++d) q->v[d] = q->v[d] + corr[d];
+        }
+        for (int s = 0; s < S; ++s) {
+            if (states) {
+                orc_wstate* w = &states[k * S + s];
+                w->cell = q->cell;
+                for (int d = 0; d < dim; ++d) w->xi[d] = q->xi[d];
+            }
+            double u[3], step[3];
+            interp(h, q->cell, q->xi, V, u);
+            for (int d = 0; d < dim; ++d) {
+                q->vext[d] = u[d];
+                step[d] = u[d] * h->dtp;
+                q->x[d] = q->x[d] + step[d];
+            }
+            if (!relocate(h, q, &rc)) return 0;
+        }
+    }
+    if (states) {
+        orc_wstate* w = &states[K * S];
+        w->cell = q->cell;
+        for (int d = 0; d < dim; ++d) w->xi[d] = q->xi[d];
+    }
+    return 1;
+}
+
+/* Forward pass of the window: final particles into fin (n entries, alive[p]
+ * set), projection into U with den (nD) kept. */
+static int window_forward(const orc_handle* h, int K, const double* V, const double* Vold, const double* v0,
+                          int empty_policy, orc_particle* fin, uint8_t* alive, double* U, double* den)
+{
+    const int dim = h->dim, nv = h->nv;
+    const int64_t nD = h->nD;
+    for (int64_t p = 0; p < h->n; ++p) {
+        fin[p] = h->P[p];
+        if (v0)
+            for (int d = 0; d < dim; ++d) fin[p].v[d] = v0[p * dim + d];
+        alive[p] = (uint8_t)window_particle(h, &fin[p], K, V, Vold, NULL);
+    }
+    for (int64_t k = 0; k < nD * dim; ++k) U[k] = 0.0;
+    for (int64_t k = 0; k < nD; ++k) den[k] = 0.0;
+    for (int64_t p = 0; p < h->n; ++p) {
+        if (!alive[p]) continue;
+        const orc_particle* q = &fin[p];
+        double N[MAXV];
+        orc_shape_values(dim, q->xi, N);
+        for (int i = 0; i < nv; ++i) {
+            const int64_t dof = h->cd[(int64_t)q->cell * nv + i];
+            for (int d = 0; d < dim; ++d) U[d * nD + dof] = U[d * nD + dof] + N[i] * q->v[d];
+            den[dof] = den[dof] + N[i];
+        }
+    }
+    for (int64_t j = 0; j < nD; ++j)
+        for (int d = 0; d < dim; ++d) {
+            if (den[j] == 0.0 && empty_policy == 1) U[d * nD + j] = V[d * nD + j];
+            else U[d * nD + j] = U[d * nD + j] / den[j];
+        }
+    return 0;
+}
+
+int orc_window_forward(orc_handle* h, int K, const double* V, const double* Vold, const double* v0,
+                       int empty_policy, double* U)
+{
+    if (!h->X || K < 0) return -1;
+    const int64_t n = h->n;
+    orc_particle* fin = (orc_particle*)malloc(sizeof(orc_particle) * (n ? n : 1));
+    uint8_t* alive = (uint8_t*)malloc(n ? n : 1);
+    double* den = (double*)malloc(sizeof(double) * (h->nD ? h->nD : 1));
+    int rc = (fin && alive && den) ? window_forward(h, K, V, Vold, v0, empty_policy, fin, alive, U, den) : -1;
+    free(fin);
+    free(alive);
+    free(den);
+    return rc;
+}
+
+/* Final particle states of the window (cell -1: deleted inside it), in the
+ * oracle's current particle order. */
+int orc_window_particles(orc_handle* h, int K, const double* V, const double* Vold, const double* v0, int32_t* cell,
+                         double* x, double* xi, double* v)
+{
+    if (!h->X || K < 0) return -1;
+    const int dim = h->dim;
+    for (int64_t p = 0; p < h->n; ++p) {
+        orc_particle q = h->P[p];
+        if (v0)
+            for (int d = 0; d < dim; ++d) q.v[d] = v0[p * dim + d];
+        const int alive = window_particle(h, &q, K, V, Vold, NULL);
+        cell[p] = alive ? q.cell : -1;
+        for (int d = 0; d < dim; ++d) {
+            x[p * dim + d] = q.x[d];
+            xi[p * dim + d] = q.xi[d];
+            v[p * dim + d] = q.v[d];
+        }
+    }
+    return 0;
+}
+
+/* Forward + backward.  gU: dJ/dU (dim x nD).  Outputs g_v0 (n x dim, the
+ * gradient with respect to the particle velocities at the window start),
+ * g_V and g_Vold (dim x nD; g_Vold = 0 without Vold).  Any output may be NULL. */
+int orc_window_adjoint(orc_handle* h, int K, const double* V, const double* Vold, const double* v0,
+                       int empty_policy, const double* gU, double* U, double* g_v0, double* g_V, double* g_Vold)
+{
+    if (!h->X || K < 0) return -1;
+    const int dim = h->dim, nv = h->nv, S = h->S;
+    const int64_t n = h->n, nD = h->nD;
+    const int T = K * S;
+    const size_t nDd = (size_t)(nD * dim) + 1;
+    orc_particle* fin = (orc_particle*)malloc(sizeof(orc_particle) * (n ? n : 1));
+    uint8_t* alive = (uint8_t*)malloc(n ? n : 1);
+    double* den = (double*)malloc(sizeof(double) * (nD ? nD : 1));
+    double* Uw = (double*)malloc(sizeof(double) * nDd);
+    double* gnum = (double*)calloc(nDd, sizeof(double));
+    double* gden = (double*)calloc((size_t)nD + 1, sizeof(double));
+    double* gadv = (double*)calloc(nDd, sizeof(double));
+    double* gdv = (double*)calloc(nDd, sizeof(double));
+    orc_wstate* st = (orc_wstate*)malloc(sizeof(orc_wstate) * (size_t)(T + 1));
+    int rc = -1;
+    if (!fin || !alive || !den || !Uw || !gnum || !gden || !gadv || !gdv || !st) goto done;
+    rc = window_forward(h, K, V, Vold, v0, empty_policy, fin, alive, Uw, den);
+    if (rc) goto done;
+    if (U)
+        for (int64_t k = 0; k < nD * dim; ++k) U[k] = Uw[k];
+    /* projection: U_j = num_j / den_j */
+    for (int64_t j = 0; j < nD; ++j) {
+        if (den[j] == 0.0) {
+            if (empty_policy == 1)
+                for (int d = 0; d < dim; ++d) gadv[d * nD + j] = gU[d * nD + j];
+            continue;
+        }
+        double s = 0.0;
+        for (int d = 0; d < dim; ++d) {
+            gnum[d * nD + j] = gU[d * nD + j] / den[j];
+            s = s + gU[d * nD + j] * Uw[d * nD + j];
+        }
+        gden[j] = -s / den[j];
+    }
+    for (int64_t p = 0; p < n; ++p) {
+        if (g_v0)
+            for (int d = 0; d < dim; ++d) g_v0[p * dim + d] = 0.0;
+        if (!alive[p]) continue;
+        /* the particle's trajectory again, with its states */
+        orc_particle q = h->P[p];
+        if (v0)
+            for (int d = 0; d < dim; ++d) q.v[d] = v0[p * dim + d];
+        window_particle(h, &q, K, V, Vold, st);
+        double N[MAXV], G[MAXV][3], gv[3] = {0.0, 0.0, 0.0}, gxi[3] = {0.0, 0.0, 0.0};
+        {
+            const orc_wstate* w = &st[T];
+            orc_shape_values(dim, w->xi, N);
+            shape_grads(dim, w->xi, G);
+            for (int i = 0; i < nv; ++i) {
+                const int64_t j = h->cd[(int64_t)w->cell * nv + i];
+                double a = gden[j];
+                for (int d = 0; d < dim; ++d) {
+                    gv[d] = gv[d] + N[i] * gnum[d * nD + j];
+                    a = a + gnum[d * nD + j] * q.v[d];
+                }
+                for (int k = 0; k < dim; ++k) gxi[k] = gxi[k] + G[i][k] * a;
+            }
+        }
+        if (g_v0)
+            for (int d = 0; d < dim; ++d) g_v0[p * dim + d] = gv[d];
+        for (int t = T - 1; t >= 0; --t) {
+            const orc_wstate* a = &st[t];
+            const orc_wstate* b = &st[t + 1];
+            double Xb[MAXV * 3], Xa[MAXV * 3], Jb[3][3], Bi[3][3], Ja[3][3], y[3], A[3][3];
+            cell_coords(h, b->cell, Xb);
+            jacobian(dim, Xb, b->xi, Jb);
+            invert(dim, Jb, Bi);
+            for (int d = 0; d < dim; ++d) { /* y = J_b^-T gxi */
+                double s = 0.0;
+                for (int k = 0; k < dim; ++k) s = s + Bi[k][d] * gxi[k];
+                y[d] = s;
+            }
+            cell_coords(h, a->cell, Xa);
+            jacobian(dim, Xa, a->xi, Ja);
+            orc_shape_values(dim, a->xi, N);
+            shape_grads(dim, a->xi, G);
+            for (int d = 0; d < dim; ++d)
+                for (int k = 0; k < dim; ++k) A[d][k] = 0.0;
+            for (int i = 0; i < nv; ++i) {
+                const int64_t j = h->cd[(int64_t)a->cell * nv + i];
+                for (int d = 0; d < dim; ++d) {
+                    const double vd = V[d * nD + j];
+                    for (int k = 0; k < dim; ++k) A[d][k] = A[d][k] + vd * G[i][k];
+                    gadv[d * nD + j] = gadv[d * nD + j] + (h->dtp * N[i]) * y[d];
+                }
+            }
+            for (int k = 0; k < dim; ++k) {
+                double s = 0.0, r = 0.0;
+                for (int d = 0; d < dim; ++d) {
+                    s = s + Ja[d][k] * y[d];
+                    r = r + A[d][k] * y[d];
+                }
+                gxi[k] = s + h->dtp * r;
+            }
+            if (Vold && t % S == 0) { /* the correction at the start of step t/S */
+                for (int i = 0; i < nv; ++i) {
+                    const int64_t j = h->cd[(int64_t)a->cell * nv + i];
+                    double c = 0.0;
+                    for (int d = 0; d < dim; ++d) {
+                        c = c + (V[d * nD + j] - Vold[d * nD + j]) * gv[d];
+                        gdv[d * nD + j] = gdv[d * nD + j] + N[i] * gv[d];
+                    }
+                    for (int k = 0; k < dim; ++k) gxi[k] = gxi[k] + G[i][k] * c;
+                }
+            }
+        }
+    }
+    for (int64_t k = 0; k < nD * dim; ++k) {
+        if (g_V) g_V[k] = gadv[k] + gdv[k];
+        if (g_Vold) g_Vold[k] = -gdv[k];
+    }
+    rc = 0;
+done:
+    free(fin);
+    free(alive);
+    free(den);
+    free(Uw);
+    free(gnum);
+    free(gden);
+    free(gadv);
+    free(gdv);
+    free(st);
+    return rc;
+}

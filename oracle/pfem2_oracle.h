@@ -84,6 +84,21 @@ int orc_set_particles(orc_handle* h, int64_t n, const uint32_t* id, const int32_
 void orc_get_stats(const orc_handle* h, orc_stats* s);
 void orc_reset_stats(orc_handle* h);
 
+/* Differentiated window (no counterpart in the reference, which has no
+ * adjoint): K steps of correct (if Vold != NULL) + sub-steps with relocation
+ * from the current particles, count correction left out, then the projection
+ * U (dim x n_dofs; empty_policy 0: NaN where no particle weighs, 1: V there).
+ * The particle set is unchanged.  v0: n x dim starting velocities or NULL.
+ * The adjoint holds every particle's cell sequence fixed and returns, for
+ * dJ/dU = gU, the gradients with respect to the starting particle velocities
+ * (g_v0, n x dim), V and Vold (dim x n_dofs).  Outputs may be NULL. */
+int orc_window_forward(orc_handle* h, int K, const double* V, const double* Vold, const double* v0,
+                       int empty_policy, double* U);
+int orc_window_particles(orc_handle* h, int K, const double* V, const double* Vold, const double* v0, int32_t* cell,
+                         double* x, double* xi, double* v);
+int orc_window_adjoint(orc_handle* h, int K, const double* V, const double* Vold, const double* v0,
+                       int empty_policy, const double* gU, double* U, double* g_v0, double* g_V, double* g_Vold);
+
 /* Geometry primitives, exposed for known-answer tests. */
 void orc_shape_values(int dim, const double* xi, double* N);
 void orc_forward_map(int dim, const double* X, const double* xi, double* x);

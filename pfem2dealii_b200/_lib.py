@@ -113,6 +113,11 @@ def load():
         "pfem2gpu_profile_report": [P, C.c_char_p, i64],
         "pfem2gpu_launch_count": [P, C.POINTER(C.c_uint64)],
         "pfem2gpu_last_error": [P, C.c_char_p, i64],
+        "pfem2gpu_window_forward_device": [P, C.c_int32, C.c_int32, dptr, dptr, dptr, dptr],
+        "pfem2gpu_window_backward_device": [P, dptr, dptr, dptr, dptr],
+        "pfem2gpu_adjoint": [P, C.c_int32, C.c_int32, dptr, dptr, dptr, dptr, dptr, dptr, dptr, dptr],
+        "pfem2gpu_window_size": [P, C.POINTER(i64)],
+        "pfem2gpu_window_particles": [P, dptr, dptr, dptr, i64, C.POINTER(i64)],
         "pfem2gpu_project_noalloc": [C.c_int, C.c_int32, C.c_int32, dptr, i64, dptr, dptr, dptr, C.c_int, dptr,
                                      C.POINTER(i64), P],
     }

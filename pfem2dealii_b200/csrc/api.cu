@@ -77,6 +77,24 @@ struct pfem2gpu_handle {
     std::vector<cudaEvent_t> ev_pool;
     std::map<std::string, std::pair<double, long long>> prof;
     std::string err;
+    // differentiated window: checkpoints, final state, projection and adjoint
+    // buffers (per-particle arrays sized ncap x segcap, the rest per mesh)
+    struct Win {
+        uint32_t ncap = 0, tsumcap = 0, n = 0;
+        int segcap = 0, tcap = -1, K = 0, C = 1, nseg = 0, rec_seg = -1;
+        bool do_correct = false, ready = false, mesh_ready = false;
+        uint32_t *slot = nullptr, *ck_cell = nullptr, *fin_cell = nullptr, *r_cell = nullptr, *rec_cell = nullptr,
+                 *order = nullptr, *order2 = nullptr, *tsum = nullptr, *ccnt = nullptr, *cstart = nullptr,
+                 *nq = nullptr;
+        uint2* q = nullptr;
+        void *ck_xi = nullptr, *fin_xi = nullptr, *fin_v = nullptr, *r_xi = nullptr, *rec_xi = nullptr;
+        double *ck_x = nullptr, *fin_x = nullptr, *r_x = nullptr, *gxi = nullptr, *gv = nullptr, *hv0 = nullptr;
+        double *part = nullptr, *U = nullptr, *den = nullptr, *gnum = nullptr, *gden = nullptr, *gadv = nullptr,
+               *gdv = nullptr, *V = nullptr, *Vold = nullptr, *gU = nullptr, *gV = nullptr, *gVold = nullptr,
+               *Vcell = nullptr, *dVcell = nullptr, *Wcell = nullptr;
+        unsigned long long* nempty = nullptr;
+        unsigned int* err = nullptr;
+    } win;
 };
 
 namespace {
@@ -217,6 +235,39 @@ void free_state(PartState& s)
         dfree(s.v[d]);
     }
     s = PartState{};
+}
+
+void free_win_particles(pfem2gpu_handle::Win& W)
+{
+    for (void* p : {(void*)W.slot, (void*)W.ck_cell, (void*)W.fin_cell, (void*)W.r_cell, (void*)W.rec_cell,
+                    (void*)W.order, (void*)W.order2, (void*)W.q, W.ck_xi, W.fin_xi, W.fin_v, W.r_xi, W.rec_xi,
+                    (void*)W.ck_x, (void*)W.fin_x, (void*)W.r_x, (void*)W.gxi, (void*)W.gv, (void*)W.hv0})
+        dfree(p);
+    W.slot = W.ck_cell = W.fin_cell = W.r_cell = W.rec_cell = W.order = W.order2 = nullptr;
+    W.q = nullptr;
+    W.ck_xi = W.fin_xi = W.fin_v = W.r_xi = W.rec_xi = nullptr;
+    W.ck_x = W.fin_x = W.r_x = W.gxi = W.gv = W.hv0 = nullptr;
+    W.ncap = 0;
+    W.segcap = 0;
+    W.tcap = -1;
+    W.ready = false;
+}
+
+void free_win_mesh(pfem2gpu_handle::Win& W)
+{
+    for (void* p : {(void*)W.tsum, (void*)W.ccnt, (void*)W.cstart, (void*)W.part, (void*)W.U, (void*)W.den,
+                    (void*)W.gnum, (void*)W.gden, (void*)W.gadv, (void*)W.gdv, (void*)W.V, (void*)W.Vold, (void*)W.gU,
+                    (void*)W.gV, (void*)W.gVold, (void*)W.nempty, (void*)W.err, (void*)W.Vcell, (void*)W.dVcell,
+                    (void*)W.Wcell, (void*)W.nq})
+        dfree(p);
+    W.tsum = W.ccnt = W.cstart = W.nq = nullptr;
+    W.part = W.U = W.den = W.gnum = W.gden = W.gadv = W.gdv = W.V = W.Vold = W.gU = W.gV = W.gVold = nullptr;
+    W.Vcell = W.dVcell = W.Wcell = nullptr;
+    W.nempty = nullptr;
+    W.err = nullptr;
+    W.tsumcap = 0;
+    W.mesh_ready = false;
+    W.ready = false;
 }
 
 cudaError_t alloc_state(pfem2gpu_handle* h, PartState& s, uint32_t cap, bool with_ids)
@@ -448,6 +499,223 @@ int maybe_grow(pfem2gpu_handle* h)
     return PFEM2GPU_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Differentiated window (window.cuh).
+// ---------------------------------------------------------------------------
+int win_reserve(pfem2gpu_handle* h, uint32_t n, uint32_t ns, int nseg, int tseg)
+{
+    auto& W = h->win;
+    const int dim = h->dim, NV = 1 << dim;
+    const size_t nc = h->nC, nd = h->nD, es = esize(h), VS = dim == 3 ? 4 : 2;
+    const bool fp64 = h->prec == PFEM2GPU_FP64;
+    if (!W.mesh_ready) {
+        CK(dalloc(&W.ccnt, nc));
+        CK(dalloc(&W.cstart, nc + 1));
+        CK(dalloc(&W.part, nc * NV * 4));
+        CK(dalloc(&W.U, nd * dim));
+        CK(dalloc(&W.den, nd));
+        CK(dalloc(&W.gnum, nd * dim));
+        CK(dalloc(&W.gden, nd));
+        CK(dalloc(&W.gadv, nc * NV * dim));
+        CK(dalloc(&W.gdv, nc * NV * dim));
+        CK(dalloc(&W.V, nd * dim));
+        CK(dalloc(&W.Vold, nd * dim));
+        CK(dalloc(&W.gU, nd * dim));
+        CK(dalloc(&W.gV, nd * dim));
+        CK(dalloc(&W.gVold, nd * dim));
+        CK(dalloc(&W.nempty, 1));
+        CK(dalloc(&W.err, 1));
+        CK(dalloc(&W.nq, 1));
+        CK(dalloc(&W.Vcell, nc * NV * VS));
+        CK(dalloc(&W.dVcell, nc * NV * VS));
+        CK(dalloc(&W.Wcell, nc * NV * VS));
+        W.mesh_ready = true;
+    }
+    const uint32_t tneed = (std::max<uint32_t>(ns, (uint32_t)nc) + WIN_TILE - 1) / WIN_TILE + 1;
+    if (tneed > W.tsumcap) {
+        dfree(W.tsum);
+        W.tsum = nullptr;
+        W.tsumcap = 0;
+        CK(dalloc(&W.tsum, tneed));
+        W.tsumcap = tneed;
+    }
+    if (n > W.ncap || nseg > W.segcap || tseg > W.tcap) {
+        CK(cudaStreamSynchronize(h->stream));
+        const uint32_t ncap = std::max<uint32_t>(std::max<uint32_t>(n, 1024), W.ncap);
+        const int segcap = std::max(nseg, W.segcap), tcap = std::max(tseg, W.tcap);
+        free_win_particles(W);
+        const size_t nck = (size_t)segcap * ncap, nrec = (size_t)(tcap + 1) * ncap;
+        CK(dalloc(&W.slot, ncap));
+        CK(dalloc(&W.ck_cell, nck));
+        CK(cudaMalloc(&W.ck_xi, nck * dim * es));
+        CK(dalloc(&W.fin_cell, ncap));
+        CK(cudaMalloc(&W.fin_xi, (size_t)ncap * dim * es));
+        CK(cudaMalloc(&W.fin_v, (size_t)ncap * dim * es));
+        CK(dalloc(&W.r_cell, ncap));
+        CK(cudaMalloc(&W.r_xi, (size_t)ncap * dim * es));
+        CK(dalloc(&W.rec_cell, nrec));
+        CK(cudaMalloc(&W.rec_xi, nrec * dim * es));
+        if (fp64) {
+            CK(dalloc(&W.ck_x, nck * dim));
+            CK(dalloc(&W.fin_x, (size_t)ncap * dim));
+            CK(dalloc(&W.r_x, (size_t)ncap * dim));
+        }
+        CK(dalloc(&W.q, ncap));
+        CK(dalloc(&W.order, ncap));
+        CK(dalloc(&W.order2, ncap));
+        CK(dalloc(&W.gxi, (size_t)ncap * dim));
+        CK(dalloc(&W.gv, (size_t)ncap * dim));
+        CK(dalloc(&W.hv0, (size_t)ncap * dim));
+        W.ncap = ncap;
+        W.segcap = segcap;
+        W.tcap = tcap;
+    }
+    return PFEM2GPU_OK;
+}
+
+WinArgs winargs(pfem2gpu_handle* h)
+{
+    auto& W = h->win;
+    WinArgs w{};
+    w.a = args(h);
+    w.n = W.n;
+    w.K = W.K;
+    w.C = W.C;
+    w.nseg = W.nseg;
+    w.do_correct = W.do_correct ? 1 : 0;
+    w.keep_empty = h->prm.empty_dof_policy == 1 ? 1 : 0;
+    w.V = W.V;
+    w.Vold = W.do_correct ? W.Vold : nullptr;
+    w.slot = W.slot;
+    const size_t es = esize(h), nck = (size_t)W.segcap * W.ncap, nrec = (size_t)(W.tcap + 1) * W.ncap;
+    w.ck_cell = W.ck_cell;
+    w.fin_cell = W.fin_cell;
+    w.r_cell = W.r_cell;
+    w.rec_cell = W.rec_cell;
+    for (int d = 0; d < h->dim; ++d) {
+        w.ck_xi[d] = (char*)W.ck_xi + d * nck * es;
+        w.ck_x[d] = W.ck_x ? W.ck_x + d * nck : nullptr;
+        w.fin_xi[d] = (char*)W.fin_xi + (size_t)d * W.ncap * es;
+        w.fin_x[d] = W.fin_x ? W.fin_x + (size_t)d * W.ncap : nullptr;
+        w.fin_v[d] = (char*)W.fin_v + (size_t)d * W.ncap * es;
+        w.r_xi[d] = (char*)W.r_xi + (size_t)d * W.ncap * es;
+        w.r_x[d] = W.r_x ? W.r_x + (size_t)d * W.ncap : nullptr;
+        w.rec_xi[d] = (char*)W.rec_xi + d * nrec * es;
+    }
+    w.q = W.q;
+    w.nq = W.nq;
+    w.ccnt = W.ccnt;
+    w.cstart = W.cstart;
+    w.tsum = W.tsum;
+    w.order = W.order;
+    w.order2 = W.order2;
+    w.part = W.part;
+    w.U = W.U;
+    w.den = W.den;
+    w.gnum = W.gnum;
+    w.gden = W.gden;
+    w.gxi = W.gxi;
+    w.gv = W.gv;
+    w.gadv = W.gadv;
+    w.gdv = W.gdv;
+    w.Wcell = W.Wcell;
+    w.dVcell = W.dVcell;
+    w.nempty = W.nempty;
+    w.err = W.err;
+    return w;
+}
+
+int window_forward_impl(pfem2gpu_handle* h, int K, int C, const double* V, const double* Vold, const double* v0,
+                        double* U_out, bool host)
+{
+    if (!h || !V || K < 0 || C < 1) return PFEM2GPU_ERR_ARG;
+    if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "window before seed");
+    if ((int64_t)C * h->pp.S > 100000) return fail(h, PFEM2GPU_ERR_ARG, "checkpoint_every x sub-steps too large");
+    int rc = apply_pending_correction(h);
+    if (rc) return rc;
+    if ((rc = sync_stats(h))) return rc;
+    auto& W = h->win;
+    const uint32_t n = (uint32_t)h->stats_h->n_particles, ns = (uint32_t)h->stats_h->n_slots;
+    const int nseg = K > 0 ? (K + C - 1) / C : 1;
+    const int tseg = std::min(C, std::max(K, 1)) * h->pp.S;
+    if ((rc = win_reserve(h, n, ns, nseg, tseg))) return rc;
+    W.ready = false;
+    W.n = n;
+    W.K = K;
+    W.C = C;
+    W.nseg = nseg;
+    W.do_correct = Vold != nullptr;
+    const size_t vbytes = (size_t)h->dim * h->nD * sizeof(double);
+    const cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    CK(cudaMemcpyAsync(W.V, V, vbytes, kind, h->stream));
+    if (Vold) CK(cudaMemcpyAsync(W.Vold, Vold, vbytes, kind, h->stream));
+    const double* v0d = v0;
+    if (v0 && host) {
+        CK(cudaMemcpyAsync(W.hv0, v0, (size_t)n * h->dim * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        v0d = W.hv0;
+    }
+    if ((rc = stage_v(h, W.V, Vold ? W.Vold : nullptr, true))) return rc;
+    // FP64 per-cell vertex velocities for the backward pass
+    WinArgs w = winargs(h);
+    run(h, "window_cells", [&] {
+        return launch_cell_v(h->dim, 0, W.V, Vold ? W.Vold : nullptr, h->cd, h->nC, h->nD, W.Vcell, W.dVcell,
+                             h->stream) +
+               launch_win_wcell(h->dim, w, W.Vcell, W.Wcell, h->stream);
+    });
+    run(h, "window_compact", [&] { return launch_win_compact(h->S0.cell, ns, (uint32_t)h->nC, W.tsum, W.slot, h->stream); });
+    run(h, "window_init", [&] { return launch_win_init(h->dim, h->prec, w, v0d, h->stream); });
+    run(h, "window_forward", [&] { return launch_win_forward(h->dim, h->prec, w, h->stream); });
+    W.rec_seg = K > 0 ? nseg - 1 : -1;
+    CK(cudaMemsetAsync(W.ccnt, 0, (size_t)h->nC * sizeof(uint32_t), h->stream));
+    CK(cudaMemsetAsync(W.nempty, 0, sizeof(unsigned long long), h->stream));
+    run(h, "window_project", [&] { return launch_win_project(h->dim, h->prec, w, h->stream); });
+    if ((rc = check_async(h))) return rc;
+    if (U_out) CK(cudaMemcpyAsync(U_out, W.U, vbytes, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, h->stream));
+    if (host) CK(cudaStreamSynchronize(h->stream));
+    W.ready = true;
+    return PFEM2GPU_OK;
+}
+
+int window_backward_impl(pfem2gpu_handle* h, const double* gU, double* g_v0, double* gV, double* gVold, bool host)
+{
+    if (!h || !gU) return PFEM2GPU_ERR_ARG;
+    auto& W = h->win;
+    if (!W.ready) return fail(h, PFEM2GPU_ERR_STATE, "window backward without a window forward");
+    int rc;
+    // the window's velocities again (other calls may have staged others since)
+    if ((rc = stage_v(h, W.V, W.do_correct ? W.Vold : nullptr, true))) return rc;
+    const size_t vbytes = (size_t)h->dim * h->nD * sizeof(double);
+    const double* gUd = gU;
+    if (host) {
+        CK(cudaMemcpyAsync(W.gU, gU, vbytes, cudaMemcpyHostToDevice, h->stream));
+        gUd = W.gU;
+    }
+    double* gv0d = host ? (g_v0 ? W.hv0 : nullptr) : g_v0;
+    double* gVd = host ? W.gV : gV;
+    double* gVoldd = host ? W.gVold : gVold;
+    const size_t nacc = (size_t)h->nC * (1 << h->dim) * h->dim * sizeof(double);
+    CK(cudaMemsetAsync(W.gadv, 0, nacc, h->stream));
+    CK(cudaMemsetAsync(W.gdv, 0, nacc, h->stream));
+    CK(cudaMemsetAsync(W.err, 0, sizeof(unsigned int), h->stream));
+    WinArgs w = winargs(h);
+    run(h, "window_backward",
+        [&] { return launch_win_backward(h->dim, h->prec, w, gUd, gv0d, gVd, gVoldd, W.rec_seg, h->stream); });
+    W.rec_seg = W.K > 0 ? 0 : -1;
+    if ((rc = check_async(h))) return rc;
+    if (host) {
+        if (g_v0) CK(cudaMemcpyAsync(g_v0, W.hv0, (size_t)W.n * h->dim * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        if (gV) CK(cudaMemcpyAsync(gV, W.gV, vbytes, cudaMemcpyDeviceToHost, h->stream));
+        if (gVold) CK(cudaMemcpyAsync(gVold, W.gVold, vbytes, cudaMemcpyDeviceToHost, h->stream));
+    }
+    unsigned int err = 0;
+    CK(cudaMemcpyAsync(&err, W.err, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->profiling) collect_profile(h);
+    if (err) return fail(h, PFEM2GPU_ERR_DEVICE, "window backward: a recomputed segment left the forward trajectory");
+    return PFEM2GPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -548,6 +816,8 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
     free_state(h->S0);
     free_state(h->S1);
     free_state(h->T);
+    free_win_particles(h->win);
+    free_win_mesh(h->win);
     if (h->stats_h) cudaFreeHost(h->stats_h);
     for (auto& row : h->move_graph)
         for (auto& g : row)
@@ -645,6 +915,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
                     (void*)h->ccount, (void*)h->cocc, (void*)h->cub, (void*)h->coff, (void*)h->tiles64,
                     (void*)h->jinv32, (void*)h->vrec32, (void*)h->dvrec32, h->partials, (void*)h->twisted})
         dfree(p);
+    free_win_mesh(h->win);
     h->has_mesh = false;
     h->nC = (int)n_cells;
     h->nV = (int)n_verts;
@@ -1071,6 +1342,63 @@ int pfem2gpu_write_vtu(pfem2gpu_handle* h, const char* path)
     for (int64_t i = 0; i < n; ++i) std::fprintf(f, "  0");
     std::fprintf(f, "\n        </DataArray>\n      </PointData>\n    </Piece>\n  </UnstructuredGrid>\n</VTKFile>\n");
     std::fclose(f);
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_window_forward_device(pfem2gpu_handle* h, int32_t steps, int32_t checkpoint_every, const double* dV,
+                                   const double* dVold, const double* dv0, double* dU_out)
+{
+    return window_forward_impl(h, steps, checkpoint_every, dV, dVold, dv0, dU_out, false);
+}
+
+int pfem2gpu_window_backward_device(pfem2gpu_handle* h, const double* dgU, double* dg_v0, double* dg_V,
+                                    double* dg_Vold)
+{
+    return window_backward_impl(h, dgU, dg_v0, dg_V, dg_Vold, false);
+}
+
+int pfem2gpu_adjoint(pfem2gpu_handle* h, int32_t steps, int32_t checkpoint_every, const double* V, const double* Vold,
+                     const double* v0, const double* gU, double* U, double* g_v0, double* g_V, double* g_Vold)
+{
+    int rc = window_forward_impl(h, steps, checkpoint_every, V, Vold, v0, U, true);
+    if (rc) return rc;
+    return window_backward_impl(h, gU, g_v0, g_V, g_Vold, true);
+}
+
+int pfem2gpu_window_particles(pfem2gpu_handle* h, int32_t* cell, double* xi, double* v, int64_t capacity, int64_t* n)
+{
+    if (!h || !n) return PFEM2GPU_ERR_ARG;
+    auto& W = h->win;
+    if (!W.ready) return fail(h, PFEM2GPU_ERR_STATE, "no window forward");
+    *n = W.n;
+    if (capacity < (int64_t)W.n) return fail(h, PFEM2GPU_ERR_ARG, "output arrays too small");
+    const int dim = h->dim;
+    const size_t n0 = W.n, es = esize(h);
+    std::vector<uint32_t> c(n0);
+    std::vector<unsigned char> buf(n0 * es);
+    CK(cudaMemcpyAsync(c.data(), W.fin_cell, n0 * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (cell)
+        for (size_t p = 0; p < n0; ++p) cell[p] = c[p] == LOST ? -1 : (int32_t)c[p];
+    for (int which = 0; which < 2; ++which) {
+        double* out = which ? v : xi;
+        if (!out) continue;
+        for (int d = 0; d < dim; ++d) {
+            const char* src = (const char*)(which ? W.fin_v : W.fin_xi) + (size_t)d * W.ncap * es;
+            CK(cudaMemcpyAsync(buf.data(), src, n0 * es, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            for (size_t p = 0; p < n0; ++p)
+                out[p * dim + d] = es == 8 ? reinterpret_cast<const double*>(buf.data())[p]
+                                           : (double)reinterpret_cast<const float*>(buf.data())[p];
+        }
+    }
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_window_size(pfem2gpu_handle* h, int64_t* n)
+{
+    if (!h || !n) return PFEM2GPU_ERR_ARG;
+    *n = h->win.ready ? (int64_t)h->win.n : -1;
     return PFEM2GPU_OK;
 }
 

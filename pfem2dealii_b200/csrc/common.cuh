@@ -124,6 +124,54 @@ struct StepArgs {
     uint32_t capacity;
 };
 
+// Differentiated window (window.cuh): device arrays of one window.
+constexpr int WIN_BT = 128;             // threads per block of the per-particle window kernels
+constexpr int WIN_TILE = 1024;          // elements per tile of the window scans
+constexpr uint32_t ERR_REPLAY = 128u;   // backward: a recomputed segment ended elsewhere than its checkpoint
+
+struct WinArgs {
+    StepArgs a;                // mesh, parameters, staged velocities (Vc/dVc or vrec32/dvrec32, Vd = V)
+    uint32_t n;                // particles in the window
+    int K, C, nseg;            // steps, steps per segment, segments
+    int do_correct;            // 1: correction with V - Vold every step
+    int keep_empty;            // empty_dof_policy 1: U = V where no particle weighs
+    const double* V;           // dim x nD component-major
+    const double* Vold;        // dim x nD or null
+    const uint32_t* slot;      // window particle -> slot of the handle's current state
+    uint32_t* ck_cell;         // nseg x n: state at the start of each segment
+    void* ck_xi[3];            // nseg x n (Real)
+    double* ck_x[3];           // nseg x n (FP64 form)
+    uint32_t* fin_cell;        // n: the forward's running state, after K steps its end (LOST: deleted)
+    void* fin_xi[3];           // n (Real)
+    double* fin_x[3];          // n (FP64 form)
+    void* fin_v[3];            // n (Real)
+    uint32_t* r_cell;          // n: running state of a segment replay
+    void* r_xi[3];             // n (Real)
+    double* r_x[3];            // n (FP64 form)
+    uint32_t* rec_cell;        // (C*S + 1) x n: states before every sub-step of one segment, then its end
+    void* rec_xi[3];           // (C*S + 1) x n (Real)
+    uint2* q;                  // n: (particle, sub-step) of the step's face crossers
+    uint32_t* nq;              // queue length
+    uint32_t* ccnt;            // nC: particles per final cell, then placement counters
+    uint32_t* cstart;          // nC + 1: exclusive scan of ccnt
+    uint32_t* tsum;            // scan tile sums
+    uint32_t* order;           // n: particles by final cell
+    uint32_t* order2;          // n: the same, ascending particle index inside each cell
+    double* part;              // nC x NV x 4: sum N_i v_d and sum N_i per (cell, vertex)
+    double* U;                 // dim x nD
+    double* den;               // nD
+    double* gnum;              // dim x nD
+    double* gden;              // nD
+    double* gxi;               // dim x n: adjoint of xi between segments
+    double* gv;                // dim x n: adjoint of the particle velocity
+    double* gadv;              // nC x NV x DIM: dJ/dV through the sub-steps
+    double* gdv;               // nC x NV x DIM: dJ/d(V - Vold) through the corrections
+    const double* Wcell;       // nC x NV x VS: X_i + h V_i per cell vertex (the sub-step map's vertices)
+    const double* dVcell;      // nC x NV x VS: V - Vold per cell vertex (FP64)
+    unsigned long long* nempty;
+    unsigned int* err;
+};
+
 template <int DIM> struct Dims {
     static constexpr int NV = 1 << DIM;
     static constexpr int VS = DIM == 3 ? 4 : 2;        // padded velocity stride

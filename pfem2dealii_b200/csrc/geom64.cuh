@@ -29,6 +29,22 @@ __device__ __forceinline__ void shape64(const double* xi, double* N)
     }
 }
 
+// dN_i/dxi_k = (b_k ? 1 : -1) prod_{m != k} (b_m ? xi_m : 1 - xi_m), product in m order.
+template <int DIM>
+__device__ __forceinline__ void shape_grad64(const double* xi, double (*G)[DIM])
+{
+#pragma unroll
+    for (int i = 0; i < (1 << DIM); ++i)
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            double g = ((i >> k) & 1) ? 1.0 : -1.0;
+#pragma unroll
+            for (int m = 0; m < DIM; ++m)
+                if (m != k) g = g * lag64((i >> m) & 1, xi[m]);
+            G[i][k] = g;
+        }
+}
+
 template <int DIM>
 __device__ __forceinline__ void fwd64(const double (*X)[DIM], const double* xi, double* x)
 {

@@ -55,4 +55,16 @@ int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const 
 int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
                       const float* jinv32, int nC, int nD, float* vrec, float* dvrec, cudaStream_t s);
 
+// window_f64.cu / window_f32.cu: the differentiated window (window.cuh)
+struct WinArgs;
+int launch_win_compact(const uint32_t* cells, uint32_t ns, uint32_t nC, uint32_t* tsum, uint32_t* slot,
+                       cudaStream_t s);
+int launch_win_scan(const uint32_t* in, uint32_t n, uint32_t* tsum, uint32_t* out, cudaStream_t s);
+int launch_win_init(int dim, int prec, const WinArgs& w, const double* v0, cudaStream_t s);
+int launch_win_forward(int dim, int prec, const WinArgs& w, cudaStream_t s);
+int launch_win_project(int dim, int prec, const WinArgs& w, cudaStream_t s);
+int launch_win_backward(int dim, int prec, const WinArgs& w, const double* gU, double* g_v0, double* gV,
+                        double* gVold, int rec_seg, cudaStream_t s);
+int launch_win_wcell(int dim, const WinArgs& w, const double* Vcell, double* Wout, cudaStream_t s);
+
 }  // namespace pfem2

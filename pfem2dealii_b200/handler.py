@@ -189,6 +189,51 @@ class ParticleHandler:
         """correct + move + project on device vectors as one CUDA graph."""
         self._ck(self.L.pfem2gpu_step_device(self.h, _ptr(dV), _ptr(dVold), _ptr(dout)))
 
+    # -- differentiated window (no counterpart in the reference) -------------
+    def window_forward_device(self, steps, checkpoint_every, dV, dVold=None, dv0=None, dU=None):
+        """K steps of correct + move without count correction from the
+        current particles, then the projection, on CUDA tensors: dV, dVold,
+        dU (dim, n_dofs) float64, dv0 (n, dim) float64 or None.  The
+        particles are not changed.  Returns dU."""
+        if dU is None:
+            import torch
+
+            dU = torch.empty_like(dV)
+        self._ck(self.L.pfem2gpu_window_forward_device(self.h, int(steps), int(checkpoint_every), _ptr(dV),
+                                                       _ptr(dVold), _ptr(dv0), _ptr(dU)))
+        return dU
+
+    def window_backward_device(self, dgU, dg_v0=None, dg_V=None, dg_Vold=None):
+        """Adjoint of the last window forward for dJ/dU = dgU (CUDA tensors)."""
+        self._ck(self.L.pfem2gpu_window_backward_device(self.h, _ptr(dgU), _ptr(dg_v0), _ptr(dg_V),
+                                                        _ptr(dg_Vold)))
+
+    def window_particles(self):
+        """End states of the last window forward: cell (-1: deleted), xi, v."""
+        n = C.c_int64()
+        self._ck(self.L.pfem2gpu_window_size(self.h, C.byref(n)))
+        k = max(n.value, 1)
+        cell = np.zeros(k, np.int32)
+        xi = np.zeros((k, self.dim))
+        v = np.zeros((k, self.dim))
+        self._ck(self.L.pfem2gpu_window_particles(self.h, _ptr(cell), _ptr(xi), _ptr(v), k, C.byref(n)))
+        return {"cell": cell[: n.value], "xi": xi[: n.value], "v": v[: n.value]}
+
+    def adjoint(self, steps, checkpoint_every, V, gU, Vold=None, v0=None):
+        """Window forward + adjoint on host arrays: (U, g_v0 (n, dim), g_V, g_Vold)."""
+        n = self.stats()["n_particles"]
+        V = _host(V, np.float64)
+        gU = _host(gU, np.float64)
+        Vold = None if Vold is None else _host(Vold, np.float64)
+        v0 = None if v0 is None else _host(v0, np.float64)
+        U = np.empty((self.dim, self.mesh.n_dofs))
+        gv0 = np.empty((max(n, 1), self.dim))
+        gV = np.empty_like(U)
+        gVo = np.empty_like(U)
+        self._ck(self.L.pfem2gpu_adjoint(self.h, int(steps), int(checkpoint_every), _ptr(V), _ptr(Vold), _ptr(v0),
+                                         _ptr(gU), _ptr(U), _ptr(gv0), _ptr(gV), _ptr(gVo)))
+        return U, gv0[:n], gV, gVo
+
     # -- particle access ------------------------------------------------------
     def particles(self):
         """Host copy of the particles (begin()/end() of the reference)."""

@@ -1,0 +1,226 @@
+"""The differentiated window and its adjoint on the GPU (through the C ABI).
+
+FP64 form: the window forward equals the oracle's window (projection sums
+to 1e-12); gradients equal the oracle's adjoint to 1e-10 (relative L2; only
+summation orders differ) and central finite differences of the GPU's own
+forward (h = 1e-6) to 1e-6 along random directions.  The checkpoint
+interval does not change the gradients.  FP32 form: gradients within the
+tolerances stated in each test of the FP64 ones.  The autograd harness
+gives the ABI's gradients.
+"""
+import numpy as np
+import pytest
+
+from pfem2dealii_b200.handler import ParticleHandler
+
+from . import cases
+from .cases import by_id
+
+pytestmark = pytest.mark.gpu
+
+G_RTOL_FP64 = 1e-10   # GPU FP64 adjoint vs oracle adjoint (relative L2)
+FD_RTOL = 1e-6        # adjoint vs central differences, h = 1e-6
+U_RTOL_FP64 = 1e-12
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def setup(case, precision="fp64", pre_steps=2, **pkw):
+    o = cases.oracle_for(case)
+    g = ParticleHandler(case.mesh.dim, cases.params(case, **pkw), precision)
+    g.initialize_maps(case.mesh)
+    o.seed(case.V)
+    g.seed_particles(case.V)
+    for _ in range(pre_steps):
+        o.step(case.V, case.Vold)
+        g.step(case.V, case.Vold)
+    return o, g
+
+
+def objective(U, n_probe=16, seed=3):
+    rng = np.random.default_rng(seed)
+    finite = np.where(np.all(np.isfinite(U), 0))[0]
+    probe = rng.choice(finite, size=min(n_probe, len(finite)), replace=False)
+    T = U[:, probe] + 0.01 * rng.standard_normal((U.shape[0], len(probe)))
+
+    def J(Ux):
+        return float(np.sum((Ux[:, probe] - T) ** 2))
+
+    def gU(Ux):
+        g = np.zeros_like(Ux)
+        g[:, probe] = 2.0 * (Ux[:, probe] - T)
+        return g
+
+    return J, gU
+
+
+def gpu_forward(g, K, C, V, Vold=None, v0=None):
+    import torch
+
+    dV = torch.tensor(V, device="cuda")
+    dVo = None if Vold is None else torch.tensor(Vold, device="cuda")
+    dv0 = None if v0 is None else torch.tensor(np.ascontiguousarray(v0), device="cuda")
+    U = g.window_forward_device(K, C, dV, dVo, dv0)
+    g.synchronize()
+    return U.cpu().numpy()
+
+
+CASES = {
+    "channel": lambda: cases.channel(32, 8, dt=0.02),
+    "duct": lambda: cases.duct(16, 4, 4, dt=0.03),
+    "cylinder": lambda: cases.cylinder(24, 12, 60, dt=4e-3),
+    "cube": lambda: cases.cube(6, q=(2, 2, 2), dt=0.05),
+}
+
+
+@pytest.mark.parametrize("which", list(CASES))
+def test_fp64_adjoint_matches_oracle(which):
+    c = CASES[which]()
+    o, g = setup(c)
+    K, C = 6, 2
+    Uo = o.window_forward(K, c.V, c.Vold)
+    J, gUf = objective(Uo)
+    gU = gUf(Uo)
+    Uo2, gv0_o, gV_o, gVo_o = o.window_adjoint(K, c.V, gU, Vold=c.Vold)
+    Ug, gv0_g, gV_g, gVo_g = g.adjoint(K, C, c.V, gU, Vold=c.Vold)
+    # the window trajectories themselves are the oracle's, bit for bit
+    Wo, Wg = o.window_particles(K, c.V, c.Vold), g.window_particles()
+    assert np.array_equal(np.isnan(Uo), np.isnan(Ug))
+    m = np.isfinite(Uo)
+    assert np.max(np.abs(Uo[m] - Ug[m])) <= U_RTOL_FP64 * np.max(np.abs(Uo[m]))
+    # per-particle gradients in id order (oracle: vector order, GPU: cell order)
+    po, pg = o.particles(), g.particles()
+    oo, og = np.argsort(po["id"]), np.argsort(pg["id"])
+    assert np.array_equal(po["id"][oo], pg["id"][og])
+    for k in ("cell", "xi", "v"):
+        assert np.array_equal(Wo[k][oo], Wg[k][og]), k
+    assert rel(gv0_g[og], gv0_o[oo]) <= G_RTOL_FP64
+    assert rel(gV_g, gV_o) <= G_RTOL_FP64
+    assert rel(gVo_g, gVo_o) <= G_RTOL_FP64
+    assert np.linalg.norm(gV_o) > 0 and np.linalg.norm(gv0_o) > 0
+
+
+@pytest.mark.parametrize("which", ["channel", "cylinder", "cube"])
+def test_fp64_adjoint_central_differences(which):
+    c = CASES[which]()
+    _, g = setup(c)
+    K, C = 5, 2
+    P = g.particles()
+    v0 = P["v"]
+    U0 = gpu_forward(g, K, C, c.V, c.Vold)
+    J, gUf = objective(U0)
+    _, gv0, gV, gVo = g.adjoint(K, C, c.V, gUf(U0), Vold=c.Vold)
+    rng = np.random.default_rng(11)
+    h = 1e-6
+    # nodal directions leave the no-slip wall DoFs (V = 0) alone: there the
+    # flow brings particles to within ~1e-7 of the wall, and a wall velocity
+    # would push them out of the mesh (deleted: J jumps)
+    free = np.any(c.V != 0.0, axis=0)
+    for name in ("v0", "V", "Vold"):
+        for _ in range(3):
+            if name == "v0":
+                d = rng.standard_normal(v0.shape)
+                Jp = J(gpu_forward(g, K, C, c.V, c.Vold, v0 + h * d))
+                Jm = J(gpu_forward(g, K, C, c.V, c.Vold, v0 - h * d))
+                ana = np.sum(gv0 * d)
+            elif name == "V":
+                d = rng.standard_normal(c.V.shape) * free
+                Jp = J(gpu_forward(g, K, C, c.V + h * d, c.Vold))
+                Jm = J(gpu_forward(g, K, C, c.V - h * d, c.Vold))
+                ana = np.sum(gV * d)
+            else:
+                d = rng.standard_normal(c.V.shape) * free
+                Jp = J(gpu_forward(g, K, C, c.V, c.Vold + h * d))
+                Jm = J(gpu_forward(g, K, C, c.V, c.Vold - h * d))
+                ana = np.sum(gVo * d)
+            fd = (Jp - Jm) / (2 * h)
+            assert abs(fd - ana) <= FD_RTOL * abs(fd), (name, fd, ana)
+
+
+def test_checkpoint_interval_does_not_change_gradients():
+    c = CASES["duct"]()
+    _, g = setup(c)
+    K = 7
+    U0 = gpu_forward(g, K, 1, c.V, c.Vold)
+    _, gUf = objective(U0)
+    gU = gUf(U0)
+    ref = None
+    for C in (1, 3, 7, 50):
+        out = g.adjoint(K, C, c.V, gU, Vold=c.Vold)
+        if ref is None:
+            ref = out
+            continue
+        assert np.array_equal(out[0], ref[0], equal_nan=True)
+        assert np.array_equal(out[1], ref[1])
+        assert rel(out[2], ref[2]) <= 1e-13 and rel(out[3], ref[3]) <= 1e-13
+
+
+def test_window_leaves_particles_and_accepts_zero_steps():
+    c = CASES["channel"]()
+    o, g = setup(c)
+    before = by_id(g.particles())
+    U = gpu_forward(g, 0, 1, c.V)
+    after = by_id(g.particles())
+    for k in before:
+        assert np.array_equal(before[k], after[k])
+    Up = g.project_particle_fields()
+    m = np.isfinite(Up)
+    assert np.max(np.abs(U[m] - Up[m])) <= 1e-12 * np.max(np.abs(Up[m]))
+    # without a correction the gradient with respect to Vold is zero
+    J, gUf = objective(U)
+    _, gv0, gV, gVo = g.adjoint(3, 2, c.V, gUf(U))
+    assert not gVo.any() and np.linalg.norm(gV) > 0
+    # a product step after the window continues from the unchanged particles
+    o.step(c.V, c.Vold)
+    g.step(c.V, c.Vold)
+    a, b = by_id(o.particles()), by_id(g.particles())
+    assert np.array_equal(a["cell"], b["cell"]) and np.array_equal(a["xi"], b["xi"])
+
+
+@pytest.mark.parametrize("which", ["duct", "cylinder"])
+def test_fp32_adjoint_against_fp64(which):
+    """FP32 form: FP32 trajectories, FP64 adjoint arithmetic along them."""
+    c = CASES[which]()
+    o, g64 = setup(c, "fp64")
+    _, g32 = setup(c, "fp32")
+    K, C = 6, 3
+    U0 = o.window_forward(K, c.V, c.Vold)
+    J, gUf = objective(U0)
+    gU = gUf(U0)
+    _, gv0_o, gV_o, gVo_o = o.window_adjoint(K, c.V, gU, Vold=c.Vold)
+    U32, gv0_32, gV_32, gVo_32 = g32.adjoint(K, C, c.V, gU, Vold=c.Vold)
+    po, p32 = o.particles(), g32.particles()
+    common, ia, ib = np.intersect1d(po["id"], p32["id"], return_indices=True)
+    assert len(common) >= 0.99 * len(po["id"])
+    assert rel(gv0_32[ib], gv0_o[ia]) <= 1e-4
+    assert rel(gV_32, gV_o) <= 1e-4
+    assert rel(gVo_32, gVo_o) <= 1e-4
+
+
+def test_autograd_harness_gives_the_abi_gradients():
+    import torch
+
+    from .adjoint_harness import window
+
+    c = CASES["cylinder"]()
+    _, g = setup(c)
+    K, C = 4, 2
+    P = g.particles()
+    v0 = torch.tensor(P["v"], device="cuda", requires_grad=True)
+    V = torch.tensor(c.V, device="cuda", requires_grad=True)
+    Vold = torch.tensor(c.Vold, device="cuda", requires_grad=True)
+    U = window(g, v0, V, Vold, K, C)
+    Un = U.detach().cpu().numpy()
+    J, gUf = objective(Un)
+    probe_mask = torch.tensor(gUf(Un) != 0, device="cuda")
+    T = torch.tensor(np.where(gUf(Un) != 0, Un - gUf(Un) / 2.0, 0.0), device="cuda")
+    Jt = torch.sum(torch.where(probe_mask, (U - T) ** 2, torch.zeros_like(U)))
+    assert abs(Jt.item() - J(Un)) <= 1e-12 * max(J(Un), 1e-300)
+    Jt.backward()
+    _, gv0, gV, gVo = g.adjoint(K, C, c.V, gUf(Un), Vold=c.Vold)
+    assert rel(v0.grad.cpu().numpy(), gv0) <= 1e-13
+    assert rel(V.grad.cpu().numpy(), gV) <= 1e-12
+    assert rel(Vold.grad.cpu().numpy(), gVo) <= 1e-12

@@ -14,6 +14,8 @@ import pytest
 from oracle.oracle import ORDER_ID, ORDER_VECTOR, Oracle, forward_map, inverse_map, key, shape_values
 from pfem2dealii_b200 import mesh as M
 
+from . import cases
+
 
 def test_shape_partition_and_linear_reproduction():
     rng = np.random.default_rng(1)
@@ -223,3 +225,46 @@ def test_reference_turek_mesh_reads_if_present():
     m = M.read_unv(p)
     assert m.n_cells == 60450 and m.n_verts == 61075
     assert np.allclose(m.vertices.min(0), [0, 0]) and np.allclose(m.vertices.max(0), [2.2, 0.41])
+
+
+@pytest.mark.parametrize("which", ["channel", "cylinder", "cube"])
+def test_oracle_window_adjoint_central_differences(which):
+    """The oracle's adjoint of the differentiated window against central
+    differences of its own window forward (h = 1e-6), along random directions
+    of the starting particle velocities, V and Vold.  The time steps are not
+    dyadic: on these uniform grids a dyadic step can land a particle exactly
+    on a cell face, where J has a kink (the projection weights are only
+    piecewise smooth) and central differences average the two sides."""
+    c = {"channel": lambda: cases.channel(16, 4, S=2, dt=0.047),
+         "cylinder": lambda: cases.cylinder(n_t=12, n_r=6, n_x=20, dt=5e-3),
+         "cube": lambda: cases.cube(n=4, q=(2, 2, 2), dt=5e-2)}[which]()
+    o = cases.oracle_for(c)
+    o.seed(c.V)
+    o.step(c.V, c.Vold)
+    K = 3
+    P = o.particles()
+    U = o.window_forward(K, c.V, c.Vold)
+    rng = np.random.default_rng(1)
+    finite = np.where(np.all(np.isfinite(U), 0))[0]
+    probe = rng.choice(finite, 8, replace=False)
+    T = U[:, probe] + 0.01
+    J = lambda Ux: float(np.sum((Ux[:, probe] - T) ** 2))  # noqa: E731
+    gU = np.zeros_like(U)
+    gU[:, probe] = 2 * (U[:, probe] - T)
+    U2, gv0, gV, gVo = o.window_adjoint(K, c.V, gU, Vold=c.Vold)
+    assert np.array_equal(U2, U, equal_nan=True)
+    h = 1e-6
+    for name in ("v0", "V", "Vold"):
+        d = rng.standard_normal(P["v"].shape if name == "v0" else c.V.shape)
+        if name == "v0":
+            Jp = J(o.window_forward(K, c.V, c.Vold, v0=P["v"] + h * d))
+            Jm = J(o.window_forward(K, c.V, c.Vold, v0=P["v"] - h * d))
+            ana = np.sum(gv0 * d)
+        elif name == "V":
+            Jp, Jm = J(o.window_forward(K, c.V + h * d, c.Vold)), J(o.window_forward(K, c.V - h * d, c.Vold))
+            ana = np.sum(gV * d)
+        else:
+            Jp, Jm = J(o.window_forward(K, c.V, c.Vold + h * d)), J(o.window_forward(K, c.V, c.Vold - h * d))
+            ana = np.sum(gVo * d)
+        fd = (Jp - Jm) / (2 * h)
+        assert abs(fd - ana) <= 1e-6 * abs(fd), (name, fd, ana)
