@@ -16,6 +16,10 @@ e2e     : FP32 form through the host C ABI (pfem2gpu_correct/move/project
           inside the timed region)
 fp64    : the plain FP64 form, same workload, device-resident
 roofline: the dominant kernel (advect) against measured HBM bandwidth
+adjoint : the differentiated window (20 steps, checkpoints every 5) and its
+          adjoint on the same particles, both forms: forward and backward
+          time, their ratio, and the gradient along the inflow amplitude
+          against FP64 central differences
 
 `--impl reference` times the CPU restatement of the reference's particle
 path (the reference itself needs deal.II/Trilinos/MPI, absent here) on all
@@ -279,16 +283,18 @@ def fd_inflow(handler_cls, m, V, Vold, prm, K, C, probe, T, torch, pre_steps=5, 
     return (js[0] - js[1]) / (2 * h)
 
 
-def adjoint_report(handler_cls, m, V, Vold, prm, torch, K=20, C=5):
+def adjoint_report(handler_cls, m, V, Vold, prm, torch, K=20, C=5, forms=("fp32", "fp64")):
     """K-step window + adjoint on the workload, both forms, with the
     directional derivative along the inflow amplitude against FP64 central
-    differences."""
+    differences (one form given: timing only)."""
     rep = {"steps": K, "checkpoint_every": C, "objective": "sum over 64 DoFs of (U - T)^2"}
-    for form in ("fp32", "fp64"):
+    for form in forms:
         r = timed_window(handler_cls, m, V, Vold, prm, form, K, C, torch)
         rep[form] = {k: r[k] for k in ("fwd_ms", "bwd_ms", "bwd_over_fwd", "particles", "dJ_da")}
-        if form == "fp32":
+        if form == forms[0]:
             probe, T = r["probe"], r["T"]
+    if len(forms) == 1:
+        return rep
     fd = fd_inflow(handler_cls, m, V, Vold, prm, K, C, probe, T, torch)
     for form in ("fp32", "fp64"):
         rep[form]["fd_rel_err"] = abs(rep[form]["dJ_da"] - fd) / abs(fd)
@@ -386,7 +392,8 @@ def main():
     m, V, Vold, prm = build_case()
     gpu_index = torch.cuda.current_device()
     if args.adjoint_only:
-        print(json.dumps(adjoint_report(ParticleHandler, m, V, Vold, prm, torch)), flush=True)
+        forms = (args.only,) if args.only else ("fp32", "fp64")
+        print(json.dumps(adjoint_report(ParticleHandler, m, V, Vold, prm, torch, forms=forms)), flush=True)
         return 0
     if args.only:
         r = timed_device_run(ParticleHandler, m, V, Vold, prm, args.only, args.steps, args.warmup, torch)
@@ -433,6 +440,8 @@ def main():
     step_ms_prof = sum(v[0] for v in prof.values()) / args.steps
     # end to end through the host ABI
     re2e = timed_host_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch)
+    # the differentiated window (K = 20, checkpoints every 5) and its adjoint
+    adj = adjoint_report(ParticleHandler, m, V, Vold, prm, torch)
     e2e_value = re2e["particle_steps"] / (re2e["ms"] / 1000.0)
     if rank != 0:
         if world > 1:
@@ -471,6 +480,7 @@ def main():
         "profiled_ms_per_step": step_ms_prof,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": re2e["h2d"],
                 "d2h_bytes_per_step": re2e["d2h"], "ms_per_step": re2e["ms"] / args.steps},
+        "adjoint": adj,
         "gpu_launches": r32["launches"],
         "clocks": clk.summary(),
         "stats": {k: r32["stats"][k] for k in ("n_particles", "lost", "removed", "seeded", "searched",

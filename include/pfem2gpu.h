@@ -140,8 +140,9 @@ int pfem2gpu_launch_count(pfem2gpu_handle* h, uint64_t* count);
  * particles, with check_particle_distribution (:356-410) left out, followed by
  * project_particle_fields (:174-215): U = P(v0, V, Vold), dim x n_dofs
  * component-major (empty_dof_policy applies to DoFs no particle reaches).
- * The per-particle arithmetic is the form's own (FP64 or FP32); the
- * projection sums of the window are FP64 and deterministic.  The handle's
+ * The trajectories are the form's own (FP64 or FP32); particle velocities,
+ * their corrections and the projection sums of the window are FP64 in both
+ * forms, and the sums are deterministic.  The handle's
  * particles are not changed; the handle's staged velocity becomes V.
  *
  * The adjoint returns, for a given gU = dJ/dU of a scalar objective J, the

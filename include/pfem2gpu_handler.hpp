@@ -212,6 +212,18 @@ public:
         return s;
     }
     void synchronize() { check(pfem2gpu_synchronize(h_), h_); }
+
+    // Differentiated window (no counterpart in the reference): `steps` steps
+    // of correct + move without count correction from the current particles,
+    // then the projection U; and the gradients of J (dJ/dU = gU) with respect
+    // to the starting particle velocities (n x dim, particles() order), V
+    // and Vold.  Vold or v0 may be null (no correction / the particles' own
+    // velocities); outputs may be null.  The particles are not changed.
+    void adjoint(int steps, int checkpoint_every, const double* V, const double* Vold, const double* v0,
+                 const double* gU, double* U, double* g_v0, double* g_V, double* g_Vold)
+    {
+        check(pfem2gpu_adjoint(h_, steps, checkpoint_every, V, Vold, v0, gU, U, g_v0, g_V, g_Vold), h_);
+    }
     pfem2gpu_handle* handle() const { return h_; }
 
 private:

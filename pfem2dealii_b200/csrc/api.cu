@@ -87,8 +87,8 @@ struct pfem2gpu_handle {
                  *order = nullptr, *order2 = nullptr, *tsum = nullptr, *ccnt = nullptr, *cstart = nullptr,
                  *nq = nullptr;
         uint2* q = nullptr;
-        void *ck_xi = nullptr, *fin_xi = nullptr, *fin_v = nullptr, *r_xi = nullptr, *rec_xi = nullptr;
-        double *ck_x = nullptr, *fin_x = nullptr, *r_x = nullptr, *gxi = nullptr, *gv = nullptr, *hv0 = nullptr;
+        void *ck_xi = nullptr, *fin_xi = nullptr, *r_xi = nullptr, *rec_xi = nullptr;
+        double *fin_v = nullptr, *ck_x = nullptr, *fin_x = nullptr, *r_x = nullptr, *gxi = nullptr, *gv = nullptr, *hv0 = nullptr;
         double *part = nullptr, *U = nullptr, *den = nullptr, *gnum = nullptr, *gden = nullptr, *gadv = nullptr,
                *gdv = nullptr, *V = nullptr, *Vold = nullptr, *gU = nullptr, *gV = nullptr, *gVold = nullptr,
                *Vcell = nullptr, *dVcell = nullptr, *Wcell = nullptr;
@@ -240,12 +240,13 @@ void free_state(PartState& s)
 void free_win_particles(pfem2gpu_handle::Win& W)
 {
     for (void* p : {(void*)W.slot, (void*)W.ck_cell, (void*)W.fin_cell, (void*)W.r_cell, (void*)W.rec_cell,
-                    (void*)W.order, (void*)W.order2, (void*)W.q, W.ck_xi, W.fin_xi, W.fin_v, W.r_xi, W.rec_xi,
+                    (void*)W.order, (void*)W.order2, (void*)W.q, W.ck_xi, W.fin_xi, (void*)W.fin_v, W.r_xi, W.rec_xi,
                     (void*)W.ck_x, (void*)W.fin_x, (void*)W.r_x, (void*)W.gxi, (void*)W.gv, (void*)W.hv0})
         dfree(p);
     W.slot = W.ck_cell = W.fin_cell = W.r_cell = W.rec_cell = W.order = W.order2 = nullptr;
     W.q = nullptr;
-    W.ck_xi = W.fin_xi = W.fin_v = W.r_xi = W.rec_xi = nullptr;
+    W.ck_xi = W.fin_xi = W.r_xi = W.rec_xi = nullptr;
+    W.fin_v = nullptr;
     W.ck_x = W.fin_x = W.r_x = W.gxi = W.gv = W.hv0 = nullptr;
     W.ncap = 0;
     W.segcap = 0;
@@ -551,7 +552,7 @@ int win_reserve(pfem2gpu_handle* h, uint32_t n, uint32_t ns, int nseg, int tseg)
         CK(cudaMalloc(&W.ck_xi, nck * dim * es));
         CK(dalloc(&W.fin_cell, ncap));
         CK(cudaMalloc(&W.fin_xi, (size_t)ncap * dim * es));
-        CK(cudaMalloc(&W.fin_v, (size_t)ncap * dim * es));
+        CK(dalloc(&W.fin_v, (size_t)ncap * dim));
         CK(dalloc(&W.r_cell, ncap));
         CK(cudaMalloc(&W.r_xi, (size_t)ncap * dim * es));
         CK(dalloc(&W.rec_cell, nrec));
@@ -598,7 +599,7 @@ WinArgs winargs(pfem2gpu_handle* h)
         w.ck_x[d] = W.ck_x ? W.ck_x + d * nck : nullptr;
         w.fin_xi[d] = (char*)W.fin_xi + (size_t)d * W.ncap * es;
         w.fin_x[d] = W.fin_x ? W.fin_x + (size_t)d * W.ncap : nullptr;
-        w.fin_v[d] = (char*)W.fin_v + (size_t)d * W.ncap * es;
+        w.fin_v[d] = W.fin_v + (size_t)d * W.ncap;
         w.r_xi[d] = (char*)W.r_xi + (size_t)d * W.ncap * es;
         w.r_x[d] = W.r_x ? W.r_x + (size_t)d * W.ncap : nullptr;
         w.rec_xi[d] = (char*)W.rec_xi + d * nrec * es;
@@ -1384,11 +1385,14 @@ int pfem2gpu_window_particles(pfem2gpu_handle* h, int32_t* cell, double* xi, dou
         double* out = which ? v : xi;
         if (!out) continue;
         for (int d = 0; d < dim; ++d) {
-            const char* src = (const char*)(which ? W.fin_v : W.fin_xi) + (size_t)d * W.ncap * es;
-            CK(cudaMemcpyAsync(buf.data(), src, n0 * es, cudaMemcpyDeviceToHost, h->stream));
+            const size_t ew = which ? 8 : es;  // velocities are FP64 in both forms
+            const char* src = which ? (const char*)(W.fin_v + (size_t)d * W.ncap)
+                                    : (const char*)W.fin_xi + (size_t)d * W.ncap * es;
+            buf.resize(n0 * ew);
+            CK(cudaMemcpyAsync(buf.data(), src, n0 * ew, cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));
             for (size_t p = 0; p < n0; ++p)
-                out[p * dim + d] = es == 8 ? reinterpret_cast<const double*>(buf.data())[p]
+                out[p * dim + d] = ew == 8 ? reinterpret_cast<const double*>(buf.data())[p]
                                            : (double)reinterpret_cast<const float*>(buf.data())[p];
         }
     }

@@ -144,7 +144,7 @@ struct WinArgs {
     uint32_t* fin_cell;        // n: the forward's running state, after K steps its end (LOST: deleted)
     void* fin_xi[3];           // n (Real)
     double* fin_x[3];          // n (FP64 form)
-    void* fin_v[3];            // n (Real)
+    double* fin_v[3];          // n: particle velocities in FP64 (both forms)
     uint32_t* r_cell;          // n: running state of a segment replay
     void* r_xi[3];             // n (Real)
     double* r_x[3];            // n (FP64 form)

@@ -191,17 +191,28 @@ __device__ __forceinline__ bool win_relocate(const WinArgs& w, uint32_t& c, Real
     return true;
 }
 
-// v += sum_i N_i(xi) (V - Vold)_i in the form's arithmetic (k_advect64/32).
+// v += sum_i N_i(xi) (V - Vold)_i in FP64.  The window keeps the particle
+// velocities (the differentiated variables) in FP64 in both forms: the FP64
+// form with k_advect64's arithmetic, the FP32 form from its FP32 xi and the
+// FP64 per-cell table of V - Vold.
 template <int DIM, typename Real>
-__device__ __forceinline__ void win_correct(const WinArgs& w, uint32_t c, const Real* xi, Real* v)
+__device__ __forceinline__ void win_correct(const WinArgs& w, uint32_t c, const Real* xi, double* v)
 {
-    Real corr[DIM];
+    double corr[DIM];
     if constexpr (std::is_same<Real, double>::value) {
         velocity64<DIM>((const double*)w.a.dVc, c, xi, corr);
     } else {
-        Rec32<DIM> dr;
-        load_rec32<DIM>(w.a.dvrec32, c, dr);
-        eval_poly<DIM>(dr.b, xi, corr);
+        double x[DIM], Dv[1 << DIM][DIM], N[1 << DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) x[d] = (double)xi[d];
+        shape64<DIM>(x, N);
+        load_vcell<DIM>(w.dVcell, c, Dv);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) corr[d] = 0.0;
+#pragma unroll
+        for (int i = 0; i < (1 << DIM); ++i)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) corr[d] = corr[d] + N[i] * Dv[i][d];
     }
 #pragma unroll
     for (int d = 0; d < DIM; ++d) v[d] = v[d] + corr[d];
@@ -232,7 +243,7 @@ __global__ void k_win_init(WinArgs w, const double* __restrict__ v0)
         for (int d = 0; d < DIM; ++d) {
             stw<Real>(w.fin_xi[d], p, ldw<Real>(S.xi[d], s));
             if constexpr (std::is_same<Real, double>::value) w.fin_x[d][p] = ldw<double>(S.x[d], s);
-            stw<Real>(w.fin_v[d], p, v0 ? (Real)v0[(size_t)p * DIM + d] : ldw<Real>(S.v[d], s));
+            w.fin_v[d][p] = v0 ? v0[(size_t)p * DIM + d] : (double)ldw<Real>(S.v[d], s);
         }
     }
 }
@@ -291,12 +302,12 @@ __global__ void __launch_bounds__(256) k_win_adv(WinArgs w, int k, int k0, int r
                     }
                 }
                 if (!REPLAY && w.do_correct) {
-                    Real v[DIM];
+                    double v[DIM];
 #pragma unroll
-                    for (int d = 0; d < DIM; ++d) v[d] = ldw<Real>(w.fin_v[d], p);
+                    for (int d = 0; d < DIM; ++d) v[d] = w.fin_v[d][p];
                     win_correct<DIM, Real>(w, c, xi, v);
 #pragma unroll
-                    for (int d = 0; d < DIM; ++d) stw<Real>(w.fin_v[d], p, v[d]);
+                    for (int d = 0; d < DIM; ++d) w.fin_v[d][p] = v[d];
                 }
                 s = win_incell<DIM, Real>(w, p, c, 0, xi, x, t0);
                 want = s < S;
@@ -387,7 +398,7 @@ __global__ void __launch_bounds__(CELL_WARPS * 32) k_win_cellsum(WinArgs w)
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
                 xi[d] = (double)ldw<Real>(w.fin_xi[d], p);
-                v[d] = (double)ldw<Real>(w.fin_v[d], p);
+                v[d] = w.fin_v[d][p];
             }
             shape64<DIM>(xi, N);
 #pragma unroll
@@ -434,7 +445,7 @@ __global__ void k_win_bwd_init(WinArgs w, double* __restrict__ g_v0)
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
                 xi[d] = (double)ldw<Real>(w.fin_xi[d], p);
-                v[d] = (double)ldw<Real>(w.fin_v[d], p);
+                v[d] = w.fin_v[d][p];
             }
             shape64<DIM>(xi, N);
             shape_grad64<DIM>(xi, G);
@@ -498,46 +509,47 @@ __device__ __forceinline__ void warp_flush(double* buf, uint32_t* keys, uint32_t
 // nodal values accumulate per particle while it stays in one cell; a change
 // of cell adds the sum alone, the segment's end adds it warp-cooperatively.
 // The thread loop is uniform across a warp (warp_flush).
-// N_i and grad N_i together from the pairwise products of the 1D factors
-// (L_m = xi_m or 1 - xi_m); the products are taken in shape64's and
+// N_i and grad N_i of one vertex from the pairwise products of the 1D
+// factors L_m = (1 - xi_m, xi_m); the products are taken in shape64's and
 // shape_grad64's order, so the values are theirs.
 template <int DIM>
-__device__ __forceinline__ void shape_and_grad64(const double* xi, double* N, double (*G)[DIM])
-{
+struct ShapeF {
     double L[DIM][2];
+    double P01[2][2], P02[2][2], P12[2][2];
+    __device__ __forceinline__ explicit ShapeF(const double* xi)
+    {
 #pragma unroll
-    for (int m = 0; m < DIM; ++m) {
-        L[m][0] = 1.0 - xi[m];
-        L[m][1] = xi[m];
-    }
-    if constexpr (DIM == 2) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int b0 = i & 1, b1 = (i >> 1) & 1;
-            N[i] = L[0][b0] * L[1][b1];
-            G[i][0] = b0 ? L[1][b1] : -L[1][b1];
-            G[i][1] = b1 ? L[0][b0] : -L[0][b0];
+        for (int m = 0; m < DIM; ++m) {
+            L[m][0] = 1.0 - xi[m];
+            L[m][1] = xi[m];
         }
-    } else {
-        double P01[2][2], P02[2][2], P12[2][2];
+        if constexpr (DIM == 3) {
 #pragma unroll
-        for (int a = 0; a < 2; ++a)
+            for (int a = 0; a < 2; ++a)
 #pragma unroll
-            for (int b = 0; b < 2; ++b) {
-                P01[a][b] = L[0][a] * L[1][b];
-                P02[a][b] = L[0][a] * L[2][b];
-                P12[a][b] = L[1][a] * L[2][b];
-            }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int b0 = i & 1, b1 = (i >> 1) & 1, b2 = (i >> 2) & 1;
-            N[i] = P01[b0][b1] * L[2][b2];
-            G[i][0] = b0 ? P12[b1][b2] : -P12[b1][b2];
-            G[i][1] = b1 ? P02[b0][b2] : -P02[b0][b2];
-            G[i][2] = b2 ? P01[b0][b1] : -P01[b0][b1];
+                for (int b = 0; b < 2; ++b) {
+                    P01[a][b] = L[0][a] * L[1][b];
+                    P02[a][b] = L[0][a] * L[2][b];
+                    P12[a][b] = L[1][a] * L[2][b];
+                }
         }
     }
-}
+    __device__ __forceinline__ double value_and_grad(int i, double* G) const
+    {
+        const int b0 = i & 1, b1 = (i >> 1) & 1;
+        if constexpr (DIM == 2) {
+            G[0] = b0 ? L[1][b1] : -L[1][b1];
+            G[1] = b1 ? L[0][b0] : -L[0][b0];
+            return L[0][b0] * L[1][b1];
+        } else {
+            const int b2 = (i >> 2) & 1;
+            G[0] = b0 ? P12[b1][b2] : -P12[b1][b2];
+            G[1] = b1 ? P02[b0][b2] : -P02[b0][b2];
+            G[2] = b2 ? P01[b0][b1] : -P01[b0][b1];
+            return P01[b0][b1] * L[2][b2];
+        }
+    }
+};
 
 template <int DIM, typename Real, bool AFF>
 __global__ void __launch_bounds__(128, 3) k_win_rev(WinArgs w, int j)
@@ -610,7 +622,7 @@ __global__ void __launch_bounds__(128, 3) k_win_rev(WinArgs w, int j)
             if (!act) continue;
             const size_t o = (size_t)t * w.n + p;
             const uint32_t ca = w.rec_cell[o];
-            double xa[DIM], y[DIM], N[NV], G[NV][DIM];
+            double xa[DIM], y[DIM];
 #pragma unroll
             for (int d = 0; d < DIM; ++d) xa[d] = (double)ldw<Real>(w.rec_xi[d], o);
 #pragma unroll
@@ -620,7 +632,6 @@ __global__ void __launch_bounds__(128, 3) k_win_rev(WinArgs w, int j)
                 for (int k = 0; k < DIM; ++k) sy = sy + Bi[k][d] * g[k];
                 y[d] = sy;
             }
-            shape_and_grad64<DIM>(xa, N, G);
             if (ca != acc_c) {  // the accumulators belong to a later cell: add them alone
                 if (acc_c != LOST) {
 #pragma unroll
@@ -638,6 +649,9 @@ __global__ void __launch_bounds__(128, 3) k_win_rev(WinArgs w, int j)
                 for (int i = 0; i < NV; ++i) accN[i] = 0.0;
                 acc_c = ca;
             }
+            // shape values and gradients per vertex from the pairwise products of
+            // the 1D factors, in shape64's / shape_grad64's multiplication order
+            ShapeF<DIM> sf(xa);
             double gn[DIM];
 #pragma unroll
             for (int k = 0; k < DIM; ++k) gn[k] = 0.0;
@@ -646,6 +660,8 @@ __global__ void __launch_bounds__(128, 3) k_win_rev(WinArgs w, int j)
             const double2* Dp = reinterpret_cast<const double2*>(w.dVcell + (size_t)ca * NV * VS);
 #pragma unroll
             for (int i = 0; i < NV; ++i) {
+                double Gi[DIM];
+                const double Ni = sf.value_and_grad(i, Gi);
                 double Wi[DIM];
                 const double2 a0 = __ldg(Wp + i * (VS / 2));
                 Wi[0] = a0.x;
@@ -664,11 +680,11 @@ __global__ void __launch_bounds__(128, 3) k_win_rev(WinArgs w, int j)
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) ci = ci + Di[d] * gv[d];
                     si = si + ci;
-                    accN[i] = accN[i] + N[i];
+                    accN[i] = accN[i] + Ni;
                 }
 #pragma unroll
-                for (int k = 0; k < DIM; ++k) gn[k] = gn[k] + G[i][k] * si;
-                const double hn = h * N[i];
+                for (int k = 0; k < DIM; ++k) gn[k] = gn[k] + Gi[k] * si;
+                const double hn = h * Ni;
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) acc[i * DIM + d] = acc[i * DIM + d] + hn * y[d];
             }
@@ -684,8 +700,10 @@ __global__ void __launch_bounds__(128, 3) k_win_rev(WinArgs w, int j)
                     bi_c = ca;
                 }
             } else {
-                double X[NV][DIM], Ja[DIM][DIM];
+                double X[NV][DIM], Ja[DIM][DIM], G[NV][DIM];
                 load_cell64<DIM>(m.cellX, ca, X);
+#pragma unroll
+                for (int i = 0; i < NV; ++i) sf.value_and_grad(i, G[i]);
 #pragma unroll
                 for (int d = 0; d < DIM; ++d)
 #pragma unroll
