@@ -46,7 +46,11 @@ struct SearchOut {
 //     particle's own cell is not retried (its inverse map is deterministic
 //     and already failed).
 // Out of line and by value, so the caller's registers stay registers.
-template <int DIM>
+// LIN (FP32 form on a mesh whose cells are all affine): the inverse map of a
+// candidate is the cell's exact affine inverse xi = A^-1 (p - b), one
+// matrix-vector product instead of the Newton iteration; the FP64 form
+// always takes the Newton restatement (bit parity with its CPU restatement).
+template <int DIM, bool LIN = false>
 __device__ __noinline__ SearchOut search64(const MeshDev m, uint32_t c, Vec<DIM> xo, Vec<DIM> ve, Vec<DIM> xp)
 {
     constexpr int NV = 1 << DIM;
@@ -121,9 +125,14 @@ __device__ __noinline__ SearchOut search64(const MeshDev m, uint32_t c, Vec<DIM>
     for (int k = 0; k < n; ++k) {
         const uint32_t cand = (uint32_t)__ldg(m.v2c_cells + b + perm[k]);
         if (cand == c) continue;
-        load_cell64<DIM>(m.cellX, cand, X);
         double xin[DIM];
-        const int st = inverse_map64<DIM>(X, m.aff + (size_t)cand * AFF, xp.v, xin);
+        int st;
+        if constexpr (LIN) {
+            st = inverse_affine64<DIM>(m.aff + (size_t)cand * AFF, xp.v, xin);
+        } else {
+            load_cell64<DIM>(m.cellX, cand, X);
+            st = inverse_map64<DIM>(X, m.aff + (size_t)cand * AFF, xp.v, xin);
+        }
         if (st) {
             out.map_failures++;
             continue;
@@ -141,8 +150,9 @@ __device__ __noinline__ SearchOut search64(const MeshDev m, uint32_t c, Vec<DIM>
 }
 
 // Full FP64 relocation of an FP32-form particle: rebuild x = F(xi) + u dt_p in
-// FP64, inverse map in the own cell, then the vertex-patch search.
-template <int DIM>
+// FP64, inverse map in the own cell, then the vertex-patch search (LIN: the
+// affine inverse, see search64).
+template <int DIM, bool LIN = false>
 __device__ __noinline__ SearchOut fallback64(const MeshDev m, uint32_t c, Vec<DIM> xo, Vec<DIM> ue, double dtp)
 {
     constexpr int AFF = Dims<DIM>::AFF;
@@ -151,7 +161,8 @@ __device__ __noinline__ SearchOut fallback64(const MeshDev m, uint32_t c, Vec<DI
     fwd64<DIM>(X, xo.v, x);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) x[d] = x[d] + ue.v[d] * dtp;
-    const int st = inverse_map64<DIM>(X, m.aff + (size_t)c * AFF, x, xin);
+    const int st = LIN ? inverse_affine64<DIM>(m.aff + (size_t)c * AFF, x, xin)
+                       : inverse_map64<DIM>(X, m.aff + (size_t)c * AFF, x, xin);
     if (st == 0 && inside_unit<DIM>(xin)) {
         SearchOut out;
         out.cell = c;
@@ -164,7 +175,7 @@ __device__ __noinline__ SearchOut fallback64(const MeshDev m, uint32_t c, Vec<DI
     Vec<DIM> xp;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) xp.v[d] = x[d];
-    SearchOut out = search64<DIM>(m, c, xo, ue, xp);
+    SearchOut out = search64<DIM, LIN>(m, c, xo, ue, xp);
     out.map_failures += st ? 1u : 0u;
     return out;
 }
@@ -374,6 +385,7 @@ constexpr int ADV64_CH = 512;
 template <int DIM>
 __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
 {
+    pdl_entry();
     extern __shared__ __align__(128) unsigned char adv_raw[];
     __shared__ uint64_t bar[2];
     auto* st = reinterpret_cast<AdvStage<DIM, double, ADV64_CH>*>(adv_raw);
@@ -431,6 +443,7 @@ __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
 template <int DIM>
 __global__ void __launch_bounds__(128) k_search64(StepArgs a)
 {
+    pdl_entry();
     const uint32_t nq = *a.nxq < a.capacity ? *a.nxq : a.capacity;
     const MeshDev& m = a.mesh;
     AdvCounters k;
@@ -601,6 +614,7 @@ __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0,
 template <int DIM, bool AFF>
 __global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
 {
+    pdl_entry();
     extern __shared__ __align__(128) unsigned char adv_raw[];
     __shared__ uint64_t bar[2];
     auto* st = reinterpret_cast<AdvStage<DIM, float, ADV_CH>*>(adv_raw);
@@ -655,9 +669,10 @@ __global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
 // Queued FP32 particles: FP64 relocation of sub-step s (x = F(xi) + u dt_p,
 // own cell first, then the vertex-patch search), then the remaining
 // sub-steps in FP32 (relocating in FP64 again whenever needed).
-template <int DIM>
+template <int DIM, bool AFF = false>
 __global__ void __launch_bounds__(128) k_cross32(StepArgs a)
 {
+    pdl_entry();
     const uint32_t nq = *a.nxq < a.capacity ? *a.nxq : a.capacity;
     const MeshDev& m = a.mesh;
     AdvCounters k;
@@ -678,7 +693,7 @@ __global__ void __launch_bounds__(128) k_cross32(StepArgs a)
             velocity_from_dofs<DIM>(m.cd, a.Vd, m.nD, c, xo.v, ue.v);
             k.fallback++;
             const uint32_t c0 = c;
-            const SearchOut so = fallback64<DIM>(m, c, xo, ue, a.pp.dtp);
+            const SearchOut so = fallback64<DIM, AFF>(m, c, xo, ue, a.pp.dtp);
             k.map_failures += so.map_failures;
             if (so.flags & SRCH_OVERFLOW) k.err |= ERR_CAND_OVERFLOW;
             if (so.cell != c0 || !(so.flags & SRCH_FOUND)) k.searched++;
@@ -693,7 +708,7 @@ __global__ void __launch_bounds__(128) k_cross32(StepArgs a)
                 const float t = (float)so.xi[d];
                 xi[d] = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
             }
-            s = substeps32<DIM>(a, c, s + 1, xi);
+            s = substeps32<DIM, AFF>(a, c, s + 1, xi);
             if (s >= a.pp.S) break;
         }
 #pragma unroll

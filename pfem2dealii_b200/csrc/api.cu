@@ -421,6 +421,7 @@ int enqueue_move(pfem2gpu_handle* h, int do_correct)
     a.do_correct = do_correct;
     CK(cudaMemsetAsync(h->nxq, 0, sizeof(uint32_t), h->stream));
     run(h, "advect", [&] { return launch_advect(h->dim, h->prec, a, h->stream); });
+    run(h, "cross", [&] { return launch_cross(h->dim, h->prec, a, h->stream); });
     return enqueue_write(h, a, 1);
 }
 

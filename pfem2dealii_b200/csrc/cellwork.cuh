@@ -478,9 +478,229 @@ __device__ uint2 write_cell_general(const StepArgs& a, WrWarp<DIM, Real>& w, uin
     return make_uint2(removed, err);
 }
 
+// Simple cell: no new particles, and no part can hold more than max+1
+// particles (the cell's count exceeds its occupied parts by at most max), so
+// every particle survives: the stayers in slot order, then the arrivals by
+// key.  Stayers and arrivals fit one round of the warp (L + na <= 32).
+template <int DIM, typename Real>
+__device__ __forceinline__ void write_cell_simple(const StepArgs& a, WrWarp<DIM, Real>& w, uint32_t c, uint32_t s0,
+                                                  uint32_t L, uint32_t na, uint32_t h, uint32_t off, uint32_t ub,
+                                                  uint32_t S, bool staged, int lane, uint32_t& err)
+{
+    const uint32_t u = (uint32_t)lane;
+    const bool st = u < L && (staged ? w.key[s0 - S + u] : a.key[s0 + u]) == c;
+    const bool ar = u >= L && u < L + na;
+    const unsigned m = __ballot_sync(0xffffffffu, st);
+    const uint32_t ns = __popc(m);
+    PData<DIM, Real> pd;
+    uint32_t pos = 0, key = 0xffffffffu;
+    if (st) {
+        if (staged) load_stage<DIM, Real>(w, s0 - S + u, s0 + u, pd);
+        else load_global<DIM, Real>(a, s0 + u, pd);
+        pos = __popc(m & ((1u << lane) - 1u));
+    } else if (ar) {
+        const uint32_t ia = arrival(a, c, u - L, h);
+        if (ia < a.capacity) {
+            load_global<DIM, Real>(a, ia, pd);
+            key = key_of(pd.id, a.pp.seed);
+        } else {
+            err |= ERR_ARRIVAL;
+        }
+    }
+    if (na > 1) {  // arrivals by key
+        uint32_t r = 0;
+        for (uint32_t t = 0; t < na; ++t) {
+            const uint32_t kl = __shfl_sync(0xffffffffu, key, (int)(L + t));
+            r += kl < key ? 1u : 0u;
+        }
+        if (ar) pos = ns + r;
+    } else if (ar) {
+        pos = ns;
+    }
+    if (st || ar) {
+        const uint32_t dst = off + pos;
+        if (dst < a.capacity) store_particle<DIM, Real>(a, dst, c, pd);
+        else err |= ERR_CAPACITY;
+        partial_row<DIM, Real>(w.tr, (int)pos, pd.xi, pd.v);
+    }
+    const uint32_t fin = ns + na;
+    if (fin != ub) err |= ERR_COUNT_UB;
+    __syncwarp();
+    PartialAcc<Real> acc;
+    partial_sum_rows<DIM, Real>(w.tr, (int)fin, lane, acc);
+    store_partial<DIM, Real>(a, c, acc, lane);
+    reset_cell(a, c, lane);
+}
+
+// Fast path of one cell (at most 64 old slots + arrivals and 64 output
+// slots), R rounds of the warp: virtual slots u = 32 r + lane, u < L the
+// cell's old slots (a stayer where its key is c), L <= u < L + na the
+// arrivals.  R = 1 when L + na <= 32, so one-round cells issue no second
+// round.
+template <int DIM, typename Real, int R>
+__device__ __forceinline__ void write_cell_fast(const StepArgs& a, WrWarp<DIM, Real>& w, uint32_t c, uint32_t s0,
+                                                uint32_t L, uint32_t na, uint32_t h, uint32_t off, uint32_t ub,
+                                                uint32_t nseed_expect, uint32_t sb, uint32_t id0, uint32_t S,
+                                                bool staged, int lane, unsigned long long& removed, uint32_t& err)
+{
+    const uint32_t cap = a.capacity;
+    const int apply = a.apply_counts, maxpp = a.pp.maxpp;
+    bool is_stay[R];
+    unsigned stm[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint32_t u = 32u * r + (uint32_t)lane;
+        is_stay[r] = u < L && (staged ? w.key[s0 - S + u] : a.key[s0 + u]) == c;
+        stm[r] = __ballot_sync(0xffffffffu, is_stay[r]);
+    }
+    uint32_t ns = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) ns += __popc(stm[r]);
+    const uint32_t n = ns + na;
+    PData<DIM, Real> pd[R];
+    bool is_arr[R], valid[R];
+    int pe[R];
+    uint32_t key[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint32_t u = 32u * r + (uint32_t)lane;
+        is_arr[r] = u >= L && u < L + na;
+        valid[r] = is_stay[r] || is_arr[r];
+        pd[r].i = 0;
+        pd[r].id = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) pd[r].xi[d] = pd[r].v[d] = Real(0);
+        if (is_stay[r]) {
+            if (staged) load_stage<DIM, Real>(w, s0 - S + u, s0 + u, pd[r]);
+            else load_global<DIM, Real>(a, s0 + u, pd[r]);
+        } else if (is_arr[r]) {
+            const uint32_t ia = arrival(a, c, u - L, h);
+            if (ia < cap) load_global<DIM, Real>(a, ia, pd[r]);
+            else err |= ERR_ARRIVAL;
+        }
+        pe[r] = valid[r] ? ext_part<DIM, Real>(pd[r].xi, a.pp) : 0;
+        key[r] = valid[r] ? key_of(pd[r].id, a.pp.seed) : 0xffffffffu;
+    }
+    int* cnt = w.cnt;
+    for (int p = lane; p < a.pp.npe; p += 32) cnt[p] = 0;
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (valid[r]) atomicAdd(cnt + pe[r], 1);
+    __syncwarp();
+    int kme[R], rank[R];
+    unsigned validm[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        kme[r] = valid[r] ? cnt[pe[r]] : 0;
+        rank[r] = 0;
+        validm[r] = __ballot_sync(0xffffffffu, valid[r]);
+    }
+    // rank inside an over-full part (by key)
+    bool over = false;
+#pragma unroll
+    for (int r = 0; r < R; ++r) over = over || kme[r] > maxpp + 1;
+    if (__any_sync(0xffffffffu, apply && over)) {
+#pragma unroll
+        for (int r2 = 0; r2 < R; ++r2) {
+            for (int l = 0; l < 32; ++l) {
+                const int pl = __shfl_sync(0xffffffffu, pe[r2], l);
+                const uint32_t kl = __shfl_sync(0xffffffffu, key[r2], l);
+                const bool vl = (validm[r2] >> l) & 1u;
+#pragma unroll
+                for (int r = 0; r < R; ++r) rank[r] += (vl && pl == pe[r] && kl < key[r]) ? 1 : 0;
+            }
+        }
+    }
+    // order: stayers (slot order), then arrivals by key
+    const unsigned ltm = (1u << lane) - 1u;
+    uint32_t seq[R];
+    seq[0] = is_stay[0] ? (uint32_t)__popc(stm[0] & ltm) : ns + (uint32_t)lane - L;
+    if constexpr (R == 2)
+        seq[R - 1] = is_stay[R - 1] ? (uint32_t)(__popc(stm[0]) + __popc(stm[R - 1] & ltm))
+                                    : ns + 32u + (uint32_t)lane - L;
+    if (na > 1) {
+        uint32_t ar[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) ar[r] = 0u;
+        for (uint32_t t = 0; t < na; ++t) {
+            const uint32_t u2 = L + t;
+            const uint32_t k0 = __shfl_sync(0xffffffffu, key[0], (int)(u2 & 31u));
+            const uint32_t k1 = R == 2 ? __shfl_sync(0xffffffffu, key[R - 1], (int)(u2 & 31u)) : 0u;
+            const uint32_t kl = (u2 >> 5) ? k1 : k0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) ar[r] += (kl < key[r]) ? 1u : 0u;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (is_arr[r]) seq[r] = ns + ar[r];
+    }
+    bool surv[R];
+    unsigned survm[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        surv[r] = valid[r] && rank[r] < survivors(kme[r], maxpp, apply);
+        survm[r] = __ballot_sync(0xffffffffu, surv[r]);
+    }
+    uint32_t nsurv = 0, pos[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        nsurv += __popc(survm[r]);
+        pos[r] = seq[r];
+    }
+    if (nsurv != n) {  // removals: survivors before in sequence order
+#pragma unroll
+        for (int r = 0; r < R; ++r) pos[r] = 0;
+#pragma unroll
+        for (int r2 = 0; r2 < R; ++r2) {
+            for (int l = 0; l < 32; ++l) {
+                const uint32_t sl = __shfl_sync(0xffffffffu, seq[r2], l);
+                const bool bl = (survm[r2] >> l) & 1u;
+#pragma unroll
+                for (int r = 0; r < R; ++r) pos[r] += (bl && sl < seq[r]) ? 1u : 0u;
+            }
+        }
+    }
+    // partial rows in registers -> shared rows when the cell's final
+    // particles fit one row block, else re-read from the new layout
+    const bool rows = nsurv + nseed_expect <= 32u;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        if (surv[r]) {
+            const uint32_t dst = off + pos[r];
+            if (dst < cap) store_particle<DIM, Real>(a, dst, c, pd[r]);
+            else err |= ERR_CAPACITY;
+            if (rows) partial_row<DIM, Real>(w.tr, (int)pos[r], pd[r].xi, pd[r].v);
+        }
+        removed += (valid[r] && !surv[r]) ? 1 : 0;
+    }
+    uint32_t nseed = 0;
+    if (nseed_expect) {
+        const uint2 sd = write_seeds<DIM, Real>(a, c, cnt, n, off + nsurv, id0, sb, rows ? w.tr : nullptr,
+                                                (int)nsurv, lane);
+        nseed = sd.x;
+        err |= sd.y;
+    }
+    const uint32_t fin = nsurv + nseed;
+    if (nseed != nseed_expect) err |= ERR_COUNT;
+    if (fin > ub) err |= ERR_COUNT_UB;
+    write_holes(a, off + fin, off + ub, lane);
+    __syncwarp();
+    if (rows) {
+        PartialAcc<Real> acc;
+        partial_sum_rows<DIM, Real>(w.tr, fin < 32u ? (int)fin : 32, lane, acc);
+        store_partial<DIM, Real>(a, c, acc, lane);
+    } else {
+        __threadfence_block();
+        partials_of_range<DIM, Real>(a, a.S1, c, off, fin < ub ? fin : ub, w.tr, lane);
+    }
+    reset_cell(a, c, lane);
+}
+
 template <int DIM, typename Real>
 __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
 {
+    pdl_entry();
     constexpr int CHC = WrCfg<DIM, Real>::CHC, UCAP = WrCfg<DIM, Real>::UCAP;
     extern __shared__ __align__(16) unsigned char wr_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -497,13 +717,14 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
         const uint32_t ncell = nC - c0 < (uint32_t)CHC ? nC - c0 : (uint32_t)CHC;
         // chunk headers, one cell per lane
         const uint32_t csl = (uint32_t)lane <= ncell ? a.cs_old[c0 + lane] : 0u;
-        uint32_t h_na = 0, h_head = LOST;
+        uint32_t h_na = 0, h_head = LOST, h_occ = 0;
         unsigned long long h_ub = 0, h_off = 0;
         if ((uint32_t)lane < ncell) {
             h_na = a.carr[c0 + lane];
             h_head = a.head[c0 + lane];
             h_ub = a.cub[c0 + lane];
             h_off = a.coff[c0 + lane];
+            for (int q = 0; q < a.pp.occw; ++q) h_occ += __popcll(a.cocc[(size_t)(c0 + lane) * a.pp.occw + q]);
         }
         const uint32_t S = __shfl_sync(0xffffffffu, csl, 0), E = __shfl_sync(0xffffffffu, csl, ncell);
         const bool staged = E - S <= (uint32_t)UCAP;
@@ -532,21 +753,16 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
             const uint32_t ub = (uint32_t)ubw, nseed_expect = (uint32_t)(ubw >> 32);
             const uint32_t off = (uint32_t)ofw, sb = (uint32_t)(ofw >> 32);
             if (lane == 0) a.cs_new[c] = off;
-            // Virtual slots u = 32 r + lane (two rounds of the warp): u < L
-            // the cell's old slots (a stayer where its key is c), L <= u < L +
-            // na the arrivals.  Cells beyond 64 take the general path.
-            const bool fast = L + na <= 64 && ub <= 64;
-            const bool two = L + na > 32;  // warp-uniform: a second round is needed
-            bool is_stay[2];
-            unsigned stm[2];
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                const uint32_t u = 32u * r + (uint32_t)lane;
-                is_stay[r] = fast && (r == 0 || two) && u < L &&
-                             (staged ? w.key[s0 - S + u] : a.key[s0 + u]) == c;
-                stm[r] = __ballot_sync(0xffffffffu, is_stay[r]);
+            const uint32_t occ = __shfl_sync(0xffffffffu, h_occ, jc);
+            // count - occupied parts <= max: no part above max + 1 particles
+            const bool no_removal = !apply || (maxpp >= 0 && ub - nseed_expect <= occ + (uint32_t)maxpp);
+            if (nseed_expect == 0 && no_removal && L + na <= 32u) {
+                write_cell_simple<DIM, Real>(a, w, c, s0, L, na, h, off, ub, S, staged, lane, err);
+                __syncwarp();
+                continue;
             }
-            if (!fast) {
+            // Cells beyond 64 particles take the general path.
+            if (!(L + na <= 64 && ub <= 64)) {
                 const uint2 gr = write_cell_general<DIM, Real>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0,
                                                                lane);
                 removed += gr.x;
@@ -556,135 +772,12 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
                 __syncwarp();
                 continue;
             }
-            const uint32_t ns = __popc(stm[0]) + __popc(stm[1]);
-            const uint32_t n = ns + na;
-            PData<DIM, Real> pd[2];
-            bool is_arr[2], valid[2];
-            int pe[2];
-            uint32_t key[2];
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                const uint32_t u = 32u * r + (uint32_t)lane;
-                is_arr[r] = (r == 0 || two) && u >= L && u < L + na;
-                valid[r] = is_stay[r] || is_arr[r];
-                pd[r].i = 0;
-                pd[r].id = 0;
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) pd[r].xi[d] = pd[r].v[d] = Real(0);
-                if (is_stay[r]) {
-                    if (staged) load_stage<DIM, Real>(w, s0 - S + u, s0 + u, pd[r]);
-                    else load_global<DIM, Real>(a, s0 + u, pd[r]);
-                } else if (is_arr[r]) {
-                    const uint32_t ia = arrival(a, c, u - L, h);
-                    if (ia < cap) load_global<DIM, Real>(a, ia, pd[r]);
-                    else err |= ERR_ARRIVAL;
-                }
-                pe[r] = valid[r] ? ext_part<DIM, Real>(pd[r].xi, a.pp) : 0;
-                key[r] = valid[r] ? key_of(pd[r].id, a.pp.seed) : 0xffffffffu;
-            }
-            int* cnt = w.cnt;
-            for (int p = lane; p < a.pp.npe; p += 32) cnt[p] = 0;
-            __syncwarp();
-#pragma unroll
-            for (int r = 0; r < 2; ++r)
-                if (valid[r]) atomicAdd(cnt + pe[r], 1);
-            __syncwarp();
-            int kme[2], rank[2] = {0, 0};
-            unsigned validm[2];
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                kme[r] = valid[r] ? cnt[pe[r]] : 0;
-                validm[r] = __ballot_sync(0xffffffffu, valid[r]);
-            }
-            // rank inside an over-full part (by key)
-            if (__any_sync(0xffffffffu, apply && (kme[0] > maxpp + 1 || kme[1] > maxpp + 1))) {
-#pragma unroll
-                for (int r2 = 0; r2 < 2; ++r2) {
-                    if (r2 == 1 && !two) break;
-                    for (int l = 0; l < 32; ++l) {
-                        const int pl = __shfl_sync(0xffffffffu, pe[r2], l);
-                        const uint32_t kl = __shfl_sync(0xffffffffu, key[r2], l);
-                        const bool vl = (validm[r2] >> l) & 1u;
-#pragma unroll
-                        for (int r = 0; r < 2; ++r) rank[r] += (vl && pl == pe[r] && kl < key[r]) ? 1 : 0;
-                    }
-                }
-            }
-            // order: stayers (slot order), then arrivals by key
-            const unsigned ltm = (1u << lane) - 1u;
-            uint32_t seq[2];
-            seq[0] = is_stay[0] ? (uint32_t)__popc(stm[0] & ltm) : ns + (uint32_t)lane - L;
-            seq[1] = is_stay[1] ? (uint32_t)(__popc(stm[0]) + __popc(stm[1] & ltm)) : ns + 32u + (uint32_t)lane - L;
-            if (na > 1) {
-                uint32_t ar[2] = {0u, 0u};
-                for (uint32_t t = 0; t < na; ++t) {
-                    const uint32_t u2 = L + t;
-                    const uint32_t k0 = __shfl_sync(0xffffffffu, key[0], (int)(u2 & 31u));
-                    const uint32_t k1 = __shfl_sync(0xffffffffu, key[1], (int)(u2 & 31u));
-                    const uint32_t kl = (u2 >> 5) ? k1 : k0;
-#pragma unroll
-                    for (int r = 0; r < 2; ++r) ar[r] += (kl < key[r]) ? 1u : 0u;
-                }
-#pragma unroll
-                for (int r = 0; r < 2; ++r)
-                    if (is_arr[r]) seq[r] = ns + ar[r];
-            }
-            bool surv[2];
-            unsigned survm[2];
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                surv[r] = valid[r] && rank[r] < survivors(kme[r], maxpp, apply);
-                survm[r] = __ballot_sync(0xffffffffu, surv[r]);
-            }
-            const uint32_t nsurv = __popc(survm[0]) + __popc(survm[1]);
-            uint32_t pos[2] = {seq[0], seq[1]};
-            if (nsurv != n) {  // removals: survivors before in sequence order
-                pos[0] = pos[1] = 0;
-#pragma unroll
-                for (int r2 = 0; r2 < 2; ++r2) {
-                    if (r2 == 1 && !two) break;
-                    for (int l = 0; l < 32; ++l) {
-                        const uint32_t sl = __shfl_sync(0xffffffffu, seq[r2], l);
-                        const bool bl = (survm[r2] >> l) & 1u;
-#pragma unroll
-                        for (int r = 0; r < 2; ++r) pos[r] += (bl && sl < seq[r]) ? 1u : 0u;
-                    }
-                }
-            }
-            // partial rows in registers -> shared rows when the cell's final
-            // particles fit one row block, else re-read from the new layout
-            const bool rows = nsurv + nseed_expect <= 32u;
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                if (surv[r]) {
-                    const uint32_t dst = off + pos[r];
-                    if (dst < cap) store_particle<DIM, Real>(a, dst, c, pd[r]);
-                    else err |= ERR_CAPACITY;
-                    if (rows) partial_row<DIM, Real>(w.tr, (int)pos[r], pd[r].xi, pd[r].v);
-                }
-                removed += (valid[r] && !surv[r]) ? 1 : 0;
-            }
-            uint32_t nseed = 0;
-            if (nseed_expect) {
-                const uint2 sd = write_seeds<DIM, Real>(a, c, cnt, n, off + nsurv, id0, sb, rows ? w.tr : nullptr,
-                                                        (int)nsurv, lane);
-                nseed = sd.x;
-                err |= sd.y;
-            }
-            const uint32_t fin = nsurv + nseed;
-            if (nseed != nseed_expect) err |= ERR_COUNT;
-            if (fin > ub) err |= ERR_COUNT_UB;
-            write_holes(a, off + fin, off + ub, lane);
-            __syncwarp();
-            if (rows) {
-                PartialAcc<Real> acc;
-                partial_sum_rows<DIM, Real>(w.tr, fin < 32u ? (int)fin : 32, lane, acc);
-                store_partial<DIM, Real>(a, c, acc, lane);
-            } else {
-                __threadfence_block();
-                partials_of_range<DIM, Real>(a, a.S1, c, off, fin < ub ? fin : ub, w.tr, lane);
-            }
-            reset_cell(a, c, lane);
+            if (L + na > 32)
+                write_cell_fast<DIM, Real, 2>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0, S, staged, lane,
+                                              removed, err);
+            else
+                write_cell_fast<DIM, Real, 1>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0, S, staged, lane,
+                                              removed, err);
             __syncwarp();
         }
     }
@@ -755,6 +848,7 @@ __device__ __forceinline__ void load4(const double* p, double* q)
 template <int DIM, typename PReal>
 __global__ void k_gather(StepArgs a, int keep_empty)
 {
+    pdl_entry();
     constexpr int NV = 1 << DIM, PW = Dims<DIM>::PW;
     const PReal* P = reinterpret_cast<const PReal*>(a.partials);
     unsigned long long nan_dofs = 0;

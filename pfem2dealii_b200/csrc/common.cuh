@@ -182,6 +182,17 @@ template <int DIM> struct Dims {
     static constexpr int REC4 = DIM == 3 ? 7 : 3;      // float4 per FP32 velocity record (coefficients + flag)
 };
 
+// Entry of a kernel of the step sequence, launched with programmatic
+// dependent launch: wait until the previous kernel on the stream has
+// completed and its writes are visible, then let the next kernel be
+// scheduled (its blocks wait in the same place).  Without the launch
+// attribute both instructions return at once.
+__device__ __forceinline__ void pdl_entry()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __host__ __device__ inline uint32_t key_of(uint32_t id, uint32_t seed)
 {
     if (!seed) return id;

@@ -333,6 +333,26 @@ __device__ __forceinline__ int inverse_map64(const double (*X)[DIM], const doubl
     return 1;
 }
 
+// Inverse of an affine cell's map from its stored inverse (aff = [A^-1 | b],
+// x = A xi + b exactly for a parallelepiped).  0 = success (1: singular cell).
+template <int DIM>
+__device__ __forceinline__ int inverse_affine64(const double* __restrict__ aff, const double* p, double* xi)
+{
+    const double a00 = __ldg(aff);
+    if (a00 != a00) return 1;
+    double r[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) r[d] = p[d] - __ldg(aff + DIM * DIM + d);
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        double acc = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) acc = acc + __ldg(aff + k * DIM + d) * r[d];
+        xi[k] = acc;
+    }
+    return 0;
+}
+
 template <int DIM>
 __device__ __forceinline__ void load_cell64(const double* __restrict__ cellX, uint32_t c, double (*X)[DIM])
 {

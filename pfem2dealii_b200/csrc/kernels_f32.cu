@@ -9,6 +9,7 @@ namespace pfem2 {
 
 int launch64_seed(int dim, const StepArgs& a, uint32_t* cs, cudaStream_t s);
 int launch64_advect(int dim, const StepArgs& a, cudaStream_t s);
+int launch64_cross(int dim, const StepArgs& a, cudaStream_t s);
 int launch64_write(int dim, const StepArgs& a, cudaStream_t s);
 int launch64_partials(int dim, const StepArgs& a, const uint32_t* cs, cudaStream_t s);
 int launch64_correct(int dim, const StepArgs& a, cudaStream_t s);
@@ -42,13 +43,19 @@ static int advect32_t(const StepArgs& a, cudaStream_t s)
     const int smem = 2 * (int)sizeof(AdvStage<DIM, float, ADV_CH>);
     if (a.mesh.all_affine) {
         static const int grid = smem_grid32(k_advect32<DIM, true>, 256, smem);
-        k_advect32<DIM, true><<<grid, 256, smem, s>>>(a);
+        return launch_pdl(k_advect32<DIM, true>, grid, 256, smem, s, a);
     } else {
         static const int grid = smem_grid32(k_advect32<DIM, false>, 256, smem);
-        k_advect32<DIM, false><<<grid, 256, smem, s>>>(a);
+        return launch_pdl(k_advect32<DIM, false>, grid, 256, smem, s, a);
     }
-    k_cross32<DIM><<<PFEM2_GRID(k_cross32<DIM>, 128), 128, 0, s>>>(a);
-    return 2;
+    return 1;
+}
+
+template <int DIM>
+static int cross32_t(const StepArgs& a, cudaStream_t s)
+{
+    if (a.mesh.all_affine) return launch_pdl(k_cross32<DIM, true>, PFEM2_GRID((k_cross32<DIM, true>), 128), 128, 0, s, a);
+    return launch_pdl(k_cross32<DIM, false>, PFEM2_GRID((k_cross32<DIM, false>), 128), 128, 0, s, a);
 }
 
 int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s)
@@ -57,12 +64,19 @@ int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s)
     return dim == 2 ? advect32_t<2>(a, s) : advect32_t<3>(a, s);
 }
 
+// The queued face crossers of the advect pass (relocation in FP64).
+int launch_cross(int dim, int prec, const StepArgs& a, cudaStream_t s)
+{
+    if (prec == 0) return launch64_cross(dim, a, s);
+    return dim == 2 ? cross32_t<2>(a, s) : cross32_t<3>(a, s);
+}
+
 template <int DIM>
 static int write32_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = WR_WARPS * (int)sizeof(WrWarp<DIM, float>);
     static const int grid = smem_grid32(k_write<DIM, float>, WR_WARPS * 32, smem);
-    k_write<DIM, float><<<grid, WR_WARPS * 32, smem, s>>>(a);
+    return launch_pdl(k_write<DIM, float>, grid, WR_WARPS * 32, smem, s, a);
     return 1;
 }
 
@@ -91,8 +105,8 @@ int launch_correct(int dim, int prec, const StepArgs& a, cudaStream_t s)
 int launch_gather(int dim, int prec, const StepArgs& a, int keep, cudaStream_t s)
 {
     if (prec == 0) return launch64_gather(dim, a, keep, s);
-    if (dim == 2) k_gather<2, float><<<PFEM2_GRID((k_gather<2, float>), 256), 256, 0, s>>>(a, keep);
-    else k_gather<3, float><<<PFEM2_GRID((k_gather<3, float>), 256), 256, 0, s>>>(a, keep);
+    if (dim == 2) return launch_pdl(k_gather<2, float>, PFEM2_GRID((k_gather<2, float>), 256), 256, 0, s, a, keep);
+    return launch_pdl(k_gather<3, float>, PFEM2_GRID((k_gather<3, float>), 256), 256, 0, s, a, keep);
     return 1;
 }
 

@@ -121,9 +121,8 @@ static int advect_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = 2 * (int)sizeof(AdvStage<DIM, double, ADV64_CH>);
     static const int grid = smem_grid(k_advect64<DIM>, 256, smem);
-    k_advect64<DIM><<<grid, 256, smem, s>>>(a);
-    k_search64<DIM><<<PFEM2_GRID(k_search64<DIM>, 128), 128, 0, s>>>(a);
-    return 2;
+    return launch_pdl(k_advect64<DIM>, grid, 256, smem, s, a);
+    return 1;
 }
 
 int launch64_advect(int dim, const StepArgs& a, cudaStream_t s)
@@ -131,12 +130,19 @@ int launch64_advect(int dim, const StepArgs& a, cudaStream_t s)
     return dim == 2 ? advect_t<2>(a, s) : advect_t<3>(a, s);
 }
 
+int launch64_cross(int dim, const StepArgs& a, cudaStream_t s)
+{
+    if (dim == 2) return launch_pdl(k_search64<2>, PFEM2_GRID(k_search64<2>, 128), 128, 0, s, a);
+    return launch_pdl(k_search64<3>, PFEM2_GRID(k_search64<3>, 128), 128, 0, s, a);
+    return 1;
+}
+
 template <int DIM>
 static int write_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = WR_WARPS * (int)sizeof(WrWarp<DIM, double>);
     static const int grid = smem_grid(k_write<DIM, double>, WR_WARPS * 32, smem);
-    k_write<DIM, double><<<grid, WR_WARPS * 32, smem, s>>>(a);
+    return launch_pdl(k_write<DIM, double>, grid, WR_WARPS * 32, smem, s, a);
     return 1;
 }
 
@@ -161,8 +167,8 @@ int launch64_correct(int dim, const StepArgs& a, cudaStream_t s)
 
 int launch64_gather(int dim, const StepArgs& a, int keep, cudaStream_t s)
 {
-    if (dim == 2) k_gather<2, double><<<PFEM2_GRID((k_gather<2, double>), 256), 256, 0, s>>>(a, keep);
-    else k_gather<3, double><<<PFEM2_GRID((k_gather<3, double>), 256), 256, 0, s>>>(a, keep);
+    if (dim == 2) return launch_pdl(k_gather<2, double>, PFEM2_GRID((k_gather<2, double>), 256), 256, 0, s, a, keep);
+    return launch_pdl(k_gather<3, double>, PFEM2_GRID((k_gather<3, double>), 256), 256, 0, s, a, keep);
     return 1;
 }
 

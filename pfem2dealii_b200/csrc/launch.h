@@ -29,11 +29,32 @@ inline int occupancy_grid(const void* kernel, int threads, size_t smem = 0)
     return g;
 }
 
+// Launch with programmatic dependent launch (the kernel calls pdl_entry()
+// first): it may be scheduled while the previous kernel drains, which hides
+// the launch gap between the dependent kernels of a step.  Returns 1 (one
+// kernel) or -1 when the launch was refused.
+template <typename... KArgs, typename... Args>
+inline int launch_pdl(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, ((KArgs)args)...) == cudaSuccess ? 1 : -1;
+}
+
 // kernels_f64.cu / kernels_f32.cu (prec: 0 = FP64 form, 1 = FP32 form)
 int launch_cell_setup(int dim, int nC, const double* verts, const int32_t* cv, double* cellX, double* aff,
                       float* geo32, float* jinv32, uint32_t* twisted, cudaStream_t s);
 int launch_seed(int dim, int prec, const StepArgs& a, uint32_t* cell_start, cudaStream_t s);
 int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s);
+int launch_cross(int dim, int prec, const StepArgs& a, cudaStream_t s);
 int launch_write(int dim, int prec, const StepArgs& a, cudaStream_t s);
 int launch_partials(int dim, int prec, const StepArgs& a, const uint32_t* cell_start, cudaStream_t s);
 int launch_correct(int dim, int prec, const StepArgs& a, cudaStream_t s);

@@ -69,6 +69,7 @@ __device__ __forceinline__ unsigned long long cell_slot_word(const StepArgs& a, 
 // Pass 1: every cell's slot word (stored to cub) and each tile's sum.
 __global__ void __launch_bounds__(SB) k_slots_reduce(StepArgs a, unsigned long long* __restrict__ tiles)
 {
+    pdl_entry();
     const uint32_t n = (uint32_t)a.mesh.nC;
     unsigned long long s = 0;
 #pragma unroll
@@ -89,6 +90,7 @@ __global__ void __launch_bounds__(SB) k_slots_reduce(StepArgs a, unsigned long l
 // and scans its rows of SB cells; coff[nC] = the grand total.
 __global__ void __launch_bounds__(SB) k_slots_down(StepArgs a, const unsigned long long* __restrict__ tiles)
 {
+    pdl_entry();
     __shared__ unsigned long long carry_s;
     const uint32_t n = (uint32_t)a.mesh.nC;
     if (threadIdx.x < 32) {
@@ -154,6 +156,7 @@ __global__ void k_fill(T* p, uint32_t n, T v)
 // the cell ranges' end.
 __global__ void k_finalize(StepArgs a, int count_step)
 {
+    pdl_entry();
     DevStats* st = a.stats;
     if (count_step) st->particle_steps += st->n_particles;
     const unsigned long long po = a.coff[a.mesh.nC];
@@ -188,6 +191,7 @@ template <int DIM, typename Real>
 __global__ void k_cell_v(const double* __restrict__ V, const double* __restrict__ Vold, const int32_t* __restrict__ cd,
                          int nC, int nD, Real* __restrict__ Vc, Real* __restrict__ dVc)
 {
+    pdl_entry();
     constexpr int NV = 1 << DIM, VS = Dims<DIM>::VS;
     const int total = nC * NV;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
@@ -246,6 +250,7 @@ __global__ void __launch_bounds__(128) k_cell_rec32(const double* __restrict__ V
                                                     const float* __restrict__ jinv32, int nC, int nD,
                                                     float* __restrict__ vrec, float* __restrict__ dvrec)
 {
+    pdl_entry();
     constexpr int NV = 1 << DIM, F = Dims<DIM>::REC4 * 4, AFF = Dims<DIM>::AFF;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nC; c += gridDim.x * blockDim.x) {
         int dof[NV];
@@ -302,8 +307,9 @@ int grid_for(const void* k, int threads) { return occupancy_grid(k, threads); }
 int launch_slots_scan(const StepArgs& a, unsigned long long* tiles, cudaStream_t s)
 {
     const uint32_t ntiles = ((uint32_t)a.mesh.nC + STILE - 1) / STILE;
-    k_slots_reduce<<<ntiles, SB, 0, s>>>(a, tiles);
-    k_slots_down<<<ntiles, SB, 0, s>>>(a, tiles);
+    const int r0 = launch_pdl(k_slots_reduce, (int)ntiles, SB, 0, s, a, tiles);
+    const int r1 = launch_pdl(k_slots_down, (int)ntiles, SB, 0, s, a, (const unsigned long long*)tiles);
+    if (r0 < 0 || r1 < 0) return -1;
     return 2;
 }
 
@@ -324,7 +330,7 @@ int launch_fill_u32(uint32_t* p, uint32_t n, uint32_t v, cudaStream_t s)
 
 int launch_finalize(const StepArgs& a, int count_step, cudaStream_t s)
 {
-    k_finalize<<<1, 1, 0, s>>>(a, count_step);
+    return launch_pdl(k_finalize, 1, 1, 0, s, a, count_step);
     return 1;
 }
 
@@ -340,10 +346,10 @@ int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const 
     const int total = nC * (1 << dim);
     const int g = (total + 255) / 256 < 8192 ? (total + 255) / 256 : 8192;
     const int grid = g > 0 ? g : 1;
-    if (dim == 2 && prec == 0) k_cell_v<2, double><<<grid, 256, 0, s>>>(V, Vold, cd, nC, nD, (double*)Vc, (double*)dVc);
-    else if (dim == 3 && prec == 0) k_cell_v<3, double><<<grid, 256, 0, s>>>(V, Vold, cd, nC, nD, (double*)Vc, (double*)dVc);
-    else if (dim == 2) k_cell_v<2, float><<<grid, 256, 0, s>>>(V, Vold, cd, nC, nD, (float*)Vc, (float*)dVc);
-    else k_cell_v<3, float><<<grid, 256, 0, s>>>(V, Vold, cd, nC, nD, (float*)Vc, (float*)dVc);
+    if (dim == 2 && prec == 0) return launch_pdl(k_cell_v<2, double>, grid, 256, 0, s, V, Vold, cd, nC, nD, (double*)Vc, (double*)dVc);
+    if (dim == 3 && prec == 0) return launch_pdl(k_cell_v<3, double>, grid, 256, 0, s, V, Vold, cd, nC, nD, (double*)Vc, (double*)dVc);
+    if (dim == 2) return launch_pdl(k_cell_v<2, float>, grid, 256, 0, s, V, Vold, cd, nC, nD, (float*)Vc, (float*)dVc);
+    return launch_pdl(k_cell_v<3, float>, grid, 256, 0, s, V, Vold, cd, nC, nD, (float*)Vc, (float*)dVc);
     return 1;
 }
 
@@ -352,8 +358,8 @@ int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_
 {
     const int g = (nC + 127) / 128;
     const int grid = g < 1 ? 1 : g;
-    if (dim == 2) k_cell_rec32<2><<<grid, 128, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
-    else k_cell_rec32<3><<<grid, 128, 0, s>>>(V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    if (dim == 2) return launch_pdl(k_cell_rec32<2>, grid, 128, 0, s, V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    return launch_pdl(k_cell_rec32<3>, grid, 128, 0, s, V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
     return 1;
 }
 

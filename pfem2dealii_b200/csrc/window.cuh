@@ -179,7 +179,8 @@ __device__ __forceinline__ bool win_relocate(const WinArgs& w, uint32_t& c, Real
 #pragma unroll
         for (int d = 0; d < DIM; ++d) xo.v[d] = (double)xi[d];
         velocity_from_dofs<DIM>(a.mesh.cd, a.Vd, a.mesh.nD, c, xo.v, ue.v);
-        const SearchOut so = fallback64<DIM>(a.mesh, c, xo, ue, a.pp.dtp);
+        const SearchOut so = a.mesh.all_affine ? fallback64<DIM, true>(a.mesh, c, xo, ue, a.pp.dtp)
+                                               : fallback64<DIM, false>(a.mesh, c, xo, ue, a.pp.dtp);
         if (!(so.flags & SRCH_FOUND)) return false;
         c = so.cell;
 #pragma unroll
