@@ -2,7 +2,7 @@
 // sequences.  One time step of the reference loop (src/pfem2solver.cpp:162-164)
 // maps to
 //   correct(V, Vold)  -> stage V, V - Vold per cell vertex (the correction is fused into move)
-//   move(V)           -> advect (staged) | FP64 relocation queue | slots per cell | scan | write | finalize
+//   move(V)           -> advect (staged) | FP64 relocation queue | slots per cell | scan | write (its last block finalises the step)
 //   project(V_out)    -> gather (per-cell partials were summed by write) | D2H
 #include <algorithm>
 #include <cmath>
@@ -403,8 +403,8 @@ void swap_state(pfem2gpu_handle* h)
 int enqueue_write(pfem2gpu_handle* h, StepArgs& a, int count_step)
 {
     run(h, "slots_scan", [&] { return launch_slots_scan(a, h->tiles64, h->stream); });
+    a.count_step = count_step;  // the write pass's last block finalises the step
     run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->stream); });
-    run(h, "finalize", [&] { return launch_finalize(a, count_step, h->stream); });
     return PFEM2GPU_OK;
 }
 

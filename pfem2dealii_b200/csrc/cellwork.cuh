@@ -712,7 +712,13 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
     const int apply = a.apply_counts, maxpp = a.pp.maxpp;
     unsigned long long removed = 0;
     uint32_t err = 0;
-    for (uint32_t ck = blockIdx.x * WR_WARPS + warp; ck < nchunks; ck += gridDim.x * WR_WARPS) {
+    // chunks of cells are handed out one at a time, so that warps that drew
+    // cheap chunks take more (cells differ in particles and arrivals)
+    while (true) {
+        uint32_t ck = 0;
+        if (lane == 0) ck = atomicAdd(&a.stats->write_next, 1u);
+        ck = __shfl_sync(0xffffffffu, ck, 0);
+        if (ck >= nchunks) break;
         const uint32_t c0 = ck * CHC;
         const uint32_t ncell = nC - c0 < (uint32_t)CHC ? nC - c0 : (uint32_t)CHC;
         // chunk headers, one cell per lane
@@ -785,6 +791,20 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
     warp_count(&a.stats->step_holes, removed);
     err = __reduce_or_sync(0xffffffffu, err);
     if (lane == 0 && err) atomicOr(&a.stats->error_flags, err);
+    // the last warp to finish finalises the step (no waiting: the others
+    // have published their counters before counting themselves done)
+    unsigned int last = 0;
+    if (lane == 0) {
+        __threadfence();
+        last = atomicAdd(&a.stats->write_done, 1u) == gridDim.x * WR_WARPS - 1 ? 1u : 0u;
+        if (last) {
+            __threadfence();
+            finalize_step(a);
+            a.stats->write_done = 0;
+            a.stats->write_next = 0;
+        }
+    }
+    (void)last;
 }
 
 // Partials of the current state (after seeding or an upload).

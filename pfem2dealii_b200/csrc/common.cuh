@@ -50,6 +50,8 @@ struct DevStats {
     unsigned long long step_holes;   // empty slots left by the last write pass
     unsigned int next_id;
     unsigned int error_flags;
+    unsigned int write_done;         // write pass: warps finished (the last one finalises the step)
+    unsigned int write_next;         // write pass: next chunk of cells to hand out
 };
 
 struct MeshDev {
@@ -103,6 +105,7 @@ struct StepArgs {
     const double* Vd;     // staged nodal velocity, component-major (nD per component)
     int do_correct;
     int apply_counts;   // write kernel: 1 = count correction, 0 = keep all (re-sort only)
+    int count_step;     // write kernel: add the step's particles to particle_steps
     uint32_t* key;      // cell after the move, or LOST
     uint32_t* head;     // nC: overflow list of particles that moved into the cell (LOST = none)
     uint32_t* next;     // next particle on the same overflow list
@@ -181,6 +184,27 @@ template <int DIM> struct Dims {
     static constexpr int JS = DIM == 3 ? 12 : 8;       // FP32 inverse Jacobian + flag, padded
     static constexpr int REC4 = DIM == 3 ? 7 : 3;      // float4 per FP32 velocity record (coefficients + flag)
 };
+
+// End of a move, run by one thread after the write pass: the new slot count
+// and particle count, the ids handed out, the cell ranges' end.
+__device__ __forceinline__ void finalize_step(const StepArgs& a)
+{
+    DevStats* st = a.stats;
+    if (a.count_step) st->particle_steps += st->n_particles;
+    const unsigned long long po = a.coff[a.mesh.nC];
+    uint32_t slots = (uint32_t)po;
+    const uint32_t seeds = (uint32_t)(po >> 32);
+    if (slots > a.capacity) {
+        st->error_flags |= ERR_CAPACITY;
+        slots = a.capacity;
+    }
+    st->n_slots = slots;
+    st->n_particles = slots - (st->step_holes < slots ? st->step_holes : slots);
+    st->step_holes = 0;
+    st->next_id += seeds;
+    st->seeded += seeds;
+    a.cs_new[a.mesh.nC] = slots;
+}
 
 // Entry of a kernel of the step sequence, launched with programmatic
 // dependent launch: wait until the previous kernel on the stream has

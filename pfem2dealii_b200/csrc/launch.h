@@ -69,7 +69,6 @@ constexpr int SCAN_MAX_TILES = 8192;  // tile sums the scan buffer holds
 int launch_slots_scan(const StepArgs& a, unsigned long long* tiles, cudaStream_t s);
 int launch_rekey(int dim, int prec, const StepArgs& a, cudaStream_t s);
 int launch_fill_u32(uint32_t* p, uint32_t n, uint32_t v, cudaStream_t s);
-int launch_finalize(const StepArgs& a, int count_step, cudaStream_t s);
 int launch_set_state(DevStats* st, long long n, long long next_id, long long add_id, cudaStream_t s);
 int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const int32_t* cd, int nC, int nD, void* Vc,
                   void* dVc, cudaStream_t s);

@@ -10,7 +10,7 @@ namespace pfem2 {
 
 namespace {
 
-constexpr int SB = 256;              // scan block
+constexpr int SB = 1024;             // scan block: one cell per thread
 constexpr int SI = SCAN_TILE / SB;   // rows of SB cells per tile
 constexpr int STILE = SCAN_TILE;     // cells per tile
 
@@ -150,28 +150,6 @@ template <typename T>
 __global__ void k_fill(T* p, uint32_t n, T v)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
-}
-
-// End of a move: the new slot count and particle count, the ids handed out,
-// the cell ranges' end.
-__global__ void k_finalize(StepArgs a, int count_step)
-{
-    pdl_entry();
-    DevStats* st = a.stats;
-    if (count_step) st->particle_steps += st->n_particles;
-    const unsigned long long po = a.coff[a.mesh.nC];
-    uint32_t slots = (uint32_t)po;
-    const uint32_t seeds = (uint32_t)(po >> 32);
-    if (slots > a.capacity) {
-        st->error_flags |= ERR_CAPACITY;
-        slots = a.capacity;
-    }
-    st->n_slots = slots;
-    st->n_particles = slots - (st->step_holes < slots ? st->step_holes : slots);
-    st->step_holes = 0;
-    st->next_id += seeds;
-    st->seeded += seeds;
-    a.cs_new[a.mesh.nC] = slots;
 }
 
 __global__ void k_set_state(DevStats* st, long long n, long long next_id, long long add_id)
@@ -328,11 +306,6 @@ int launch_fill_u32(uint32_t* p, uint32_t n, uint32_t v, cudaStream_t s)
     return 1;
 }
 
-int launch_finalize(const StepArgs& a, int count_step, cudaStream_t s)
-{
-    return launch_pdl(k_finalize, 1, 1, 0, s, a, count_step);
-    return 1;
-}
 
 int launch_set_state(DevStats* st, long long n, long long next_id, long long add_id, cudaStream_t s)
 {
