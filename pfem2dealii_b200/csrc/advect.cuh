@@ -283,10 +283,14 @@ __device__ __forceinline__ void stage_chunk(const StepArgs& a, AdvStage<DIM, Rea
 
 // The chunk loop shared by both forms: double-buffered staging, f(stage, t,
 // i, active) per particle slot (every lane of every warp calls it, so warp
-// collectives are allowed inside).
+// collectives are allowed inside).  Chunks are handed out one at a time from
+// a counter (stats->adv_next, reset when the step is finalised), so blocks
+// that drew cheap chunks take more; a block holds tickets for the chunk it
+// processes and the one being staged.
 template <int DIM, typename Real, int CH, typename F>
 __device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Real, CH>* st, uint64_t* bar, F&& f)
 {
+    __shared__ uint32_t tk[2];
     const uint32_t n = (uint32_t)a.stats->n_slots;
     const uint32_t nchunks = (n + CH - 1) / CH;
     if (threadIdx.x == 0) {
@@ -296,17 +300,22 @@ __device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Rea
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        if (blockIdx.x < nchunks) stage_chunk<DIM, Real, CH>(a, st[0], &bar[0], blockIdx.x, n);
-        if (blockIdx.x + gridDim.x < nchunks) stage_chunk<DIM, Real, CH>(a, st[1], &bar[1], blockIdx.x + gridDim.x, n);
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            tk[b] = atomicAdd(&a.stats->adv_next, 1u);
+            if (tk[b] < nchunks) stage_chunk<DIM, Real, CH>(a, st[b], &bar[b], tk[b], n);
+        }
     }
-    uint32_t it = 0;
-    for (uint32_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x, ++it) {
+    __syncthreads();
+    for (uint32_t it = 0;; ++it) {
         const int sidx = it & 1;
+        const uint32_t chunk = tk[sidx];
+        if (chunk >= nchunks) break;  // tickets grow: the other buffer holds nothing in flight
         const bool ok = mbar_wait(&bar[sidx], (it >> 1) & 1u);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicOr(&a.stats->error_flags, ERR_TIMEOUT);
-            // let the copies still in flight land before the block leaves
-            mbar_wait(&bar[sidx ^ 1], ((it + 1) >> 1) & 1u);
+            // let the copy still in flight land before the block leaves
+            if (tk[sidx ^ 1] < nchunks) mbar_wait(&bar[sidx ^ 1], ((it + 1) >> 1) & 1u);
             return;
         }
         const uint32_t base = chunk * CH;
@@ -314,11 +323,15 @@ __device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Rea
 #pragma unroll 1
         for (uint32_t t = threadIdx.x; t < (uint32_t)CH; t += blockDim.x) f(st[sidx], t, base + t, t < cnt);
         __syncthreads();
-        const uint32_t nxt = chunk + 2 * gridDim.x;
-        if (threadIdx.x == 0 && nxt < nchunks) {
-            fence_proxy_async();
-            stage_chunk<DIM, Real, CH>(a, st[sidx], &bar[sidx], nxt, n);
+        if (threadIdx.x == 0) {
+            const uint32_t nxt = atomicAdd(&a.stats->adv_next, 1u);
+            tk[sidx] = nxt;
+            if (nxt < nchunks) {
+                fence_proxy_async();
+                stage_chunk<DIM, Real, CH>(a, st[sidx], &bar[sidx], nxt, n);
+            }
         }
+        __syncthreads();
     }
 }
 

@@ -52,6 +52,7 @@ struct DevStats {
     unsigned int error_flags;
     unsigned int write_done;         // write pass: warps finished (the last one finalises the step)
     unsigned int write_next;         // write pass: next chunk of cells to hand out
+    unsigned int adv_next;           // advect pass: next chunk of particles to hand out
 };
 
 struct MeshDev {
@@ -198,6 +199,7 @@ __device__ __forceinline__ void finalize_step(const StepArgs& a)
         st->error_flags |= ERR_CAPACITY;
         slots = a.capacity;
     }
+    st->adv_next = 0;  // the advect pass of this step has finished
     st->n_slots = slots;
     st->n_particles = slots - (st->step_holes < slots ? st->step_holes : slots);
     st->step_holes = 0;

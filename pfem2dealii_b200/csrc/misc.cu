@@ -222,59 +222,80 @@ __device__ __forceinline__ void store_rec(float* r, const float* w, float flag)
     }
 }
 
+// One thread per cell, tiles of REC_TILE consecutive cells per block: the
+// records are built in shared memory and written back as contiguous float4
+// rows (the per-cell 112-byte records would otherwise be stored at a 112-byte
+// stride, half sectors per instruction).
+constexpr int REC_TILE = 128;
+
 template <int DIM>
-__global__ void __launch_bounds__(128) k_cell_rec32(const double* __restrict__ V, const double* __restrict__ Vold,
-                                                    const int32_t* __restrict__ cd, const double* __restrict__ aff,
-                                                    const float* __restrict__ jinv32, int nC, int nD,
-                                                    float* __restrict__ vrec, float* __restrict__ dvrec)
+__global__ void __launch_bounds__(REC_TILE) k_cell_rec32(const double* __restrict__ V, const double* __restrict__ Vold,
+                                                         const int32_t* __restrict__ cd, const double* __restrict__ aff,
+                                                         const float* __restrict__ jinv32, int nC, int nD,
+                                                         float* __restrict__ vrec, float* __restrict__ dvrec)
 {
     pdl_entry();
-    constexpr int NV = 1 << DIM, F = Dims<DIM>::REC4 * 4, AFF = Dims<DIM>::AFF;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nC; c += gridDim.x * blockDim.x) {
-        int dof[NV];
+    constexpr int NV = 1 << DIM, F = Dims<DIM>::REC4 * 4, F4 = Dims<DIM>::REC4, AFF = Dims<DIM>::AFF;
+    __shared__ __align__(16) float rec_s[2][REC_TILE * F];
+    for (int c0 = blockIdx.x * REC_TILE; c0 < nC; c0 += gridDim.x * REC_TILE) {
+        const int c = c0 + threadIdx.x;
+        if (c < nC) {
+            int dof[NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) dof[k] = __ldg(cd + (size_t)c * NV + k);
-        double f[NV][DIM], g[NV][DIM];
-#pragma unroll
-        for (int k = 0; k < NV; ++k)
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                f[k][d] = __ldg(V + (size_t)d * nD + dof[k]);
-                g[k][d] = Vold ? f[k][d] - __ldg(Vold + (size_t)d * nD + dof[k]) : 0.0;
-            }
-        moebius<DIM>(f);
-        const bool affine = __ldg(jinv32 + (size_t)c * Dims<DIM>::JS + DIM * DIM) != 0.0f;
-        float w[NV * DIM];
-        if (affine) {
-            double A[DIM][DIM];
-#pragma unroll
-            for (int d = 0; d < DIM; ++d)
-#pragma unroll
-                for (int e = 0; e < DIM; ++e) A[d][e] = __ldg(aff + (size_t)c * AFF + d * DIM + e);
+            for (int k = 0; k < NV; ++k) dof[k] = __ldg(cd + (size_t)c * NV + k);
+            double f[NV][DIM], g[NV][DIM];
 #pragma unroll
             for (int k = 0; k < NV; ++k)
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) {
-                    double t = 0.0;
-#pragma unroll
-                    for (int e = 0; e < DIM; ++e) t += A[d][e] * f[k][e];
-                    w[k * DIM + d] = (float)t;
+                    f[k][d] = __ldg(V + (size_t)d * nD + dof[k]);
+                    g[k][d] = Vold ? f[k][d] - __ldg(Vold + (size_t)d * nD + dof[k]) : 0.0;
                 }
-        } else {
+            moebius<DIM>(f);
+            const bool affine = __ldg(jinv32 + (size_t)c * Dims<DIM>::JS + DIM * DIM) != 0.0f;
+            float w[NV * DIM];
+            if (affine) {
+                double A[DIM][DIM];
 #pragma unroll
-            for (int k = 0; k < NV; ++k)
+                for (int d = 0; d < DIM; ++d)
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) w[k * DIM + d] = (float)f[k][d];
+                    for (int e = 0; e < DIM; ++e) A[d][e] = __ldg(aff + (size_t)c * AFF + d * DIM + e);
+#pragma unroll
+                for (int k = 0; k < NV; ++k)
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        double t = 0.0;
+#pragma unroll
+                        for (int e = 0; e < DIM; ++e) t += A[d][e] * f[k][e];
+                        w[k * DIM + d] = (float)t;
+                    }
+            } else {
+#pragma unroll
+                for (int k = 0; k < NV; ++k)
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) w[k * DIM + d] = (float)f[k][d];
+            }
+            store_rec<DIM>(&rec_s[0][threadIdx.x * F], w, affine ? 1.0f : 0.0f);
+            if (Vold) {
+                moebius<DIM>(g);
+#pragma unroll
+                for (int k = 0; k < NV; ++k)
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) w[k * DIM + d] = (float)g[k][d];
+                store_rec<DIM>(&rec_s[1][threadIdx.x * F], w, 0.0f);
+            }
         }
-        store_rec<DIM>(vrec + (size_t)c * F, w, affine ? 1.0f : 0.0f);
-        if (Vold) {
-            moebius<DIM>(g);
-#pragma unroll
-            for (int k = 0; k < NV; ++k)
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) w[k * DIM + d] = (float)g[k][d];
-            store_rec<DIM>(dvrec + (size_t)c * F, w, 0.0f);
+        __syncthreads();
+        const int ncell = nC - c0 < REC_TILE ? nC - c0 : REC_TILE;
+        const float4* s0 = reinterpret_cast<const float4*>(rec_s[0]);
+        const float4* s1 = reinterpret_cast<const float4*>(rec_s[1]);
+        float4* d0 = reinterpret_cast<float4*>(vrec + (size_t)c0 * F);
+        float4* d1 = reinterpret_cast<float4*>(dvrec + (size_t)c0 * F);
+        for (int j = threadIdx.x; j < ncell * F4; j += REC_TILE) {
+            d0[j] = s0[j];
+            if (Vold) d1[j] = s1[j];
         }
+        __syncthreads();
     }
 }
 
@@ -329,10 +350,10 @@ int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const 
 int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
                       const float* jinv32, int nC, int nD, float* vrec, float* dvrec, cudaStream_t s)
 {
-    const int g = (nC + 127) / 128;
+    const int g = (nC + REC_TILE - 1) / REC_TILE;
     const int grid = g < 1 ? 1 : g;
-    if (dim == 2) return launch_pdl(k_cell_rec32<2>, grid, 128, 0, s, V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
-    return launch_pdl(k_cell_rec32<3>, grid, 128, 0, s, V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    if (dim == 2) return launch_pdl(k_cell_rec32<2>, grid, REC_TILE, 0, s, V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    return launch_pdl(k_cell_rec32<3>, grid, REC_TILE, 0, s, V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
     return 1;
 }
 
