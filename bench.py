@@ -48,8 +48,17 @@ WORKLOAD = "3D duct 128x32x32 Q1 hexes, 27 ppc (3,538,944 particles), max 2/part
 # Algorithmic bytes per particle of the advect kernel (3D): read cell u32 +
 # xi[3] + v[3], write xi[3] + v[3] + key u32 + slot u32.
 ADVECT_BYTES = {"fp32": 4 + 12 + 12 + 12 + 12 + 4 + 4, "fp64": 4 + 24 * 3 + 24 * 3 + 4 + 4}
+# ... of the write pass (FP32, 3D): read key u32 + id u32 + moved xi[3] + v[3],
+# write cell u32 + id u32 + xi[3] + v[3]; plus the cell's projection partials
+# (32 floats = 128 B per cell, 27 particles per cell: ~5 B per particle).
+WRITE_BYTES = {"fp32": 4 + 4 + 12 + 12 + 4 + 4 + 12 + 12 + 5}
 # Per particle-step, whole step (compulsory passes 5s + 8, s = 4 + 2*dim*w).
 STEP_BYTES = {"fp32": 5 * (4 + 24) + 8, "fp64": 5 * (4 + 48) + 8}
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# two main kernels, from one ncu capture at time step 11 of this workload with
+# the L2 not flushed between kernels (profiles/duct_fp32_step_traffic.md).
+TRAFFIC_WRITE = 245.1e6  # bytes per launch (115.2 MB read + 129.8 MB written)
+TRAFFIC_ADVECT = 222.8e6  # bytes per launch (123.4 MB read + 99.4 MB written)
 
 
 def env_rank():
@@ -434,9 +443,11 @@ def main():
     rp = timed_device_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch, profile=True)
     prof = rp["profile"]
     adv_ms, adv_n = prof.get("advect", [0.0, 1])
+    wr_ms, wr_n = prof.get("write", [0.0, 1])
     per_launch_particles = rp["particle_steps"] / max(adv_n, 1)
     peak, peak_kind = load_peak()
     achieved = ADVECT_BYTES["fp32"] * per_launch_particles / (adv_ms / adv_n / 1000.0) / 1e9
+    achieved_w = WRITE_BYTES["fp32"] * per_launch_particles / (wr_ms / wr_n / 1000.0) / 1e9
     step_ms_prof = sum(v[0] for v in prof.values()) / args.steps
     # end to end through the host ABI
     re2e = timed_host_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch)
@@ -472,10 +483,16 @@ def main():
                                 "steps": args.warmup + args.steps,
                                 "fixed_vold_0.9v": err_fixed},
         "step_effective_gbs": STEP_BYTES["fp32"] * value / 1e9,
-        "roofline": {"bound": "hbm", "kernel": "k_advect32<3>", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                     "bytes_per_particle": ADVECT_BYTES["fp32"], "peak_source": peak_kind,
-                     "launch_ms": adv_ms / adv_n},
+        "roofline": {"bound": "hbm", "kernel": "k_write<3,float>", "achieved": achieved_w, "peak": peak,
+                     "unit": "GB/s", "frac": achieved_w / peak, "traffic": TRAFFIC_WRITE,
+                     "bytes_per_particle": WRITE_BYTES["fp32"], "peak_source": peak_kind,
+                     "launch_ms": wr_ms / wr_n,
+                     "advect": {"kernel": "k_advect32<3,1>", "achieved": achieved, "frac": achieved / peak,
+                                "bytes_per_particle": ADVECT_BYTES["fp32"], "launch_ms": adv_ms / adv_n,
+                                "traffic": TRAFFIC_ADVECT},
+                     "step": {"achieved": STEP_BYTES["fp32"] * value / 1e9,
+                              "frac": STEP_BYTES["fp32"] * value / 1e9 / peak,
+                              "bytes_per_particle_step": STEP_BYTES["fp32"]}},
         "kernel_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items())},
         "profiled_ms_per_step": step_ms_prof,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": re2e["h2d"],
