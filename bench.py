@@ -115,10 +115,25 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def build_case():
+WORKLOADS = {
+    "duct": WORKLOAD,
+    "cube": "3D perturbed cube [0,2pi]^3, 80^3 Q1 hexes (interior vertices moved by up to +-0.1 h, seed 0), "
+            "64 ppc (32,768,000 particles), max 2/part, 3 sub-steps, dt 1e-3, u = (sin x cos y cos z, "
+            "-cos x sin y cos z, 0)",
+}
+ADJOINT_K = {"duct": 20, "cube": 10}
+
+
+def build_case(name="duct"):
     from pfem2dealii_b200 import mesh as M
     from pfem2dealii_b200.handler import ParticleParams
 
+    if name == "cube":
+        m = M.perturbed_cube(80, amplitude=0.1, seed=0)
+        V = M.field_at_dofs(m, M.taylor_green_3d())
+        prm = ParticleParams(particles_per_cell=(4, 4, 4), max_particles_per_cell_part=2,
+                             particle_integration_steps=3, time_step=1e-3)
+        return m, V, 0.9 * V, prm
     m = M.hyper_rectangle((0.0, 0.0, 0.0), (8.0, 1.0, 1.0), (128, 32, 32), "duct")
     V = M.field_at_dofs(m, M.duct_profile(1.0))
     prm = ParticleParams(particles_per_cell=(3, 3, 3), max_particles_per_cell_part=2,
@@ -311,7 +326,7 @@ def adjoint_report(handler_cls, m, V, Vold, prm, torch, K=20, C=5, forms=("fp32"
     return rep
 
 
-def cpu_baseline(m, V, Vold, prm, budget_s=20.0, max_steps=None, warmup=0):
+def cpu_baseline(m, V, Vold, prm, budget_s=20.0, max_steps=None, warmup=0, workload=WORKLOAD):
     """The FP64 CPU restatement (reference removal order) on all host cores,
     on the full workload; `warmup` untimed steps, then steps until the time
     budget is spent."""
@@ -333,7 +348,7 @@ def cpu_baseline(m, V, Vold, prm, budget_s=20.0, max_steps=None, warmup=0):
         ps += n
         done += 1
     return {"value": ps / t, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{done} time step(s) of the full {WORKLOAD} workload, FP64 restatement, "
+            "sample": f"{done} time step(s) of the full {workload} workload, FP64 restatement, "
                       f"{cores} threads (not the reference binary: deal.II/Trilinos/MPI absent)",
             "steps": done, "seconds": t}
 
@@ -377,6 +392,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="duct",
+                    help="duct: the headline configuration; cube: the 32.8 M-particle perturbed-cube stress case")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="time the differentiated window and its adjoint only (prints one JSON object)")
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
@@ -398,11 +415,13 @@ def main():
         torch.cuda.set_device(0)
     from pfem2dealii_b200.handler import ParticleHandler
 
-    m, V, Vold, prm = build_case()
+    m, V, Vold, prm = build_case(args.workload)
+    workload = WORKLOADS[args.workload]
     gpu_index = torch.cuda.current_device()
     if args.adjoint_only:
         forms = (args.only,) if args.only else ("fp32", "fp64")
-        print(json.dumps(adjoint_report(ParticleHandler, m, V, Vold, prm, torch, forms=forms)), flush=True)
+        print(json.dumps(adjoint_report(ParticleHandler, m, V, Vold, prm, torch, K=ADJOINT_K[args.workload],
+                                        forms=forms)), flush=True)
         return 0
     if args.only:
         r = timed_device_run(ParticleHandler, m, V, Vold, prm, args.only, args.steps, args.warmup, torch)
@@ -452,7 +471,7 @@ def main():
     # end to end through the host ABI
     re2e = timed_host_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch)
     # the differentiated window (K = 20, checkpoints every 5) and its adjoint
-    adj = adjoint_report(ParticleHandler, m, V, Vold, prm, torch)
+    adj = adjoint_report(ParticleHandler, m, V, Vold, prm, torch, K=ADJOINT_K[args.workload])
     e2e_value = re2e["particle_steps"] / (re2e["ms"] / 1000.0)
     if rank != 0:
         if world > 1:
@@ -460,7 +479,7 @@ def main():
         return 0
     cb = None
     if not args.no_cpu_baseline:
-        cb = cpu_baseline(m, V, Vold, prm, budget_s=args.cpu_budget, max_steps=3)
+        cb = cpu_baseline(m, V, Vold, prm, budget_s=args.cpu_budget, max_steps=3, workload=workload)
     line = {
         "metric": METRIC,
         "value": value,
@@ -474,7 +493,7 @@ def main():
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": "fp32", "particles": r32["n_particles"],
+        "config": {"workload": workload, "form": "fp32", "particles": r32["n_particles"],
                    "l2": "inputs larger than L2 (particle arrays ~300 MB per form)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "fp64": {"value": v64, "unit": UNIT, "ms_per_step": r64["ms"] / args.steps, "dtype": "f64",

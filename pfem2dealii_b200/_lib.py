@@ -10,7 +10,9 @@ import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_build", "libpfem2gpu.so")
+# PFEM2GPU_LIB selects another build of the same library (for comparing two
+# builds in one process environment); by default the in-tree build.
+LIB_PATH = os.environ.get("PFEM2GPU_LIB") or os.path.join(HERE, "_build", "libpfem2gpu.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "pfem2gpu.h")
 
 OK = 0
