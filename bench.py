@@ -193,6 +193,43 @@ def timed_device_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, tor
     return res
 
 
+def timed_output(handler_cls, m, V, Vold, prm, torch, steps=5, reps=5):
+    """output_particle_solution's data for the workload after a few steps:
+    packing on the device plus one pinned device-to-host copy (best of reps,
+    CUDA events on the handler's stream)."""
+    g = handler_cls(3, prm, "fp32")
+    g.initialize_maps(m)
+    dev = torch.device("cuda:0")
+    dV = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
+    dVo = torch.from_numpy(np.ascontiguousarray(Vold)).to(dev)
+    out = torch.empty_like(dV)
+    g.seed_particles_device(dV)
+    for k in range(steps):
+        a, b = ((dVo, dV), (dV, dVo))[k & 1]
+        g.step_device(a, b, out)
+    g.synchronize()
+    n = g.stats()["n_particles"]
+    dout = torch.empty(6 * n, dtype=torch.float32, device=dev)
+    hout = torch.empty(6 * n, dtype=torch.float32).pin_memory()
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+    best = None
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.pack_output_device(dout)
+        with torch.cuda.stream(stream):
+            hout.copy_(dout, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1)
+        best = t if best is None else min(best, t)
+    # release the buffers used on the handler's stream before the stream goes
+    del hout, dout
+    torch.cuda.synchronize()
+    g.close()
+    return {"particles": n, "ms": best, "bytes": 24 * n}
+
+
 def timed_host_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, torch):
     """The same steps through the host C ABI with pinned vectors: H2D of V
     and Vold, D2H of the projected velocity, every step."""
@@ -470,6 +507,8 @@ def main():
     step_ms_prof = sum(v[0] for v in prof.values()) / args.steps
     # end to end through the host ABI
     re2e = timed_host_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch)
+    # output_particle_solution's data: packing on the device + one copy
+    outp = timed_output(ParticleHandler, m, V, Vold, prm, torch)
     # the differentiated window (K = 20, checkpoints every 5) and its adjoint
     adj = adjoint_report(ParticleHandler, m, V, Vold, prm, torch, K=ADJOINT_K[args.workload])
     e2e_value = re2e["particle_steps"] / (re2e["ms"] / 1000.0)
@@ -517,6 +556,8 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": re2e["h2d"],
                 "d2h_bytes_per_step": re2e["d2h"], "ms_per_step": re2e["ms"] / args.steps},
         "adjoint": adj,
+        "output_pack": {"particles": outp["particles"], "ms": outp["ms"], "bytes": outp["bytes"],
+                        "gbs": outp["bytes"] / (outp["ms"] / 1000.0) / 1e9},
         "gpu_launches": r32["launches"],
         "clocks": clk.summary(),
         "stats": {k: r32["stats"][k] for k in ("n_particles", "lost", "removed", "seeded", "searched",

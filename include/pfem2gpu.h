@@ -113,8 +113,17 @@ int pfem2gpu_get_particles(pfem2gpu_handle* h, uint32_t* id, int32_t* cell, doub
  * x is used by the FP64 form, ignored by the FP32 form. */
 int pfem2gpu_set_particles(pfem2gpu_handle* h, int64_t n, const uint32_t* id, const int32_t* cell, const double* x,
                            const double* xi, const double* v, uint32_t next_id);
-/* Particle VTU file as output_particle_solution writes it (rank 0 of 1). */
+/* Particle VTU file as output_particle_solution writes it (rank 0 of 1);
+ * the data come from pfem2gpu_pack_output_device in one copy. */
 int pfem2gpu_write_vtu(pfem2gpu_handle* h, const char* path);
+/* The data of output_particle_solution (:218-317) packed on the device as the
+ * Float32 values its file holds: d_out[3k .. 3k+2] = position of the k-th
+ * particle (pfem2gpu_get_particles order), d_out[3n + 3k .. 3n + 3k+2] = its
+ * velocity (2D: third components 0).  d_out: device array of >= 6 x capacity
+ * floats; *n gets the particle count (PFEM2GPU_ERR_ARG if capacity is
+ * smaller).  Asynchronous on the handle's stream: synchronise before reading
+ * d_out from another stream or the host. */
+int pfem2gpu_pack_output_device(pfem2gpu_handle* h, float* d_out, int64_t capacity, int64_t* n);
 
 int pfem2gpu_get_stats(pfem2gpu_handle* h, pfem2gpu_stats* out);
 int pfem2gpu_reset_stats(pfem2gpu_handle* h);

@@ -105,6 +105,7 @@ def load():
         "pfem2gpu_get_particles": [P, dptr, dptr, dptr, dptr, dptr, i64, C.POINTER(i64)],
         "pfem2gpu_set_particles": [P, i64, dptr, dptr, dptr, dptr, dptr, u32],
         "pfem2gpu_write_vtu": [P, C.c_char_p],
+        "pfem2gpu_pack_output_device": [P, dptr, i64, C.POINTER(i64)],
         "pfem2gpu_get_stats": [P, C.POINTER(Stats)],
         "pfem2gpu_reset_stats": [P],
         "pfem2gpu_synchronize": [P],

@@ -77,6 +77,10 @@ struct pfem2gpu_handle {
     std::vector<cudaEvent_t> ev_pool;
     std::map<std::string, std::pair<double, long long>> prof;
     std::string err;
+    // output packing: live-slot list, its scan tiles, the packed floats
+    uint32_t *out_slot = nullptr, *out_tsum = nullptr;
+    float *out_dev = nullptr, *out_host = nullptr;
+    uint32_t out_cap = 0, out_tcap = 0, out_dcap = 0;
     // differentiated window: checkpoints, final state, projection and adjoint
     // buffers (per-particle arrays sized ncap x segcap, the rest per mesh)
     struct Win {
@@ -718,6 +722,39 @@ int window_backward_impl(pfem2gpu_handle* h, const double* gU, double* g_v0, dou
     return PFEM2GPU_OK;
 }
 
+// Packed Float32 positions and velocities of the live particles (slot
+// order) into dst (device, >= 6 n floats); n = the particle count.
+int pack_output(pfem2gpu_handle* h, float* dst, int64_t capacity, int64_t* n)
+{
+    *n = 0;
+    if (!h->has_particles) return PFEM2GPU_OK;
+    int rc = apply_pending_correction(h);
+    if (rc) return rc;
+    if ((rc = sync_stats(h))) return rc;
+    const uint32_t np = (uint32_t)h->stats_h->n_particles, ns = (uint32_t)h->stats_h->n_slots;
+    *n = np;
+    if (capacity < (int64_t)np) return fail(h, PFEM2GPU_ERR_ARG, "output buffer too small");
+    if (np > h->out_cap) {
+        dfree(h->out_slot);
+        h->out_slot = nullptr;
+        h->out_cap = 0;
+        CK(dalloc(&h->out_slot, np));
+        h->out_cap = np;
+    }
+    const uint32_t tneed = (ns + WIN_TILE - 1) / WIN_TILE + 1;
+    if (tneed > h->out_tcap) {
+        dfree(h->out_tsum);
+        h->out_tsum = nullptr;
+        h->out_tcap = 0;
+        CK(dalloc(&h->out_tsum, tneed));
+        h->out_tcap = tneed;
+    }
+    StepArgs a = args(h);
+    run(h, "output_compact", [&] { return launch_win_compact(h->S0.cell, ns, (uint32_t)h->nC, h->out_tsum, h->out_slot, h->stream); });
+    run(h, "output_pack", [&] { return launch_pack_output(h->dim, h->prec, a, h->out_slot, np, dst, h->stream); });
+    return check_async(h);
+}
+
 }  // namespace
 
 extern "C" {
@@ -820,6 +857,10 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
     free_state(h->T);
     free_win_particles(h->win);
     free_win_mesh(h->win);
+    dfree(h->out_slot);
+    dfree(h->out_tsum);
+    dfree(h->out_dev);
+    if (h->out_host) cudaFreeHost(h->out_host);
     if (h->stats_h) cudaFreeHost(h->stats_h);
     for (auto& row : h->move_graph)
         for (auto& g : row)
@@ -1309,25 +1350,46 @@ int pfem2gpu_launch_count(pfem2gpu_handle* h, uint64_t* count)
     return PFEM2GPU_OK;
 }
 
+int pfem2gpu_pack_output_device(pfem2gpu_handle* h, float* d_out, int64_t capacity, int64_t* n)
+{
+    if (!h || !n || (capacity > 0 && !d_out)) return PFEM2GPU_ERR_ARG;
+    return pack_output(h, d_out, capacity, n);
+}
+
 int pfem2gpu_write_vtu(pfem2gpu_handle* h, const char* path)
 {
     if (!h || !path) return PFEM2GPU_ERR_ARG;
+    // the live particles' positions and velocities packed on the device as
+    // the Float32 values the file holds, one device-to-host copy
+    int rc = apply_pending_correction(h);
+    if (rc) return rc;
+    if (h->has_particles && (rc = sync_stats(h))) return rc;
+    const int64_t want = h->has_particles ? (int64_t)h->stats_h->n_particles : 0;
+    if (want > 0 && (uint64_t)want > h->out_dcap) {
+        dfree(h->out_dev);
+        if (h->out_host) cudaFreeHost(h->out_host);
+        h->out_dev = nullptr;
+        h->out_host = nullptr;
+        h->out_dcap = 0;
+        CK(dalloc(&h->out_dev, (size_t)want * 6));
+        CK(cudaMallocHost(&h->out_host, (size_t)want * 6 * sizeof(float)));
+        h->out_dcap = (uint32_t)want;
+    }
     int64_t n = 0;
-    int rc = pfem2gpu_get_particles(h, nullptr, nullptr, nullptr, nullptr, nullptr, 0, &n);
-    if (rc && rc != PFEM2GPU_ERR_ARG) return rc;
-    std::vector<double> x((size_t)std::max<int64_t>(n, 1) * h->dim), v(x.size());
-    if ((rc = pfem2gpu_get_particles(h, nullptr, nullptr, x.data(), nullptr, v.data(), n, &n))) return rc;
+    if ((rc = pack_output(h, h->out_dev, want, &n))) return rc;
+    if (n > 0) CK(cudaMemcpyAsync(h->out_host, h->out_dev, (size_t)n * 6 * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const float* xp = h->out_host;
+    const float* vp = h->out_host ? h->out_host + (size_t)n * 3 : nullptr;
     FILE* f = std::fopen(path, "w");
     if (!f) return fail(h, PFEM2GPU_ERR_ARG, std::string("cannot open ") + path);
-    const int dim = h->dim;
     // layout of output_particle_solution, src/pfem2particlehandler.cpp:223-291
     std::fprintf(f, "<?xml version=\"1.0\" ?> \n<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" "
                     "byte_order=\"LittleEndian\">\n  <UnstructuredGrid>\n");
     std::fprintf(f, "    <Piece NumberOfPoints=\"%lld\" NumberOfCells=\"%lld\">\n", (long long)n, (long long)n);
     std::fprintf(f, "      <Points>\n        <DataArray type=\"Float32\" NumberOfComponents=\"3\" Format=\"ascii\">\n");
     for (int64_t i = 0; i < n; ++i)
-        std::fprintf(f, "          %g %.6f %.6f\n", x[i * dim], dim > 1 ? x[i * dim + 1] : 0.0,
-                     dim > 2 ? x[i * dim + 2] : 0.0);
+        std::fprintf(f, "          %g %.6f %.6f\n", (double)xp[3 * i], (double)xp[3 * i + 1], (double)xp[3 * i + 2]);
     std::fprintf(f, "        </DataArray>\n      </Points>\n      <Cells>\n");
     std::fprintf(f, "        <DataArray type=\"Int32\" Name=\"connectivity\" Format=\"ascii\">\n");
     for (int64_t i = 0; i < n; ++i) std::fprintf(f, "          %lld\n", (long long)i);
@@ -1338,8 +1400,7 @@ int pfem2gpu_write_vtu(pfem2gpu_handle* h, const char* path)
     std::fprintf(f, "\n        </DataArray>\n      </Cells>\n      <PointData Scalars=\"scalars\">\n");
     std::fprintf(f, "        <DataArray type=\"Float32\" Name=\"velocity\" NumberOfComponents=\"3\" Format=\"ascii\">\n");
     for (int64_t i = 0; i < n; ++i)
-        std::fprintf(f, "          %g %.6f %.6f\n", v[i * dim], dim > 1 ? v[i * dim + 1] : 0.0,
-                     dim > 2 ? v[i * dim + 2] : 0.0);
+        std::fprintf(f, "          %g %.6f %.6f\n", (double)vp[3 * i], (double)vp[3 * i + 1], (double)vp[3 * i + 2]);
     std::fprintf(f, "        </DataArray>\n        <DataArray type=\"Float32\" Name=\"subdomain\" Format=\"ascii\">\n        ");
     for (int64_t i = 0; i < n; ++i) std::fprintf(f, "  0");
     std::fprintf(f, "\n        </DataArray>\n      </PointData>\n    </Piece>\n  </UnstructuredGrid>\n</VTKFile>\n");

@@ -929,4 +929,33 @@ __global__ void k_positions32(StepArgs a, double* xout)
     }
 }
 
+// Output packing (output_particle_solution, src/pfem2particlehandler.cpp:
+// 218-317, writes positions and velocities as Float32): for the k-th live
+// particle (slot[k], in slot order) out[3k..3k+2] = x and
+// out[3n + 3k..] = v as floats, x = the FP64 position (FP64 form) or F(xi)
+// in FP64 (FP32 form); 2D pads the third component with 0.
+template <int DIM, typename Real>
+__global__ void k_pack_output(StepArgs a, const uint32_t* __restrict__ slot, uint32_t n, float* __restrict__ out)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = slot[k];
+        double x[3] = {0.0, 0.0, 0.0};
+        if constexpr (std::is_same<Real, double>::value) {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) x[d] = ldr<double>(a.S0.x[d], i);
+        } else {
+            double X[1 << DIM][DIM], xi[DIM];
+            load_cell64<DIM>(a.mesh.cellX, a.S0.cell[i], X);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) xi[d] = (double)ldr<float>(a.S0.xi[d], i);
+            fwd64<DIM>(X, xi, x);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            out[(size_t)3 * k + d] = (float)x[d];
+            out[(size_t)3 * n + (size_t)3 * k + d] = d < DIM ? (float)ldr<Real>(a.S0.v[d], i) : 0.0f;
+        }
+    }
+}
+
 }  // namespace pfem2

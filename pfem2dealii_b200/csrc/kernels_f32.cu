@@ -110,6 +110,17 @@ int launch_gather(int dim, int prec, const StepArgs& a, int keep, cudaStream_t s
     return 1;
 }
 
+int launch64_pack_output(int dim, const StepArgs& a, const uint32_t* slot, uint32_t n, float* out, cudaStream_t s);
+
+int launch_pack_output(int dim, int prec, const StepArgs& a, const uint32_t* slot, uint32_t n, float* out,
+                       cudaStream_t s)
+{
+    if (prec == 0) return launch64_pack_output(dim, a, slot, n, out, s);
+    if (dim == 2) k_pack_output<2, float><<<PFEM2_GRID((k_pack_output<2, float>), 256), 256, 0, s>>>(a, slot, n, out);
+    else k_pack_output<3, float><<<PFEM2_GRID((k_pack_output<3, float>), 256), 256, 0, s>>>(a, slot, n, out);
+    return 1;
+}
+
 int launch_positions32(int dim, const StepArgs& a, double* xout, cudaStream_t s)
 {
     if (dim == 2) k_positions32<2><<<PFEM2_GRID(k_positions32<2>, 256), 256, 0, s>>>(a, xout);

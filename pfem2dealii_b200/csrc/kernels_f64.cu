@@ -172,4 +172,11 @@ int launch64_gather(int dim, const StepArgs& a, int keep, cudaStream_t s)
     return 1;
 }
 
+int launch64_pack_output(int dim, const StepArgs& a, const uint32_t* slot, uint32_t n, float* out, cudaStream_t s)
+{
+    if (dim == 2) k_pack_output<2, double><<<PFEM2_GRID((k_pack_output<2, double>), 256), 256, 0, s>>>(a, slot, n, out);
+    else k_pack_output<3, double><<<PFEM2_GRID((k_pack_output<3, double>), 256), 256, 0, s>>>(a, slot, n, out);
+    return 1;
+}
+
 }  // namespace pfem2

@@ -60,6 +60,8 @@ int launch_partials(int dim, int prec, const StepArgs& a, const uint32_t* cell_s
 int launch_correct(int dim, int prec, const StepArgs& a, cudaStream_t s);
 int launch_gather(int dim, int prec, const StepArgs& a, int keep_empty, cudaStream_t s);
 int launch_positions32(int dim, const StepArgs& a, double* xout, cudaStream_t s);
+int launch_pack_output(int dim, int prec, const StepArgs& a, const uint32_t* slot, uint32_t n, float* out,
+                       cudaStream_t s);
 
 // misc.cu
 constexpr int SCAN_TILE = 1024;       // cells per tile of the slot-offset scan

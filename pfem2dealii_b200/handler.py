@@ -256,6 +256,20 @@ class ParticleHandler:
                 _host(P["xi"], np.float64), _host(P["v"], np.float64)]
         self._ck(self.L.pfem2gpu_set_particles(self.h, n, *[_ptr(a) for a in arrs], next_id))
 
+    def pack_output_device(self, dout=None):
+        """Float32 positions and velocities of the particles packed on the
+        device (a CUDA tensor of 6 n floats: n x 3 positions, then n x 3
+        velocities), the data of output_particle_solution.  Returns the
+        tensor and n."""
+        import torch
+
+        n = self.stats()["n_particles"]
+        if dout is None:
+            dout = torch.empty(max(6 * n, 1), dtype=torch.float32, device="cuda")
+        got = C.c_int64()
+        self._ck(self.L.pfem2gpu_pack_output_device(self.h, _ptr(dout), dout.numel() // 6, C.byref(got)))
+        return dout, got.value
+
     def output_particle_solution(self, timestep_number: int, directory: str = "."):
         """particles-NN.000.vtu plus particles-NN.pvtu
         (src/pfem2particlehandler.cpp:218-317, one rank)."""

@@ -279,3 +279,33 @@ def test_step_device_graph_replay(precision):
         m = np.isfinite(Vh)
         assert np.array_equal(Vh[m], Vg[m])
         assert_same_particles(h.particles(), g.particles())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("which", ["channel", "duct", "cylinder"])
+def test_pack_output_matches_particles(precision, which):
+    """pfem2gpu_pack_output_device: the live particles' positions and
+    velocities as Float32, in get_particles order (empty slots skipped:
+    the runs include removals and losses)."""
+    import torch
+
+    c = {"channel": lambda: cases.channel(16, 4, q=(4, 4), maxpp=0, dt=0.03),
+         "duct": lambda: cases.duct(16, 4, 4, maxpp=0, dt=0.05),
+         "cylinder": lambda: cases.cylinder(24, 12, 60, dt=4e-3)}[which]()
+    _, g = make(c, precision)
+    g.seed_particles(c.V)
+    for _ in range(4):
+        g.step(c.V, c.Vold)
+    assert g.stats()["removed"] > 0 or which == "cylinder"
+    out, n = g.pack_output_device()
+    g.synchronize()
+    P = g.particles()
+    assert n == len(P["id"])
+    o = out.cpu().numpy()
+    dim = c.mesh.dim
+    x = o[: 3 * n].reshape(n, 3)
+    v = o[3 * n: 6 * n].reshape(n, 3)
+    assert np.array_equal(x[:, :dim], P["x"].astype(np.float32))
+    assert np.array_equal(v[:, :dim], P["v"].astype(np.float32))
+    if dim == 2:
+        assert not x[:, 2].any() and not v[:, 2].any()
