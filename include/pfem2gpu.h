@@ -79,10 +79,19 @@ int pfem2gpu_destroy(pfem2gpu_handle* h);
  * lexicographic vertex order (the DoF of vertex i is cell->vertex_dof_index(i,0),
  * src/pfem2particle.cpp:83-87).  The vertex maps (GridTools::vertex_to_cell_map,
  * vertex_to_cell_centers_directions) may be passed (offsets n_verts+1, cells
- * ascending, unit directions dim per entry) or NULL to have them built. */
+ * ascending, unit directions dim per entry) or NULL to have them built on the
+ * device (counting sort by vertex, cells ascending, FP64 directions centre -
+ * vertex normalised by the square root of the sum of squares). */
 int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int64_t n_dofs,
                       const double* vertices, const int32_t* cell_vertices, const int32_t* cell_dofs,
                       const int32_t* v2c_offsets, const int32_t* v2c_cells, const double* v2c_dirs);
+
+/* The vertex maps in use (given or built), copied to host arrays: offsets
+ * n_verts+1, cells and dirs (dim per entry) of >= capacity entries; *n = the
+ * number of entries.  With cells and dirs NULL only offsets and *n are
+ * read (the query for the capacity). */
+int pfem2gpu_get_vertex_maps(pfem2gpu_handle* h, int32_t* offsets, int32_t* cells, double* dirs, int64_t capacity,
+                             int64_t* n);
 
 /* seed_particles (src/pfem2particlehandler.cpp:43-109). */
 int pfem2gpu_seed(pfem2gpu_handle* h, const double* V);

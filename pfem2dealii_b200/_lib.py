@@ -121,6 +121,7 @@ def load():
         "pfem2gpu_adjoint": [P, C.c_int32, C.c_int32, dptr, dptr, dptr, dptr, dptr, dptr, dptr, dptr],
         "pfem2gpu_window_size": [P, C.POINTER(i64)],
         "pfem2gpu_window_particles": [P, dptr, dptr, dptr, i64, C.POINTER(i64)],
+        "pfem2gpu_get_vertex_maps": [P, dptr, dptr, dptr, i64, C.POINTER(i64)],
         "pfem2gpu_project_noalloc": [C.c_int, C.c_int32, C.c_int32, dptr, i64, dptr, dptr, dptr, C.c_int, dptr,
                                      C.POINTER(i64), P],
     }

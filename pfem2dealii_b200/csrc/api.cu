@@ -877,6 +877,67 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
     return PFEM2GPU_OK;
 }
 
+// Counting sorts on the device (cv, cd and verts already resident): dof ->
+// entries k = cell * NV + i ascending per dof, and, unless the caller gave
+// them, vertex -> cells ascending with the unit vertex -> centre directions.
+// One host read of the vertex map's length sizes its arrays.
+static cudaError_t build_maps(pfem2gpu_handle* h, size_t nc, size_t nvx, size_t nd, bool given,
+                              const int32_t* v2c_offsets, const int32_t* v2c_cells, const double* v2c_dirs)
+{
+    const int dim = h->dim, NV = 1 << dim;
+    const size_t nmax = std::max(nvx, nd), ntiles = (nmax + WIN_TILE - 1) / WIN_TILE + 1;
+    uint32_t *cnt = nullptr, *fill = nullptr, *tsum = nullptr;
+    cudaError_t e = cudaSuccess;
+    auto done = [&](cudaError_t r) {
+        dfree(cnt);
+        dfree(fill);
+        dfree(tsum);
+        return r;
+    };
+#define BM(x)                                      \
+    do {                                           \
+        if ((e = (x)) != cudaSuccess) return done(e); \
+    } while (0)
+    BM(dalloc(&cnt, nmax));
+    BM(dalloc(&fill, nmax));
+    BM(dalloc(&tsum, ntiles));
+    cudaStream_t s = h->stream;
+    // dof -> (cell, local vertex)
+    BM(cudaMemsetAsync(cnt, 0, nd * 4, s));
+    BM(cudaMemsetAsync(fill, 0, nd * 4, s));
+    launch_d2c_count((long long)(nc * NV), h->cd, cnt, s);
+    launch_win_scan(cnt, (uint32_t)nd, tsum, (uint32_t*)h->d2c_off, s);
+    launch_d2c_build((long long)(nc * NV), (int)nd, h->cd, (const uint32_t*)h->d2c_off, fill, h->d2c_ent, s);
+    BM(cudaGetLastError());
+    // vertex -> cells
+    int32_t total = 0;
+    if (given) {
+        total = v2c_offsets[nvx];
+        BM(dalloc(&h->v2c_cells, std::max<size_t>(total, 1)));
+        BM(dalloc(&h->v2c_dirs, std::max<size_t>((size_t)total * dim, 1)));
+        BM(cudaMemcpyAsync(h->v2c_off, v2c_offsets, (nvx + 1) * 4, cudaMemcpyHostToDevice, s));
+        BM(cudaMemcpyAsync(h->v2c_cells, v2c_cells, (size_t)total * 4, cudaMemcpyHostToDevice, s));
+        BM(cudaMemcpyAsync(h->v2c_dirs, v2c_dirs, (size_t)total * dim * 8, cudaMemcpyHostToDevice, s));
+        BM(cudaStreamSynchronize(s));
+        return done(cudaSuccess);
+    }
+    BM(cudaMemsetAsync(cnt, 0, nvx * 4, s));
+    BM(cudaMemsetAsync(fill, 0, nvx * 4, s));
+    launch_v2c_count(dim, (int)nc, h->cv, cnt, s);
+    launch_win_scan(cnt, (uint32_t)nvx, tsum, (uint32_t*)h->v2c_off, s);
+    BM(cudaGetLastError());
+    BM(cudaMemcpyAsync(&total, h->v2c_off + nvx, 4, cudaMemcpyDeviceToHost, s));
+    BM(cudaStreamSynchronize(s));
+    BM(dalloc(&h->v2c_cells, std::max<size_t>(total, 1)));
+    BM(dalloc(&h->v2c_dirs, std::max<size_t>((size_t)total * dim, 1)));
+    launch_v2c_build(dim, (int)nc, (int)nvx, h->verts, h->cv, (const uint32_t*)h->v2c_off, fill, h->v2c_cells,
+                     h->v2c_dirs, s);
+    BM(cudaGetLastError());
+    BM(cudaStreamSynchronize(s));
+#undef BM
+    return done(cudaSuccess);
+}
+
 int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int64_t n_dofs, const double* vertices,
                       const int32_t* cell_vertices, const int32_t* cell_dofs, const int32_t* v2c_offsets,
                       const int32_t* v2c_cells, const double* v2c_dirs)
@@ -892,72 +953,28 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
         if (cell_vertices[k] < 0 || cell_vertices[k] >= n_verts) return fail(h, PFEM2GPU_ERR_ARG, "bad cell vertex");
         if (cell_dofs[k] < 0 || cell_dofs[k] >= n_dofs) return fail(h, PFEM2GPU_ERR_ARG, "bad cell dof");
     }
-    // vertex -> cells (ascending) and unit vertex -> centre directions
-    std::vector<int32_t> off, cells;
-    std::vector<double> dirs;
-    if (v2c_offsets && v2c_cells && v2c_dirs) {
-        off.assign(v2c_offsets, v2c_offsets + n_verts + 1);
-        if (off[0] != 0) return fail(h, PFEM2GPU_ERR_ARG, "v2c offsets must start at 0");
+    if (n_cells * NV > (int64_t)INT32_MAX) return fail(h, PFEM2GPU_ERR_ARG, "mesh too large");
+    // vertex -> cells (ascending) and unit vertex -> centre directions: the
+    // caller's maps, checked here, or built on the device further down
+    const bool given_maps = v2c_offsets && v2c_cells && v2c_dirs;
+    if (given_maps) {
+        if (v2c_offsets[0] != 0) return fail(h, PFEM2GPU_ERR_ARG, "v2c offsets must start at 0");
         for (int64_t v = 0; v < n_verts; ++v)
-            if (off[v + 1] < off[v]) return fail(h, PFEM2GPU_ERR_ARG, "v2c offsets not monotone");
-        cells.assign(v2c_cells, v2c_cells + off[n_verts]);
-        for (int32_t c : cells)
-            if (c < 0 || c >= n_cells) return fail(h, PFEM2GPU_ERR_ARG, "bad v2c cell");
-        dirs.assign(v2c_dirs, v2c_dirs + (size_t)off[n_verts] * dim);
-    } else {
-        off.assign(n_verts + 1, 0);
-        std::vector<int32_t> last(n_verts, -1);
-        for (int64_t c = 0; c < n_cells; ++c)
-            for (int i = 0; i < NV; ++i) {
-                const int32_t v = cell_vertices[c * NV + i];
-                if (last[v] != (int32_t)c) {
-                    last[v] = (int32_t)c;
-                    off[v + 1]++;
-                }
-            }
-        for (int64_t v = 0; v < n_verts; ++v) off[v + 1] += off[v];
-        cells.assign(off[n_verts], 0);
-        dirs.assign((size_t)off[n_verts] * dim, 0.0);
-        std::vector<int32_t> fill(off.begin(), off.end() - 1);
-        std::fill(last.begin(), last.end(), -1);
-        for (int64_t c = 0; c < n_cells; ++c)
-            for (int i = 0; i < NV; ++i) {
-                const int32_t v = cell_vertices[c * NV + i];
-                if (last[v] == (int32_t)c) continue;
-                last[v] = (int32_t)c;
-                cells[fill[v]++] = (int32_t)c;
-            }
-        for (int64_t v = 0; v < n_verts; ++v)
-            for (int32_t k = off[v]; k < off[v + 1]; ++k) {
-                const int64_t c = cells[k];
-                double dir[3], s = 0.0;
-                for (int d = 0; d < dim; ++d) {
-                    double ctr = 0.0;
-                    for (int i = 0; i < NV; ++i) ctr = ctr + vertices[(size_t)cell_vertices[c * NV + i] * dim + d];
-                    ctr = ctr / (double)NV;
-                    dir[d] = ctr - vertices[v * dim + d];
-                }
-                for (int d = 0; d < dim; ++d) s = s + dir[d] * dir[d];
-                s = std::sqrt(s);
-                for (int d = 0; d < dim; ++d) dirs[(size_t)k * dim + d] = dir[d] / s;
-            }
+            if (v2c_offsets[v + 1] < v2c_offsets[v]) return fail(h, PFEM2GPU_ERR_ARG, "v2c offsets not monotone");
+        for (int64_t k = 0; k < v2c_offsets[n_verts]; ++k)
+            if (v2c_cells[k] < 0 || v2c_cells[k] >= n_cells) return fail(h, PFEM2GPU_ERR_ARG, "bad v2c cell");
     }
-    // dof -> (cell, local vertex), cells ascending
-    std::vector<int32_t> doff(n_dofs + 1, 0), dent((size_t)n_cells * NV);
-    for (int64_t k = 0; k < n_cells * NV; ++k) doff[cell_dofs[k] + 1]++;
-    for (int64_t d = 0; d < n_dofs; ++d) doff[d + 1] += doff[d];
-    {
-        std::vector<int32_t> fill(doff.begin(), doff.end() - 1);
-        for (int64_t k = 0; k < n_cells * NV; ++k) dent[fill[cell_dofs[k]]++] = (int32_t)k;
+    // release an older mesh (a failure further down leaves no dangling pointer)
+    for (void** p : {(void**)&h->cv, (void**)&h->cd, (void**)&h->v2c_off, (void**)&h->v2c_cells, (void**)&h->d2c_off,
+                     (void**)&h->d2c_ent, (void**)&h->verts, (void**)&h->cellX, (void**)&h->aff,
+                     (void**)&h->v2c_dirs, (void**)&h->geo32, (void**)&h->Vstage, (void**)&h->Vstage2,
+                     (void**)&h->Vout, (void**)&h->Vc, (void**)&h->dVc, (void**)&h->head, (void**)&h->cs0,
+                     (void**)&h->cs1, (void**)&h->carr, (void**)&h->carrs, (void**)&h->ccount, (void**)&h->cocc,
+                     (void**)&h->cub, (void**)&h->coff, (void**)&h->tiles64, (void**)&h->jinv32, (void**)&h->vrec32,
+                     (void**)&h->dvrec32, (void**)&h->partials, (void**)&h->twisted}) {
+        dfree(*p);
+        *p = nullptr;
     }
-    // release an older mesh
-    for (void* p : {(void*)h->cv, (void*)h->cd, (void*)h->v2c_off, (void*)h->v2c_cells, (void*)h->d2c_off,
-                    (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
-                    (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vc, h->dVc,
-                    (void*)h->head, (void*)h->cs0, (void*)h->cs1, (void*)h->carr, (void*)h->carrs,
-                    (void*)h->ccount, (void*)h->cocc, (void*)h->cub, (void*)h->coff, (void*)h->tiles64,
-                    (void*)h->jinv32, (void*)h->vrec32, (void*)h->dvrec32, h->partials, (void*)h->twisted})
-        dfree(p);
     free_win_mesh(h->win);
     h->has_mesh = false;
     h->nC = (int)n_cells;
@@ -969,10 +986,8 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(dalloc(&h->cd, nc * NV));
     CK(dalloc(&h->verts, nvx * dim));
     CK(dalloc(&h->v2c_off, nvx + 1));
-    CK(dalloc(&h->v2c_cells, cells.size()));
-    CK(dalloc(&h->v2c_dirs, dirs.size()));
     CK(dalloc(&h->d2c_off, nd + 1));
-    CK(dalloc(&h->d2c_ent, dent.size()));
+    CK(dalloc(&h->d2c_ent, nc * NV));
     CK(dalloc(&h->cellX, nc * NV * dim));
     CK(dalloc(&h->aff, nc * AFF));
     CK(dalloc(&h->geo32, nc * GS));
@@ -1010,11 +1025,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(cudaMemcpyAsync(h->cv, cell_vertices, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->cd, cell_dofs, nc * NV * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->verts, vertices, nvx * dim * 8, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->v2c_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->v2c_cells, cells.data(), cells.size() * 4, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->v2c_dirs, dirs.data(), dirs.size() * 8, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d2c_off, doff.data(), doff.size() * 4, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d2c_ent, dent.data(), dent.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(build_maps(h, nc, nvx, nd, given_maps, v2c_offsets, v2c_cells, v2c_dirs));
     CK(cudaMemsetAsync(h->Vc, 0, vcn * esize(h), h->stream));
     CK(cudaMemsetAsync(h->dVc, 0, vcn * esize(h), h->stream));
     run(h, "fill", [&] { return launch_fill_u32(h->head, (uint32_t)nc, LOST, h->stream); });
@@ -1426,6 +1437,23 @@ int pfem2gpu_adjoint(pfem2gpu_handle* h, int32_t steps, int32_t checkpoint_every
     int rc = window_forward_impl(h, steps, checkpoint_every, V, Vold, v0, U, true);
     if (rc) return rc;
     return window_backward_impl(h, gU, g_v0, g_V, g_Vold, true);
+}
+
+int pfem2gpu_get_vertex_maps(pfem2gpu_handle* h, int32_t* offsets, int32_t* cells, double* dirs, int64_t capacity,
+                             int64_t* n)
+{
+    if (!h || !n) return PFEM2GPU_ERR_ARG;
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "no mesh");
+    int32_t total = 0;
+    CK(cudaMemcpyAsync(&total, h->v2c_off + h->nV, 4, cudaMemcpyDeviceToHost, h->stream));
+    if (offsets) CK(cudaMemcpyAsync(offsets, h->v2c_off, ((size_t)h->nV + 1) * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *n = total;
+    if ((cells || dirs) && capacity < total) return fail(h, PFEM2GPU_ERR_ARG, "output arrays too small");
+    if (cells) CK(cudaMemcpyAsync(cells, h->v2c_cells, (size_t)total * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (dirs) CK(cudaMemcpyAsync(dirs, h->v2c_dirs, (size_t)total * h->dim * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PFEM2GPU_OK;
 }
 
 int pfem2gpu_window_particles(pfem2gpu_handle* h, int32_t* cell, double* xi, double* v, int64_t capacity, int64_t* n)

@@ -179,4 +179,158 @@ int launch64_pack_output(int dim, const StepArgs& a, const uint32_t* slot, uint3
     return 1;
 }
 
+// ---------------------------------------------------------------------------
+// Vertex -> cell map on the device (initialize_maps,
+// src/pfem2particlehandler.cpp:320-324: GridTools::vertex_to_cell_map and
+// vertex_to_cell_centers_directions): per vertex the cells around it in
+// ascending order, each with the unit direction from the vertex to the cell
+// centre, the same FP64 operations as the host builder (this file is
+// compiled with --fmad=false).
+// ---------------------------------------------------------------------------
+namespace {
+
+// A cell's vertex that appears earlier in the same cell is not counted again.
+template <int DIM>
+__device__ __forceinline__ bool first_in_cell(const int32_t* __restrict__ cv, int c, int i)
+{
+    constexpr int NV = 1 << DIM;
+    const int32_t v = cv[(size_t)c * NV + i];
+    for (int j = 0; j < i; ++j)
+        if (cv[(size_t)c * NV + j] == v) return false;
+    return true;
+}
+
+template <int DIM>
+__global__ void k_v2c_count(int nC, const int32_t* __restrict__ cv, uint32_t* __restrict__ cnt)
+{
+    constexpr int NV = 1 << DIM;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nC * NV;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / NV), i = (int)(t % NV);
+        if (first_in_cell<DIM>(cv, c, i)) atomicAdd(cnt + cv[t], 1u);
+    }
+}
+
+template <int DIM>
+__global__ void k_v2c_place(int nC, const int32_t* __restrict__ cv, const uint32_t* __restrict__ off,
+                            uint32_t* __restrict__ fill, int32_t* __restrict__ cells)
+{
+    constexpr int NV = 1 << DIM;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nC * NV;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / NV), i = (int)(t % NV);
+        if (!first_in_cell<DIM>(cv, c, i)) continue;
+        const int32_t v = cv[t];
+        cells[off[v] + atomicAdd(fill + v, 1u)] = c;
+    }
+}
+
+// Per vertex: its cells in ascending order, then the unit directions.
+template <int DIM>
+__global__ void k_v2c_finish(int nV, const double* __restrict__ verts, const int32_t* __restrict__ cv,
+                             const uint32_t* __restrict__ off, int32_t* __restrict__ cells, double* __restrict__ dirs)
+{
+    constexpr int NV = 1 << DIM;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nV; v += gridDim.x * blockDim.x) {
+        const uint32_t b = off[v], e = off[v + 1];
+        for (uint32_t k = b + 1; k < e; ++k) {  // insertion sort (a handful of cells)
+            const int32_t x = cells[k];
+            uint32_t j = k;
+            while (j > b && cells[j - 1] > x) {
+                cells[j] = cells[j - 1];
+                --j;
+            }
+            cells[j] = x;
+        }
+        for (uint32_t k = b; k < e; ++k) {
+            const int c = cells[k];
+            double dir[DIM], s = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                double ctr = 0.0;
+#pragma unroll
+                for (int i = 0; i < NV; ++i) ctr = ctr + verts[(size_t)cv[(size_t)c * NV + i] * DIM + d];
+                ctr = ctr / (double)NV;
+                dir[d] = ctr - verts[(size_t)v * DIM + d];
+            }
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) s = s + dir[d] * dir[d];
+            s = sqrt(s);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) dirs[(size_t)k * DIM + d] = dir[d] / s;
+        }
+    }
+}
+
+// dof -> (cell, local vertex) entries k = cell * NV + i, ascending per dof.
+__global__ void k_d2c_count(long long nE, const int32_t* __restrict__ cd, uint32_t* __restrict__ cnt)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nE; k += (long long)gridDim.x * blockDim.x)
+        atomicAdd(cnt + cd[k], 1u);
+}
+
+__global__ void k_d2c_place(long long nE, const int32_t* __restrict__ cd, const uint32_t* __restrict__ off,
+                            uint32_t* __restrict__ fill, int32_t* __restrict__ ent)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nE; k += (long long)gridDim.x * blockDim.x) {
+        const int32_t d = cd[k];
+        ent[off[d] + atomicAdd(fill + d, 1u)] = (int32_t)k;
+    }
+}
+
+__global__ void k_d2c_sort(int nD, const uint32_t* __restrict__ off, int32_t* __restrict__ ent)
+{
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nD; d += gridDim.x * blockDim.x) {
+        const uint32_t b = off[d], e = off[d + 1];
+        for (uint32_t k = b + 1; k < e; ++k) {
+            const int32_t x = ent[k];
+            uint32_t j = k;
+            while (j > b && ent[j - 1] > x) {
+                ent[j] = ent[j - 1];
+                --j;
+            }
+            ent[j] = x;
+        }
+    }
+}
+
+}  // namespace
+
+int launch_d2c_count(long long nE, const int32_t* cd, uint32_t* cnt, cudaStream_t s)
+{
+    k_d2c_count<<<PFEM2_GRID(k_d2c_count, 256), 256, 0, s>>>(nE, cd, cnt);
+    return 1;
+}
+
+int launch_d2c_build(long long nE, int nD, const int32_t* cd, const uint32_t* off, uint32_t* fill, int32_t* ent,
+                     cudaStream_t s)
+{
+    k_d2c_place<<<PFEM2_GRID(k_d2c_place, 256), 256, 0, s>>>(nE, cd, off, fill, ent);
+    k_d2c_sort<<<PFEM2_GRID(k_d2c_sort, 128), 128, 0, s>>>(nD, off, ent);
+    return 2;
+}
+
+// Counts per vertex into cnt (zeroed by the caller), then, once the caller
+// has their exclusive scan in off (nV + 1), the ascending lists and the
+// directions; fill (nV, zeroed) is the placement counter.
+int launch_v2c_count(int dim, int nC, const int32_t* cv, uint32_t* cnt, cudaStream_t s)
+{
+    if (dim == 2) k_v2c_count<2><<<PFEM2_GRID(k_v2c_count<2>, 256), 256, 0, s>>>(nC, cv, cnt);
+    else k_v2c_count<3><<<PFEM2_GRID(k_v2c_count<3>, 256), 256, 0, s>>>(nC, cv, cnt);
+    return 1;
+}
+
+int launch_v2c_build(int dim, int nC, int nV, const double* verts, const int32_t* cv, const uint32_t* off,
+                     uint32_t* fill, int32_t* cells, double* dirs, cudaStream_t s)
+{
+    if (dim == 2) {
+        k_v2c_place<2><<<PFEM2_GRID(k_v2c_place<2>, 256), 256, 0, s>>>(nC, cv, off, fill, cells);
+        k_v2c_finish<2><<<PFEM2_GRID(k_v2c_finish<2>, 128), 128, 0, s>>>(nV, verts, cv, off, cells, dirs);
+    } else {
+        k_v2c_place<3><<<PFEM2_GRID(k_v2c_place<3>, 256), 256, 0, s>>>(nC, cv, off, fill, cells);
+        k_v2c_finish<3><<<PFEM2_GRID(k_v2c_finish<3>, 128), 128, 0, s>>>(nV, verts, cv, off, cells, dirs);
+    }
+    return 2;
+}
+
 }  // namespace pfem2

@@ -63,6 +63,14 @@ int launch_positions32(int dim, const StepArgs& a, double* xout, cudaStream_t s)
 int launch_pack_output(int dim, int prec, const StepArgs& a, const uint32_t* slot, uint32_t n, float* out,
                        cudaStream_t s);
 
+// kernels_f64.cu: vertex -> cell and dof -> cell maps built on the device
+int launch_v2c_count(int dim, int nC, const int32_t* cv, uint32_t* cnt, cudaStream_t s);
+int launch_v2c_build(int dim, int nC, int nV, const double* verts, const int32_t* cv, const uint32_t* off,
+                     uint32_t* fill, int32_t* cells, double* dirs, cudaStream_t s);
+int launch_d2c_count(long long nE, const int32_t* cd, uint32_t* cnt, cudaStream_t s);
+int launch_d2c_build(long long nE, int nD, const int32_t* cd, const uint32_t* off, uint32_t* fill, int32_t* ent,
+                     cudaStream_t s);
+
 // misc.cu
 constexpr int SCAN_TILE = 1024;       // cells per tile of the slot-offset scan
 constexpr int SCAN_MAX_TILES = 8192;  // tile sums the scan buffer holds

@@ -130,8 +130,10 @@ class ParticleHandler:
         _lib.check(rc, self.h)
 
     # -- mesh -----------------------------------------------------------------
-    def initialize_maps(self, mesh: Mesh, with_maps: bool = True):
-        """Mesh upload plus initialize_maps (src/pfem2particlehandler.cpp:320-324)."""
+    def initialize_maps(self, mesh: Mesh, host_maps: bool = False):
+        """Mesh upload plus initialize_maps (src/pfem2particlehandler.cpp:320-324).
+        The vertex maps are built on the device, or, with host_maps, by
+        mesh.vertex_maps and passed in."""
         assert mesh.dim == self.dim
         self.mesh = mesh
         self._keep = [
@@ -140,7 +142,7 @@ class ParticleHandler:
             _host(mesh.cell_dofs, np.int32),
         ]
         maps = [None, None, None]
-        if with_maps:
+        if host_maps:
             off, cells, dirs = vertex_maps(mesh)
             maps = [_host(off, np.int32), _host(cells, np.int32), _host(dirs, np.float64)]
             self._keep += maps
@@ -207,6 +209,17 @@ class ParticleHandler:
         """Adjoint of the last window forward for dJ/dU = dgU (CUDA tensors)."""
         self._ck(self.L.pfem2gpu_window_backward_device(self.h, _ptr(dgU), _ptr(dg_v0), _ptr(dg_V),
                                                         _ptr(dg_Vold)))
+
+    def vertex_maps(self):
+        """The vertex -> cell maps in use: (offsets, cells, dirs (n, dim))."""
+        off = np.zeros(self.mesh.n_verts + 1, np.int32)
+        n = C.c_int64()
+        self._ck(self.L.pfem2gpu_get_vertex_maps(self.h, _ptr(off), None, None, 0, C.byref(n)))
+        k = max(n.value, 1)
+        cells = np.zeros(k, np.int32)
+        dirs = np.zeros((k, self.dim))
+        self._ck(self.L.pfem2gpu_get_vertex_maps(self.h, _ptr(off), _ptr(cells), _ptr(dirs), k, C.byref(n)))
+        return off, cells[: n.value], dirs[: n.value]
 
     def window_particles(self):
         """End states of the last window forward: cell (-1: deleted), xi, v."""

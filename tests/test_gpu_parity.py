@@ -309,3 +309,63 @@ def test_pack_output_matches_particles(precision, which):
     assert np.array_equal(v[:, :dim], P["v"].astype(np.float32))
     if dim == 2:
         assert not x[:, 2].any() and not v[:, 2].any()
+
+
+def _maps_case(which):
+    if which == "cube_big":
+        return cases.cube(n=96)
+    return getattr(cases, which)()
+
+
+@pytest.mark.parametrize("which", ["channel", "duct", "cylinder", "cube", "cube_big"])
+def test_device_vertex_maps_equal_host_builder(which):
+    """initialize_maps built on the device (src/pfem2particlehandler.cpp:320-324):
+    offsets and ascending cells equal mesh.vertex_maps, the unit directions
+    bit for bit."""
+    case = _maps_case(which)
+    g = ParticleHandler(case.mesh.dim, cases.params(case), "fp64")
+    g.initialize_maps(case.mesh)
+    off, cells, dirs = g.vertex_maps()
+    o2, c2, d2 = M.vertex_maps(case.mesh)
+    assert np.array_equal(off, o2)
+    assert np.array_equal(cells, c2)
+    assert dirs.shape == d2.shape and dirs.tobytes() == d2.tobytes()
+    g.close()
+
+
+def test_given_vertex_maps_kept_and_runs_identical():
+    """Maps passed by the caller are used as given; a run on them equals the
+    run on device-built maps bit for bit."""
+    case = cases.cylinder()
+    runs = []
+    for host_maps in (True, False):
+        g = ParticleHandler(case.mesh.dim, cases.params(case), "fp64")
+        g.initialize_maps(case.mesh, host_maps=host_maps)
+        if host_maps:
+            off, cells, dirs = g.vertex_maps()
+            o2, c2, d2 = M.vertex_maps(case.mesh)
+            assert np.array_equal(off, o2) and np.array_equal(cells, c2) and dirs.tobytes() == d2.tobytes()
+        g.seed_particles(case.V)
+        for _ in range(5):
+            U = g.step(case.V, case.Vold)
+        runs.append((by_id(g.particles()), U))
+        g.close()
+    (a, Ua), (b, Ub) = runs
+    for k in ("id", "cell", "x", "xi", "v"):
+        assert np.array_equal(a[k], b[k]), k
+    assert Ua.tobytes() == Ub.tobytes()
+
+
+def test_device_vertex_maps_collapsed_cell():
+    """A cell listing one vertex twice counts it once (the map is a set per
+    vertex), as GridTools::vertex_to_cell_map does."""
+    verts = np.array([[0, 0], [1, 0], [0, 1], [1, 1], [2, 0], [2, 1]], np.float64)
+    cells = np.array([[0, 1, 2, 3], [1, 4, 3, 3]], np.int32)
+    m = M.Mesh(2, verts, cells, cells.copy(), verts.shape[0], "collapsed")
+    g = ParticleHandler(2, cases.params(cases.channel()), "fp64")
+    g.initialize_maps(m)
+    off, cl, dirs = g.vertex_maps()
+    o2, c2, d2 = M.vertex_maps(m)
+    assert np.array_equal(off, o2) and np.array_equal(cl, c2) and dirs.tobytes() == d2.tobytes()
+    assert off[4] - off[3] == 2
+    g.close()
