@@ -452,6 +452,8 @@ def main():
                     help="time the differentiated window and its adjoint only (prints one JSON object)")
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
                     help="run one device-resident pass of one form and print its timing (profiling runs)")
+    ap.add_argument("--kernels", action="store_true",
+                    help="with --only: also the per-kernel times of a profiled run (CUDA events)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -479,8 +481,13 @@ def main():
         return 0
     if args.only:
         r = timed_device_run(ParticleHandler, m, V, Vold, prm, args.only, args.steps, args.warmup, torch)
-        print(json.dumps({"form": args.only, "ms_per_step": r["ms"] / args.steps,
-                          "value": r["particle_steps"] / (r["ms"] / 1000.0), "unit": UNIT}), flush=True)
+        out = {"form": args.only, "ms_per_step": r["ms"] / args.steps,
+               "value": r["particle_steps"] / (r["ms"] / 1000.0), "unit": UNIT}
+        if args.kernels:
+            rp = timed_device_run(ParticleHandler, m, V, Vold, prm, args.only, args.steps, args.warmup, torch,
+                                  profile=True)
+            out["kernel_ms_per_step"] = {k: v[0] / args.steps for k, v in sorted(rp["profile"].items())}
+        print(json.dumps(out), flush=True)
         return 0
 
     def barrier():

@@ -93,6 +93,20 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
 int pfem2gpu_get_vertex_maps(pfem2gpu_handle* h, int32_t* offsets, int32_t* cells, double* dirs, int64_t capacity,
                              int64_t* n);
 
+/* GridIn::read_unv as the reference's solver calls it
+ * (src/pfem2solver.cpp:116-119), host only (no device needed): datasets 2411
+ * (nodes) and 2412 (elements) of an I-DEAS universal file; quads (44, 94) in
+ * 2D, hexes (115) in 3D become cells in deal.II's lexicographic vertex order,
+ * left-handed cells get their first two directions swapped, nodes no cell
+ * uses are dropped and vertices are numbered by ascending node label.  dim 0
+ * takes it from the elements (*dim_out: the mesh's).  With vertices and
+ * cell_vertices NULL only the counts are returned; then arrays of
+ * n_verts x dim and n_cells x 2^dim.
+ * The reason of a failure: pfem2gpu_read_unv_error(). */
+int pfem2gpu_read_unv(const char* path, int dim, int32_t* dim_out, int64_t* n_verts, int64_t* n_cells,
+                      double* vertices, int32_t* cell_vertices, int64_t verts_capacity, int64_t cells_capacity);
+const char* pfem2gpu_read_unv_error(void);
+
 /* seed_particles (src/pfem2particlehandler.cpp:43-109). */
 int pfem2gpu_seed(pfem2gpu_handle* h, const double* V);
 /* correct_particle_velocity (:112-139): v += sum N_i (V - Vold)_i; applied

@@ -122,6 +122,9 @@ def load():
         "pfem2gpu_window_size": [P, C.POINTER(i64)],
         "pfem2gpu_window_particles": [P, dptr, dptr, dptr, i64, C.POINTER(i64)],
         "pfem2gpu_get_vertex_maps": [P, dptr, dptr, dptr, i64, C.POINTER(i64)],
+        "pfem2gpu_read_unv": [C.c_char_p, C.c_int, C.POINTER(C.c_int32), C.POINTER(i64), C.POINTER(i64), dptr, dptr,
+                              i64, i64],
+        "pfem2gpu_read_unv_error": [],
         "pfem2gpu_project_noalloc": [C.c_int, C.c_int32, C.c_int32, dptr, i64, dptr, dptr, dptr, C.c_int, dptr,
                                      C.POINTER(i64), P],
     }
@@ -131,6 +134,7 @@ def load():
         f.restype = C.c_int
     L.pfem2gpu_error_string.argtypes = [C.c_int]
     L.pfem2gpu_error_string.restype = C.c_char_p
+    L.pfem2gpu_read_unv_error.restype = C.c_char_p
     _lib = L
     return L
 

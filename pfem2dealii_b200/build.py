@@ -29,6 +29,7 @@ SOURCES = {
     "noalloc.cu": ["--fmad=false"],
     "window_f64.cu": ["--fmad=false"],
     "window_f32.cu": [],
+    "mesh_io.cu": [],
 }
 
 

@@ -260,6 +260,44 @@ def read_unv(src, dim=None) -> Mesh:
     return Mesh(dim, verts, cells, cells.copy(), verts.shape[0], "unv")
 
 
+def read_unv_native(src, dim=None) -> Mesh:
+    """read_unv through the library's C++ reader (pfem2gpu_read_unv, host
+    only): the same mesh, for large files.  ``src`` is a .unv path or a .tgz
+    archive holding one (extracted to a temporary file first)."""
+    import ctypes as C
+    import tempfile
+
+    from . import _lib
+
+    L = _lib.load()
+    p = os.fspath(src)
+    tmp = None
+    if p.endswith((".tgz", ".tar.gz")):
+        with tarfile.open(p) as tf:
+            mem = [m for m in tf.getmembers() if m.name.endswith(".unv")][0]
+            tmp = tempfile.NamedTemporaryFile(suffix=".unv", delete=False)
+            tmp.write(tf.extractfile(mem).read())
+            tmp.close()
+            p = tmp.name
+    try:
+        nv, nc, dd = C.c_int64(), C.c_int64(), C.c_int32()
+        path = p.encode()
+        rc = L.pfem2gpu_read_unv(path, int(dim or 0), C.byref(dd), C.byref(nv), C.byref(nc), None, None, 0, 0)
+        if rc != _lib.OK:
+            raise ValueError(L.pfem2gpu_read_unv_error().decode())
+        d = dd.value
+        verts = np.empty((nv.value, d), np.float64)
+        cells = np.empty((nc.value, 1 << d), np.int32)
+        rc = L.pfem2gpu_read_unv(path, d, None, C.byref(nv), C.byref(nc), verts.ctypes.data_as(C.c_void_p),
+                                 cells.ctypes.data_as(C.c_void_p), nv.value, nc.value)
+        if rc != _lib.OK:
+            raise ValueError(L.pfem2gpu_read_unv_error().decode())
+    finally:
+        if tmp is not None:
+            os.unlink(tmp.name)
+    return Mesh(d, verts, cells, cells.copy(), verts.shape[0], "unv")
+
+
 def write_unv(mesh: Mesh, stream: io.TextIOBase):
     """Write a mesh as UNV datasets 2411/2412 (nodes and quad/hex cells)."""
     lex_to_ucd = [0, 1, 3, 2] if mesh.dim == 2 else [0, 1, 3, 2, 4, 5, 7, 6]

@@ -268,3 +268,64 @@ def test_oracle_window_adjoint_central_differences(which):
             ana = np.sum(gVo * d)
         fd = (Jp - Jm) / (2 * h)
         assert abs(fd - ana) <= 1e-6 * abs(fd), (name, fd, ana)
+
+
+def _unv_file(tmp_path, m, name):
+    p = tmp_path / name
+    with open(p, "w") as f:
+        M.write_unv(m, f)
+    return str(p)
+
+
+@pytest.mark.parametrize("which", ["channel2d", "turek", "box3d", "cube3d"])
+def test_native_unv_reader_matches_python(tmp_path, which):
+    """pfem2gpu_read_unv (the library's C++ reader, host only) gives the same
+    vertices and cells as mesh.read_unv."""
+    m = {"channel2d": lambda: M.hyper_rectangle((0, 0), (4, 1), (16, 4)),
+         "turek": lambda: M.turek_channel(8, 4, 10),
+         "box3d": lambda: M.hyper_rectangle((0, 0, 0), (2, 1, 1), (4, 3, 2)),
+         "cube3d": lambda: M.perturbed_cube(5)}[which]()
+    p = _unv_file(tmp_path, m, which + ".unv")
+    a = M.read_unv(p)
+    b = M.read_unv_native(p)
+    assert b.dim == a.dim == m.dim
+    assert np.array_equal(a.vertices, b.vertices)
+    assert np.array_equal(a.cells, b.cells)
+    assert np.array_equal(b.cells, m.cells)
+
+
+def test_native_unv_reader_flips_left_handed_cells(tmp_path):
+    """Cells written with their first two directions swapped (negative
+    Jacobian) come back right-handed, as in the Python reader."""
+    m = M.hyper_rectangle((0, 0, 0), (1, 1, 1), (2, 2, 2))
+    bad = m.cells.copy()
+    bad[::2] = bad[::2][:, [0, 2, 1, 3, 4, 6, 5, 7]]
+    mb = M.Mesh(3, m.vertices, bad, bad.copy(), m.n_verts, "flipped")
+    p = _unv_file(tmp_path, mb, "flipped.unv")
+    b = M.read_unv_native(p)
+    assert np.array_equal(b.cells, M.read_unv(p).cells)
+    assert np.array_equal(b.cells, m.cells)
+
+
+def test_native_unv_reader_errors(tmp_path):
+    from pfem2dealii_b200 import _lib
+    import ctypes as C
+
+    L = _lib.load()
+    nv, nc = C.c_int64(), C.c_int64()
+    assert L.pfem2gpu_read_unv(b"/nonexistent.unv", 0, None, C.byref(nv), C.byref(nc), None, None, 0, 0) != 0
+    assert b"cannot open" in L.pfem2gpu_read_unv_error()
+    p = _unv_file(tmp_path, M.hyper_rectangle((0, 0), (1, 1), (2, 2)), "q.unv")
+    assert L.pfem2gpu_read_unv(p.encode(), 3, None, C.byref(nv), C.byref(nc), None, None, 0, 0) != 0
+    assert b"2D" in L.pfem2gpu_read_unv_error()
+
+
+def test_native_unv_reader_reference_mesh_if_present():
+    import os
+
+    p = "/root/reference/cases/TurekBenchmark/Mesh3.tgz"
+    if not os.path.exists(p):
+        pytest.skip("reference tree not mounted")
+    a = M.read_unv(p)
+    b = M.read_unv_native(p)
+    assert np.array_equal(a.vertices, b.vertices) and np.array_equal(a.cells, b.cells)
