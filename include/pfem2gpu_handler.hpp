@@ -59,6 +59,24 @@ struct Mesh {
     std::vector<int32_t> cell_vertices, cell_dofs;
 };
 
+// GridIn::read_unv (src/pfem2solver.cpp:116-119) through pfem2gpu_read_unv:
+// the mesh of a UNV file, each vertex its own DoF (vertex_dof_index = vertex
+// index, deal.II's Q1 numbering before any renumbering).
+inline Mesh read_unv(const std::string& path, int dim)
+{
+    Mesh m;
+    int32_t d = 0;
+    if (pfem2gpu_read_unv(path.c_str(), dim, &d, &m.n_verts, &m.n_cells, nullptr, nullptr, 0, 0) != PFEM2GPU_OK)
+        throw Error(PFEM2GPU_ERR_ARG, std::string("pfem2gpu: ") + pfem2gpu_read_unv_error());
+    m.vertices.resize((size_t)m.n_verts * d);
+    m.cell_vertices.resize((size_t)m.n_cells << d);
+    check(pfem2gpu_read_unv(path.c_str(), d, nullptr, &m.n_verts, &m.n_cells, m.vertices.data(),
+                            m.cell_vertices.data(), m.n_verts, m.n_cells));
+    m.cell_dofs = m.cell_vertices;
+    m.n_dofs = m.n_verts;
+    return m;
+}
+
 // The particle record of the reference (src/pfem2particle.h:63-72), without
 // the per-particle DoF copy (the cell's DoFs are a per-cell table here).
 template <int dim>

@@ -90,3 +90,37 @@ def test_cpp_mirror_matches_oracle(tmp_path, which):
     a, b = by_id(o.particles()), by_id(P)
     for k in ("id", "cell", "x", "xi", "v"):
         assert np.array_equal(a[k], b[k].reshape(a[k].shape)), k
+
+
+def test_cpp_read_unv_matches_python(tmp_path):
+    """pfem2gpu::read_unv of the C++ mirror (host only, no device needed)
+    gives mesh.read_unv's vertices and cells, each vertex its own DoF."""
+    from pfem2dealii_b200 import mesh as M
+
+    exe = str(tmp_path / "unv_driver")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "unv_driver.cpp"), "-L", LIBDIR, "-lpfem2gpu",
+           f"-Wl,-rpath,{LIBDIR}", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    for m in (M.turek_channel(8, 4, 10), M.perturbed_cube(4)):
+        src = str(tmp_path / "m.unv")
+        with open(src, "w") as f:
+            M.write_unv(m, f)
+        out = str(tmp_path / "m.bin")
+        r = subprocess.run([exe, src, out], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        raw = open(out, "rb").read()
+        dim, nv, nc, nd = np.frombuffer(raw[:32], np.int64)
+        o = 32
+        verts = np.frombuffer(raw[o:o + nv * dim * 8], np.float64).reshape(nv, dim)
+        o += nv * dim * 8
+        cells = np.frombuffer(raw[o:o + nc * (1 << dim) * 4], np.int32).reshape(nc, 1 << dim)
+        o += nc * (1 << dim) * 4
+        dofs = np.frombuffer(raw[o:], np.int32).reshape(nc, 1 << dim)
+        ref = M.read_unv(src)
+        assert dim == ref.dim and nd == nv
+        assert np.array_equal(verts, ref.vertices) and np.array_equal(cells, ref.cells)
+        assert np.array_equal(dofs, cells)
+    r = subprocess.run([exe, str(tmp_path / "missing.unv"), str(tmp_path / "x.bin")], capture_output=True, text=True)
+    assert r.returncode == 3 and "cannot open" in r.stderr
