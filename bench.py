@@ -121,13 +121,22 @@ WORKLOADS = {
             "64 ppc (32,768,000 particles), max 2/part, 3 sub-steps, dt 1e-3, u = (sin x cos y cos z, "
             "-cos x sin y cos z, 0)",
 }
-ADJOINT_K = {"duct": 20, "cube": 10}
+WORKLOADS["turek"] = ("2D channel 2.2x0.41 with a cylinder of radius 0.05 at (0.2, 0.2), synthetic Turek-type "
+                      "unstructured mesh of 64,512 Q1 quads, 16 ppc (1,032,192 particles), max 2/part, 3 sub-steps, "
+                      "dt 5e-4, parabolic inflow Umax 1.5, zero on the walls and the cylinder")
+ADJOINT_K = {"duct": 20, "cube": 10, "turek": 20}
 
 
 def build_case(name="duct"):
     from pfem2dealii_b200 import mesh as M
     from pfem2dealii_b200.handler import ParticleParams
 
+    if name == "turek":
+        m = M.turek_channel(96, 48, 480)
+        V = M.field_at_dofs(m, M.cylinder_inflow(1.5))
+        prm = ParticleParams(particles_per_cell=(4, 4), max_particles_per_cell_part=2,
+                             particle_integration_steps=3, time_step=5e-4)
+        return m, V, 0.9 * V, prm
     if name == "cube":
         m = M.perturbed_cube(80, amplitude=0.1, seed=0)
         V = M.field_at_dofs(m, M.taylor_green_3d())
@@ -146,7 +155,7 @@ def timed_device_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, tor
     """Seed, warm up, then time `steps` device-resident steps with CUDA events
     on the handler's stream.  alternate: step k runs with (V_k, V_{k-1}) where
     V_k alternates between V and Vold; otherwise (V, Vold) every step."""
-    g = handler_cls(3, prm, precision)
+    g = handler_cls(m.dim, prm, precision)
     g.initialize_maps(m)
     dev = torch.device("cuda:0")
     dV = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
@@ -197,7 +206,7 @@ def timed_output(handler_cls, m, V, Vold, prm, torch, steps=5, reps=5):
     """output_particle_solution's data for the workload after a few steps:
     packing on the device plus one pinned device-to-host copy (best of reps,
     CUDA events on the handler's stream)."""
-    g = handler_cls(3, prm, "fp32")
+    g = handler_cls(m.dim, prm, "fp32")
     g.initialize_maps(m)
     dev = torch.device("cuda:0")
     dV = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
@@ -209,8 +218,8 @@ def timed_output(handler_cls, m, V, Vold, prm, torch, steps=5, reps=5):
         g.step_device(a, b, out)
     g.synchronize()
     n = g.stats()["n_particles"]
-    dout = torch.empty(6 * n, dtype=torch.float32, device=dev)
-    hout = torch.empty(6 * n, dtype=torch.float32).pin_memory()
+    dout = torch.empty(2 * m.dim * n, dtype=torch.float32, device=dev)
+    hout = torch.empty(2 * m.dim * n, dtype=torch.float32).pin_memory()
     stream = torch.cuda.ExternalStream(g.stream_handle())
     best = None
     for _ in range(reps):
@@ -227,7 +236,7 @@ def timed_output(handler_cls, m, V, Vold, prm, torch, steps=5, reps=5):
     del hout, dout
     torch.cuda.synchronize()
     g.close()
-    return {"particles": n, "ms": best, "bytes": 24 * n}
+    return {"particles": n, "ms": best, "bytes": 8 * m.dim * n}
 
 
 def timed_mesh_setup(handler_cls, m, prm, torch, reps=3):
@@ -250,7 +259,7 @@ def timed_mesh_setup(handler_cls, m, prm, torch, reps=3):
 def timed_host_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, torch):
     """The same steps through the host C ABI with pinned vectors: H2D of V
     and Vold, D2H of the projected velocity, every step."""
-    g = handler_cls(3, prm, precision)
+    g = handler_cls(m.dim, prm, precision)
     g.initialize_maps(m)
     hV = torch.from_numpy(np.ascontiguousarray(V)).pin_memory()
     hVo = torch.from_numpy(np.ascontiguousarray(Vold)).pin_memory()
@@ -296,7 +305,7 @@ def timed_window(handler_cls, m, V, Vold, prm, precision, K, C, torch, pre_steps
     reps).  Also the directional derivative along the inflow amplitude
     (V -> a V at the DoFs where V != 0) against central differences of the
     FP64 form's window (h = 1e-6)."""
-    g = handler_cls(3, prm, precision)
+    g = handler_cls(m.dim, prm, precision)
     g.initialize_maps(m)
     dev = torch.device("cuda:0")
     dV = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
@@ -341,7 +350,7 @@ def timed_window(handler_cls, m, V, Vold, prm, precision, K, C, torch, pre_steps
 
 def fd_inflow(handler_cls, m, V, Vold, prm, K, C, probe, T, torch, pre_steps=5, h=1e-6):
     """Central difference of J along V -> (1 + t) V with the FP64 form."""
-    g = handler_cls(3, prm, "fp64")
+    g = handler_cls(m.dim, prm, "fp64")
     g.initialize_maps(m)
     dev = torch.device("cuda:0")
     dV = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
@@ -407,6 +416,20 @@ def cpu_baseline(m, V, Vold, prm, budget_s=20.0, max_steps=None, warmup=0, workl
             "steps": done, "seconds": t}
 
 
+def config2_report(handler_cls, torch, steps=200, warmup=3):
+    """The 2D obstacle workload (the reference's Turek-type case): both forms
+    over the same velocity sequence, and their projected-velocity error."""
+    m, V, Vold, prm = build_case("turek")
+    r32 = timed_device_run(handler_cls, m, V, Vold, prm, "fp32", steps, warmup, torch)
+    r64 = timed_device_run(handler_cls, m, V, Vold, prm, "fp64", steps, warmup, torch)
+    v32 = r32["particle_steps"] / (r32["ms"] / 1000.0)
+    v64 = r64["particle_steps"] / (r64["ms"] / 1000.0)
+    return {"workload": WORKLOADS["turek"], "steps": steps, "particles": r32["n_particles"],
+            "fp32": {"value": v32, "ms_per_step": r32["ms"] / steps},
+            "fp64": {"value": v64, "ms_per_step": r64["ms"] / steps}, "fp32_over_fp64": v32 / v64,
+            "fp32_vs_fp64_rel_l2": rel_l2(r64["V"], r32["V"]), "tolerance": 1e-4, "unit": UNIT}
+
+
 def rel_l2(a, b):
     m = np.isfinite(a) & np.isfinite(b)
     return float(np.linalg.norm((a - b)[m]) / np.linalg.norm(a[m]))
@@ -447,7 +470,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="duct",
-                    help="duct: the headline configuration; cube: the 32.8 M-particle perturbed-cube stress case")
+                    help="duct: the headline configuration; cube: the 32.8 M-particle perturbed-cube stress case; "
+                         "turek: the 2D obstacle case (1.03 M particles)")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="time the differentiated window and its adjoint only (prints one JSON object)")
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
@@ -534,6 +558,7 @@ def main():
     # output_particle_solution's data: packing on the device + one copy
     outp = timed_output(ParticleHandler, m, V, Vold, prm, torch)
     mesh_setup = timed_mesh_setup(ParticleHandler, m, prm, torch)
+    cfg2 = config2_report(ParticleHandler, torch) if args.workload == "duct" else None
     # the differentiated window (K = 20, checkpoints every 5) and its adjoint
     adj = adjoint_report(ParticleHandler, m, V, Vold, prm, torch, K=ADJOINT_K[args.workload])
     e2e_value = re2e["particle_steps"] / (re2e["ms"] / 1000.0)
@@ -584,6 +609,7 @@ def main():
         "output_pack": {"particles": outp["particles"], "ms": outp["ms"], "bytes": outp["bytes"],
                         "gbs": outp["bytes"] / (outp["ms"] / 1000.0) / 1e9},
         "mesh_setup": mesh_setup,
+        "obstacle_2d": cfg2,
         "gpu_launches": r32["launches"],
         "clocks": clk.summary(),
         "stats": {k: r32["stats"][k] for k in ("n_particles", "lost", "removed", "seeded", "searched",

@@ -102,6 +102,60 @@ __device__ __noinline__ SearchOut search64(const MeshDev m, uint32_t c, Vec<DIM>
         out.flags |= SRCH_OVERFLOW;
         n = MAX_CAND;
     }
+    if constexpr (LIN) {
+        // Up to REG_CAND candidates stay in registers: the next one tried is
+        // the untried maximum of the dot products, the first of equal ones
+        // (the order of the stable descending sort below), selected only
+        // when the ones before it have failed.
+        if (n <= REG_CAND) {
+            double dk[REG_CAND];
+            uint32_t ck[REG_CAND];
+#pragma unroll
+            for (int k = 0; k < REG_CAND; ++k) {
+                dk[k] = 0.0;
+                ck[k] = c;
+                if (k < n) {
+                    const double* cd = m.v2c_dirs + (size_t)(b + k) * DIM;
+                    double s = __ldg(cd) * vtp[0];
+#pragma unroll
+                    for (int d = 1; d < DIM; ++d) s = s + __ldg(cd + d) * vtp[d];
+                    dk[k] = s;
+                    ck[k] = (uint32_t)__ldg(m.v2c_cells + b + k);
+                }
+            }
+            uint32_t tried = 0;
+            for (int t = 0; t < n; ++t) {
+                int bi = -1;
+                double bv = 0.0;
+                uint32_t cand = c;
+#pragma unroll
+                for (int k = 0; k < REG_CAND; ++k) {
+                    const bool open = k < n && !((tried >> k) & 1u);
+                    if (open && (bi < 0 || dk[k] > bv)) {
+                        bi = k;
+                        bv = dk[k];
+                        cand = ck[k];
+                    }
+                }
+                tried |= 1u << bi;
+                if (cand == c) continue;
+                double xin[DIM];
+                if (inverse_affine64<DIM>(m.aff + (size_t)cand * AFF, xp.v, xin)) {
+                    out.map_failures++;
+                    continue;
+                }
+                if (inside_unit<DIM>(xin)) {
+                    out.cell = cand;
+                    out.flags |= SRCH_FOUND;
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) out.xi[d] = xin[d];
+                    if (near_face64<DIM>(xin)) out.flags |= SRCH_NEAR;
+                    return out;
+                }
+            }
+            return out;
+        }
+    }
     double dots[MAX_CAND];
     uint8_t perm[MAX_CAND];
     for (int k = 0; k < n; ++k) {

@@ -332,7 +332,10 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
     CK(dalloc(&h->next, cap));
     CK(dalloc(&h->xq, cap));
     CK(dalloc(&h->gscr, cap));
-    if (!h->nxq) CK(dalloc(&h->nxq, 1));
+    if (!h->nxq) {
+        CK(dalloc(&h->nxq, 1));
+        CK(cudaMemsetAsync(h->nxq, 0, sizeof(uint32_t), h->stream));
+    }
     if (h->prec == PFEM2GPU_FP32) CK(dalloc(&h->xtmp, cap * h->dim));
     h->cap = (uint32_t)cap;
     h->gen++;
@@ -353,17 +356,18 @@ int stage_v(pfem2gpu_handle* h, const double* V, const double* Vold, bool device
             CK(cudaMemcpyAsync(h->Vstage2, Vold, bytes, cudaMemcpyHostToDevice, h->stream));
             vo = h->Vstage2;
         }
-    } else if (V != h->Vstage) {
-        CK(cudaMemcpyAsync(h->Vstage, V, bytes, cudaMemcpyDeviceToDevice, h->stream));
     }
+    // device vectors: the staging kernel also writes the kept copy of V
+    double* vcopy = device && V != h->Vstage ? h->Vstage : nullptr;
     if (h->prec == PFEM2GPU_FP64) {
         run(h, "stage_velocity", [&] {
-            return launch_cell_v(h->dim, h->prec, v, vo, h->cd, h->nC, h->nD, h->Vc, Vold ? h->dVc : nullptr, h->stream);
+            return launch_cell_v(h->dim, h->prec, v, vo, h->cd, h->nC, h->nD, h->Vc, Vold ? h->dVc : nullptr, vcopy,
+                                 h->stream);
         });
     } else {
         run(h, "stage_velocity", [&] {
             return launch_cell_rec32(h->dim, v, vo, h->cd, h->aff, h->jinv32, h->nC, h->nD, h->vrec32,
-                                     Vold ? h->dvrec32 : nullptr, h->stream);
+                                     Vold ? h->dvrec32 : nullptr, vcopy, h->stream);
         });
     }
     h->vaos_valid = true;
@@ -404,8 +408,9 @@ void swap_state(pfem2gpu_handle* h)
 
 // The write pass (count correction, new layout, projection partials) and
 // the counters of the step.
-int enqueue_write(pfem2gpu_handle* h, StepArgs& a, int count_step)
+int enqueue_write(pfem2gpu_handle* h, StepArgs& a, int count_step, int reset_nan = 0)
 {
+    a.reset_nan = reset_nan;
     run(h, "slots_scan", [&] { return launch_slots_scan(a, h->tiles64, h->stream); });
     a.count_step = count_step;  // the write pass's last block finalises the step
     run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->stream); });
@@ -419,14 +424,15 @@ int write_and_swap(pfem2gpu_handle* h, StepArgs& a, int count_step)
     return check_async(h);
 }
 
-int enqueue_move(pfem2gpu_handle* h, int do_correct)
+// The crossing queue's counter is zero here: set at allocation, and reset by
+// the write pass that ends every move.
+int enqueue_move(pfem2gpu_handle* h, int do_correct, int reset_nan = 0)
 {
     StepArgs a = args(h);
     a.do_correct = do_correct;
-    CK(cudaMemsetAsync(h->nxq, 0, sizeof(uint32_t), h->stream));
     run(h, "advect", [&] { return launch_advect(h->dim, h->prec, a, h->stream); });
     run(h, "cross", [&] { return launch_cross(h->dim, h->prec, a, h->stream); });
-    return enqueue_write(h, a, 1);
+    return enqueue_write(h, a, 1, reset_nan);
 }
 
 // Run `enqueue` through a cached CUDA graph: eager on the first use of a
@@ -666,7 +672,7 @@ int window_forward_impl(pfem2gpu_handle* h, int K, int C, const double* V, const
     WinArgs w = winargs(h);
     run(h, "window_cells", [&] {
         return launch_cell_v(h->dim, 0, W.V, Vold ? W.Vold : nullptr, h->cd, h->nC, h->nD, W.Vcell, W.dVcell,
-                             h->stream) +
+                             nullptr, h->stream) +
                launch_win_wcell(h->dim, w, W.Vcell, W.Wcell, h->stream);
     });
     run(h, "window_compact", [&] { return launch_win_compact(h->S0.cell, ns, (uint32_t)h->nC, W.tsum, W.slot, h->stream); });
@@ -1134,14 +1140,14 @@ int pfem2gpu_step_device(pfem2gpu_handle* h, const double* dV, const double* dVo
     int rc = apply_pending_correction(h);
     if (rc) return rc;
     rc = graphed(h, h->step_graph[h->parity], dV, dVold, dV_out, [&]() -> int {
+        // kernels only: the staging kernel keeps the copy of V, the write
+        // pass resets the counters, the gather writes the caller's vector
         int r = stage_v(h, dV, dVold, true);
         if (r) return r;
-        if ((r = enqueue_move(h, 1))) return r;
+        if ((r = enqueue_move(h, 1, 1))) return r;
         StepArgs a = args(h);
-        CK(cudaMemsetAsync(&h->stats->nan_dofs, 0, sizeof(unsigned long long), h->stream));
+        a.Vout = dV_out;
         run(h, "gather", [&] { return launch_gather(h->dim, h->prec, a, h->prm.empty_dof_policy == 1, h->stream); });
-        CK(cudaMemcpyAsync(dV_out, h->Vout, (size_t)h->dim * h->nD * sizeof(double), cudaMemcpyDeviceToDevice,
-                           h->stream));
         return PFEM2GPU_OK;
     });
     if (rc) return rc;

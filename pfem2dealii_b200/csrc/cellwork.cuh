@@ -23,6 +23,7 @@
 #include "common.cuh"
 #include "geom32.cuh"
 #include "geom64.cuh"
+#include "staging.cuh"
 
 namespace pfem2 {
 
@@ -241,6 +242,73 @@ __device__ __forceinline__ void partials_of_range(const StepArgs& a, const PartS
     store_partial<DIM, Real>(a, c, acc, lane);
 }
 
+// FP32 cells of at most 32 particles, one per lane (lanes without a particle
+// add zeros): the first level of the pairwise tree, rows u + (u + 16), is
+// taken through one shuffle instead of shared memory.  Lane u < 16 keeps the
+// entries of the vertices whose highest reference-coordinate bit is clear,
+// lane u + 16 those with it set, and receives them from its partner, so each
+// entry crosses the warp once and 16 rows of PW entries are staged; the
+// tree's other levels and the compensated add follow.  Shape values and
+// products are those of partial_row (N = (x0 factor * x1 factor) * x2 factor).
+template <int DIM>
+__device__ __forceinline__ void partial_pairs32(float (*tr)[TRW], bool active, const float* xi, const float* v,
+                                                int lane, PartialAcc<float>& acc)
+{
+    constexpr int NV = 1 << DIM, H = NV / 2, PW = Dims<DIM>::PW;
+    const bool hi = lane >= 16;
+    float x[DIM], w[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        x[d] = active ? xi[d] : 0.0f;
+        w[d] = active ? v[d] : 0.0f;
+    }
+    float lowN[H];  // products of the factors below the highest direction
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+        float n = (k & 1) ? x[0] : 1.0f - x[0];
+        if (DIM > 2) n *= ((k >> 1) & 1) ? x[1] : 1.0f - x[1];
+        lowN[k] = n;
+    }
+    // a lane without a particle adds nothing (its shape values are zero too)
+    const float top = x[DIM - 1], bot = 1.0f - x[DIM - 1];
+    const float fk = active ? (hi ? top : bot) : 0.0f, fs = active ? (hi ? bot : top) : 0.0f;
+    float keep[4 * H];
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+        const float nk = lowN[k] * fk, ns = lowN[k] * fs;
+        float e[4], f[4];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            e[d] = nk * w[d];
+            f[d] = ns * w[d];
+        }
+        e[DIM] = nk;
+        f[DIM] = ns;
+        if (DIM == 2) e[3] = f[3] = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) keep[4 * k + j] = e[j] + __shfl_xor_sync(0xffffffffu, f[j], 16);
+    }
+    const int row = lane & 15, col0 = hi ? 4 * H : 0;
+#pragma unroll
+    for (int k = 0; k < H; ++k)
+        *reinterpret_cast<float4*>(&tr[row][col0 + 4 * k]) =
+            make_float4(keep[4 * k], keep[4 * k + 1], keep[4 * k + 2], keep[4 * k + 3]);
+    __syncwarp();
+    if (lane < PW) {
+        float t[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) t[r] = tr[r][lane];
+#pragma unroll
+        for (int wd = 8; wd >= 1; wd >>= 1)
+#pragma unroll
+            for (int r = 0; r < wd; ++r) t[r] = t[r] + t[r + wd];
+        const float y = t[0] - acc.c;
+        const float sm = acc.s + y;
+        acc.c = (sm - acc.s) - y;
+        acc.s = sm;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Write pass.  A warp takes CHC consecutive cells; their old ranges are
 // contiguous, so the stayers' data (key, id, xi, v[, x]) of the whole chunk
@@ -266,6 +334,7 @@ struct __align__(16) WrWarp {
     Real x[HX ? DIM : 1][HX ? UCAP : 4];
     int cnt[NPE_MAX];
     Real tr[32][TRW];
+    uint64_t bar;  // completion of the chunk's bulk copies
 };
 
 template <int DIM, typename Real>
@@ -493,6 +562,7 @@ __device__ __forceinline__ void write_cell_simple(const StepArgs& a, WrWarp<DIM,
     const unsigned m = __ballot_sync(0xffffffffu, st);
     const uint32_t ns = __popc(m);
     PData<DIM, Real> pd;
+    bool loaded = st;
     uint32_t pos = 0, key = 0xffffffffu;
     if (st) {
         if (staged) load_stage<DIM, Real>(w, s0 - S + u, s0 + u, pd);
@@ -502,32 +572,53 @@ __device__ __forceinline__ void write_cell_simple(const StepArgs& a, WrWarp<DIM,
         const uint32_t ia = arrival(a, c, u - L, h);
         if (ia < a.capacity) {
             load_global<DIM, Real>(a, ia, pd);
+            loaded = true;
             key = key_of(pd.id, a.pp.seed);
         } else {
             err |= ERR_ARRIVAL;
         }
     }
-    if (na > 1) {  // arrivals by key
-        uint32_t r = 0;
+    uint32_t rank = 0;  // of an arrival among the cell's arrivals, by key
+    if (na > 1) {
         for (uint32_t t = 0; t < na; ++t) {
             const uint32_t kl = __shfl_sync(0xffffffffu, key, (int)(L + t));
-            r += kl < key ? 1u : 0u;
+            rank += kl < key ? 1u : 0u;
         }
-        if (ar) pos = ns + r;
-    } else if (ar) {
-        pos = ns;
     }
+    if (ar) pos = ns + rank;
     if (st || ar) {
         const uint32_t dst = off + pos;
         if (dst < a.capacity) store_particle<DIM, Real>(a, dst, c, pd);
         else err |= ERR_CAPACITY;
-        partial_row<DIM, Real>(w.tr, (int)pos, pd.xi, pd.v);
+        if constexpr (!std::is_same<Real, float>::value) partial_row<DIM, Real>(w.tr, (int)pos, pd.xi, pd.v);
     }
     const uint32_t fin = ns + na;
     if (fin != ub) err |= ERR_COUNT_UB;
-    __syncwarp();
     PartialAcc<Real> acc;
-    partial_sum_rows<DIM, Real>(w.tr, (int)fin, lane, acc);
+    if constexpr (std::is_same<Real, float>::value) {
+        // rows are lanes: stayers in slot order; the arrival of rank r moves
+        // to lane L + r, so the sum's order does not depend on the order in
+        // which the arrivals were recorded
+        int from = lane;
+        bool act = st;
+        for (uint32_t t = 0; t < na; ++t) {
+            const unsigned b = __ballot_sync(0xffffffffu, ar && loaded && rank == t);
+            if (u == L + t) {
+                from = b ? __ffs(b) - 1 : lane;
+                act = b != 0;
+            }
+        }
+        float xs[DIM], vs[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            xs[d] = __shfl_sync(0xffffffffu, pd.xi[d], from);
+            vs[d] = __shfl_sync(0xffffffffu, pd.v[d], from);
+        }
+        partial_pairs32<DIM>(w.tr, act, xs, vs, lane, acc);
+    } else {
+        __syncwarp();
+        partial_sum_rows<DIM, Real>(w.tr, (int)fin, lane, acc);
+    }
     store_partial<DIM, Real>(a, c, acc, lane);
     reset_cell(a, c, lane);
 }
@@ -712,6 +803,13 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
     const int apply = a.apply_counts, maxpp = a.pp.maxpp;
     unsigned long long removed = 0;
     uint32_t err = 0;
+    if (lane == 0) {
+        mbar_init(&w.bar, 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+    uint32_t phase = 0;
+    bool stage_ok = true;  // cleared for good if a copy ever fails to land in time
     // chunks of cells are handed out one at a time, so that warps that drew
     // cheap chunks take more (cells differ in particles and arrivals)
     while (true) {
@@ -732,19 +830,37 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
             h_off = a.coff[c0 + lane];
             for (int q = 0; q < a.pp.occw; ++q) h_occ += __popcll(a.cocc[(size_t)(c0 + lane) * a.pp.occw + q]);
         }
+        // the chunk's old slot range [S, E), staged by bulk copies of whole
+        // 16-byte pieces [SA, EA) (the capacity is a multiple of 4 slots)
         const uint32_t S = __shfl_sync(0xffffffffu, csl, 0), E = __shfl_sync(0xffffffffu, csl, ncell);
-        const bool staged = E - S <= (uint32_t)UCAP;
-        if (staged) {
-            for (uint32_t j = lane; j < E - S; j += 32) {
-                const uint32_t i = S + j;
-                w.key[j] = a.key[i];
-                w.id[j] = a.S0.id[i];
+        const uint32_t SA = S & ~3u, EA = (E + 3u) & ~3u;
+        bool staged = stage_ok && EA - SA <= (uint32_t)UCAP;
+        if (staged && EA > SA) {
+            const uint32_t nb = EA - SA;
+            if (lane == 0) {
+                fence_proxy_async();  // the previous chunk's reads of the stage come first
+                constexpr uint32_t per = 8u + 2u * DIM * sizeof(Real) + (WrCfg<DIM, Real>::HX ? DIM * 8u : 0u);
+                mbar_expect_tx(&w.bar, nb * per);
+                bulk_g2s(w.key, a.key + SA, nb * 4u, &w.bar);
+                bulk_g2s(w.id, a.S0.id + SA, nb * 4u, &w.bar);
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) {
-                    w.xi[d][j] = ldr<Real>(a.T.xi[d], i);
-                    w.v[d][j] = ldr<Real>(a.T.v[d], i);
-                    if constexpr (WrCfg<DIM, Real>::HX) w.x[d][j] = ldr<double>(a.T.x[d], i);
+                    bulk_g2s(w.xi[d], reinterpret_cast<const Real*>(a.T.xi[d]) + SA, nb * (uint32_t)sizeof(Real),
+                             &w.bar);
+                    bulk_g2s(w.v[d], reinterpret_cast<const Real*>(a.T.v[d]) + SA, nb * (uint32_t)sizeof(Real),
+                             &w.bar);
+                    if constexpr (WrCfg<DIM, Real>::HX)
+                        bulk_g2s(w.x[d], reinterpret_cast<const double*>(a.T.x[d]) + SA, nb * 8u, &w.bar);
                 }
+            }
+            const uint32_t par = phase;
+            phase ^= 1u;
+            if (!__all_sync(0xffffffffu, mbar_wait(&w.bar, par))) {
+                // give the copy one more bounded wait, then stop staging
+                err |= ERR_TIMEOUT;
+                mbar_wait(&w.bar, par);
+                staged = false;
+                stage_ok = false;
             }
         }
         __syncwarp();
@@ -763,7 +879,7 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
             // count - occupied parts <= max: no part above max + 1 particles
             const bool no_removal = !apply || (maxpp >= 0 && ub - nseed_expect <= occ + (uint32_t)maxpp);
             if (nseed_expect == 0 && no_removal && L + na <= 32u) {
-                write_cell_simple<DIM, Real>(a, w, c, s0, L, na, h, off, ub, S, staged, lane, err);
+                write_cell_simple<DIM, Real>(a, w, c, s0, L, na, h, off, ub, SA, staged, lane, err);
                 __syncwarp();
                 continue;
             }
@@ -779,10 +895,10 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
                 continue;
             }
             if (L + na > 32)
-                write_cell_fast<DIM, Real, 2>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0, S, staged, lane,
+                write_cell_fast<DIM, Real, 2>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0, SA, staged, lane,
                                               removed, err);
             else
-                write_cell_fast<DIM, Real, 1>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0, S, staged, lane,
+                write_cell_fast<DIM, Real, 1>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0, SA, staged, lane,
                                               removed, err);
             __syncwarp();
         }

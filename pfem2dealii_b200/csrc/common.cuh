@@ -17,6 +17,7 @@ namespace pfem2 {
 constexpr uint32_t LOST = 0xFFFFFFFFu;  // no cell / end of a list
 constexpr uint32_t HOLE = 0xFFFFFFFEu;  // cell of an empty slot (where a removed particle would have gone)
 constexpr int MAX_CAND = 64;   // cells around one vertex tried by the relocation search
+constexpr int REG_CAND = 12;   // FP32 form on affine meshes: candidates kept in registers
 constexpr int NPE_MAX = 256;   // extended cell parts (q0+1)(q1+1)(q2+1)
 constexpr int OCCW_MAX = 4;    // 64-bit part-occupancy words per cell
 constexpr int ARRCAP = 4;      // arrival slots per cell before the overflow list
@@ -107,6 +108,7 @@ struct StepArgs {
     int do_correct;
     int apply_counts;   // write kernel: 1 = count correction, 0 = keep all (re-sort only)
     int count_step;     // write kernel: add the step's particles to particle_steps
+    int reset_nan;      // write kernel: zero nan_dofs for the projection that follows
     uint32_t* key;      // cell after the move, or LOST
     uint32_t* head;     // nC: overflow list of particles that moved into the cell (LOST = none)
     uint32_t* next;     // next particle on the same overflow list
@@ -200,6 +202,8 @@ __device__ __forceinline__ void finalize_step(const StepArgs& a)
         slots = a.capacity;
     }
     st->adv_next = 0;  // the advect pass of this step has finished
+    *a.nxq = 0;        // and the crossing queue has been drained
+    if (a.reset_nan) st->nan_dofs = 0;
     st->n_slots = slots;
     st->n_particles = slots - (st->step_holes < slots ? st->step_holes : slots);
     st->step_holes = 0;

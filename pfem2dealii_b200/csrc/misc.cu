@@ -165,11 +165,22 @@ __global__ void k_set_state(DevStats* st, long long n, long long next_id, long l
 // Per-cell copy of the nodal velocity (and V - Vold, deltaV of
 // src/pfem2particlehandler.cpp:120-124) for every cell vertex, padded to
 // VS components (FP64 form).
+// The staged copy of V (component-major, ncopy values) written by the kernel
+// that reads V first, so a step needs no separate copy.
+__device__ __forceinline__ void copy_v(const double* __restrict__ V, double* __restrict__ Vcopy, size_t ncopy)
+{
+    if (!Vcopy) return;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < ncopy; i += (size_t)gridDim.x * blockDim.x)
+        Vcopy[i] = V[i];
+}
+
 template <int DIM, typename Real>
 __global__ void k_cell_v(const double* __restrict__ V, const double* __restrict__ Vold, const int32_t* __restrict__ cd,
-                         int nC, int nD, Real* __restrict__ Vc, Real* __restrict__ dVc)
+                         int nC, int nD, Real* __restrict__ Vc, Real* __restrict__ dVc, double* __restrict__ Vcopy,
+                         size_t ncopy)
 {
     pdl_entry();
+    copy_v(V, Vcopy, ncopy);
     constexpr int NV = 1 << DIM, VS = Dims<DIM>::VS;
     const int total = nC * NV;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
@@ -232,9 +243,11 @@ template <int DIM>
 __global__ void __launch_bounds__(REC_TILE) k_cell_rec32(const double* __restrict__ V, const double* __restrict__ Vold,
                                                          const int32_t* __restrict__ cd, const double* __restrict__ aff,
                                                          const float* __restrict__ jinv32, int nC, int nD,
-                                                         float* __restrict__ vrec, float* __restrict__ dvrec)
+                                                         float* __restrict__ vrec, float* __restrict__ dvrec,
+                                                         double* __restrict__ Vcopy, size_t ncopy)
 {
     pdl_entry();
+    copy_v(V, Vcopy, ncopy);
     constexpr int NV = 1 << DIM, F = Dims<DIM>::REC4 * 4, F4 = Dims<DIM>::REC4, AFF = Dims<DIM>::AFF;
     __shared__ __align__(16) float rec_s[2][REC_TILE * F];
     for (int c0 = blockIdx.x * REC_TILE; c0 < nC; c0 += gridDim.x * REC_TILE) {
@@ -335,25 +348,27 @@ int launch_set_state(DevStats* st, long long n, long long next_id, long long add
 }
 
 int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const int32_t* cd, int nC, int nD, void* Vc,
-                  void* dVc, cudaStream_t s)
+                  void* dVc, double* Vcopy, cudaStream_t s)
 {
+    const size_t nc = Vcopy ? (size_t)dim * nD : 0;
     const int total = nC * (1 << dim);
     const int g = (total + 255) / 256 < 8192 ? (total + 255) / 256 : 8192;
     const int grid = g > 0 ? g : 1;
-    if (dim == 2 && prec == 0) return launch_pdl(k_cell_v<2, double>, grid, 256, 0, s, V, Vold, cd, nC, nD, (double*)Vc, (double*)dVc);
-    if (dim == 3 && prec == 0) return launch_pdl(k_cell_v<3, double>, grid, 256, 0, s, V, Vold, cd, nC, nD, (double*)Vc, (double*)dVc);
-    if (dim == 2) return launch_pdl(k_cell_v<2, float>, grid, 256, 0, s, V, Vold, cd, nC, nD, (float*)Vc, (float*)dVc);
-    return launch_pdl(k_cell_v<3, float>, grid, 256, 0, s, V, Vold, cd, nC, nD, (float*)Vc, (float*)dVc);
+    if (dim == 2 && prec == 0) return launch_pdl(k_cell_v<2, double>, grid, 256, 0, s, V, Vold, cd, nC, nD, (double*)Vc, (double*)dVc, Vcopy, nc);
+    if (dim == 3 && prec == 0) return launch_pdl(k_cell_v<3, double>, grid, 256, 0, s, V, Vold, cd, nC, nD, (double*)Vc, (double*)dVc, Vcopy, nc);
+    if (dim == 2) return launch_pdl(k_cell_v<2, float>, grid, 256, 0, s, V, Vold, cd, nC, nD, (float*)Vc, (float*)dVc, Vcopy, nc);
+    return launch_pdl(k_cell_v<3, float>, grid, 256, 0, s, V, Vold, cd, nC, nD, (float*)Vc, (float*)dVc, Vcopy, nc);
     return 1;
 }
 
 int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
-                      const float* jinv32, int nC, int nD, float* vrec, float* dvrec, cudaStream_t s)
+                      const float* jinv32, int nC, int nD, float* vrec, float* dvrec, double* Vcopy, cudaStream_t s)
 {
+    const size_t nc = Vcopy ? (size_t)dim * nD : 0;
     const int g = (nC + REC_TILE - 1) / REC_TILE;
     const int grid = g < 1 ? 1 : g;
-    if (dim == 2) return launch_pdl(k_cell_rec32<2>, grid, REC_TILE, 0, s, V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
-    return launch_pdl(k_cell_rec32<3>, grid, REC_TILE, 0, s, V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec);
+    if (dim == 2) return launch_pdl(k_cell_rec32<2>, grid, REC_TILE, 0, s, V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec, Vcopy, nc);
+    return launch_pdl(k_cell_rec32<3>, grid, REC_TILE, 0, s, V, Vold, cd, aff, jinv32, nC, nD, vrec, dvrec, Vcopy, nc);
     return 1;
 }
 
