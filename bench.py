@@ -416,6 +416,22 @@ def cpu_baseline(m, V, Vold, prm, budget_s=20.0, max_steps=None, warmup=0, workl
             "steps": done, "seconds": t}
 
 
+def form_difference(V64, V32, particles64, particles32):
+    """FP32 vs FP64 projected velocity: the relative L2 error, and how much of
+    it sits on DoFs where the two forms' particle sets parted (a count
+    correction or part decision taken differently moves such a DoF by the
+    order of the velocity itself): DoFs off by more than 1e-3 of max |V|,
+    and the relative L2 error over the other DoFs."""
+    m = np.isfinite(V64) & np.isfinite(V32)
+    d = np.where(m, np.abs(V64 - V32), 0.0)
+    scale = float(np.max(np.abs(V64[m]))) if m.any() else 1.0
+    off = (d > 1e-3 * scale).any(axis=0)
+    keep = m & ~off[None, :]
+    rest = float(np.linalg.norm((V64 - V32)[keep]) / np.linalg.norm(V64[keep])) if keep.any() else 0.0
+    return {"rel_l2": rel_l2(V64, V32), "dofs_off_by_1e-3_of_max": int(off.sum()), "dofs": int(V64.shape[1]),
+            "rel_l2_other_dofs": rest, "particles_fp64": int(particles64), "particles_fp32": int(particles32)}
+
+
 def config2_report(handler_cls, torch, steps=200, warmup=3):
     """The 2D obstacle workload (the reference's Turek-type case): both forms
     over the same velocity sequence, and their projected-velocity error."""
@@ -427,7 +443,8 @@ def config2_report(handler_cls, torch, steps=200, warmup=3):
     return {"workload": WORKLOADS["turek"], "steps": steps, "particles": r32["n_particles"],
             "fp32": {"value": v32, "ms_per_step": r32["ms"] / steps},
             "fp64": {"value": v64, "ms_per_step": r64["ms"] / steps}, "fp32_over_fp64": v32 / v64,
-            "fp32_vs_fp64_rel_l2": rel_l2(r64["V"], r32["V"]), "tolerance": 1e-4, "unit": UNIT}
+            "fp32_vs_fp64_rel_l2": rel_l2(r64["V"], r32["V"]), "tolerance": 1e-4, "unit": UNIT,
+            "difference": form_difference(r64["V"], r32["V"], r64["n_particles"], r32["n_particles"])}
 
 
 def rel_l2(a, b):
@@ -476,6 +493,8 @@ def main():
                     help="time the differentiated window and its adjoint only (prints one JSON object)")
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
                     help="run one device-resident pass of one form and print its timing (profiling runs)")
+    ap.add_argument("--e2e", action="store_true",
+                    help="with --only: also the same steps through the host ABI (pinned H2D/D2H each step)")
     ap.add_argument("--kernels", action="store_true",
                     help="with --only: also the per-kernel times of a profiled run (CUDA events)")
     args = ap.parse_args()
@@ -507,6 +526,9 @@ def main():
         r = timed_device_run(ParticleHandler, m, V, Vold, prm, args.only, args.steps, args.warmup, torch)
         out = {"form": args.only, "ms_per_step": r["ms"] / args.steps,
                "value": r["particle_steps"] / (r["ms"] / 1000.0), "unit": UNIT}
+        if args.e2e:
+            re = timed_host_run(ParticleHandler, m, V, Vold, prm, args.only, args.steps, args.warmup, torch)
+            out["e2e"] = {"value": re["particle_steps"] / (re["ms"] / 1000.0), "ms_per_step": re["ms"] / args.steps}
         if args.kernels:
             rp = timed_device_run(ParticleHandler, m, V, Vold, prm, args.only, args.steps, args.warmup, torch,
                                   profile=True)
@@ -589,7 +611,9 @@ def main():
                  "fp32_over_fp64": value / v64},
         "fp32_vs_fp64_rel_l2": {"projected_velocity": err, "tolerance": 1e-4,
                                 "steps": args.warmup + args.steps,
-                                "fixed_vold_0.9v": err_fixed},
+                                "fixed_vold_0.9v": err_fixed,
+                                "fixed_vold_0.9v_difference": form_difference(f64["V"], f32["V"], f64["n_particles"],
+                                                                              f32["n_particles"])},
         "step_effective_gbs": STEP_BYTES["fp32"] * value / 1e9,
         "roofline": {"bound": "hbm", "kernel": "k_write<3,float>", "achieved": achieved_w, "peak": peak,
                      "unit": "GB/s", "frac": achieved_w / peak, "traffic": TRAFFIC_WRITE,
