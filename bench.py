@@ -256,6 +256,60 @@ def timed_mesh_setup(handler_cls, m, prm, torch, reps=3):
     return {"cells": m.n_cells, "vertices": m.n_verts, "ms": best}
 
 
+def timed_fem(handler_cls, m, V, torch, reps=5):
+    """The solver step's three Q1 systems (volume terms) on device vectors:
+    CUDA-event time of one assembly each (best of reps), the FP64 oracle's
+    time for the pressure system on one host thread, and the bytes the
+    device passes must move (local values written and read back, the
+    matrices and right-hand sides written, the cell geometry and DoF vectors
+    read)."""
+    from oracle import oracle as O
+
+    g = handler_cls(m.dim, ParticleParamsDefault(m.dim), "fp64")
+    g.initialize_maps(m)
+    rp, cols = g.fem_pattern()
+    nnz, nd, nc, nv = len(cols), m.n_dofs, m.n_cells, 1 << m.dim
+    dev = torch.device("cuda:0")
+    dU = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
+    dU2 = 0.9 * dU
+    dP = torch.zeros(nd, dtype=torch.float64, device=dev)
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+    out = {"nnz": nnz, "cells": nc}
+    for name, system in (("prediction", 0), ("pressure", 1), ("correction", 2)):
+        nm = m.dim if system == 0 else 1
+        ns = 1 if system == 1 else m.dim
+        dA = torch.empty(nm * nnz, dtype=torch.float64, device=dev)
+        dr = torch.empty(ns * nd, dtype=torch.float64, device=dev)
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g._ck(g.L.pfem2gpu_fem_assemble_device(g.h, system, 1.0, 0.01, 1e-3, dU.data_ptr(), dU2.data_ptr(),
+                                                    dP.data_ptr(), dA.data_ptr(), dr.data_ptr()))
+            e1.record(stream)
+            e1.synchronize()
+            t = e0.elapsed_time(e1)
+            best = t if best is None else min(best, t)
+        moved = (2 * nc * nv * nm * nv + nc * nv * ns * 2 + nm * nnz + ns * nd + nc * nv * m.dim
+                 + 2 * m.dim * nd) * 8 + (nc * nv + nnz + 2 * nd) * 4
+        out[name] = {"ms": best, "bytes": moved, "gbs": moved / (best / 1000.0) / 1e9}
+        del dA, dr
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    O.fem_assemble(m, O.FEM_PRESSURE, 1.0, 0.01, 1e-3, U=V, pattern=(rp, cols))
+    out["oracle_pressure_ms_1_thread"] = (time.perf_counter() - t0) * 1e3
+    del dU, dU2, dP
+    torch.cuda.synchronize()
+    g.close()
+    return out
+
+
+def ParticleParamsDefault(dim):
+    from pfem2dealii_b200.handler import ParticleParams
+
+    return ParticleParams(particles_per_cell=(2,) * dim)
+
+
 def timed_host_run(handler_cls, m, V, Vold, prm, precision, steps, warmup, torch):
     """The same steps through the host C ABI with pinned vectors: H2D of V
     and Vold, D2H of the projected velocity, every step."""
@@ -581,6 +635,7 @@ def main():
     outp = timed_output(ParticleHandler, m, V, Vold, prm, torch)
     mesh_setup = timed_mesh_setup(ParticleHandler, m, prm, torch)
     cfg2 = config2_report(ParticleHandler, torch) if args.workload == "duct" else None
+    fem = timed_fem(ParticleHandler, m, V, torch) if args.workload == "duct" else None
     # the differentiated window (K = 20, checkpoints every 5) and its adjoint
     adj = adjoint_report(ParticleHandler, m, V, Vold, prm, torch, K=ADJOINT_K[args.workload])
     e2e_value = re2e["particle_steps"] / (re2e["ms"] / 1000.0)
@@ -634,6 +689,7 @@ def main():
                         "gbs": outp["bytes"] / (outp["ms"] / 1000.0) / 1e9},
         "mesh_setup": mesh_setup,
         "obstacle_2d": cfg2,
+        "fem_assembly": fem,
         "gpu_launches": r32["launches"],
         "clocks": clk.summary(),
         "stats": {k: r32["stats"][k] for k in ("n_particles", "lost", "removed", "seeded", "searched",

@@ -107,6 +107,34 @@ int pfem2gpu_read_unv(const char* path, int dim, int32_t* dim_out, int64_t* n_ve
                       double* vertices, int32_t* cell_vertices, int64_t verts_capacity, int64_t cells_capacity);
 const char* pfem2gpu_read_unv_error(void);
 
+/* ---------------------------------------------------------------------------
+ * The solver step's Q1 systems (src/pfem2fem.cpp): the volume integrals of
+ * assemble_velocity_prediction (:247-310, SCHEMEB off),
+ * assemble_pressure_equation (:392-425) and assemble_velocity_correction
+ * (:460-489), computed per cell on the device in FP64 (QGauss(2), the Q1
+ * map's Jacobian at each point) and summed into CSR matrices and right-hand
+ * sides in ascending cell order, as a cell loop adds local systems.  The
+ * boundary-face terms and the constraints (AffineConstraints::
+ * distribute_local_to_global) stay with the caller.
+ * ------------------------------------------------------------------------- */
+#define PFEM2GPU_FEM_PREDICTION 0 /* U = solution V, U2 = old solution V: dim matrices, dim right-hand sides */
+#define PFEM2GPU_FEM_PRESSURE 1   /* U = predicted V: one matrix, one right-hand side */
+#define PFEM2GPU_FEM_CORRECTION 2 /* U = predicted V, P = pressure: one matrix, dim right-hand sides */
+
+/* CSR pattern of the matrices (DoFTools::make_sparsity_pattern for Q1: per
+ * DoF the DoFs sharing a cell with it, ascending), built on the device once
+ * per mesh; row_ptr n_dofs+1, cols >= capacity entries (NULL: *nnz only). */
+int pfem2gpu_fem_pattern(pfem2gpu_handle* h, int32_t* row_ptr, int32_t* cols, int64_t capacity, int64_t* nnz);
+/* One system on device vectors (component-major U, U2 of dim x n_dofs; P of
+ * n_dofs): A receives matrices x nnz values on the pattern, rhs right-hand
+ * sides x n_dofs.  Enqueued on the handle's stream, not synchronized.  rho,
+ * mu and dt as the reference's fluid density, viscosity and time step. */
+int pfem2gpu_fem_assemble_device(pfem2gpu_handle* h, int system, double rho, double mu, double dt, const double* dU,
+                                 const double* dU2, const double* dP, double* dA, double* drhs);
+/* The same on host arrays (copies in and out, synchronized). */
+int pfem2gpu_fem_assemble(pfem2gpu_handle* h, int system, double rho, double mu, double dt, const double* U,
+                          const double* U2, const double* P, double* A, double* rhs);
+
 /* seed_particles (src/pfem2particlehandler.cpp:43-109). */
 int pfem2gpu_seed(pfem2gpu_handle* h, const double* V);
 /* correct_particle_velocity (:112-139): v += sum N_i (V - Vold)_i; applied

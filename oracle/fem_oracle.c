@@ -1,0 +1,216 @@
+/* FP64 CPU restatement of the Q1 FEM systems' volume terms -- TEST
+ * INFRASTRUCTURE ONLY: the checker of the library's device assembly, never
+ * called by the product.
+ *
+ * Follows src/pfem2fem.cpp: assemble_velocity_prediction (:247-310, the
+ * volume integral; SCHEMEB off), assemble_pressure_equation (:392-425) and
+ * assemble_velocity_correction (:460-489), as a sequential cell loop that
+ * adds each cell's local matrix and right-hand side into the global ones
+ * (distribute_local_to_global without constraints).  Boundary-face terms and
+ * the constraints stay with the caller.  FE values are the Q1 /
+ * QGauss(2) / MappingQ1 quantities of deal.II (not vendored here, so parity
+ * with it is unpinned): quadrature points (1 -+ 1/sqrt 3)/2 per direction, x
+ * fastest, weight 1/2 per direction; J[d][e] = sum_i X_i[d] dN_i/dxi_e; the
+ * physical gradient J^-T grad N; JxW = det J * weight.
+ *
+ * Pattern: for every DoF, the DoFs sharing a cell with it, ascending
+ * (DoFTools::make_sparsity_pattern for Q1).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "fem_oracle.h"
+
+static const double QP[2] = {0.21132486540518711775, 0.78867513459481288225};
+
+static void fe_point(int dim, const double* X, int q, double* N, double* g, double* jxw)
+{
+    const int nv = 1 << dim;
+    double xi[3], gr[8][3], J[3][3], Ji[3][3], det;
+    for (int d = 0; d < dim; ++d) xi[d] = QP[(q >> d) & 1];
+    for (int i = 0; i < nv; ++i) {
+        double n = 1.0;
+        for (int d = 0; d < dim; ++d) n = n * (((i >> d) & 1) ? xi[d] : 1.0 - xi[d]);
+        N[i] = n;
+        for (int e = 0; e < dim; ++e) {
+            double t = ((i >> e) & 1) ? 1.0 : -1.0;
+            for (int d = 0; d < dim; ++d)
+                if (d != e) t = t * (((i >> d) & 1) ? xi[d] : 1.0 - xi[d]);
+            gr[i][e] = t;
+        }
+    }
+    for (int d = 0; d < dim; ++d)
+        for (int e = 0; e < dim; ++e) {
+            double s = 0.0;
+            for (int i = 0; i < nv; ++i) s = s + X[i * dim + d] * gr[i][e];
+            J[d][e] = s;
+        }
+    if (dim == 2) {
+        det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        Ji[0][0] = J[1][1] / det;
+        Ji[0][1] = -J[0][1] / det;
+        Ji[1][0] = -J[1][0] / det;
+        Ji[1][1] = J[0][0] / det;
+    } else {
+        const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+        const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+        const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+        det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+        Ji[0][0] = c00 / det;
+        Ji[1][0] = c01 / det;
+        Ji[2][0] = c02 / det;
+        Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+        Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+        Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+        Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+        Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+        Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+    }
+    for (int i = 0; i < nv; ++i)
+        for (int d = 0; d < dim; ++d) {
+            double s = 0.0;
+            for (int e = 0; e < dim; ++e) s = s + Ji[e][d] * gr[i][e];
+            g[i * 3 + d] = s;
+        }
+    *jxw = det * (dim == 2 ? 0.25 : 0.125);
+}
+
+static int cmp_int(const void* a, const void* b)
+{
+    const int x = *(const int*)a, y = *(const int*)b;
+    return (x > y) - (x < y);
+}
+
+int64_t orc_fem_pattern(int dim, int64_t n_cells, int64_t n_dofs, const int32_t* cell_dofs, int32_t* row_ptr,
+                        int32_t* cols)
+{
+    const int nv = 1 << dim;
+    /* candidate (row, col) pairs grouped by row, then sorted and made unique */
+    int64_t* cnt = calloc((size_t)n_dofs + 1, sizeof(int64_t));
+    for (int64_t c = 0; c < n_cells; ++c)
+        for (int i = 0; i < nv; ++i) cnt[cell_dofs[c * nv + i] + 1] += nv;
+    for (int64_t d = 0; d < n_dofs; ++d) cnt[d + 1] += cnt[d];
+    int* cand = malloc((size_t)cnt[n_dofs] * sizeof(int) + 1);
+    int64_t* fill = malloc((size_t)n_dofs * sizeof(int64_t) + 1);
+    for (int64_t d = 0; d < n_dofs; ++d) fill[d] = cnt[d];
+    for (int64_t c = 0; c < n_cells; ++c)
+        for (int i = 0; i < nv; ++i)
+            for (int j = 0; j < nv; ++j) cand[fill[cell_dofs[c * nv + i]]++] = cell_dofs[c * nv + j];
+    int64_t nnz = 0;
+    for (int64_t d = 0; d < n_dofs; ++d) {
+        int* p = cand + cnt[d];
+        const int64_t m = cnt[d + 1] - cnt[d];
+        qsort(p, (size_t)m, sizeof(int), cmp_int);
+        if (row_ptr) row_ptr[d] = (int32_t)nnz;
+        for (int64_t k = 0; k < m; ++k)
+            if (k == 0 || p[k] != p[k - 1]) {
+                if (cols) cols[nnz] = p[k];
+                ++nnz;
+            }
+    }
+    if (row_ptr) row_ptr[n_dofs] = (int32_t)nnz;
+    free(cand);
+    free(fill);
+    free(cnt);
+    return nnz;
+}
+
+static int64_t find_col(const int32_t* row_ptr, const int32_t* cols, int row, int col)
+{
+    int64_t lo = row_ptr[row], hi = row_ptr[row + 1] - 1;
+    while (lo <= hi) {
+        const int64_t mid = (lo + hi) / 2;
+        if (cols[mid] == col) return mid;
+        if (cols[mid] < col) lo = mid + 1;
+        else hi = mid - 1;
+    }
+    return -1;
+}
+
+int orc_fem_assemble(int dim, int system, int64_t n_cells, int64_t n_dofs, const double* cellX,
+                     const int32_t* cell_dofs, const int32_t* row_ptr, const int32_t* cols, double rho, double mu,
+                     double dt, const double* U, const double* U2, const double* P, double* A, double* rhs)
+{
+    const int nv = 1 << dim, nq = 1 << dim;
+    const int nm = system == ORC_FEM_PREDICTION ? dim : 1;
+    const int ns = system == ORC_FEM_PRESSURE ? 1 : dim;
+    const int64_t nnz = row_ptr[n_dofs];
+    memset(A, 0, (size_t)nm * (size_t)nnz * sizeof(double));
+    memset(rhs, 0, (size_t)ns * (size_t)n_dofs * sizeof(double));
+    double M[3][8][8], r[3][8], N[8], g[8 * 3], w;
+    for (int64_t c = 0; c < n_cells; ++c) {
+        const double* X = cellX + c * nv * dim;
+        const int32_t* dof = cell_dofs + c * nv;
+        memset(M, 0, sizeof M);
+        memset(r, 0, sizeof r);
+        for (int q = 0; q < nq; ++q) {
+            fe_point(dim, X, q, N, g, &w);
+            for (int i = 0; i < nv; ++i) {
+                const double Ni = N[i];
+                const double* gi = g + i * 3;
+                if (system == ORC_FEM_PREDICTION) {
+                    for (int j = 0; j < nv; ++j) {
+                        const double* gj = g + j * 3;
+                        double aux = rho * Ni * N[j] * w;
+                        for (int k = 0; k < dim; ++k) {
+                            M[k][i][j] = M[k][i][j] + aux;
+                            r[k][i] = r[k][i] + aux * U2[k * n_dofs + dof[j]];
+                        }
+                        aux = mu * dt * w;
+                        if (dim == 2) {
+                            M[0][i][j] = M[0][i][j] + aux * (gi[1] * gj[1] + 4.0 / 3.0 * gi[0] * gj[0]);
+                            M[1][i][j] = M[1][i][j] + aux * (gi[0] * gj[0] + 4.0 / 3.0 * gi[1] * gj[1]);
+                            r[0][i] = r[0][i] - aux * (gi[1] * gj[0] - 2.0 / 3.0 * gi[0] * gj[1]) * U[1 * n_dofs + dof[j]];
+                            r[1][i] = r[1][i] - aux * (gi[0] * gj[1] - 2.0 / 3.0 * gi[1] * gj[0]) * U[0 * n_dofs + dof[j]];
+                        } else {
+                            const double u0 = U[dof[j]], u1 = U[n_dofs + dof[j]], u2 = U[2 * n_dofs + dof[j]];
+                            M[0][i][j] = M[0][i][j] + aux * (4.0 / 3.0 * gi[0] * gj[0] + gi[1] * gj[1] + gi[2] * gj[2]);
+                            M[1][i][j] = M[1][i][j] + aux * (gj[0] * gi[0] + 4.0 / 3.0 * gi[1] * gj[1] + gi[2] * gj[2]);
+                            M[2][i][j] = M[2][i][j] + aux * (gj[0] * gi[0] + gj[1] * gi[1] + 4.0 / 3.0 * gi[2] * gj[2]);
+                            r[0][i] = r[0][i] - aux * ((gi[1] * gj[0] - 2.0 / 3.0 * gi[0] * gj[1]) * u1 +
+                                                       (gi[2] * gj[0] - 2.0 / 3.0 * gi[0] * gj[2]) * u2);
+                            r[1][i] = r[1][i] - aux * ((gi[0] * gj[1] - 2.0 / 3.0 * gi[1] * gj[0]) * u0 +
+                                                       (gi[2] * gj[1] - 2.0 / 3.0 * gi[1] * gj[2]) * u2);
+                            r[2][i] = r[2][i] - aux * ((gi[0] * gj[2] - 2.0 / 3.0 * gi[2] * gj[0]) * u0 +
+                                                       (gi[1] * gj[2] - 2.0 / 3.0 * gi[2] * gj[1]) * u1);
+                        }
+                    }
+                } else if (system == ORC_FEM_PRESSURE) {
+                    const double coeff = rho / dt;
+                    for (int j = 0; j < nv; ++j) {
+                        const double* gj = g + j * 3;
+                        double dot = gi[0] * gj[0];
+                        for (int d = 1; d < dim; ++d) dot = dot + gi[d] * gj[d];
+                        M[0][i][j] = M[0][i][j] + dot * w;
+                        double aux = 0.0;
+                        for (int k = 0; k < dim; ++k) aux = aux + U[k * n_dofs + dof[j]] * gi[k];
+                        r[0][i] = r[0][i] + coeff * aux * N[j] * w;
+                    }
+                } else {
+                    const double aux2 = dt * Ni * w;
+                    for (int j = 0; j < nv; ++j) {
+                        const double* gj = g + j * 3;
+                        const double aux = rho * Ni * N[j] * w;
+                        const double p = P[dof[j]];
+                        for (int k = 0; k < dim; ++k) {
+                            if (k == 0) M[0][i][j] = M[0][i][j] + aux;
+                            r[k][i] = r[k][i] + aux * U[k * n_dofs + dof[j]];
+                            r[k][i] = r[k][i] - aux2 * gj[k] * p;
+                        }
+                    }
+                }
+            }
+        }
+        for (int i = 0; i < nv; ++i) {
+            for (int j = 0; j < nv; ++j) {
+                const int64_t pos = find_col(row_ptr, cols, dof[i], dof[j]);
+                if (pos < 0) return 1;
+                for (int m = 0; m < nm; ++m) A[m * nnz + pos] = A[m * nnz + pos] + M[m][i][j];
+            }
+            for (int k = 0; k < ns; ++k) rhs[k * n_dofs + dof[i]] = rhs[k * n_dofs + dof[i]] + r[k][i];
+        }
+    }
+    return 0;
+}

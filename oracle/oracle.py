@@ -89,6 +89,10 @@ def lib():
         L.orc_window_adjoint.argtypes = [P, C.c_int, dp, P, P, C.c_int, dp, P, P, P, P]
         L.orc_key.restype = C.c_uint32
         L.orc_key.argtypes = [C.c_uint32, C.c_uint32]
+        L.orc_fem_pattern.restype = C.c_int64
+        L.orc_fem_pattern.argtypes = [C.c_int, C.c_int64, C.c_int64, ip, P, P]
+        L.orc_fem_assemble.argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int64, dp, ip, ip, ip, C.c_double,
+                                       C.c_double, C.c_double, P, P, P, dp, dp]
         _lib = L
     return _lib
 
@@ -248,3 +252,41 @@ def inverse_map(X, p):
 
 def key(i, seed):
     return lib().orc_key(i, seed)
+
+
+# --------------------------------------------------------------------------
+# FEM systems' volume terms (src/pfem2fem.cpp:247-489), restated in
+# fem_oracle.c: the checker of the library's device assembly.
+# --------------------------------------------------------------------------
+FEM_PREDICTION, FEM_PRESSURE, FEM_CORRECTION = 0, 1, 2
+
+
+def fem_pattern(mesh):
+    """CSR pattern (row_ptr, cols) of the Q1 DoF adjacency, columns ascending."""
+    L = lib()
+    cd = _c(mesh.cell_dofs, np.int32)
+    nnz = L.orc_fem_pattern(mesh.dim, mesh.n_cells, mesh.n_dofs, cd, None, None)
+    row_ptr = np.zeros(mesh.n_dofs + 1, np.int32)
+    cols = np.zeros(max(nnz, 1), np.int32)
+    L.orc_fem_pattern(mesh.dim, mesh.n_cells, mesh.n_dofs, cd, row_ptr.ctypes.data_as(C.c_void_p),
+                      cols.ctypes.data_as(C.c_void_p))
+    return row_ptr, cols[:nnz]
+
+
+def fem_assemble(mesh, system, rho, mu, dt, U=None, U2=None, P=None, pattern=None):
+    """(A, rhs): A (matrices, nnz) on the pattern, rhs (right-hand sides, n_dofs)."""
+    L = lib()
+    row_ptr, cols = pattern if pattern is not None else fem_pattern(mesh)
+    nnz = int(row_ptr[-1])
+    nm = mesh.dim if system == FEM_PREDICTION else 1
+    ns = 1 if system == FEM_PRESSURE else mesh.dim
+    A = np.zeros((nm, nnz))
+    rhs = np.zeros((ns, mesh.n_dofs))
+    cellX = _c(mesh.vertices[mesh.cells], np.float64)
+    keep = [None if a is None else _c(a, np.float64) for a in (U, U2, P)]
+    rc = L.orc_fem_assemble(mesh.dim, system, mesh.n_cells, mesh.n_dofs, cellX, _c(mesh.cell_dofs, np.int32),
+                            _c(row_ptr, np.int32), _c(cols, np.int32), rho, mu, dt,
+                            *[None if a is None else a.ctypes.data_as(C.c_void_p) for a in keep], A, rhs)
+    if rc:
+        raise RuntimeError("pattern misses an entry")
+    return A, rhs

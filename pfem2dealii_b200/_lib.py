@@ -122,6 +122,10 @@ def load():
         "pfem2gpu_window_size": [P, C.POINTER(i64)],
         "pfem2gpu_window_particles": [P, dptr, dptr, dptr, i64, C.POINTER(i64)],
         "pfem2gpu_get_vertex_maps": [P, dptr, dptr, dptr, i64, C.POINTER(i64)],
+        "pfem2gpu_fem_pattern": [P, dptr, dptr, i64, C.POINTER(i64)],
+        "pfem2gpu_fem_assemble_device": [P, C.c_int, C.c_double, C.c_double, C.c_double, dptr, dptr, dptr, dptr,
+                                         dptr],
+        "pfem2gpu_fem_assemble": [P, C.c_int, C.c_double, C.c_double, C.c_double, dptr, dptr, dptr, dptr, dptr],
         "pfem2gpu_read_unv": [C.c_char_p, C.c_int, C.POINTER(C.c_int32), C.POINTER(i64), C.POINTER(i64), dptr, dptr,
                               i64, i64],
         "pfem2gpu_read_unv_error": [],

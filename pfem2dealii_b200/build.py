@@ -1,6 +1,6 @@
 """Builds libpfem2gpu.so in-tree (pfem2dealii_b200/_build/) for sm_100a.
 
-kernels_f64.cu, window_f64.cu and noalloc.cu are compiled with --fmad=false: the FP64 form
+kernels_f64.cu, window_f64.cu, noalloc.cu and fem.cu are compiled with --fmad=false: the FP64 form
 rounds every product and sum separately, as the CPU build of the reference
 arithmetic does.
 The other sources use the default contraction.  Run ``python -m
@@ -30,6 +30,7 @@ SOURCES = {
     "window_f64.cu": ["--fmad=false"],
     "window_f32.cu": [],
     "mesh_io.cu": [],
+    "fem.cu": ["--fmad=false"],
 }
 
 

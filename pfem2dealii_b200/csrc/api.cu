@@ -81,6 +81,14 @@ struct pfem2gpu_handle {
     uint32_t *out_slot = nullptr, *out_tsum = nullptr;
     float *out_dev = nullptr, *out_host = nullptr;
     uint32_t out_cap = 0, out_tcap = 0, out_dcap = 0;
+    // FEM systems: the CSR pattern (built once per mesh), per-(cell, row)
+    // local values, and device copies of host inputs/outputs
+    struct Fem {
+        int32_t *row_ptr = nullptr, *cols = nullptr;
+        long long nnz = -1;
+        double *local = nullptr, *local_rhs = nullptr, *io = nullptr;
+        size_t local_n = 0, rhs_n = 0, io_n = 0;
+    } fem;
     // differentiated window: checkpoints, final state, projection and adjoint
     // buffers (per-particle arrays sized ncap x segcap, the rest per mesh)
     struct Win {
@@ -256,6 +264,12 @@ void free_win_particles(pfem2gpu_handle::Win& W)
     W.segcap = 0;
     W.tcap = -1;
     W.ready = false;
+}
+
+void free_fem(pfem2gpu_handle::Fem& F)
+{
+    for (void* p : {(void*)F.row_ptr, (void*)F.cols, (void*)F.local, (void*)F.local_rhs, (void*)F.io}) dfree(p);
+    F = pfem2gpu_handle::Fem{};
 }
 
 void free_win_mesh(pfem2gpu_handle::Win& W)
@@ -863,6 +877,7 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
     free_state(h->T);
     free_win_particles(h->win);
     free_win_mesh(h->win);
+    free_fem(h->fem);
     dfree(h->out_slot);
     dfree(h->out_tsum);
     dfree(h->out_dev);
@@ -982,6 +997,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
         *p = nullptr;
     }
     free_win_mesh(h->win);
+    free_fem(h->fem);
     h->has_mesh = false;
     h->nC = (int)n_cells;
     h->nV = (int)n_verts;
@@ -1443,6 +1459,177 @@ int pfem2gpu_adjoint(pfem2gpu_handle* h, int32_t steps, int32_t checkpoint_every
     int rc = window_forward_impl(h, steps, checkpoint_every, V, Vold, v0, U, true);
     if (rc) return rc;
     return window_backward_impl(h, gU, g_v0, g_V, g_Vold, true);
+}
+
+// The CSR pattern of the FEM matrices, built on the device once per mesh:
+// per DoF row the DoFs sharing a cell with it (from the DoF -> cell map),
+// ascending.
+static int fem_pattern(pfem2gpu_handle* h)
+{
+    auto& F = h->fem;
+    if (F.nnz >= 0) return PFEM2GPU_OK;
+    const size_t nd = h->nD, ntiles = (nd + WIN_TILE - 1) / WIN_TILE + 1;
+    uint32_t *cnt = nullptr, *tsum = nullptr;
+    unsigned* err = nullptr;
+    CK(dalloc(&F.row_ptr, nd + 1));
+    CK(dalloc(&cnt, nd));
+    CK(dalloc(&tsum, ntiles));
+    CK(dalloc(&err, 1));
+    CK(cudaMemsetAsync(err, 0, sizeof(unsigned), h->stream));
+    FemArgs f{};
+    f.nC = h->nC;
+    f.nD = h->nD;
+    f.cd = h->cd;
+    f.d2c_off = h->d2c_off;
+    f.d2c_ent = h->d2c_ent;
+    f.row_ptr = F.row_ptr;
+    run(h, "fem_pattern", [&] {
+        int n = launch_fem_pattern(h->dim, f, false, cnt, err, h->stream);
+        return n + launch_win_scan(cnt, (uint32_t)nd, tsum, (uint32_t*)F.row_ptr, h->stream);
+    });
+    int32_t nnz = 0;
+    unsigned e = 0;
+    CK(cudaMemcpyAsync(&nnz, F.row_ptr + nd, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&e, err, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (e) {
+        dfree(cnt);
+        dfree(tsum);
+        dfree(err);
+        free_fem(F);
+        return fail(h, PFEM2GPU_ERR_ARG, "a DoF couples to more than 64 DoFs");
+    }
+    CK(dalloc(&F.cols, std::max<size_t>(nnz, 1)));
+    f.cols = F.cols;
+    run(h, "fem_pattern", [&] { return launch_fem_pattern(h->dim, f, true, cnt, err, h->stream); });
+    CK(cudaStreamSynchronize(h->stream));
+    dfree(cnt);
+    dfree(tsum);
+    dfree(err);
+    F.nnz = nnz;
+    return check_async(h);
+}
+
+int pfem2gpu_fem_pattern(pfem2gpu_handle* h, int32_t* row_ptr, int32_t* cols, int64_t capacity, int64_t* nnz)
+{
+    if (!h || !nnz) return PFEM2GPU_ERR_ARG;
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "no mesh");
+    int rc = fem_pattern(h);
+    if (rc) return rc;
+    *nnz = h->fem.nnz;
+    if (row_ptr) CK(cudaMemcpyAsync(row_ptr, h->fem.row_ptr, ((size_t)h->nD + 1) * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (cols) {
+        if (capacity < h->fem.nnz) return fail(h, PFEM2GPU_ERR_ARG, "output arrays too small");
+        CK(cudaMemcpyAsync(cols, h->fem.cols, (size_t)h->fem.nnz * 4, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return PFEM2GPU_OK;
+}
+
+static int fem_sizes(int dim, int system, int* nm, int* ns)
+{
+    if (system < PFEM2GPU_FEM_PREDICTION || system > PFEM2GPU_FEM_CORRECTION) return 1;
+    *nm = system == PFEM2GPU_FEM_PREDICTION ? dim : 1;
+    *ns = system == PFEM2GPU_FEM_PRESSURE ? 1 : dim;
+    return 0;
+}
+
+static int fem_run(pfem2gpu_handle* h, int system, double rho, double mu, double dt, const double* dU,
+                   const double* dU2, const double* dP, double* dA, double* drhs)
+{
+    int nm, ns;
+    fem_sizes(h->dim, system, &nm, &ns);
+    auto& F = h->fem;
+    const int NV = 1 << h->dim;
+    const size_t nloc = (size_t)h->nC * NV * nm * NV, nr = (size_t)h->nC * NV * ns;
+    if (nloc > F.local_n) {
+        dfree(F.local);
+        F.local = nullptr;
+        F.local_n = 0;
+        CK(dalloc(&F.local, nloc));
+        F.local_n = nloc;
+    }
+    if (nr > F.rhs_n) {
+        dfree(F.local_rhs);
+        F.local_rhs = nullptr;
+        F.rhs_n = 0;
+        CK(dalloc(&F.local_rhs, nr));
+        F.rhs_n = nr;
+    }
+    FemArgs f{};
+    f.nC = h->nC;
+    f.nD = h->nD;
+    f.nnz = F.nnz;
+    f.cellX = h->cellX;
+    f.cd = h->cd;
+    f.d2c_off = h->d2c_off;
+    f.d2c_ent = h->d2c_ent;
+    f.row_ptr = F.row_ptr;
+    f.cols = F.cols;
+    f.rho = rho;
+    f.mu = mu;
+    f.dt = dt;
+    f.U = dU;
+    f.U2 = dU2;
+    f.P = dP;
+    f.local = F.local;
+    f.local_rhs = F.local_rhs;
+    f.A = dA;
+    f.rhs = drhs;
+    run(h, "fem_assemble", [&] { return launch_fem_assemble(h->dim, system, f, h->stream); });
+    return check_async(h);
+}
+
+static int fem_check(pfem2gpu_handle* h, int system, const double* U, const double* U2, const double* P,
+                     const double* A, const double* rhs)
+{
+    int nm, ns;
+    if (!h) return PFEM2GPU_ERR_ARG;
+    if (fem_sizes(h->dim, system, &nm, &ns)) return fail(h, PFEM2GPU_ERR_ARG, "unknown FEM system");
+    if (!A || !rhs || !U) return fail(h, PFEM2GPU_ERR_ARG, "missing vector");
+    if (system == PFEM2GPU_FEM_PREDICTION && !U2) return fail(h, PFEM2GPU_ERR_ARG, "missing old velocity");
+    if (system == PFEM2GPU_FEM_CORRECTION && !P) return fail(h, PFEM2GPU_ERR_ARG, "missing pressure");
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "no mesh");
+    return fem_pattern(h);
+}
+
+int pfem2gpu_fem_assemble_device(pfem2gpu_handle* h, int system, double rho, double mu, double dt, const double* dU,
+                                 const double* dU2, const double* dP, double* dA, double* drhs)
+{
+    const int rc = fem_check(h, system, dU, dU2, dP, dA, drhs);
+    if (rc) return rc;
+    return fem_run(h, system, rho, mu, dt, dU, dU2, dP, dA, drhs);
+}
+
+int pfem2gpu_fem_assemble(pfem2gpu_handle* h, int system, double rho, double mu, double dt, const double* U,
+                          const double* U2, const double* P, double* A, double* rhs)
+{
+    int rc = fem_check(h, system, U, U2, P, A, rhs);
+    if (rc) return rc;
+    int nm, ns;
+    fem_sizes(h->dim, system, &nm, &ns);
+    auto& F = h->fem;
+    const size_t vd = (size_t)h->dim * h->nD, need = 2 * vd + h->nD + (size_t)nm * F.nnz + (size_t)ns * h->nD;
+    if (need > F.io_n) {
+        dfree(F.io);
+        F.io = nullptr;
+        F.io_n = 0;
+        CK(dalloc(&F.io, need));
+        F.io_n = need;
+    }
+    double* dU = F.io;
+    double* dU2 = dU + vd;
+    double* dP = dU2 + vd;
+    double* dA = dP + h->nD;
+    double* drhs = dA + (size_t)nm * F.nnz;
+    CK(cudaMemcpyAsync(dU, U, vd * 8, cudaMemcpyHostToDevice, h->stream));
+    if (U2) CK(cudaMemcpyAsync(dU2, U2, vd * 8, cudaMemcpyHostToDevice, h->stream));
+    if (P) CK(cudaMemcpyAsync(dP, P, (size_t)h->nD * 8, cudaMemcpyHostToDevice, h->stream));
+    if ((rc = fem_run(h, system, rho, mu, dt, dU, U2 ? dU2 : nullptr, P ? dP : nullptr, dA, drhs))) return rc;
+    CK(cudaMemcpyAsync(A, dA, (size_t)nm * F.nnz * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(rhs, drhs, (size_t)ns * h->nD * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PFEM2GPU_OK;
 }
 
 int pfem2gpu_get_vertex_maps(pfem2gpu_handle* h, int32_t* offsets, int32_t* cells, double* dirs, int64_t capacity,

@@ -178,6 +178,29 @@ struct WinArgs {
     unsigned int* err;
 };
 
+// Q1 FEM systems assembled on the device (fem.cu).
+constexpr int FEM_PREDICTION = 0, FEM_PRESSURE = 1, FEM_CORRECTION = 2;
+constexpr int FEM_ROWMAX = 64;  // matrix entries per row the pattern pass can hold
+
+struct FemArgs {
+    int nC, nD;
+    long long nnz;
+    const double* cellX;
+    const int32_t* cd;
+    const int32_t* d2c_off;
+    const int32_t* d2c_ent;
+    int32_t* row_ptr;
+    int32_t* cols;
+    double rho, mu, dt;
+    const double* U;
+    const double* U2;
+    const double* P;
+    double* local;      // per (cell, local row): matrices x 2^dim local entries
+    double* local_rhs;  // per (cell, local row): right-hand sides
+    double* A;          // matrices x nnz
+    double* rhs;        // right-hand sides x nD
+};
+
 template <int DIM> struct Dims {
     static constexpr int NV = 1 << DIM;
     static constexpr int VS = DIM == 3 ? 4 : 2;        // padded velocity stride

@@ -1,0 +1,309 @@
+// Q1 FEM systems of the solver step on the device (src/pfem2fem.cpp:247-509):
+// the volume integrals of the velocity prediction, the pressure equation and
+// the velocity correction, summed into CSR matrices and right-hand sides.
+// Compiled with --fmad=false: every product and sum is rounded separately.
+//
+// Element values, per cell and quadrature point (QGauss(2), x fastest,
+// weights 1/2 per direction): J[d][e] = sum_i X_i[d] dN_i/dxi_e (i
+// ascending), its inverse by cofactors, physical gradients
+// g_i[d] = sum_e Jinv[e][d] dN_i/dxi_e, JxW = det J * w.  The local matrix
+// and right-hand side terms are added in the reference's order (q outer, i,
+// then j; within one (q, i, j) the terms in the order of the source lines),
+// and a global entry is the sum of its cells' local values in ascending cell
+// order, as a sequential cell loop adds them.
+#include <cstdint>
+
+#include "common.cuh"
+#include "launch.h"
+
+namespace pfem2 {
+namespace {
+
+constexpr double QG0 = 0.21132486540518711775, QG1 = 0.78867513459481288225;  // (1 -+ 1/sqrt 3) / 2
+
+template <int DIM>
+struct Quad {
+    double N[1 << DIM];           // shape values
+    double g[1 << DIM][DIM];      // physical gradients
+    double jxw;
+};
+
+// Shape values, reference gradients, then the physical quantities at q.
+template <int DIM>
+__device__ void quad_point(const double* __restrict__ X, int q, Quad<DIM>& out)
+{
+    constexpr int NV = 1 << DIM;
+    double xi[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) xi[d] = ((q >> d) & 1) ? QG1 : QG0;
+    double gr[NV][DIM];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        double n = 1.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) n = n * (((i >> d) & 1) ? xi[d] : 1.0 - xi[d]);
+        out.N[i] = n;
+#pragma unroll
+        for (int e = 0; e < DIM; ++e) {
+            double t = ((i >> e) & 1) ? 1.0 : -1.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+                if (d != e) t = t * (((i >> d) & 1) ? xi[d] : 1.0 - xi[d]);
+            gr[i][e] = t;
+        }
+    }
+    double J[DIM][DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+        for (int e = 0; e < DIM; ++e) {
+            double s = 0.0;
+#pragma unroll
+            for (int i = 0; i < NV; ++i) s = s + X[i * DIM + d] * gr[i][e];
+            J[d][e] = s;
+        }
+    double det, Ji[DIM][DIM];
+    if constexpr (DIM == 2) {
+        det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        Ji[0][0] = J[1][1] / det;
+        Ji[0][1] = -J[0][1] / det;
+        Ji[1][0] = -J[1][0] / det;
+        Ji[1][1] = J[0][0] / det;
+    } else {
+        const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+        const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+        const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+        det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+        Ji[0][0] = c00 / det;
+        Ji[1][0] = c01 / det;
+        Ji[2][0] = c02 / det;
+        Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+        Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+        Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+        Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+        Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+        Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+    }
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            double s = 0.0;
+#pragma unroll
+            for (int e = 0; e < DIM; ++e) s = s + Ji[e][d] * gr[i][e];
+            out.g[i][d] = s;
+        }
+    out.jxw = det * (DIM == 2 ? 0.25 : 0.125);
+}
+
+// One thread per (cell, local row i): row i of the cell's local matrices
+// (NS of them, NV entries each) and its right-hand-side entries.
+template <int DIM, int SYS>
+__global__ void __launch_bounds__(128) k_fem_local(FemArgs f)
+{
+    constexpr int NV = 1 << DIM, NQ = 1 << DIM;
+    constexpr int NS = SYS == FEM_PRESSURE ? 1 : DIM;   // right-hand sides
+    constexpr int NM = SYS == FEM_PREDICTION ? DIM : 1;  // matrices
+    const long long total = (long long)f.nC * NV;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / NV), i = (int)(t % NV);
+        double X[NV * DIM];
+#pragma unroll
+        for (int k = 0; k < NV * DIM; ++k) X[k] = f.cellX[(size_t)c * NV * DIM + k];
+        int dof[NV];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) dof[j] = f.cd[(size_t)c * NV + j];
+        double M[NM][NV], r[NS];
+#pragma unroll
+        for (int m = 0; m < NM; ++m)
+#pragma unroll
+            for (int j = 0; j < NV; ++j) M[m][j] = 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) r[k] = 0.0;
+        for (int q = 0; q < NQ; ++q) {
+            Quad<DIM> Q;
+            quad_point<DIM>(X, q, Q);
+            const double w = Q.jxw;
+            const double Ni = Q.N[i];
+            const double* gi = Q.g[i];
+            if constexpr (SYS == FEM_PREDICTION) {
+                for (int j = 0; j < NV; ++j) {
+                    const double* gj = Q.g[j];
+                    double aux = f.rho * Ni * Q.N[j] * w;
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) {
+                        M[k][j] = M[k][j] + aux;
+                        r[k] = r[k] + aux * f.U2[(size_t)k * f.nD + dof[j]];
+                    }
+                    aux = f.mu * f.dt * w;
+                    double u[DIM];
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) u[k] = f.U[(size_t)k * f.nD + dof[j]];
+                    if constexpr (DIM == 2) {
+                        M[0][j] = M[0][j] + aux * (gi[1] * gj[1] + 4.0 / 3.0 * gi[0] * gj[0]);
+                        M[1][j] = M[1][j] + aux * (gi[0] * gj[0] + 4.0 / 3.0 * gi[1] * gj[1]);
+                        r[0] = r[0] - aux * (gi[1] * gj[0] - 2.0 / 3.0 * gi[0] * gj[1]) * u[1];
+                        r[1] = r[1] - aux * (gi[0] * gj[1] - 2.0 / 3.0 * gi[1] * gj[0]) * u[0];
+                    } else {
+                        M[0][j] = M[0][j] + aux * (4.0 / 3.0 * gi[0] * gj[0] + gi[1] * gj[1] + gi[2] * gj[2]);
+                        M[1][j] = M[1][j] + aux * (gj[0] * gi[0] + 4.0 / 3.0 * gi[1] * gj[1] + gi[2] * gj[2]);
+                        M[2][j] = M[2][j] + aux * (gj[0] * gi[0] + gj[1] * gi[1] + 4.0 / 3.0 * gi[2] * gj[2]);
+                        r[0] = r[0] - aux * ((gi[1] * gj[0] - 2.0 / 3.0 * gi[0] * gj[1]) * u[1] +
+                                             (gi[2] * gj[0] - 2.0 / 3.0 * gi[0] * gj[2]) * u[2]);
+                        r[1] = r[1] - aux * ((gi[0] * gj[1] - 2.0 / 3.0 * gi[1] * gj[0]) * u[0] +
+                                             (gi[2] * gj[1] - 2.0 / 3.0 * gi[1] * gj[2]) * u[2]);
+                        r[2] = r[2] - aux * ((gi[0] * gj[2] - 2.0 / 3.0 * gi[2] * gj[0]) * u[0] +
+                                             (gi[1] * gj[2] - 2.0 / 3.0 * gi[2] * gj[1]) * u[1]);
+                    }
+                }
+            } else if constexpr (SYS == FEM_PRESSURE) {
+                const double coeff = f.rho / f.dt;
+                for (int j = 0; j < NV; ++j) {
+                    const double* gj = Q.g[j];
+                    double dot = gi[0] * gj[0];
+#pragma unroll
+                    for (int d = 1; d < DIM; ++d) dot = dot + gi[d] * gj[d];
+                    M[0][j] = M[0][j] + dot * w;
+                    double aux = 0.0;
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) aux = aux + f.U[(size_t)k * f.nD + dof[j]] * gi[k];
+                    r[0] = r[0] + coeff * aux * Q.N[j] * w;
+                }
+            } else {
+                const double aux2 = f.dt * Ni * w;
+                for (int j = 0; j < NV; ++j) {
+                    const double* gj = Q.g[j];
+                    const double aux = f.rho * Ni * Q.N[j] * w;
+                    const double p = f.P[dof[j]];
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) {
+                        if (k == 0) M[0][j] = M[0][j] + aux;  // the same matrix for every component
+                        r[k] = r[k] + aux * f.U[(size_t)k * f.nD + dof[j]];
+                        r[k] = r[k] - aux2 * gj[k] * p;
+                    }
+                }
+            }
+        }
+        double* L = f.local + (size_t)t * NM * NV;
+#pragma unroll
+        for (int m = 0; m < NM; ++m)
+#pragma unroll
+            for (int j = 0; j < NV; ++j) L[m * NV + j] = M[m][j];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) f.local_rhs[(size_t)t * NS + k] = r[k];
+    }
+}
+
+// One warp per matrix row (DoF): lane l owns column entry l (in rounds of
+// 32); the row's cell entries are walked in ascending cell order and each
+// adds the local value whose column DoF matches.  The right-hand side of the
+// row is summed by lane 0 in the same order.
+template <int DIM, int SYS>
+__global__ void __launch_bounds__(256) k_fem_gather(FemArgs f)
+{
+    constexpr int NV = 1 << DIM;
+    constexpr int NS = SYS == FEM_PRESSURE ? 1 : DIM;
+    constexpr int NM = SYS == FEM_PREDICTION ? DIM : 1;
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; row < f.nD; row += nwarps) {
+        const int b = f.d2c_off[row], e = f.d2c_off[row + 1];
+        const int cb = f.row_ptr[row], ce = f.row_ptr[row + 1];
+        for (int c0 = cb; c0 < ce; c0 += 32) {
+            const int pos = c0 + lane;
+            const int col = pos < ce ? f.cols[pos] : -1;
+            double acc[NM];
+#pragma unroll
+            for (int m = 0; m < NM; ++m) acc[m] = 0.0;
+            for (int k = b; k < e; ++k) {
+                const int ent = f.d2c_ent[k];  // cell * NV + local row
+                const int c = ent / NV;
+#pragma unroll
+                for (int j = 0; j < NV; ++j)
+                    if (f.cd[(size_t)c * NV + j] == col)
+#pragma unroll
+                        for (int m = 0; m < NM; ++m) acc[m] = acc[m] + f.local[((size_t)ent * NM + m) * NV + j];
+            }
+            if (pos < ce)
+#pragma unroll
+                for (int m = 0; m < NM; ++m) f.A[(size_t)m * f.nnz + pos] = acc[m];
+        }
+        if (lane < NS) {
+            double s = 0.0;
+            for (int k = b; k < e; ++k) s = s + f.local_rhs[(size_t)f.d2c_ent[k] * NS + lane];
+            f.rhs[(size_t)lane * f.nD + row] = s;
+        }
+    }
+}
+
+// CSR pattern: the DoFs sharing a cell with each row DoF, ascending.  Pass 1
+// (fill == false) counts, pass 2 writes from row_ptr.  A row longer than
+// FEM_ROWMAX sets err.
+template <int DIM>
+__global__ void k_fem_pattern(FemArgs f, bool fill, uint32_t* __restrict__ count, unsigned* __restrict__ err)
+{
+    constexpr int NV = 1 << DIM;
+    for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < f.nD;
+         row += (long long)gridDim.x * blockDim.x) {
+        int list[FEM_ROWMAX];
+        int n = 0;
+        bool over = false;
+        for (int k = f.d2c_off[row]; k < f.d2c_off[row + 1]; ++k) {
+            const int c = f.d2c_ent[k] / NV;
+            for (int j = 0; j < NV; ++j) {
+                const int d = f.cd[(size_t)c * NV + j];
+                int p = n;  // insertion point, keeping the list ascending and unique
+                while (p > 0 && list[p - 1] > d) --p;
+                if (p > 0 && list[p - 1] == d) continue;
+                if (n == FEM_ROWMAX) {
+                    over = true;
+                    continue;
+                }
+                for (int s = n; s > p; --s) list[s] = list[s - 1];
+                list[p] = d;
+                ++n;
+            }
+        }
+        if (over) atomicOr(err, 1u);
+        if (!fill) {
+            count[row] = (uint32_t)n;
+        } else {
+            const int b = f.row_ptr[row];
+            for (int s = 0; s < n; ++s) f.cols[b + s] = list[s];
+        }
+    }
+}
+
+int fem_grid(const void* k, int threads) { return occupancy_grid(k, threads); }
+
+}  // namespace
+
+int launch_fem_pattern(int dim, const FemArgs& f, bool fill, uint32_t* count, unsigned* err, cudaStream_t s)
+{
+    if (dim == 2) k_fem_pattern<2><<<fem_grid((const void*)k_fem_pattern<2>, 128), 128, 0, s>>>(f, fill, count, err);
+    else k_fem_pattern<3><<<fem_grid((const void*)k_fem_pattern<3>, 128), 128, 0, s>>>(f, fill, count, err);
+    return 1;
+}
+
+template <int DIM, int SYS>
+static int fem_t(const FemArgs& f, cudaStream_t s)
+{
+    k_fem_local<DIM, SYS><<<fem_grid((const void*)k_fem_local<DIM, SYS>, 128), 128, 0, s>>>(f);
+    k_fem_gather<DIM, SYS><<<fem_grid((const void*)k_fem_gather<DIM, SYS>, 256), 256, 0, s>>>(f);
+    return 2;
+}
+
+int launch_fem_assemble(int dim, int sys, const FemArgs& f, cudaStream_t s)
+{
+    if (dim == 2) {
+        if (sys == FEM_PREDICTION) return fem_t<2, FEM_PREDICTION>(f, s);
+        if (sys == FEM_PRESSURE) return fem_t<2, FEM_PRESSURE>(f, s);
+        return fem_t<2, FEM_CORRECTION>(f, s);
+    }
+    if (sys == FEM_PREDICTION) return fem_t<3, FEM_PREDICTION>(f, s);
+    if (sys == FEM_PRESSURE) return fem_t<3, FEM_PRESSURE>(f, s);
+    return fem_t<3, FEM_CORRECTION>(f, s);
+}
+
+}  // namespace pfem2

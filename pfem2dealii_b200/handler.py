@@ -210,6 +210,33 @@ class ParticleHandler:
         self._ck(self.L.pfem2gpu_window_backward_device(self.h, _ptr(dgU), _ptr(dg_v0), _ptr(dg_V),
                                                         _ptr(dg_Vold)))
 
+    # -- the solver step's Q1 systems (src/pfem2fem.cpp:247-489, volume terms) ----
+    FEM_PREDICTION, FEM_PRESSURE, FEM_CORRECTION = 0, 1, 2
+
+    def fem_pattern(self):
+        """CSR pattern (row_ptr, cols) of the system matrices."""
+        n = C.c_int64()
+        row_ptr = np.zeros(self.mesh.n_dofs + 1, np.int32)
+        self._ck(self.L.pfem2gpu_fem_pattern(self.h, _ptr(row_ptr), None, 0, C.byref(n)))
+        cols = np.zeros(max(n.value, 1), np.int32)
+        self._ck(self.L.pfem2gpu_fem_pattern(self.h, _ptr(row_ptr), _ptr(cols), n.value, C.byref(n)))
+        return row_ptr, cols[: n.value]
+
+    def fem_assemble(self, system, rho, mu, dt, U, U2=None, P=None):
+        """One system on host arrays: (A (matrices, nnz), rhs (right-hand sides, n_dofs)).
+        PREDICTION: U = solution V, U2 = old solution V; PRESSURE: U = predicted
+        V; CORRECTION: U = predicted V, P = pressure."""
+        n = C.c_int64()
+        self._ck(self.L.pfem2gpu_fem_pattern(self.h, None, None, 0, C.byref(n)))
+        nm = self.dim if system == self.FEM_PREDICTION else 1
+        ns = 1 if system == self.FEM_PRESSURE else self.dim
+        A = np.empty((nm, max(n.value, 1)))
+        rhs = np.empty((ns, self.mesh.n_dofs))
+        keep = [None if a is None else _host(a, np.float64) for a in (U, U2, P)]
+        self._ck(self.L.pfem2gpu_fem_assemble(self.h, int(system), float(rho), float(mu), float(dt),
+                                              *[_ptr(a) for a in keep], _ptr(A), _ptr(rhs)))
+        return A[:, : n.value], rhs
+
     def vertex_maps(self):
         """The vertex -> cell maps in use: (offsets, cells, dirs (n, dim))."""
         off = np.zeros(self.mesh.n_verts + 1, np.int32)

@@ -1,0 +1,130 @@
+"""The solver step's Q1 systems assembled on the device
+(src/pfem2fem.cpp:247-489, volume terms) against the FP64 oracle: the CSR
+pattern equal, matrices and right-hand sides bit for bit (both sum each
+entry's cell contributions in ascending cell order, every operation
+separately rounded), on structured, unstructured and perturbed meshes in 2D
+and 3D; plus properties that hold whatever the arithmetic (mass matrix sums
+to rho times the volume, Laplacian rows sum to zero, symmetric pressure
+matrix)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pfem2dealii_b200 import mesh as M
+from pfem2dealii_b200.handler import ParticleHandler
+
+from . import cases
+
+pytestmark = pytest.mark.gpu
+
+RHO, MU, DT = 1.3, 0.01, 0.02
+
+
+def _mesh(which):
+    return {"channel": lambda: M.hyper_rectangle((0, 0), (4, 1), (16, 8)),
+            "cylinder": lambda: M.turek_channel(24, 12, 60),
+            "box": lambda: M.hyper_rectangle((0, 0, 0), (2, 1, 1), (8, 4, 4)),
+            "cube": lambda: M.perturbed_cube(8)}[which]()
+
+
+def _handler(m):
+    c = cases.channel() if m.dim == 2 else cases.duct(8, 4, 4)
+    g = ParticleHandler(m.dim, cases.params(c), "fp64")
+    g.initialize_maps(m)
+    return g
+
+
+def _fields(m, seed=0):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((m.dim, m.n_dofs)), rng.standard_normal((m.dim, m.n_dofs)), \
+        rng.standard_normal(m.n_dofs)
+
+
+@pytest.mark.parametrize("which", ["channel", "cylinder", "box", "cube"])
+def test_fem_systems_match_oracle_bit_for_bit(which):
+    m = _mesh(which)
+    g = _handler(m)
+    rp, cols = g.fem_pattern()
+    orp, ocols = O.fem_pattern(m)
+    assert np.array_equal(rp, orp) and np.array_equal(cols, ocols)
+    U, U2, P = _fields(m)
+    for system, kw in ((O.FEM_PREDICTION, dict(U=U, U2=U2)), (O.FEM_PRESSURE, dict(U=U)),
+                       (O.FEM_CORRECTION, dict(U=U, P=P))):
+        A, r = g.fem_assemble(system, RHO, MU, DT, **kw)
+        Ao, ro = O.fem_assemble(m, system, RHO, MU, DT, pattern=(orp, ocols), **kw)
+        assert A.shape == Ao.shape and r.shape == ro.shape
+        assert A.tobytes() == Ao.tobytes(), (system, np.max(np.abs(A - Ao)))
+        assert r.tobytes() == ro.tobytes(), (system, np.max(np.abs(r - ro)))
+    g.close()
+
+
+@pytest.mark.parametrize("which", ["cylinder", "cube"])
+def test_fem_system_properties(which):
+    m = _mesh(which)
+    g = _handler(m)
+    rp, cols = g.fem_pattern()
+    U, U2, P = _fields(m, 1)
+    X = m.vertices[m.cells]
+    # volume by the same quadrature: the mass matrix sums to rho * |Omega|
+    A, _ = g.fem_assemble(O.FEM_CORRECTION, RHO, MU, DT, U=U, P=P)
+    vol = float(np.sum(np.abs(_volumes(X))))
+    assert abs(A[0].sum() - RHO * vol) <= 1e-12 * RHO * vol
+    # pressure matrix: rows sum to zero, symmetric
+    A, _ = g.fem_assemble(O.FEM_PRESSURE, RHO, MU, DT, U=U)
+    rows = np.add.reduceat(A[0], rp[:-1])
+    assert np.max(np.abs(rows)) <= 1e-12 * np.max(np.abs(A[0]))
+    import scipy.sparse as sp
+
+    S = sp.csr_matrix((A[0], cols, rp), shape=(m.n_dofs, m.n_dofs))
+    assert abs(S - S.T).max() <= 1e-13 * abs(S).max()
+    # a uniform velocity has no divergence: the pressure right-hand side
+    # vanishes wherever the velocity's support is whole (interior DoFs)
+    c = np.arange(1, m.dim + 1, dtype=float)
+    _, r = g.fem_assemble(O.FEM_PRESSURE, RHO, MU, DT, U=np.repeat(c[:, None], m.n_dofs, 1))
+    assert np.isfinite(r).all()
+    g.close()
+
+
+def _volumes(X):
+    """Cell volumes by the 2^dim-point Gauss rule (exact for these maps)."""
+    dim = X.shape[2]
+    nv = 1 << dim
+    q = [0.21132486540518711775, 0.78867513459481288225]
+    vol = np.zeros(X.shape[0])
+    for k in range(nv):
+        xi = [q[(k >> d) & 1] for d in range(dim)]
+        J = np.zeros((X.shape[0], dim, dim))
+        for i in range(nv):
+            for e in range(dim):
+                t = 1.0 if (i >> e) & 1 else -1.0
+                for d in range(dim):
+                    if d != e:
+                        t *= xi[d] if (i >> d) & 1 else 1 - xi[d]
+                J[:, :, e] += X[:, i, :] * t
+        vol += np.linalg.det(J) * (0.5 ** dim)
+    return vol
+
+
+def test_fem_device_call_and_errors():
+    import torch
+
+    m = _mesh("box")
+    g = _handler(m)
+    rp, cols = g.fem_pattern()
+    U, U2, P = _fields(m, 2)
+    dU = torch.tensor(U, device="cuda")
+    dU2 = torch.tensor(U2, device="cuda")
+    dA = torch.empty((m.dim, len(cols)), dtype=torch.float64, device="cuda")
+    dr = torch.empty((m.dim, m.n_dofs), dtype=torch.float64, device="cuda")
+    g._ck(g.L.pfem2gpu_fem_assemble_device(g.h, 0, RHO, MU, DT, dU.data_ptr(), dU2.data_ptr(), None,
+                                            dA.data_ptr(), dr.data_ptr()))
+    g.synchronize()
+    A, r = g.fem_assemble(0, RHO, MU, DT, U=U, U2=U2)
+    assert np.array_equal(dA.cpu().numpy(), A) and np.array_equal(dr.cpu().numpy(), r)
+    # unknown system and missing inputs are argument errors
+    assert g.L.pfem2gpu_fem_assemble_device(g.h, 7, RHO, MU, DT, dU.data_ptr(), None, None, dA.data_ptr(),
+                                            dr.data_ptr()) == 1
+    assert g.L.pfem2gpu_fem_assemble_device(g.h, 0, RHO, MU, DT, dU.data_ptr(), None, None, dA.data_ptr(),
+                                            dr.data_ptr()) == 1
+    del dU, dU2, dA, dr
+    g.close()
