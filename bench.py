@@ -547,6 +547,8 @@ def main():
                     help="time the differentiated window and its adjoint only (prints one JSON object)")
     ap.add_argument("--only", choices=["fp32", "fp64"], default=None,
                     help="run one device-resident pass of one form and print its timing (profiling runs)")
+    ap.add_argument("--fem-only", action="store_true",
+                    help="time the three FEM system assemblies on the workload mesh only (prints one JSON object)")
     ap.add_argument("--e2e", action="store_true",
                     help="with --only: also the same steps through the host ABI (pinned H2D/D2H each step)")
     ap.add_argument("--kernels", action="store_true",
@@ -575,6 +577,9 @@ def main():
         forms = (args.only,) if args.only else ("fp32", "fp64")
         print(json.dumps(adjoint_report(ParticleHandler, m, V, Vold, prm, torch, K=ADJOINT_K[args.workload],
                                         forms=forms)), flush=True)
+        return 0
+    if args.fem_only:
+        print(json.dumps(timed_fem(ParticleHandler, m, V, torch)), flush=True)
         return 0
     if args.only:
         r = timed_device_run(ParticleHandler, m, V, Vold, prm, args.only, args.steps, args.warmup, torch)

@@ -96,102 +96,122 @@ __device__ void quad_point(const double* __restrict__ X, int q, Quad<DIM>& out)
     out.jxw = det * (DIM == 2 ? 0.25 : 0.125);
 }
 
-// One thread per (cell, local row i): row i of the cell's local matrices
-// (NS of them, NV entries each) and its right-hand-side entries.
+// One lane per (cell, local row i), 32 / 2^dim cells per warp.  The cell's
+// 2^dim quadrature points are computed once, lane i taking point i, into
+// shared memory; then lane i accumulates row i of the cell's local matrices
+// (NM of them, NV entries each) and its right-hand-side entries, reading the
+// points in order.
+constexpr int FEM_WARPS = 4;
+
 template <int DIM, int SYS>
-__global__ void __launch_bounds__(128) k_fem_local(FemArgs f)
+__global__ void __launch_bounds__(FEM_WARPS * 32) k_fem_local(FemArgs f)
 {
-    constexpr int NV = 1 << DIM, NQ = 1 << DIM;
+    constexpr int NV = 1 << DIM, NQ = 1 << DIM, CPW = 32 / NV;
     constexpr int NS = SYS == FEM_PRESSURE ? 1 : DIM;   // right-hand sides
     constexpr int NM = SYS == FEM_PREDICTION ? DIM : 1;  // matrices
-    const long long total = (long long)f.nC * NV;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(t / NV), i = (int)(t % NV);
-        double X[NV * DIM];
+    __shared__ Quad<DIM> qd[FEM_WARPS][CPW][NQ];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int jc = lane / NV, i = lane % NV;
+    const long long nwarps = (long long)gridDim.x * FEM_WARPS;
+    for (long long gw = (long long)blockIdx.x * FEM_WARPS + warp; gw * CPW < f.nC; gw += nwarps) {
+        const long long c = gw * CPW + jc;
+        const bool valid = c < f.nC;
+        if (valid) {
+            double X[NV * DIM];
 #pragma unroll
-        for (int k = 0; k < NV * DIM; ++k) X[k] = f.cellX[(size_t)c * NV * DIM + k];
-        int dof[NV];
+            for (int k = 0; k < NV * DIM; ++k) X[k] = f.cellX[(size_t)c * NV * DIM + k];
+            quad_point<DIM>(X, i, qd[warp][jc][i]);
+        }
+        __syncwarp();
+        if (valid) {
+            int dof[NV];
 #pragma unroll
-        for (int j = 0; j < NV; ++j) dof[j] = f.cd[(size_t)c * NV + j];
-        double M[NM][NV], r[NS];
+            for (int j = 0; j < NV; ++j) dof[j] = f.cd[(size_t)c * NV + j];
+            double M[NM][NV], r[NS];
 #pragma unroll
-        for (int m = 0; m < NM; ++m)
+            for (int m = 0; m < NM; ++m)
 #pragma unroll
-            for (int j = 0; j < NV; ++j) M[m][j] = 0.0;
+                for (int j = 0; j < NV; ++j) M[m][j] = 0.0;
 #pragma unroll
-        for (int k = 0; k < NS; ++k) r[k] = 0.0;
-        for (int q = 0; q < NQ; ++q) {
-            Quad<DIM> Q;
-            quad_point<DIM>(X, q, Q);
-            const double w = Q.jxw;
-            const double Ni = Q.N[i];
-            const double* gi = Q.g[i];
-            if constexpr (SYS == FEM_PREDICTION) {
-                for (int j = 0; j < NV; ++j) {
-                    const double* gj = Q.g[j];
-                    double aux = f.rho * Ni * Q.N[j] * w;
+            for (int k = 0; k < NS; ++k) r[k] = 0.0;
+            for (int q = 0; q < NQ; ++q) {
+                const Quad<DIM>& Q = qd[warp][jc][q];
+                const double w = Q.jxw;
+                const double Ni = Q.N[i];
+                double gi[DIM];
 #pragma unroll
-                    for (int k = 0; k < DIM; ++k) {
-                        M[k][j] = M[k][j] + aux;
-                        r[k] = r[k] + aux * f.U2[(size_t)k * f.nD + dof[j]];
+                for (int d = 0; d < DIM; ++d) gi[d] = Q.g[i][d];
+                if constexpr (SYS == FEM_PREDICTION) {
+#pragma unroll
+                    for (int j = 0; j < NV; ++j) {
+                        const double* gj = Q.g[j];
+                        double aux = f.rho * Ni * Q.N[j] * w;
+#pragma unroll
+                        for (int k = 0; k < DIM; ++k) {
+                            M[k][j] = M[k][j] + aux;
+                            r[k] = r[k] + aux * f.U2[(size_t)k * f.nD + dof[j]];
+                        }
+                        aux = f.mu * f.dt * w;
+                        double u[DIM];
+#pragma unroll
+                        for (int k = 0; k < DIM; ++k) u[k] = f.U[(size_t)k * f.nD + dof[j]];
+                        if constexpr (DIM == 2) {
+                            M[0][j] = M[0][j] + aux * (gi[1] * gj[1] + 4.0 / 3.0 * gi[0] * gj[0]);
+                            M[1][j] = M[1][j] + aux * (gi[0] * gj[0] + 4.0 / 3.0 * gi[1] * gj[1]);
+                            r[0] = r[0] - aux * (gi[1] * gj[0] - 2.0 / 3.0 * gi[0] * gj[1]) * u[1];
+                            r[1] = r[1] - aux * (gi[0] * gj[1] - 2.0 / 3.0 * gi[1] * gj[0]) * u[0];
+                        } else {
+                            M[0][j] = M[0][j] + aux * (4.0 / 3.0 * gi[0] * gj[0] + gi[1] * gj[1] + gi[2] * gj[2]);
+                            M[1][j] = M[1][j] + aux * (gj[0] * gi[0] + 4.0 / 3.0 * gi[1] * gj[1] + gi[2] * gj[2]);
+                            M[2][j] = M[2][j] + aux * (gj[0] * gi[0] + gj[1] * gi[1] + 4.0 / 3.0 * gi[2] * gj[2]);
+                            r[0] = r[0] - aux * ((gi[1] * gj[0] - 2.0 / 3.0 * gi[0] * gj[1]) * u[1] +
+                                                 (gi[2] * gj[0] - 2.0 / 3.0 * gi[0] * gj[2]) * u[2]);
+                            r[1] = r[1] - aux * ((gi[0] * gj[1] - 2.0 / 3.0 * gi[1] * gj[0]) * u[0] +
+                                                 (gi[2] * gj[1] - 2.0 / 3.0 * gi[1] * gj[2]) * u[2]);
+                            r[2] = r[2] - aux * ((gi[0] * gj[2] - 2.0 / 3.0 * gi[2] * gj[0]) * u[0] +
+                                                 (gi[1] * gj[2] - 2.0 / 3.0 * gi[2] * gj[1]) * u[1]);
+                        }
                     }
-                    aux = f.mu * f.dt * w;
-                    double u[DIM];
+                } else if constexpr (SYS == FEM_PRESSURE) {
+                    const double coeff = f.rho / f.dt;
 #pragma unroll
-                    for (int k = 0; k < DIM; ++k) u[k] = f.U[(size_t)k * f.nD + dof[j]];
-                    if constexpr (DIM == 2) {
-                        M[0][j] = M[0][j] + aux * (gi[1] * gj[1] + 4.0 / 3.0 * gi[0] * gj[0]);
-                        M[1][j] = M[1][j] + aux * (gi[0] * gj[0] + 4.0 / 3.0 * gi[1] * gj[1]);
-                        r[0] = r[0] - aux * (gi[1] * gj[0] - 2.0 / 3.0 * gi[0] * gj[1]) * u[1];
-                        r[1] = r[1] - aux * (gi[0] * gj[1] - 2.0 / 3.0 * gi[1] * gj[0]) * u[0];
-                    } else {
-                        M[0][j] = M[0][j] + aux * (4.0 / 3.0 * gi[0] * gj[0] + gi[1] * gj[1] + gi[2] * gj[2]);
-                        M[1][j] = M[1][j] + aux * (gj[0] * gi[0] + 4.0 / 3.0 * gi[1] * gj[1] + gi[2] * gj[2]);
-                        M[2][j] = M[2][j] + aux * (gj[0] * gi[0] + gj[1] * gi[1] + 4.0 / 3.0 * gi[2] * gj[2]);
-                        r[0] = r[0] - aux * ((gi[1] * gj[0] - 2.0 / 3.0 * gi[0] * gj[1]) * u[1] +
-                                             (gi[2] * gj[0] - 2.0 / 3.0 * gi[0] * gj[2]) * u[2]);
-                        r[1] = r[1] - aux * ((gi[0] * gj[1] - 2.0 / 3.0 * gi[1] * gj[0]) * u[0] +
-                                             (gi[2] * gj[1] - 2.0 / 3.0 * gi[1] * gj[2]) * u[2]);
-                        r[2] = r[2] - aux * ((gi[0] * gj[2] - 2.0 / 3.0 * gi[2] * gj[0]) * u[0] +
-                                             (gi[1] * gj[2] - 2.0 / 3.0 * gi[2] * gj[1]) * u[1]);
+                    for (int j = 0; j < NV; ++j) {
+                        const double* gj = Q.g[j];
+                        double dot = gi[0] * gj[0];
+#pragma unroll
+                        for (int d = 1; d < DIM; ++d) dot = dot + gi[d] * gj[d];
+                        M[0][j] = M[0][j] + dot * w;
+                        double aux = 0.0;
+#pragma unroll
+                        for (int k = 0; k < DIM; ++k) aux = aux + f.U[(size_t)k * f.nD + dof[j]] * gi[k];
+                        r[0] = r[0] + coeff * aux * Q.N[j] * w;
                     }
-                }
-            } else if constexpr (SYS == FEM_PRESSURE) {
-                const double coeff = f.rho / f.dt;
-                for (int j = 0; j < NV; ++j) {
-                    const double* gj = Q.g[j];
-                    double dot = gi[0] * gj[0];
+                } else {
+                    const double aux2 = f.dt * Ni * w;
 #pragma unroll
-                    for (int d = 1; d < DIM; ++d) dot = dot + gi[d] * gj[d];
-                    M[0][j] = M[0][j] + dot * w;
-                    double aux = 0.0;
+                    for (int j = 0; j < NV; ++j) {
+                        const double* gj = Q.g[j];
+                        const double aux = f.rho * Ni * Q.N[j] * w;
+                        const double p = f.P[dof[j]];
 #pragma unroll
-                    for (int k = 0; k < DIM; ++k) aux = aux + f.U[(size_t)k * f.nD + dof[j]] * gi[k];
-                    r[0] = r[0] + coeff * aux * Q.N[j] * w;
-                }
-            } else {
-                const double aux2 = f.dt * Ni * w;
-                for (int j = 0; j < NV; ++j) {
-                    const double* gj = Q.g[j];
-                    const double aux = f.rho * Ni * Q.N[j] * w;
-                    const double p = f.P[dof[j]];
-#pragma unroll
-                    for (int k = 0; k < DIM; ++k) {
-                        if (k == 0) M[0][j] = M[0][j] + aux;  // the same matrix for every component
-                        r[k] = r[k] + aux * f.U[(size_t)k * f.nD + dof[j]];
-                        r[k] = r[k] - aux2 * gj[k] * p;
+                        for (int k = 0; k < DIM; ++k) {
+                            if (k == 0) M[0][j] = M[0][j] + aux;  // the same matrix for every component
+                            r[k] = r[k] + aux * f.U[(size_t)k * f.nD + dof[j]];
+                            r[k] = r[k] - aux2 * gj[k] * p;
+                        }
                     }
                 }
             }
+            const size_t t = (size_t)c * NV + i;
+            double* L = f.local + t * NM * NV;
+#pragma unroll
+            for (int m = 0; m < NM; ++m)
+#pragma unroll
+                for (int j = 0; j < NV; ++j) L[m * NV + j] = M[m][j];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) f.local_rhs[t * NS + k] = r[k];
         }
-        double* L = f.local + (size_t)t * NM * NV;
-#pragma unroll
-        for (int m = 0; m < NM; ++m)
-#pragma unroll
-            for (int j = 0; j < NV; ++j) L[m * NV + j] = M[m][j];
-#pragma unroll
-        for (int k = 0; k < NS; ++k) f.local_rhs[(size_t)t * NS + k] = r[k];
+        __syncwarp();
     }
 }
 
@@ -289,7 +309,7 @@ int launch_fem_pattern(int dim, const FemArgs& f, bool fill, uint32_t* count, un
 template <int DIM, int SYS>
 static int fem_t(const FemArgs& f, cudaStream_t s)
 {
-    k_fem_local<DIM, SYS><<<fem_grid((const void*)k_fem_local<DIM, SYS>, 128), 128, 0, s>>>(f);
+    k_fem_local<DIM, SYS><<<fem_grid((const void*)k_fem_local<DIM, SYS>, FEM_WARPS * 32), FEM_WARPS * 32, 0, s>>>(f);
     k_fem_gather<DIM, SYS><<<fem_grid((const void*)k_fem_gather<DIM, SYS>, 256), 256, 0, s>>>(f);
     return 2;
 }
