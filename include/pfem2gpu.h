@@ -109,9 +109,9 @@ const char* pfem2gpu_read_unv_error(void);
 
 /* ---------------------------------------------------------------------------
  * The solver step's Q1 systems (src/pfem2fem.cpp): the volume integrals of
- * assemble_velocity_prediction (:247-310, SCHEMEB off),
- * assemble_pressure_equation (:392-425) and assemble_velocity_correction
- * (:460-489), computed per cell on the device in FP64 (QGauss(2), the Q1
+ * assemble_velocity_prediction (:247-319, SCHEMEB off),
+ * assemble_pressure_equation (:393-435) and assemble_velocity_correction
+ * (:461-510), computed per cell on the device in FP64 (QGauss(2), the Q1
  * map's Jacobian at each point) and summed into CSR matrices and right-hand
  * sides in ascending cell order, as a cell loop adds local systems.  The
  * boundary-face terms and the constraints (AffineConstraints::

@@ -2,9 +2,9 @@
  * INFRASTRUCTURE ONLY: the checker of the library's device assembly, never
  * called by the product.
  *
- * Follows src/pfem2fem.cpp: assemble_velocity_prediction (:247-310, the
- * volume integral; SCHEMEB off), assemble_pressure_equation (:392-425) and
- * assemble_velocity_correction (:460-489), as a sequential cell loop that
+ * Follows src/pfem2fem.cpp: assemble_velocity_prediction (:247-319, the
+ * volume integral; SCHEMEB off), assemble_pressure_equation (:393-435) and
+ * assemble_velocity_correction (:461-510), as a sequential cell loop that
  * adds each cell's local matrix and right-hand side into the global ones
  * (distribute_local_to_global without constraints).  Boundary-face terms and
  * the constraints stay with the caller.  FE values are the Q1 /

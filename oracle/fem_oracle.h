@@ -1,5 +1,5 @@
 /* FP64 CPU restatement of the Q1 FEM systems' volume terms
- * (src/pfem2fem.cpp:247-489) -- test infrastructure only. */
+ * (src/pfem2fem.cpp:247-510) -- test infrastructure only. */
 #ifndef FEM_ORACLE_H
 #define FEM_ORACLE_H
 #include <stdint.h>

@@ -255,7 +255,7 @@ def key(i, seed):
 
 
 # --------------------------------------------------------------------------
-# FEM systems' volume terms (src/pfem2fem.cpp:247-489), restated in
+# FEM systems' volume terms (src/pfem2fem.cpp:247-510), restated in
 # fem_oracle.c: the checker of the library's device assembly.
 # --------------------------------------------------------------------------
 FEM_PREDICTION, FEM_PRESSURE, FEM_CORRECTION = 0, 1, 2

@@ -210,7 +210,7 @@ class ParticleHandler:
         self._ck(self.L.pfem2gpu_window_backward_device(self.h, _ptr(dgU), _ptr(dg_v0), _ptr(dg_V),
                                                         _ptr(dg_Vold)))
 
-    # -- the solver step's Q1 systems (src/pfem2fem.cpp:247-489, volume terms) ----
+    # -- the solver step's Q1 systems (src/pfem2fem.cpp:247-510, volume terms) ----
     FEM_PREDICTION, FEM_PRESSURE, FEM_CORRECTION = 0, 1, 2
 
     def fem_pattern(self):

@@ -1,5 +1,5 @@
 """The solver step's Q1 systems assembled on the device
-(src/pfem2fem.cpp:247-489, volume terms) against the FP64 oracle: the CSR
+(src/pfem2fem.cpp:247-510, volume terms) against the FP64 oracle: the CSR
 pattern equal, matrices and right-hand sides bit for bit (both sum each
 entry's cell contributions in ascending cell order, every operation
 separately rounded), on structured, unstructured and perturbed meshes in 2D
