@@ -113,9 +113,11 @@ const char* pfem2gpu_read_unv_error(void);
  * assemble_pressure_equation (:393-435) and assemble_velocity_correction
  * (:461-510), computed per cell on the device in FP64 (QGauss(2), the Q1
  * map's Jacobian at each point) and summed into CSR matrices and right-hand
- * sides in ascending cell order, as a cell loop adds local systems.  The
- * boundary-face terms and the constraints (AffineConstraints::
- * distribute_local_to_global) stay with the caller.
+ * sides in ascending cell order, as a cell loop adds local systems.  With
+ * boundary ids set (pfem2gpu_fem_set_boundary), the boundary-face terms of
+ * the prediction (:320-383) and of the pressure equation (:436-449) are
+ * added on the faces outside the Dirichlet sets.  The constraints
+ * (AffineConstraints::distribute_local_to_global) stay with the caller.
  * ------------------------------------------------------------------------- */
 #define PFEM2GPU_FEM_PREDICTION 0 /* U = solution V, U2 = old solution V: dim matrices, dim right-hand sides */
 #define PFEM2GPU_FEM_PRESSURE 1   /* U = predicted V: one matrix, one right-hand side */
@@ -125,6 +127,15 @@ const char* pfem2gpu_read_unv_error(void);
  * DoF the DoFs sharing a cell with it, ascending), built on the device once
  * per mesh; row_ptr n_dofs+1, cols >= capacity entries (NULL: *nnz only). */
 int pfem2gpu_fem_pattern(pfem2gpu_handle* h, int32_t* row_ptr, int32_t* cols, int64_t capacity, int64_t* nnz);
+/* Boundary ids per cell and face (n_cells x 2 dim, deal.II face numbering:
+ * face 2d lies at xi_d = 0, face 2d+1 at xi_d = 1; -1 for an interior face)
+ * and the Dirichlet sets (getVelocityDirichletBCpatchIDs,
+ * getPressureDirichletBCpatchIDs): the prediction gets face terms on
+ * boundary faces outside the velocity set, the pressure equation on those
+ * outside the pressure set.  face_ids NULL: no face terms. */
+int pfem2gpu_fem_set_boundary(pfem2gpu_handle* h, const int32_t* face_ids, int32_t n_velocity_dirichlet,
+                              const int32_t* velocity_dirichlet, int32_t n_pressure_dirichlet,
+                              const int32_t* pressure_dirichlet);
 /* One system on device vectors (component-major U, U2 of dim x n_dofs; P of
  * n_dofs): A receives matrices x nnz values on the pattern, rhs right-hand
  * sides x n_dofs.  Enqueued on the handle's stream, not synchronized.  rho,

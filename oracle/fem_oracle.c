@@ -77,6 +77,72 @@ static void fe_point(int dim, const double* X, int q, double* N, double* g, doub
     *jxw = det * (dim == 2 ? 0.25 : 0.125);
 }
 
+/* Face f (xi_{f/2} = f%2), face point qf: the other directions ascending,
+ * the first fastest, weight 1/2 each; outward normal J^-T nhat normalised,
+ * surface element det J |J^-T nhat| w (deal.II FEFaceValues, MappingQ1). */
+static void fe_face_point(int dim, const double* X, int f, int qf, double* N, double* g, double* n, double* jxw)
+{
+    const int nv = 1 << dim, fd = f >> 1, side = f & 1;
+    double xi[3], gr[8][3], J[3][3], Ji[3][3], det;
+    int k = 0;
+    for (int d = 0; d < dim; ++d) {
+        if (d == fd) xi[d] = side ? 1.0 : 0.0;
+        else xi[d] = QP[(qf >> k++) & 1];
+    }
+    for (int i = 0; i < nv; ++i) {
+        double nn = 1.0;
+        for (int d = 0; d < dim; ++d) nn = nn * (((i >> d) & 1) ? xi[d] : 1.0 - xi[d]);
+        N[i] = nn;
+        for (int e = 0; e < dim; ++e) {
+            double t = ((i >> e) & 1) ? 1.0 : -1.0;
+            for (int d = 0; d < dim; ++d)
+                if (d != e) t = t * (((i >> d) & 1) ? xi[d] : 1.0 - xi[d]);
+            gr[i][e] = t;
+        }
+    }
+    for (int d = 0; d < dim; ++d)
+        for (int e = 0; e < dim; ++e) {
+            double sum = 0.0;
+            for (int i = 0; i < nv; ++i) sum = sum + X[i * dim + d] * gr[i][e];
+            J[d][e] = sum;
+        }
+    if (dim == 2) {
+        det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        Ji[0][0] = J[1][1] / det;
+        Ji[0][1] = -J[0][1] / det;
+        Ji[1][0] = -J[1][0] / det;
+        Ji[1][1] = J[0][0] / det;
+    } else {
+        const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+        const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+        const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+        det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+        Ji[0][0] = c00 / det;
+        Ji[1][0] = c01 / det;
+        Ji[2][0] = c02 / det;
+        Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+        Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+        Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+        Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+        Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+        Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+    }
+    for (int i = 0; i < nv; ++i)
+        for (int d = 0; d < dim; ++d) {
+            double sum = 0.0;
+            for (int e = 0; e < dim; ++e) sum = sum + Ji[e][d] * gr[i][e];
+            g[i * 3 + d] = sum;
+        }
+    double v[3], nrm = 0.0;
+    for (int a = 0; a < dim; ++a) {
+        v[a] = side ? Ji[fd][a] : -Ji[fd][a];
+        nrm = nrm + v[a] * v[a];
+    }
+    nrm = sqrt(nrm);
+    for (int a = 0; a < dim; ++a) n[a] = v[a] / nrm;
+    *jxw = det * nrm * (dim == 2 ? 0.5 : 0.25);
+}
+
 static int cmp_int(const void* a, const void* b)
 {
     const int x = *(const int*)a, y = *(const int*)b;
@@ -131,7 +197,8 @@ static int64_t find_col(const int32_t* row_ptr, const int32_t* cols, int row, in
 
 int orc_fem_assemble(int dim, int system, int64_t n_cells, int64_t n_dofs, const double* cellX,
                      const int32_t* cell_dofs, const int32_t* row_ptr, const int32_t* cols, double rho, double mu,
-                     double dt, const double* U, const double* U2, const double* P, double* A, double* rhs)
+                     double dt, const double* U, const double* U2, const double* P, const uint16_t* fmask, double* A,
+                     double* rhs)
 {
     const int nv = 1 << dim, nq = 1 << dim;
     const int nm = system == ORC_FEM_PREDICTION ? dim : 1;
@@ -199,6 +266,63 @@ int orc_fem_assemble(int dim, int system, int64_t n_cells, int64_t n_dofs, const
                             r[k][i] = r[k][i] + aux * U[k * n_dofs + dof[j]];
                             r[k][i] = r[k][i] - aux2 * gj[k] * p;
                         }
+                    }
+                }
+            }
+        }
+        /* boundary faces outside the Dirichlet set: :320-383 (prediction), :436-449 (pressure) */
+        const unsigned faces = !fmask ? 0u
+                               : system == ORC_FEM_PREDICTION ? (fmask[c] & 0xffu)
+                               : system == ORC_FEM_PRESSURE   ? ((unsigned)fmask[c] >> 8)
+                                                              : 0u;
+        for (int f = 0; f < 2 * dim; ++f) {
+            if (!((faces >> f) & 1u)) continue;
+            for (int qf = 0; qf < (1 << (dim - 1)); ++qf) {
+                double nrm[3];
+                fe_face_point(dim, X, f, qf, N, g, nrm, &w);
+                if (system == ORC_FEM_PREDICTION && dim == 2) {
+                    for (int i = 0; i < nv; ++i)
+                        for (int j = 0; j < nv; ++j) {
+                            const double* gj = g + j * 3;
+                            const double u0 = U[dof[j]], u1 = U[n_dofs + dof[j]];
+                            M[0][i][j] = M[0][i][j] - mu * dt * N[i] * 4.0 / 3.0 * gj[0] * nrm[0] * w;
+                            r[0][i] = r[0][i] + mu * dt * N[i] * (-2.0 / 3.0) * gj[1] * u1 * nrm[0] * w;
+                            M[1][i][j] = M[1][i][j] - mu * dt * N[i] * gj[0] * nrm[0] * w;
+                            r[1][i] = r[1][i] + mu * dt * N[i] * gj[1] * u0 * nrm[0] * w;
+                        }
+                } else if (system == ORC_FEM_PREDICTION) {
+                    double tX[3] = {0, 0, 0}, tY[3] = {0, 0, 0}, tZ[3] = {0, 0, 0};
+                    for (int ii = 0; ii < nv; ++ii) {
+                        const double* gg = g + ii * 3;
+                        const double v0 = 0.0, v1 = U[n_dofs + dof[ii]], v2 = U[2 * n_dofs + dof[ii]];
+                        tX[0] = tX[0] + ((4.0 / 3.0) * gg[0] * v0 - (2.0 / 3.0) * gg[1] * v1 - (2.0 / 3.0) * gg[2] * v2);
+                        tX[1] = tX[1] + (gg[1] * v0 + gg[0] * v1);
+                        tX[2] = tX[2] + (gg[2] * v0 + gg[0] * v2);
+                        tY[0] = tY[0] + (gg[1] * v0 + gg[0] * v1);
+                        tY[1] = tY[1] + ((-2.0 / 3.0) * gg[0] * v0 + (4.0 / 3.0) * gg[1] * v1 - (2.0 / 3.0) * gg[2] * v2);
+                        tY[2] = tY[2] + (gg[2] * v1 + gg[1] * v2);
+                        tZ[0] = tZ[0] + (gg[2] * v0 + gg[0] * v2);
+                        tZ[1] = tZ[1] + (gg[2] * v1 + gg[1] * v2);
+                        tZ[2] = tZ[2] + ((-2.0 / 3.0) * gg[0] * v0 - (2.0 / 3.0) * gg[1] * v1 + (4.0 / 3.0) * gg[2] * v2);
+                    }
+                    const double* T[3] = {tX, tY, tZ};
+                    for (int i = 0; i < nv; ++i) {
+                        const double aux = mu * dt * N[i] * w;
+                        for (int k = 0; k < 3; ++k) {
+                            double dot = (aux * T[k][0]) * nrm[0];
+                            for (int d = 1; d < 3; ++d) dot = dot + (aux * T[k][d]) * nrm[d];
+                            r[k][i] = r[k][i] + dot;
+                        }
+                    }
+                } else {
+                    const double coeff = rho / dt;
+                    double Vq[3] = {0, 0, 0};
+                    for (int ii = 0; ii < nv; ++ii)
+                        for (int k = 0; k < dim; ++k) Vq[k] = Vq[k] + N[ii] * U[k * n_dofs + dof[ii]];
+                    for (int i = 0; i < nv; ++i) {
+                        double dot = (coeff * N[i] * Vq[0]) * nrm[0];
+                        for (int d = 1; d < dim; ++d) dot = dot + (coeff * N[i] * Vq[d]) * nrm[d];
+                        r[0][i] = r[0][i] - dot * w;
                     }
                 }
             }

@@ -15,9 +15,12 @@ extern "C" {
 int64_t orc_fem_pattern(int dim, int64_t n_cells, int64_t n_dofs, const int32_t* cell_dofs, int32_t* row_ptr,
                         int32_t* cols);
 /* A: (matrices x nnz), rhs: (right-hand sides x n_dofs); cellX: n_cells x 2^dim x dim. */
+/* fmask (may be NULL): per cell, bit f = boundary face f with prediction
+ * face terms, bit 8 + f = with pressure face terms. */
 int orc_fem_assemble(int dim, int system, int64_t n_cells, int64_t n_dofs, const double* cellX,
                      const int32_t* cell_dofs, const int32_t* row_ptr, const int32_t* cols, double rho, double mu,
-                     double dt, const double* U, const double* U2, const double* P, double* A, double* rhs);
+                     double dt, const double* U, const double* U2, const double* P, const uint16_t* fmask, double* A,
+                     double* rhs);
 #ifdef __cplusplus
 }
 #endif

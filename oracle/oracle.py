@@ -92,7 +92,7 @@ def lib():
         L.orc_fem_pattern.restype = C.c_int64
         L.orc_fem_pattern.argtypes = [C.c_int, C.c_int64, C.c_int64, ip, P, P]
         L.orc_fem_assemble.argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int64, dp, ip, ip, ip, C.c_double,
-                                       C.c_double, C.c_double, P, P, P, dp, dp]
+                                       C.c_double, C.c_double, P, P, P, P, dp, dp]
         _lib = L
     return _lib
 
@@ -273,7 +273,19 @@ def fem_pattern(mesh):
     return row_ptr, cols[:nnz]
 
 
-def fem_assemble(mesh, system, rho, mu, dt, U=None, U2=None, P=None, pattern=None):
+def fem_face_mask(face_ids, velocity_dirichlet=(), pressure_dirichlet=()):
+    """Per cell: bit f = boundary face f outside the velocity Dirichlet set,
+    bit 8 + f = outside the pressure Dirichlet set."""
+    fid = np.asarray(face_ids)
+    mask = np.zeros(fid.shape[0], np.uint16)
+    for f in range(fid.shape[1]):
+        b = fid[:, f] >= 0
+        mask |= ((b & ~np.isin(fid[:, f], list(velocity_dirichlet))).astype(np.uint16) << f)
+        mask |= ((b & ~np.isin(fid[:, f], list(pressure_dirichlet))).astype(np.uint16) << (8 + f))
+    return mask
+
+
+def fem_assemble(mesh, system, rho, mu, dt, U=None, U2=None, P=None, pattern=None, face_mask=None):
     """(A, rhs): A (matrices, nnz) on the pattern, rhs (right-hand sides, n_dofs)."""
     L = lib()
     row_ptr, cols = pattern if pattern is not None else fem_pattern(mesh)
@@ -284,9 +296,11 @@ def fem_assemble(mesh, system, rho, mu, dt, U=None, U2=None, P=None, pattern=Non
     rhs = np.zeros((ns, mesh.n_dofs))
     cellX = _c(mesh.vertices[mesh.cells], np.float64)
     keep = [None if a is None else _c(a, np.float64) for a in (U, U2, P)]
+    fm = None if face_mask is None else _c(face_mask, np.uint16)
     rc = L.orc_fem_assemble(mesh.dim, system, mesh.n_cells, mesh.n_dofs, cellX, _c(mesh.cell_dofs, np.int32),
                             _c(row_ptr, np.int32), _c(cols, np.int32), rho, mu, dt,
-                            *[None if a is None else a.ctypes.data_as(C.c_void_p) for a in keep], A, rhs)
+                            *[None if a is None else a.ctypes.data_as(C.c_void_p) for a in keep],
+                            None if fm is None else fm.ctypes.data_as(C.c_void_p), A, rhs)
     if rc:
         raise RuntimeError("pattern misses an entry")
     return A, rhs

@@ -88,6 +88,7 @@ struct pfem2gpu_handle {
         long long nnz = -1;
         double *local = nullptr, *local_rhs = nullptr, *io = nullptr;
         size_t local_n = 0, rhs_n = 0, io_n = 0;
+        uint16_t* fmask = nullptr;  // per cell: faces with prediction / pressure face terms
     } fem;
     // differentiated window: checkpoints, final state, projection and adjoint
     // buffers (per-particle arrays sized ncap x segcap, the rest per mesh)
@@ -268,7 +269,8 @@ void free_win_particles(pfem2gpu_handle::Win& W)
 
 void free_fem(pfem2gpu_handle::Fem& F)
 {
-    for (void* p : {(void*)F.row_ptr, (void*)F.cols, (void*)F.local, (void*)F.local_rhs, (void*)F.io}) dfree(p);
+    for (void* p : {(void*)F.row_ptr, (void*)F.cols, (void*)F.local, (void*)F.local_rhs, (void*)F.io, (void*)F.fmask})
+        dfree(p);
     F = pfem2gpu_handle::Fem{};
 }
 
@@ -1576,6 +1578,7 @@ static int fem_run(pfem2gpu_handle* h, int system, double rho, double mu, double
     f.local_rhs = F.local_rhs;
     f.A = dA;
     f.rhs = drhs;
+    f.fmask = F.fmask;
     run(h, "fem_assemble", [&] { return launch_fem_assemble(h->dim, system, f, h->stream); });
     return check_async(h);
 }
@@ -1591,6 +1594,39 @@ static int fem_check(pfem2gpu_handle* h, int system, const double* U, const doub
     if (system == PFEM2GPU_FEM_CORRECTION && !P) return fail(h, PFEM2GPU_ERR_ARG, "missing pressure");
     if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "no mesh");
     return fem_pattern(h);
+}
+
+int pfem2gpu_fem_set_boundary(pfem2gpu_handle* h, const int32_t* face_ids, int32_t n_velocity_dirichlet,
+                              const int32_t* velocity_dirichlet, int32_t n_pressure_dirichlet,
+                              const int32_t* pressure_dirichlet)
+{
+    if (!h) return PFEM2GPU_ERR_ARG;
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "no mesh");
+    auto& F = h->fem;
+    dfree(F.fmask);
+    F.fmask = nullptr;
+    if (!face_ids) return PFEM2GPU_OK;
+    if ((n_velocity_dirichlet > 0 && !velocity_dirichlet) || (n_pressure_dirichlet > 0 && !pressure_dirichlet) ||
+        n_velocity_dirichlet < 0 || n_pressure_dirichlet < 0)
+        return fail(h, PFEM2GPU_ERR_ARG, "bad Dirichlet id list");
+    const int nf = 2 * h->dim;
+    std::vector<uint16_t> mask(h->nC, 0);
+    auto in = [](int32_t id, int32_t n, const int32_t* ids) {
+        for (int32_t k = 0; k < n; ++k)
+            if (ids[k] == id) return true;
+        return false;
+    };
+    for (int c = 0; c < h->nC; ++c)
+        for (int f = 0; f < nf; ++f) {
+            const int32_t id = face_ids[(size_t)c * nf + f];
+            if (id < 0) continue;  // interior face
+            if (!in(id, n_velocity_dirichlet, velocity_dirichlet)) mask[c] |= (uint16_t)(1u << f);
+            if (!in(id, n_pressure_dirichlet, pressure_dirichlet)) mask[c] |= (uint16_t)(1u << (8 + f));
+        }
+    CK(dalloc(&F.fmask, (size_t)h->nC));
+    CK(cudaMemcpyAsync(F.fmask, mask.data(), (size_t)h->nC * sizeof(uint16_t), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PFEM2GPU_OK;
 }
 
 int pfem2gpu_fem_assemble_device(pfem2gpu_handle* h, int system, double rho, double mu, double dt, const double* dU,

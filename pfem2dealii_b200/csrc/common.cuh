@@ -199,6 +199,8 @@ struct FemArgs {
     double* local_rhs;  // per (cell, local row): right-hand sides
     double* A;          // matrices x nnz
     double* rhs;        // right-hand sides x nD
+    const uint16_t* fmask;  // per cell: bit f = boundary face f with prediction face terms,
+                            // bit 8 + f = with pressure face terms (null: none)
 };
 
 template <int DIM> struct Dims {

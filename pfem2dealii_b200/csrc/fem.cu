@@ -96,6 +96,175 @@ __device__ void quad_point(const double* __restrict__ X, int q, Quad<DIM>& out)
     out.jxw = det * (DIM == 2 ? 0.25 : 0.125);
 }
 
+// Face f (deal.II numbering: xi_{f/2} = f%2), face point qf of QGauss(2) in
+// the face's other directions (ascending, the first fastest; weight 1/2
+// each): shape values and gradients as in the cell, the outward unit normal
+// n = J^-T nhat / |J^-T nhat| and the surface element det J |J^-T nhat| w.
+template <int DIM>
+struct FaceQuad {
+    double N[1 << DIM];
+    double g[1 << DIM][DIM];
+    double n[DIM];
+    double jxw;
+};
+
+template <int DIM>
+__device__ void face_point(const double* __restrict__ X, int f, int qf, FaceQuad<DIM>& out)
+{
+    constexpr int NV = 1 << DIM;
+    const int fd = f >> 1, side = f & 1;
+    double xi[DIM];
+    int k = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        if (d == fd) {
+            xi[d] = side ? 1.0 : 0.0;
+        } else {
+            xi[d] = ((qf >> k) & 1) ? QG1 : QG0;
+            ++k;
+        }
+    }
+    double gr[NV][DIM];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        double nn = 1.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) nn = nn * (((i >> d) & 1) ? xi[d] : 1.0 - xi[d]);
+        out.N[i] = nn;
+#pragma unroll
+        for (int e = 0; e < DIM; ++e) {
+            double t = ((i >> e) & 1) ? 1.0 : -1.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+                if (d != e) t = t * (((i >> d) & 1) ? xi[d] : 1.0 - xi[d]);
+            gr[i][e] = t;
+        }
+    }
+    double J[DIM][DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+        for (int e = 0; e < DIM; ++e) {
+            double sum = 0.0;
+#pragma unroll
+            for (int i = 0; i < NV; ++i) sum = sum + X[i * DIM + d] * gr[i][e];
+            J[d][e] = sum;
+        }
+    double det, Ji[DIM][DIM];
+    if constexpr (DIM == 2) {
+        det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        Ji[0][0] = J[1][1] / det;
+        Ji[0][1] = -J[0][1] / det;
+        Ji[1][0] = -J[1][0] / det;
+        Ji[1][1] = J[0][0] / det;
+    } else {
+        const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+        const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+        const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+        det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+        Ji[0][0] = c00 / det;
+        Ji[1][0] = c01 / det;
+        Ji[2][0] = c02 / det;
+        Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+        Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+        Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+        Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+        Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+        Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+    }
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            double sum = 0.0;
+#pragma unroll
+            for (int e = 0; e < DIM; ++e) sum = sum + Ji[e][d] * gr[i][e];
+            out.g[i][d] = sum;
+        }
+    double v[DIM], nrm = 0.0;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+        v[a] = side ? Ji[fd][a] : -Ji[fd][a];
+        nrm = nrm + v[a] * v[a];
+    }
+    nrm = sqrt(nrm);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) out.n[a] = v[a] / nrm;
+    out.jxw = det * nrm * (DIM == 2 ? 0.5 : 0.25);
+}
+
+// Boundary-face terms of row i (the faces set in the cell's mask for this
+// system, ascending; their points in order), after the volume terms:
+// assemble_velocity_prediction :320-383, assemble_pressure_equation
+// :436-449.  The 3D prediction term takes velocity components 1..dim-1 of
+// the cell's DoFs, component 0 as zero, as the reference's loop does.
+template <int DIM, int SYS, int NM, int NS>
+__device__ void face_terms(const FemArgs& f, long long c, int i, const int* dof, double (*M)[1 << DIM], double* r)
+{
+    constexpr int NV = 1 << DIM;
+    const unsigned mk = f.fmask[c];
+    const unsigned faces = SYS == FEM_PREDICTION ? (mk & 0xffu) : (mk >> 8);
+    if (!faces) return;
+    double X[NV * DIM];
+#pragma unroll
+    for (int k = 0; k < NV * DIM; ++k) X[k] = f.cellX[(size_t)c * NV * DIM + k];
+    for (int fc = 0; fc < 2 * DIM; ++fc) {
+        if (!((faces >> fc) & 1u)) continue;
+        for (int qf = 0; qf < (1 << (DIM - 1)); ++qf) {
+            FaceQuad<DIM> F;
+            face_point<DIM>(X, fc, qf, F);
+            const double Ni = F.N[i];
+            if constexpr (SYS == FEM_PREDICTION) {
+                if constexpr (DIM == 2) {
+                    for (int j = 0; j < NV; ++j) {
+                        const double u0 = f.U[dof[j]], u1 = f.U[(size_t)f.nD + dof[j]];
+                        M[0][j] = M[0][j] - f.mu * f.dt * Ni * 4.0 / 3.0 * F.g[j][0] * F.n[0] * F.jxw;
+                        r[0] = r[0] + f.mu * f.dt * Ni * (-2.0 / 3.0) * F.g[j][1] * u1 * F.n[0] * F.jxw;
+                        M[1][j] = M[1][j] - f.mu * f.dt * Ni * F.g[j][0] * F.n[0] * F.jxw;
+                        r[1] = r[1] + f.mu * f.dt * Ni * F.g[j][1] * u0 * F.n[0] * F.jxw;
+                    }
+                } else {
+                    double tX[3] = {0.0, 0.0, 0.0}, tY[3] = {0.0, 0.0, 0.0}, tZ[3] = {0.0, 0.0, 0.0};
+                    for (int ii = 0; ii < NV; ++ii) {
+                        const double* g = F.g[ii];
+                        const double v0 = 0.0, v1 = f.U[(size_t)f.nD + dof[ii]], v2 = f.U[(size_t)2 * f.nD + dof[ii]];
+                        tX[0] = tX[0] + ((4.0 / 3.0) * g[0] * v0 - (2.0 / 3.0) * g[1] * v1 - (2.0 / 3.0) * g[2] * v2);
+                        tX[1] = tX[1] + (g[1] * v0 + g[0] * v1);
+                        tX[2] = tX[2] + (g[2] * v0 + g[0] * v2);
+                        tY[0] = tY[0] + (g[1] * v0 + g[0] * v1);
+                        tY[1] = tY[1] + ((-2.0 / 3.0) * g[0] * v0 + (4.0 / 3.0) * g[1] * v1 - (2.0 / 3.0) * g[2] * v2);
+                        tY[2] = tY[2] + (g[2] * v1 + g[1] * v2);
+                        tZ[0] = tZ[0] + (g[2] * v0 + g[0] * v2);
+                        tZ[1] = tZ[1] + (g[2] * v1 + g[1] * v2);
+                        tZ[2] = tZ[2] + ((-2.0 / 3.0) * g[0] * v0 - (2.0 / 3.0) * g[1] * v1 + (4.0 / 3.0) * g[2] * v2);
+                    }
+                    const double aux = f.mu * f.dt * Ni * F.jxw;
+                    const double* T[3] = {tX, tY, tZ};
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        double dot = (aux * T[k][0]) * F.n[0];
+#pragma unroll
+                        for (int d = 1; d < 3; ++d) dot = dot + (aux * T[k][d]) * F.n[d];
+                        r[k] = r[k] + dot;
+                    }
+                }
+            } else if constexpr (SYS == FEM_PRESSURE) {
+                const double coeff = f.rho / f.dt;
+                double Vq[DIM];
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) Vq[k] = 0.0;
+                for (int ii = 0; ii < NV; ++ii)
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) Vq[k] = Vq[k] + F.N[ii] * f.U[(size_t)k * f.nD + dof[ii]];
+                double dot = (coeff * Ni * Vq[0]) * F.n[0];
+#pragma unroll
+                for (int d = 1; d < DIM; ++d) dot = dot + (coeff * Ni * Vq[d]) * F.n[d];
+                r[0] = r[0] - dot * F.jxw;
+            }
+        }
+    }
+}
+
 // One lane per (cell, local row i), 32 / 2^dim cells per warp.  The cell's
 // 2^dim quadrature points are computed once, lane i taking point i, into
 // shared memory; then lane i accumulates row i of the cell's local matrices
@@ -215,6 +384,43 @@ __global__ void __launch_bounds__(FEM_WARPS * 32) k_fem_local(FemArgs f)
     }
 }
 
+// Boundary-face terms, added to the finished volume values of row i of each
+// cell with such faces (the same additions, in the same order, as adding
+// them to the accumulators after the volume loop).
+template <int DIM, int SYS>
+__global__ void __launch_bounds__(128) k_fem_faces(FemArgs f)
+{
+    constexpr int NV = 1 << DIM;
+    constexpr int NS = SYS == FEM_PRESSURE ? 1 : DIM;
+    constexpr int NM = SYS == FEM_PREDICTION ? DIM : 1;
+    const long long total = (long long)f.nC * NV;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long c = t / NV;
+        const int i = (int)(t % NV);
+        const unsigned mk = f.fmask[c];
+        if (!(SYS == FEM_PREDICTION ? (mk & 0xffu) : (mk >> 8))) continue;
+        int dof[NV];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) dof[j] = f.cd[(size_t)c * NV + j];
+        double M[NM][NV], r[NS];
+        double* L = f.local + (size_t)t * NM * NV;
+#pragma unroll
+        for (int m = 0; m < NM; ++m)
+#pragma unroll
+            for (int j = 0; j < NV; ++j) M[m][j] = L[m * NV + j];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) r[k] = f.local_rhs[(size_t)t * NS + k];
+        face_terms<DIM, SYS, NM, NS>(f, c, i, dof, M, r);
+#pragma unroll
+        for (int m = 0; m < NM; ++m)
+#pragma unroll
+            for (int j = 0; j < NV; ++j) L[m * NV + j] = M[m][j];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) f.local_rhs[(size_t)t * NS + k] = r[k];
+    }
+}
+
 // One warp per matrix row (DoF): lane l owns column entry l (in rounds of
 // 32); the row's cell entries are walked in ascending cell order and each
 // adds the local value whose column DoF matches.  The right-hand side of the
@@ -310,8 +516,15 @@ template <int DIM, int SYS>
 static int fem_t(const FemArgs& f, cudaStream_t s)
 {
     k_fem_local<DIM, SYS><<<fem_grid((const void*)k_fem_local<DIM, SYS>, FEM_WARPS * 32), FEM_WARPS * 32, 0, s>>>(f);
+    int n = 2;
+    if constexpr (SYS != FEM_CORRECTION) {
+        if (f.fmask) {
+            k_fem_faces<DIM, SYS><<<fem_grid((const void*)k_fem_faces<DIM, SYS>, 128), 128, 0, s>>>(f);
+            n = 3;
+        }
+    }
     k_fem_gather<DIM, SYS><<<fem_grid((const void*)k_fem_gather<DIM, SYS>, 256), 256, 0, s>>>(f);
-    return 2;
+    return n;
 }
 
 int launch_fem_assemble(int dim, int sys, const FemArgs& f, cudaStream_t s)

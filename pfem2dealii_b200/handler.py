@@ -222,6 +222,18 @@ class ParticleHandler:
         self._ck(self.L.pfem2gpu_fem_pattern(self.h, _ptr(row_ptr), _ptr(cols), n.value, C.byref(n)))
         return row_ptr, cols[: n.value]
 
+    def fem_set_boundary(self, face_ids, velocity_dirichlet=(), pressure_dirichlet=()):
+        """Boundary ids per cell and face (mesh.boundary_face_ids) and the
+        Dirichlet id sets; None clears (no face terms)."""
+        if face_ids is None:
+            self._ck(self.L.pfem2gpu_fem_set_boundary(self.h, None, 0, None, 0, None))
+            return
+        fid = _host(face_ids, np.int32)
+        vd = np.asarray(list(velocity_dirichlet) or [0], np.int32)
+        pd = np.asarray(list(pressure_dirichlet) or [0], np.int32)
+        self._ck(self.L.pfem2gpu_fem_set_boundary(self.h, _ptr(fid), len(velocity_dirichlet), _ptr(vd),
+                                                  len(pressure_dirichlet), _ptr(pd)))
+
     def fem_assemble(self, system, rho, mu, dt, U, U2=None, P=None):
         """One system on host arrays: (A (matrices, nnz), rhs (right-hand sides, n_dofs)).
         PREDICTION: U = solution V, U2 = old solution V; PRESSURE: U = predicted

@@ -298,6 +298,45 @@ def read_unv_native(src, dim=None) -> Mesh:
     return Mesh(d, verts, cells, cells.copy(), verts.shape[0], "unv")
 
 
+def boundary_face_ids(mesh: Mesh, classify=None) -> np.ndarray:
+    """Per cell and face (deal.II face numbering: face 2d has xi_d = 0, face
+    2d+1 has xi_d = 1), the boundary id of a face no other cell shares, -1
+    for interior faces.  ``classify(centre) -> id`` names the boundary part
+    from the face centre; by default the id is the face number of the
+    bounding box side the face lies on (as GridGenerator::hyper_rectangle
+    with colorize), or 2*dim for a face inside the box (an obstacle)."""
+    dim, nv = mesh.dim, mesh.nv
+    faces = {}
+    keys = np.zeros((mesh.n_cells, 2 * dim), dtype=object)
+    for f in range(2 * dim):
+        d, side = f // 2, f % 2
+        loc = [i for i in range(nv) if ((i >> d) & 1) == side]
+        fv = np.sort(mesh.cells[:, loc], axis=1)
+        for c in range(mesh.n_cells):
+            k = tuple(fv[c])
+            keys[c, f] = k
+            faces[k] = faces.get(k, 0) + 1
+    lo, hi = mesh.vertices.min(0), mesh.vertices.max(0)
+    span = np.maximum(hi - lo, 1e-300)
+    out = np.full((mesh.n_cells, 2 * dim), -1, np.int32)
+    for c in range(mesh.n_cells):
+        for f in range(2 * dim):
+            if faces[keys[c, f]] != 1:
+                continue
+            centre = mesh.vertices[list(keys[c, f])].mean(0)
+            if classify is not None:
+                out[c, f] = int(classify(centre))
+                continue
+            bid = 2 * dim
+            for d in range(dim):
+                if abs(centre[d] - lo[d]) <= 1e-9 * span[d]:
+                    bid = 2 * d
+                elif abs(centre[d] - hi[d]) <= 1e-9 * span[d]:
+                    bid = 2 * d + 1
+            out[c, f] = bid
+    return out
+
+
 def write_unv(mesh: Mesh, stream: io.TextIOBase):
     """Write a mesh as UNV datasets 2411/2412 (nodes and quad/hex cells)."""
     lex_to_ucd = [0, 1, 3, 2] if mesh.dim == 2 else [0, 1, 3, 2, 4, 5, 7, 6]

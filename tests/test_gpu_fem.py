@@ -128,3 +128,55 @@ def test_fem_device_call_and_errors():
                                             dr.data_ptr()) == 1
     del dU, dU2, dA, dr
     g.close()
+
+
+BOUNDARY = {  # velocity Dirichlet ids, pressure Dirichlet ids (the rest gets face terms)
+    "channel": ((0, 2, 3), (1,)),
+    "cylinder": ((0, 2, 3, 4), (1,)),
+    "box": ((0, 2, 3, 4, 5), (1,)),
+    "cube": ((0, 1, 2, 3), (4, 5)),
+}
+
+
+@pytest.mark.parametrize("which", ["channel", "cylinder", "box", "cube"])
+def test_fem_face_terms_match_oracle_bit_for_bit(which):
+    """With boundary ids and Dirichlet sets, the prediction and pressure
+    systems carry the boundary-face terms (src/pfem2fem.cpp:320-383,
+    436-449) on the other boundary faces; device and oracle agree bit for
+    bit, and clearing the ids gives the volume-only systems back."""
+    m = _mesh(which)
+    g = _handler(m)
+    fid = M.boundary_face_ids(m)
+    vd, pd = BOUNDARY[which]
+    g.fem_set_boundary(fid, vd, pd)
+    mask = O.fem_face_mask(fid, vd, pd)
+    assert mask.any()
+    pat = O.fem_pattern(m)
+    U, U2, P = _fields(m, 3)
+    for system, kw in ((O.FEM_PREDICTION, dict(U=U, U2=U2)), (O.FEM_PRESSURE, dict(U=U)),
+                       (O.FEM_CORRECTION, dict(U=U, P=P))):
+        A, r = g.fem_assemble(system, RHO, MU, DT, **kw)
+        Ao, ro = O.fem_assemble(m, system, RHO, MU, DT, pattern=pat, face_mask=mask, **kw)
+        assert A.tobytes() == Ao.tobytes(), (system, np.max(np.abs(A - Ao)))
+        assert r.tobytes() == ro.tobytes(), (system, np.max(np.abs(r - ro)))
+    g.fem_set_boundary(None)
+    A, r = g.fem_assemble(O.FEM_PRESSURE, RHO, MU, DT, U=U)
+    Ao, ro = O.fem_assemble(m, O.FEM_PRESSURE, RHO, MU, DT, pattern=pat, U=U)
+    assert A.tobytes() == Ao.tobytes() and r.tobytes() == ro.tobytes()
+    g.close()
+
+
+@pytest.mark.parametrize("which", ["channel", "cylinder", "cube"])
+def test_fem_pressure_face_term_is_the_outflux(which):
+    """With face terms on the whole boundary, the pressure right-hand side
+    sums to -rho/dt times the outflux of the velocity, here u = (x, 0, 0):
+    the domain's volume (the divergence theorem on the discrete normals)."""
+    m = _mesh(which)
+    g = _handler(m)
+    g.fem_set_boundary(M.boundary_face_ids(m), (), ())
+    U = np.zeros((m.dim, m.n_dofs))
+    U[0] = m.vertices[:, 0]
+    _, r = g.fem_assemble(O.FEM_PRESSURE, 1.0, 0.0, 1.0, U=U)
+    vol = float(np.sum(_volumes(m.vertices[m.cells])))
+    assert abs(r.sum() + vol) <= 1e-12 * vol
+    g.close()
