@@ -61,6 +61,21 @@ TRAFFIC_WRITE = 245.1e6  # bytes per launch (115.2 MB read + 129.8 MB written)
 TRAFFIC_ADVECT = 222.8e6  # bytes per launch (123.4 MB read + 99.4 MB written)
 
 
+def reduce_over_ranks(ms, particle_steps, world, device):
+    """Whole-job figures of N replicas: the slowest rank's time (max) and the
+    particle-steps of all ranks (sum).  Every rank calls it once, in the same
+    place."""
+    if world <= 1:
+        return float(ms), float(particle_steps)
+    import torch
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ps = torch.tensor([float(particle_steps)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(ps)
+    return float(t.item()), float(ps.item())
+
+
 def env_rank():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
         os.environ.get("LOCAL_RANK", "0"))
@@ -606,15 +621,7 @@ def main():
         r32 = timed_device_run(ParticleHandler, m, V, Vold, prm, "fp32", args.steps, args.warmup, torch)
         barrier()
     ms = r32["ms"]
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        ps = torch.tensor([float(r32["particle_steps"])], device="cuda")
-        torch.distributed.all_reduce(ps)
-        total_ps = float(ps.item())
-    else:
-        total_ps = float(r32["particle_steps"])
+    ms, total_ps = reduce_over_ranks(ms, r32["particle_steps"], world, "cuda")
     value = total_ps / (ms / 1000.0)
     # FP64 form (plain) and the FP32 vs FP64 error after the same steps
     r64 = timed_device_run(ParticleHandler, m, V, Vold, prm, "fp64", args.steps, args.warmup, torch)
