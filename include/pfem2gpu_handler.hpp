@@ -244,6 +244,14 @@ public:
     }
     pfem2gpu_handle* handle() const { return h_; }
 
+    const Mesh& mesh() const { return mesh_; }
+    // The handle, with the mesh uploaded (for FemSystems and direct C calls).
+    pfem2gpu_handle* handle()
+    {
+        initialize_maps();
+        return h_;
+    }
+
 private:
     template <typename T>
     static T* need(T* p)
@@ -259,6 +267,67 @@ private:
     const double* Vold_ = nullptr;
     double* Vout_ = nullptr;
     std::vector<Particle<dim>> pending_;
+};
+
+// pfem2Fem's assembly methods (src/pfem2fem.cpp:247-510) on the mesh of a
+// ParticleHandler: setup_system's sparsity pattern once, then per step the
+// three systems (volume and boundary-face terms) into caller arrays, as
+// matrices x nnz values on that pattern and right-hand sides x n_dofs.  The
+// constraints and the solves stay with the caller.
+template <int dim>
+class FemSystems {
+public:
+    FemSystems(ParticleHandler<dim>& particles, double rho, double mu)
+        : h_(particles.handle()), rho_(rho), mu_(mu), n_dofs_(particles.mesh().n_dofs)
+    {
+    }
+
+    // DoFTools::make_sparsity_pattern for Q1 (setup_system, :78-94).
+    void setup_system(std::vector<int32_t>& row_ptr, std::vector<int32_t>& cols)
+    {
+        int64_t nnz = 0;
+        check(pfem2gpu_fem_pattern(h_, nullptr, nullptr, 0, &nnz), h_);
+        cols.resize((size_t)nnz);
+        row_ptr.resize((size_t)n_dofs_ + 1);
+        check(pfem2gpu_fem_pattern(h_, row_ptr.data(), cols.data(), nnz, &nnz), h_);
+        nnz_ = nnz;
+    }
+    // Boundary id of every cell face (-1 interior) and the Dirichlet id sets
+    // (getVelocityDirichletBCpatchIDs, getPressureDirichletBCpatchIDs).
+    void set_boundary(const std::vector<int32_t>& face_ids, const std::vector<int32_t>& velocity_dirichlet,
+                      const std::vector<int32_t>& pressure_dirichlet)
+    {
+        check(pfem2gpu_fem_set_boundary(h_, face_ids.data(), (int32_t)velocity_dirichlet.size(),
+                                        velocity_dirichlet.data(), (int32_t)pressure_dirichlet.size(),
+                                        pressure_dirichlet.data()),
+              h_);
+    }
+    // assemble_velocity_prediction (:247-383): dim matrices, dim right-hand sides.
+    void assemble_velocity_prediction(double time_step, const double* V, const double* Vold, double* A, double* rhs)
+    {
+        check(pfem2gpu_fem_assemble(h_, PFEM2GPU_FEM_PREDICTION, rho_, mu_, time_step, V, Vold, nullptr, A, rhs), h_);
+    }
+    // assemble_pressure_equation (:393-449): one matrix, one right-hand side.
+    void assemble_pressure_equation(double time_step, const double* predictionV, double* A, double* rhs)
+    {
+        check(pfem2gpu_fem_assemble(h_, PFEM2GPU_FEM_PRESSURE, rho_, mu_, time_step, predictionV, nullptr, nullptr, A,
+                                    rhs),
+              h_);
+    }
+    // assemble_velocity_correction (:461-510): one matrix, dim right-hand sides.
+    void assemble_velocity_correction(double time_step, const double* predictionV, const double* P, double* A,
+                                      double* rhs)
+    {
+        check(pfem2gpu_fem_assemble(h_, PFEM2GPU_FEM_CORRECTION, rho_, mu_, time_step, predictionV, nullptr, P, A,
+                                    rhs),
+              h_);
+    }
+    int64_t nnz() const { return nnz_; }
+
+private:
+    pfem2gpu_handle* h_;
+    double rho_, mu_;
+    int64_t n_dofs_, nnz_ = 0;
 };
 
 }  // namespace pfem2gpu

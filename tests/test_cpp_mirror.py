@@ -124,3 +124,56 @@ def test_cpp_read_unv_matches_python(tmp_path):
         assert np.array_equal(dofs, cells)
     r = subprocess.run([exe, str(tmp_path / "missing.unv"), str(tmp_path / "x.bin")], capture_output=True, text=True)
     assert r.returncode == 3 and "cannot open" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["cylinder", "cube"])
+def test_cpp_fem_systems_match_oracle(tmp_path, which):
+    """pfem2gpu::FemSystems, driven as pfem2Fem calls its assembly methods
+    (setup_system, then prediction, pressure, correction with boundary
+    ids), gives the oracle's pattern, matrices and right-hand sides bit for
+    bit."""
+    from oracle import oracle as O
+    from pfem2dealii_b200 import mesh as M
+
+    m = M.turek_channel(24, 12, 60) if which == "cylinder" else M.perturbed_cube(6)
+    fid = M.boundary_face_ids(m)
+    vd, pd = ((0, 2, 3, 4), (1,)) if which == "cylinder" else ((0, 1, 2, 3), (4, 5))
+    rng = np.random.default_rng(5)
+    U, U2, P = rng.standard_normal((m.dim, m.n_dofs)), rng.standard_normal((m.dim, m.n_dofs)), \
+        rng.standard_normal(m.n_dofs)
+    rho, mu, dt = 1.3, 0.01, 0.02
+    exe = str(tmp_path / "fem_driver")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "fem_driver.cpp"), "-L", LIBDIR, "-lpfem2gpu",
+           f"-Wl,-rpath,{LIBDIR}", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    src, dst = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    with open(src, "wb") as f:
+        f.write(np.array([m.dim, m.n_cells, m.n_verts, m.n_dofs, len(vd), len(pd)], np.int64).tobytes())
+        f.write(np.array([rho, mu, dt], np.float64).tobytes())
+        for a, t in ((m.vertices, np.float64), (m.cells, np.int32), (m.cell_dofs, np.int32), (fid, np.int32),
+                     (np.array(vd), np.int32), (np.array(pd), np.int32), (U, np.float64), (U2, np.float64),
+                     (P, np.float64)):
+            f.write(np.ascontiguousarray(a, t).tobytes())
+    r = subprocess.run([exe, src, dst], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    raw = open(dst, "rb").read()
+    nnz = int(np.frombuffer(raw[:8], np.int64)[0])
+    o = 8
+    rp = np.frombuffer(raw[o:o + 4 * (m.n_dofs + 1)], np.int32)
+    o += 4 * (m.n_dofs + 1)
+    cols = np.frombuffer(raw[o:o + 4 * nnz], np.int32)
+    o += 4 * nnz
+    orp, ocols = O.fem_pattern(m)
+    assert np.array_equal(rp, orp) and np.array_equal(cols, ocols)
+    mask = O.fem_face_mask(fid, vd, pd)
+    for system, nm, ns, kw in ((O.FEM_PREDICTION, m.dim, m.dim, dict(U=U, U2=U2)), (O.FEM_PRESSURE, 1, 1, dict(U=U)),
+                               (O.FEM_CORRECTION, 1, m.dim, dict(U=U, P=P))):
+        A = np.frombuffer(raw[o:o + 8 * nm * nnz], np.float64).reshape(nm, nnz)
+        o += 8 * nm * nnz
+        rhs = np.frombuffer(raw[o:o + 8 * ns * m.n_dofs], np.float64).reshape(ns, m.n_dofs)
+        o += 8 * ns * m.n_dofs
+        Ao, ro = O.fem_assemble(m, system, rho, mu, dt, pattern=(orp, ocols), face_mask=mask, **kw)
+        assert A.tobytes() == Ao.tobytes() and rhs.tobytes() == ro.tobytes(), system
