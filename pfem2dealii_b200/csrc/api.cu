@@ -84,7 +84,7 @@ struct pfem2gpu_handle {
     // FEM systems: the CSR pattern (built once per mesh), per-(cell, row)
     // local values, and device copies of host inputs/outputs
     struct Fem {
-        int32_t *row_ptr = nullptr, *cols = nullptr;
+        int32_t *row_ptr = nullptr, *cols = nullptr, *con_off = nullptr, *con = nullptr;
         long long nnz = -1;
         double *local = nullptr, *local_rhs = nullptr, *io = nullptr;
         size_t local_n = 0, rhs_n = 0, io_n = 0;
@@ -269,7 +269,8 @@ void free_win_particles(pfem2gpu_handle::Win& W)
 
 void free_fem(pfem2gpu_handle::Fem& F)
 {
-    for (void* p : {(void*)F.row_ptr, (void*)F.cols, (void*)F.local, (void*)F.local_rhs, (void*)F.io, (void*)F.fmask})
+    for (void* p : {(void*)F.row_ptr, (void*)F.cols, (void*)F.con_off, (void*)F.con, (void*)F.local,
+                    (void*)F.local_rhs, (void*)F.io, (void*)F.fmask})
         dfree(p);
     F = pfem2gpu_handle::Fem{};
 }
@@ -1470,6 +1471,8 @@ static int fem_pattern(pfem2gpu_handle* h)
 {
     auto& F = h->fem;
     if (F.nnz >= 0) return PFEM2GPU_OK;
+    const size_t NV = (size_t)1 << h->dim;
+    if ((size_t)h->nC * NV * NV > (size_t)INT32_MAX) return fail(h, PFEM2GPU_ERR_ARG, "mesh too large for the FEM lists");
     const size_t nd = h->nD, ntiles = (nd + WIN_TILE - 1) / WIN_TILE + 1;
     uint32_t *cnt = nullptr, *tsum = nullptr;
     unsigned* err = nullptr;
@@ -1504,10 +1507,29 @@ static int fem_pattern(pfem2gpu_handle* h)
     CK(dalloc(&F.cols, std::max<size_t>(nnz, 1)));
     f.cols = F.cols;
     run(h, "fem_pattern", [&] { return launch_fem_pattern(h->dim, f, true, cnt, err, h->stream); });
+    // contribution lists of the entries (count, scan, fill)
+    const size_t nz = (size_t)nnz, ztiles = (nz + WIN_TILE - 1) / WIN_TILE + 1;
+    uint32_t *zcnt = nullptr, *ztsum = nullptr;
+    CK(dalloc(&zcnt, std::max<size_t>(nz, 1)));
+    CK(dalloc(&ztsum, ztiles));
+    CK(dalloc(&F.con_off, nz + 1));
+    f.con_off = F.con_off;
+    run(h, "fem_pattern", [&] {
+        int n = launch_fem_contrib(h->dim, f, false, zcnt, h->stream);
+        return n + launch_win_scan(zcnt, (uint32_t)nz, ztsum, (uint32_t*)F.con_off, h->stream);
+    });
+    int32_t ncon = 0;
+    CK(cudaMemcpyAsync(&ncon, F.con_off + nz, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    CK(dalloc(&F.con, std::max<size_t>(ncon, 1)));
+    f.con = F.con;
+    run(h, "fem_pattern", [&] { return launch_fem_contrib(h->dim, f, true, zcnt, h->stream); });
     CK(cudaStreamSynchronize(h->stream));
     dfree(cnt);
     dfree(tsum);
     dfree(err);
+    dfree(zcnt);
+    dfree(ztsum);
     F.nnz = nnz;
     return check_async(h);
 }
@@ -1568,6 +1590,8 @@ static int fem_run(pfem2gpu_handle* h, int system, double rho, double mu, double
     f.d2c_ent = h->d2c_ent;
     f.row_ptr = F.row_ptr;
     f.cols = F.cols;
+    f.con_off = F.con_off;
+    f.con = F.con;
     f.rho = rho;
     f.mu = mu;
     f.dt = dt;

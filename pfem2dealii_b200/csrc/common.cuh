@@ -191,6 +191,8 @@ struct FemArgs {
     const int32_t* d2c_ent;
     int32_t* row_ptr;
     int32_t* cols;
+    int32_t* con_off;   // per matrix entry: its contributions, in ascending cell order
+    int32_t* con;       // (cell * NV + local row) * NV + local column
     double rho, mu, dt;
     const double* U;
     const double* U2;

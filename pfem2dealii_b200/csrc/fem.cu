@@ -421,16 +421,14 @@ __global__ void __launch_bounds__(128) k_fem_faces(FemArgs f)
     }
 }
 
-// One warp per matrix row (DoF): lane l owns column entry l (in rounds of
-// 32); the row's cell entries are walked in ascending cell order and each
-// adds the local value whose column DoF matches.  The right-hand side of the
-// row is summed by lane 0 in the same order.
-template <int DIM, int SYS>
-__global__ void __launch_bounds__(256) k_fem_gather(FemArgs f)
+// Contribution lists, built once per mesh: for every matrix entry the local
+// values (cell, local row, local column) that add into it, in ascending cell
+// order -- the order in which a cell loop adds them.  One warp per row, a
+// lane per entry; pass 1 (fill == false) counts, pass 2 writes from con_off.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_fem_contrib(FemArgs f, bool fill, uint32_t* __restrict__ count)
 {
     constexpr int NV = 1 << DIM;
-    constexpr int NS = SYS == FEM_PRESSURE ? 1 : DIM;
-    constexpr int NM = SYS == FEM_PREDICTION ? DIM : 1;
     const int lane = threadIdx.x & 31;
     const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
     for (long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; row < f.nD; row += nwarps) {
@@ -439,27 +437,58 @@ __global__ void __launch_bounds__(256) k_fem_gather(FemArgs f)
         for (int c0 = cb; c0 < ce; c0 += 32) {
             const int pos = c0 + lane;
             const int col = pos < ce ? f.cols[pos] : -1;
-            double acc[NM];
-#pragma unroll
-            for (int m = 0; m < NM; ++m) acc[m] = 0.0;
+            int n = 0, base = (fill && pos < ce) ? f.con_off[pos] : 0;
             for (int k = b; k < e; ++k) {
                 const int ent = f.d2c_ent[k];  // cell * NV + local row
                 const int c = ent / NV;
 #pragma unroll
                 for (int j = 0; j < NV; ++j)
-                    if (f.cd[(size_t)c * NV + j] == col)
-#pragma unroll
-                        for (int m = 0; m < NM; ++m) acc[m] = acc[m] + f.local[((size_t)ent * NM + m) * NV + j];
+                    if (f.cd[(size_t)c * NV + j] == col) {
+                        if (fill) f.con[base + n] = ent * NV + j;
+                        ++n;
+                    }
             }
-            if (pos < ce)
+            if (!fill && pos < ce) count[pos] = (uint32_t)n;
+        }
+    }
+}
+
+// Matrix values: one thread per entry, the sum of its local values in list
+// order.  Right-hand sides: one thread per DoF, its cells in ascending order.
+template <int DIM, int SYS>
+__global__ void __launch_bounds__(256) k_fem_gather(FemArgs f)
+{
+    constexpr int NV = 1 << DIM;
+    constexpr int NS = SYS == FEM_PRESSURE ? 1 : DIM;
+    constexpr int NM = SYS == FEM_PREDICTION ? DIM : 1;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < f.nnz; e += stride) {
+        double acc[NM];
 #pragma unroll
-                for (int m = 0; m < NM; ++m) f.A[(size_t)m * f.nnz + pos] = acc[m];
+        for (int m = 0; m < NM; ++m) acc[m] = 0.0;
+        const int kb = f.con_off[e], ke = f.con_off[e + 1];
+        for (int k = kb; k < ke; ++k) {
+            const int tj = f.con[k];
+            const size_t t = (size_t)(tj / NV);
+            const int j = tj % NV;
+#pragma unroll
+            for (int m = 0; m < NM; ++m) acc[m] = acc[m] + f.local[(t * NM + m) * NV + j];
         }
-        if (lane < NS) {
-            double s = 0.0;
-            for (int k = b; k < e; ++k) s = s + f.local_rhs[(size_t)f.d2c_ent[k] * NS + lane];
-            f.rhs[(size_t)lane * f.nD + row] = s;
+#pragma unroll
+        for (int m = 0; m < NM; ++m) f.A[(size_t)m * f.nnz + e] = acc[m];
+    }
+    for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < f.nD; row += stride) {
+        const int b = f.d2c_off[row], e = f.d2c_off[row + 1];
+        double s[NS];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) s[k] = 0.0;
+        for (int k = b; k < e; ++k) {
+            const size_t t = (size_t)f.d2c_ent[k];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) s[q] = s[q] + f.local_rhs[t * NS + q];
         }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) f.rhs[(size_t)q * f.nD + row] = s[q];
     }
 }
 
@@ -504,6 +533,13 @@ __global__ void k_fem_pattern(FemArgs f, bool fill, uint32_t* __restrict__ count
 int fem_grid(const void* k, int threads) { return occupancy_grid(k, threads); }
 
 }  // namespace
+
+int launch_fem_contrib(int dim, const FemArgs& f, bool fill, uint32_t* count, cudaStream_t s)
+{
+    if (dim == 2) k_fem_contrib<2><<<fem_grid((const void*)k_fem_contrib<2>, 256), 256, 0, s>>>(f, fill, count);
+    else k_fem_contrib<3><<<fem_grid((const void*)k_fem_contrib<3>, 256), 256, 0, s>>>(f, fill, count);
+    return 1;
+}
 
 int launch_fem_pattern(int dim, const FemArgs& f, bool fill, uint32_t* count, unsigned* err, cudaStream_t s)
 {

@@ -74,6 +74,7 @@ int launch_d2c_build(long long nE, int nD, const int32_t* cd, const uint32_t* of
 // fem.cu: the Q1 FEM systems' volume terms
 int launch_fem_pattern(int dim, const FemArgs& f, bool fill, uint32_t* count, unsigned* err, cudaStream_t s);
 int launch_fem_assemble(int dim, int sys, const FemArgs& f, cudaStream_t s);
+int launch_fem_contrib(int dim, const FemArgs& f, bool fill, uint32_t* count, cudaStream_t s);
 
 // misc.cu
 constexpr int SCAN_TILE = 1024;       // cells per tile of the slot-offset scan
