@@ -57,8 +57,8 @@ STEP_BYTES = {"fp32": 5 * (4 + 24) + 8, "fp64": 5 * (4 + 48) + 8}
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # two main kernels, from one ncu capture at time step 11 of this workload with
 # the L2 not flushed between kernels (profiles/duct_fp32_step_traffic.md).
-TRAFFIC_WRITE = 245.1e6  # bytes per launch (115.2 MB read + 129.8 MB written)
-TRAFFIC_ADVECT = 222.8e6  # bytes per launch (123.4 MB read + 99.4 MB written)
+TRAFFIC_WRITE = 244.2e6  # bytes per launch (116.1 MB read + 128.1 MB written)
+TRAFFIC_ADVECT = 222.6e6  # bytes per launch (123.7 MB read + 98.9 MB written)
 
 
 def reduce_over_ranks(ms, particle_steps, world, device):
