@@ -275,6 +275,22 @@ void free_fem(pfem2gpu_handle::Fem& F)
     F = pfem2gpu_handle::Fem{};
 }
 
+// Device scratch of one call, released on every return path.
+struct Scratch {
+    std::vector<void*> p;
+    template <typename T>
+    cudaError_t get(T** ptr, size_t n)
+    {
+        cudaError_t e = dalloc(ptr, n);
+        if (e == cudaSuccess) p.push_back(*ptr);
+        return e;
+    }
+    ~Scratch()
+    {
+        for (void* q : p) dfree(q);
+    }
+};
+
 void free_win_mesh(pfem2gpu_handle::Win& W)
 {
     for (void* p : {(void*)W.tsum, (void*)W.ccnt, (void*)W.cstart, (void*)W.part, (void*)W.U, (void*)W.den,
@@ -1464,22 +1480,21 @@ int pfem2gpu_adjoint(pfem2gpu_handle* h, int32_t steps, int32_t checkpoint_every
     return window_backward_impl(h, gU, g_v0, g_V, g_Vold, true);
 }
 
-// The CSR pattern of the FEM matrices, built on the device once per mesh:
-// per DoF row the DoFs sharing a cell with it (from the DoF -> cell map),
-// ascending.
-static int fem_pattern(pfem2gpu_handle* h)
+// The CSR pattern of the FEM matrices: per DoF row the DoFs sharing a cell
+// with it (from the DoF -> cell map), ascending.
+static int fem_pattern_build(pfem2gpu_handle* h)
 {
     auto& F = h->fem;
-    if (F.nnz >= 0) return PFEM2GPU_OK;
     const size_t NV = (size_t)1 << h->dim;
     if ((size_t)h->nC * NV * NV > (size_t)INT32_MAX) return fail(h, PFEM2GPU_ERR_ARG, "mesh too large for the FEM lists");
     const size_t nd = h->nD, ntiles = (nd + WIN_TILE - 1) / WIN_TILE + 1;
+    Scratch sc;
     uint32_t *cnt = nullptr, *tsum = nullptr;
     unsigned* err = nullptr;
     CK(dalloc(&F.row_ptr, nd + 1));
-    CK(dalloc(&cnt, nd));
-    CK(dalloc(&tsum, ntiles));
-    CK(dalloc(&err, 1));
+    CK(sc.get(&cnt, nd));
+    CK(sc.get(&tsum, ntiles));
+    CK(sc.get(&err, 1));
     CK(cudaMemsetAsync(err, 0, sizeof(unsigned), h->stream));
     FemArgs f{};
     f.nC = h->nC;
@@ -1497,21 +1512,15 @@ static int fem_pattern(pfem2gpu_handle* h)
     CK(cudaMemcpyAsync(&nnz, F.row_ptr + nd, 4, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(&e, err, 4, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    if (e) {
-        dfree(cnt);
-        dfree(tsum);
-        dfree(err);
-        free_fem(F);
-        return fail(h, PFEM2GPU_ERR_ARG, "a DoF couples to more than 64 DoFs");
-    }
+    if (e) return fail(h, PFEM2GPU_ERR_ARG, "a DoF couples to more than 64 DoFs");
     CK(dalloc(&F.cols, std::max<size_t>(nnz, 1)));
     f.cols = F.cols;
     run(h, "fem_pattern", [&] { return launch_fem_pattern(h->dim, f, true, cnt, err, h->stream); });
     // contribution lists of the entries (count, scan, fill)
     const size_t nz = (size_t)nnz, ztiles = (nz + WIN_TILE - 1) / WIN_TILE + 1;
     uint32_t *zcnt = nullptr, *ztsum = nullptr;
-    CK(dalloc(&zcnt, std::max<size_t>(nz, 1)));
-    CK(dalloc(&ztsum, ztiles));
+    CK(sc.get(&zcnt, std::max<size_t>(nz, 1)));
+    CK(sc.get(&ztsum, ztiles));
     CK(dalloc(&F.con_off, nz + 1));
     f.con_off = F.con_off;
     run(h, "fem_pattern", [&] {
@@ -1525,13 +1534,22 @@ static int fem_pattern(pfem2gpu_handle* h)
     f.con = F.con;
     run(h, "fem_pattern", [&] { return launch_fem_contrib(h->dim, f, true, zcnt, h->stream); });
     CK(cudaStreamSynchronize(h->stream));
-    dfree(cnt);
-    dfree(tsum);
-    dfree(err);
-    dfree(zcnt);
-    dfree(ztsum);
-    F.nnz = nnz;
-    return check_async(h);
+    int rc = check_async(h);
+    if (rc == PFEM2GPU_OK) F.nnz = nnz;
+    return rc;
+}
+
+// The CSR pattern of the FEM matrices and the entries' contribution lists,
+// built on the device once per mesh (a failure leaves nothing half built).
+static int fem_pattern(pfem2gpu_handle* h)
+{
+    if (h->fem.nnz >= 0) return PFEM2GPU_OK;
+    uint16_t* keep = h->fem.fmask;  // the boundary ids survive a failed build
+    h->fem.fmask = nullptr;
+    const int rc = fem_pattern_build(h);
+    if (rc != PFEM2GPU_OK) free_fem(h->fem);
+    h->fem.fmask = keep;
+    return rc;
 }
 
 int pfem2gpu_fem_pattern(pfem2gpu_handle* h, int32_t* row_ptr, int32_t* cols, int64_t capacity, int64_t* nnz)
