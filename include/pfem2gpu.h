@@ -145,6 +145,20 @@ int pfem2gpu_fem_assemble_device(pfem2gpu_handle* h, int system, double rho, dou
 /* The same on host arrays (copies in and out, synchronized). */
 int pfem2gpu_fem_assemble(pfem2gpu_handle* h, int system, double rho, double mu, double dt, const double* U,
                           const double* U2, const double* P, double* A, double* rhs);
+/* Dirichlet rows on an assembled system: the effect, summed over the cells,
+ * of AffineConstraints::distribute_local_to_global for constraints
+ * x_r = g_r without coupling (interpolate_boundary_values, and the
+ * inhomogeneities of velocity_prediction_bc, src/pfem2fem.cpp:150-245).  A
+ * constrained row keeps its diagonal A_rr alone and its right-hand side
+ * becomes A_rr g_r; every other row moves A_rc g_c of each constrained
+ * column c (ascending) to its right-hand side and zeroes A_rc.  rows: n
+ * distinct DoFs; values: one set of n values per right-hand side of the
+ * system (right-hand side q uses matrix min(q, matrices - 1)).  The _device
+ * form works on device A and rhs (rows and values are host arrays). */
+int pfem2gpu_fem_constrain(pfem2gpu_handle* h, int system, int32_t n, const int32_t* rows, const double* values,
+                           double* A, double* rhs);
+int pfem2gpu_fem_constrain_device(pfem2gpu_handle* h, int system, int32_t n, const int32_t* rows,
+                                  const double* values, double* dA, double* drhs);
 
 /* seed_particles (src/pfem2particlehandler.cpp:43-109). */
 int pfem2gpu_seed(pfem2gpu_handle* h, const double* V);

@@ -304,3 +304,45 @@ def fem_assemble(mesh, system, rho, mu, dt, U=None, U2=None, P=None, pattern=Non
     if rc:
         raise RuntimeError("pattern misses an entry")
     return A, rhs
+
+
+def fem_constrain(row_ptr, cols, A, rhs, rows, values):
+    """Dirichlet rows on an assembled system, restated: a constrained row
+    keeps its diagonal alone and its right-hand side becomes A_rr g_r; every
+    other row moves A_rc g_c of each constrained column (ascending) to its
+    right-hand side and zeroes A_rc.  Right-hand side q uses matrix
+    min(q, matrices - 1).  Returns new (A, rhs)."""
+    A = np.array(A, dtype=np.float64)
+    rhs = np.array(rhs, dtype=np.float64)
+    values = np.asarray(values, np.float64)
+    nm, ns, nd = A.shape[0], rhs.shape[0], rhs.shape[1]
+    idx = -np.ones(nd, np.int64)
+    idx[np.asarray(rows, np.int64)] = np.arange(len(rows))
+    for r in range(nd):
+        b, e = int(row_ptr[r]), int(row_ptr[r + 1])
+        cs = cols[b:e]
+        if idx[r] >= 0:
+            for q in range(ns):
+                m = min(q, nm - 1)
+                diag = 0.0
+                for k in range(b, e):
+                    if cols[k] == r:
+                        diag = float(A[m, k])
+                rhs[q, r] = diag * float(values[q][idx[r]])
+            for m in range(nm):
+                A[m, b:e][cs != r] = 0.0
+            continue
+        hit = idx[cs] >= 0
+        if not hit.any():
+            continue
+        for q in range(ns):
+            m = min(q, nm - 1)
+            s = float(rhs[q, r])
+            for k in range(b, e):
+                ic = idx[cols[k]]
+                if ic >= 0:
+                    s = s - float(A[m, k]) * float(values[q][ic])
+            rhs[q, r] = s
+        for m in range(nm):
+            A[m, b:e][hit] = 0.0
+    return A, rhs

@@ -89,6 +89,9 @@ struct pfem2gpu_handle {
         double *local = nullptr, *local_rhs = nullptr, *io = nullptr;
         size_t local_n = 0, rhs_n = 0, io_n = 0;
         uint16_t* fmask = nullptr;  // per cell: faces with prediction / pressure face terms
+        int32_t* con_idx = nullptr;  // per DoF: index among the constrained rows, or -1
+        double* con_val = nullptr;
+        size_t con_val_n = 0;
     } fem;
     // differentiated window: checkpoints, final state, projection and adjoint
     // buffers (per-particle arrays sized ncap x segcap, the rest per mesh)
@@ -270,7 +273,7 @@ void free_win_particles(pfem2gpu_handle::Win& W)
 void free_fem(pfem2gpu_handle::Fem& F)
 {
     for (void* p : {(void*)F.row_ptr, (void*)F.cols, (void*)F.con_off, (void*)F.con, (void*)F.local,
-                    (void*)F.local_rhs, (void*)F.io, (void*)F.fmask})
+                    (void*)F.local_rhs, (void*)F.io, (void*)F.fmask, (void*)F.con_idx, (void*)F.con_val})
         dfree(p);
     F = pfem2gpu_handle::Fem{};
 }
@@ -1667,6 +1670,79 @@ int pfem2gpu_fem_set_boundary(pfem2gpu_handle* h, const int32_t* face_ids, int32
         }
     CK(dalloc(&F.fmask, (size_t)h->nC));
     CK(cudaMemcpyAsync(F.fmask, mask.data(), (size_t)h->nC * sizeof(uint16_t), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PFEM2GPU_OK;
+}
+
+static int fem_constrain(pfem2gpu_handle* h, int system, int32_t n, const int32_t* rows, const double* values,
+                         double* dA, double* drhs)
+{
+    int nm, ns;
+    if (!h) return PFEM2GPU_ERR_ARG;
+    if (fem_sizes(h->dim, system, &nm, &ns)) return fail(h, PFEM2GPU_ERR_ARG, "unknown FEM system");
+    if (n < 0 || (n > 0 && (!rows || !values)) || !dA || !drhs) return fail(h, PFEM2GPU_ERR_ARG, "bad constraint arrays");
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "no mesh");
+    int rc = fem_pattern(h);
+    if (rc) return rc;
+    auto& F = h->fem;
+    std::vector<int32_t> idx(h->nD, -1);
+    for (int32_t k = 0; k < n; ++k) {
+        if (rows[k] < 0 || rows[k] >= h->nD) return fail(h, PFEM2GPU_ERR_ARG, "constrained row out of range");
+        if (idx[rows[k]] >= 0) return fail(h, PFEM2GPU_ERR_ARG, "constrained row listed twice");
+        idx[rows[k]] = k;
+    }
+    if (!F.con_idx) CK(dalloc(&F.con_idx, (size_t)h->nD));
+    const size_t nv = std::max<size_t>((size_t)ns * n, 1);
+    if (nv > F.con_val_n) {
+        dfree(F.con_val);
+        F.con_val = nullptr;
+        F.con_val_n = 0;
+        CK(dalloc(&F.con_val, nv));
+        F.con_val_n = nv;
+    }
+    CK(cudaMemcpyAsync(F.con_idx, idx.data(), (size_t)h->nD * 4, cudaMemcpyHostToDevice, h->stream));
+    if (n > 0) CK(cudaMemcpyAsync(F.con_val, values, (size_t)ns * n * 8, cudaMemcpyHostToDevice, h->stream));
+    run(h, "fem_constrain", [&] {
+        return launch_fem_constrain(h->nD, F.nnz, nm, ns, F.row_ptr, F.cols, F.con_idx, n, F.con_val, dA, drhs,
+                                    h->stream);
+    });
+    // the host arrays above must outlive the copies
+    CK(cudaStreamSynchronize(h->stream));
+    return check_async(h);
+}
+
+int pfem2gpu_fem_constrain_device(pfem2gpu_handle* h, int system, int32_t n, const int32_t* rows,
+                                  const double* values, double* dA, double* drhs)
+{
+    return fem_constrain(h, system, n, rows, values, dA, drhs);
+}
+
+int pfem2gpu_fem_constrain(pfem2gpu_handle* h, int system, int32_t n, const int32_t* rows, const double* values,
+                           double* A, double* rhs)
+{
+    int nm, ns;
+    if (!h) return PFEM2GPU_ERR_ARG;
+    if (fem_sizes(h->dim, system, &nm, &ns)) return fail(h, PFEM2GPU_ERR_ARG, "unknown FEM system");
+    if (!A || !rhs) return fail(h, PFEM2GPU_ERR_ARG, "missing matrix or right-hand side");
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "no mesh");
+    int rc = fem_pattern(h);
+    if (rc) return rc;
+    auto& F = h->fem;
+    const size_t na = (size_t)nm * F.nnz, nr = (size_t)ns * h->nD;
+    if (na + nr > F.io_n) {
+        dfree(F.io);
+        F.io = nullptr;
+        F.io_n = 0;
+        CK(dalloc(&F.io, na + nr));
+        F.io_n = na + nr;
+    }
+    double* dA = F.io;
+    double* dr = F.io + na;
+    CK(cudaMemcpyAsync(dA, A, na * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(dr, rhs, nr * 8, cudaMemcpyHostToDevice, h->stream));
+    if ((rc = fem_constrain(h, system, n, rows, values, dA, dr))) return rc;
+    CK(cudaMemcpyAsync(A, dA, na * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(rhs, dr, nr * 8, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return PFEM2GPU_OK;
 }

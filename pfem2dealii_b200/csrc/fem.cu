@@ -530,9 +530,60 @@ __global__ void k_fem_pattern(FemArgs f, bool fill, uint32_t* __restrict__ count
     }
 }
 
+// Dirichlet rows (the effect of AffineConstraints::distribute_local_to_global
+// for constraints without coupling, summed over the cells): one thread per
+// row.  A constrained row keeps its diagonal A_rr and nothing else, its
+// right-hand side becomes A_rr g_r; in every other row each constrained
+// column c, ascending, moves A_rc g_c to the right-hand side and is zeroed.
+// con_val[r] = index of r among the constrained rows or -1; g holds ns
+// value sets (one per right-hand side) of n_con values; right-hand side q
+// uses matrix min(q, nm - 1).
+__global__ void __launch_bounds__(256) k_fem_constrain(int nD, long long nnz, int nm, int ns, const int32_t* row_ptr,
+                                                       const int32_t* cols, const int32_t* con_idx, int n_con,
+                                                       const double* g, double* A, double* rhs)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < nD; r += (long long)gridDim.x * blockDim.x) {
+        const int b = row_ptr[r], e = row_ptr[r + 1];
+        const int ir = con_idx[r];
+        if (ir >= 0) {
+            for (int q = 0; q < ns; ++q) {
+                const int m = q < nm ? q : nm - 1;
+                double diag = 0.0;
+                for (int k = b; k < e; ++k)
+                    if (cols[k] == (int)r) diag = A[(size_t)m * nnz + k];
+                rhs[(size_t)q * nD + r] = diag * g[(size_t)q * n_con + ir];
+            }
+            for (int m = 0; m < nm; ++m)
+                for (int k = b; k < e; ++k)
+                    if (cols[k] != (int)r) A[(size_t)m * nnz + k] = 0.0;
+            continue;
+        }
+        for (int q = 0; q < ns; ++q) {
+            const int m = q < nm ? q : nm - 1;
+            double s = rhs[(size_t)q * nD + r];
+            for (int k = b; k < e; ++k) {
+                const int ic = con_idx[cols[k]];
+                if (ic >= 0) s = s - A[(size_t)m * nnz + k] * g[(size_t)q * n_con + ic];
+            }
+            rhs[(size_t)q * nD + r] = s;
+        }
+        for (int m = 0; m < nm; ++m)
+            for (int k = b; k < e; ++k)
+                if (con_idx[cols[k]] >= 0) A[(size_t)m * nnz + k] = 0.0;
+    }
+}
+
 int fem_grid(const void* k, int threads) { return occupancy_grid(k, threads); }
 
 }  // namespace
+
+int launch_fem_constrain(int nD, long long nnz, int nm, int ns, const int32_t* row_ptr, const int32_t* cols,
+                         const int32_t* con_idx, int n_con, const double* g, double* A, double* rhs, cudaStream_t s)
+{
+    k_fem_constrain<<<fem_grid((const void*)k_fem_constrain, 256), 256, 0, s>>>(nD, nnz, nm, ns, row_ptr, cols, con_idx,
+                                                                                  n_con, g, A, rhs);
+    return 1;
+}
 
 int launch_fem_contrib(int dim, const FemArgs& f, bool fill, uint32_t* count, cudaStream_t s)
 {

@@ -75,6 +75,8 @@ int launch_d2c_build(long long nE, int nD, const int32_t* cd, const uint32_t* of
 int launch_fem_pattern(int dim, const FemArgs& f, bool fill, uint32_t* count, unsigned* err, cudaStream_t s);
 int launch_fem_assemble(int dim, int sys, const FemArgs& f, cudaStream_t s);
 int launch_fem_contrib(int dim, const FemArgs& f, bool fill, uint32_t* count, cudaStream_t s);
+int launch_fem_constrain(int nD, long long nnz, int nm, int ns, const int32_t* row_ptr, const int32_t* cols,
+                         const int32_t* con_idx, int n_con, const double* g, double* A, double* rhs, cudaStream_t s);
 
 // misc.cu
 constexpr int SCAN_TILE = 1024;       // cells per tile of the slot-offset scan

@@ -249,6 +249,18 @@ class ParticleHandler:
                                               *[_ptr(a) for a in keep], _ptr(A), _ptr(rhs)))
         return A[:, : n.value], rhs
 
+    def fem_constrain(self, system, A, rhs, rows, values):
+        """Dirichlet rows (pfem2gpu_fem_constrain) on host copies of an
+        assembled system: returns the constrained (A, rhs).  values: one row
+        of len(rows) values per right-hand side."""
+        A = np.array(A, dtype=np.float64, order="C")
+        rhs = np.array(rhs, dtype=np.float64, order="C")
+        r = np.ascontiguousarray(rows, np.int32)
+        v = np.ascontiguousarray(values, np.float64)
+        self._ck(self.L.pfem2gpu_fem_constrain(self.h, int(system), len(r), _ptr(r) if len(r) else None,
+                                               _ptr(v) if len(r) else None, _ptr(A), _ptr(rhs)))
+        return A, rhs
+
     def vertex_maps(self):
         """The vertex -> cell maps in use: (offsets, cells, dirs (n, dim))."""
         off = np.zeros(self.mesh.n_verts + 1, np.int32)
