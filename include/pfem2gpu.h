@@ -155,6 +155,18 @@ int pfem2gpu_fem_assemble(pfem2gpu_handle* h, int system, double rho, double mu,
  * distinct DoFs; values: one set of n values per right-hand side of the
  * system (right-hand side q uses matrix min(q, matrices - 1)).  The _device
  * form works on device A and rhs (rows and values are host arrays). */
+/* velocity_prediction_bc (src/pfem2fem.cpp:150-245): the values of the
+ * prediction's Dirichlet rows, on the DoFs of the boundary faces in the
+ * velocity Dirichlet set of pfem2gpu_fem_set_boundary: the face integral of
+ * the pressure gradient, times dt / rho, divided by the face integral of the
+ * shape function, plus the Dirichlet velocity of the boundary id (ids[k] ->
+ * velocities[k * dim ..]; of the last such face in cell and face order, as
+ * the reference's map keeps; an id not listed counts as zero).  P: pressure
+ * at the DoFs.  Out: rows (ascending) and values[d * n + k]; NULL arrays
+ * return *n only.  Feed them to pfem2gpu_fem_constrain. */
+int pfem2gpu_fem_velocity_bc(pfem2gpu_handle* h, double rho, double dt, const double* P, int32_t n_ids,
+                             const int32_t* ids, const double* velocities, int32_t* rows, double* values,
+                             int64_t capacity, int64_t* n);
 int pfem2gpu_fem_constrain(pfem2gpu_handle* h, int system, int32_t n, const int32_t* rows, const double* values,
                            double* A, double* rhs);
 int pfem2gpu_fem_constrain_device(pfem2gpu_handle* h, int system, int32_t n, const int32_t* rows,

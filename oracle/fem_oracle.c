@@ -338,3 +338,66 @@ int orc_fem_assemble(int dim, int system, int64_t n_cells, int64_t n_dofs, const
     }
     return 0;
 }
+
+/* velocity_prediction_bc (src/pfem2fem.cpp:150-245) and
+ * fill_velocity_boundary_dofs_list (:128-148): per cell (ascending) and
+ * boundary face in the velocity Dirichlet set (ascending), at each face
+ * point, the pressure gradient sum_j grad N_j p_j times N_i and N_i added to
+ * vertex i; summed into the DoFs in cell order; on DoFs of such faces
+ * value_d = grad_d * (dt / rho) / weight + the velocity of the last such
+ * face's id.  flags[r] = 1 on those DoFs. */
+void orc_fem_velocity_bc(int dim, int64_t n_cells, int64_t n_dofs, const double* cellX, const int32_t* cell_dofs,
+                         const int32_t* face_ids, int n_vd, const int32_t* vd, int n_ids, const int32_t* ids,
+                         const double* velocities, double rho, double dt, const double* P, int32_t* flags,
+                         double* values)
+{
+    const int nv = 1 << dim, nf = 2 * dim;
+    double* pg = calloc((size_t)n_dofs * (dim + 1), sizeof(double));
+    int32_t* last = malloc((size_t)n_dofs * sizeof(int32_t));
+    for (int64_t r = 0; r < n_dofs; ++r) last[r] = -1;
+    double N[8], g[8 * 3], nrm[3], w;
+    for (int64_t c = 0; c < n_cells; ++c) {
+        const double* X = cellX + c * nv * dim;
+        const int32_t* dof = cell_dofs + c * nv;
+        double loc[8][4];
+        int lid[8];
+        memset(loc, 0, sizeof loc);
+        for (int i = 0; i < nv; ++i) lid[i] = -1;
+        for (int f = 0; f < nf; ++f) {
+            const int32_t id = face_ids[c * nf + f];
+            if (id < 0) continue;
+            int isd = 0;
+            for (int k = 0; k < n_vd; ++k) isd |= vd[k] == id;
+            if (!isd) continue;
+            for (int i = 0; i < nv; ++i)
+                if (((i >> (f >> 1)) & 1) == (f & 1)) lid[i] = id;
+            for (int qf = 0; qf < (1 << (dim - 1)); ++qf) {
+                fe_face_point(dim, X, f, qf, N, g, nrm, &w);
+                double gp[3] = {0, 0, 0};
+                for (int j = 0; j < nv; ++j)
+                    for (int d = 0; d < dim; ++d) gp[d] = gp[d] + g[j * 3 + d] * P[dof[j]];
+                for (int i = 0; i < nv; ++i) {
+                    for (int d = 0; d < dim; ++d) loc[i][d] = loc[i][d] + N[i] * gp[d];
+                    loc[i][dim] = loc[i][dim] + N[i];
+                }
+            }
+        }
+        for (int i = 0; i < nv; ++i) {
+            for (int q = 0; q <= dim; ++q) pg[dof[i] * (dim + 1) + q] = pg[dof[i] * (dim + 1) + q] + loc[i][q];
+            if (lid[i] >= 0) last[dof[i]] = lid[i];
+        }
+    }
+    const double coeff = dt / rho;
+    for (int64_t r = 0; r < n_dofs; ++r) {
+        flags[r] = last[r] >= 0;
+        int slot = -1;
+        for (int k = 0; k < n_ids; ++k)
+            if (ids[k] == last[r]) slot = k;
+        for (int d = 0; d < dim; ++d)
+            values[d * n_dofs + r] = last[r] >= 0 ? pg[r * (dim + 1) + d] * coeff / pg[r * (dim + 1) + dim] +
+                                                         (slot >= 0 ? velocities[slot * dim + d] : 0.0)
+                                                   : 0.0;
+    }
+    free(pg);
+    free(last);
+}

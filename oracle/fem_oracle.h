@@ -21,6 +21,11 @@ int orc_fem_assemble(int dim, int system, int64_t n_cells, int64_t n_dofs, const
                      const int32_t* cell_dofs, const int32_t* row_ptr, const int32_t* cols, double rho, double mu,
                      double dt, const double* U, const double* U2, const double* P, const uint16_t* fmask, double* A,
                      double* rhs);
+/* velocity_prediction_bc: flags (n_dofs) and values (dim x n_dofs) of the prediction's Dirichlet rows. */
+void orc_fem_velocity_bc(int dim, int64_t n_cells, int64_t n_dofs, const double* cellX, const int32_t* cell_dofs,
+                         const int32_t* face_ids, int n_vd, const int32_t* vd, int n_ids, const int32_t* ids,
+                         const double* velocities, double rho, double dt, const double* P, int32_t* flags,
+                         double* values);
 #ifdef __cplusplus
 }
 #endif

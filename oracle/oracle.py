@@ -93,6 +93,8 @@ def lib():
         L.orc_fem_pattern.argtypes = [C.c_int, C.c_int64, C.c_int64, ip, P, P]
         L.orc_fem_assemble.argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int64, dp, ip, ip, ip, C.c_double,
                                        C.c_double, C.c_double, P, P, P, P, dp, dp]
+        L.orc_fem_velocity_bc.argtypes = [C.c_int, C.c_int64, C.c_int64, dp, ip, ip, C.c_int, ip, C.c_int, ip, dp,
+                                          C.c_double, C.c_double, dp, ip, dp]
         _lib = L
     return _lib
 
@@ -346,3 +348,20 @@ def fem_constrain(row_ptr, cols, A, rhs, rows, values):
         for m in range(nm):
             A[m, b:e][hit] = 0.0
     return A, rhs
+
+
+def fem_velocity_bc(mesh, face_ids, velocity_dirichlet, velocity_bc, rho, dt, P):
+    """velocity_prediction_bc restated: (rows, values (dim, n)) of the
+    prediction's Dirichlet rows.  velocity_bc maps an id to its velocity."""
+    L = lib()
+    ids = np.asarray(sorted(velocity_bc), np.int32)
+    vel = np.ascontiguousarray([velocity_bc[i] for i in ids], np.float64).reshape(-1)
+    vd = np.asarray(list(velocity_dirichlet), np.int32)
+    flags = np.zeros(mesh.n_dofs, np.int32)
+    vals = np.zeros((mesh.dim, mesh.n_dofs))
+    L.orc_fem_velocity_bc(mesh.dim, mesh.n_cells, mesh.n_dofs, _c(mesh.vertices[mesh.cells], np.float64),
+                          _c(mesh.cell_dofs, np.int32), _c(face_ids, np.int32), len(vd), vd if len(vd) else
+                          np.zeros(1, np.int32), len(ids), ids if len(ids) else np.zeros(1, np.int32),
+                          vel if len(vel) else np.zeros(1), rho, dt, _c(P, np.float64), flags, vals)
+    rows = np.nonzero(flags)[0].astype(np.int32)
+    return rows, np.ascontiguousarray(vals[:, rows])

@@ -125,6 +125,8 @@ def load():
         "pfem2gpu_fem_pattern": [P, dptr, dptr, i64, C.POINTER(i64)],
         "pfem2gpu_fem_set_boundary": [P, dptr, C.c_int32, dptr, C.c_int32, dptr],
         "pfem2gpu_fem_constrain": [P, C.c_int, C.c_int32, dptr, dptr, dptr, dptr],
+        "pfem2gpu_fem_velocity_bc": [P, C.c_double, C.c_double, dptr, C.c_int32, dptr, dptr, dptr, dptr, i64,
+                                     C.POINTER(i64)],
         "pfem2gpu_fem_constrain_device": [P, C.c_int, C.c_int32, dptr, dptr, dptr, dptr],
         "pfem2gpu_fem_assemble_device": [P, C.c_int, C.c_double, C.c_double, C.c_double, dptr, dptr, dptr, dptr,
                                          dptr],

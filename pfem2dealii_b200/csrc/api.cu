@@ -89,6 +89,8 @@ struct pfem2gpu_handle {
         double *local = nullptr, *local_rhs = nullptr, *io = nullptr;
         size_t local_n = 0, rhs_n = 0, io_n = 0;
         uint16_t* fmask = nullptr;  // per cell: faces with prediction / pressure face terms
+        uint8_t* dmask = nullptr;    // per cell: boundary faces in the velocity Dirichlet set
+        int32_t* face_id = nullptr;  // per cell and face: boundary id, -1 interior
         int32_t* con_idx = nullptr;  // per DoF: index among the constrained rows, or -1
         double* con_val = nullptr;
         size_t con_val_n = 0;
@@ -273,7 +275,8 @@ void free_win_particles(pfem2gpu_handle::Win& W)
 void free_fem(pfem2gpu_handle::Fem& F)
 {
     for (void* p : {(void*)F.row_ptr, (void*)F.cols, (void*)F.con_off, (void*)F.con, (void*)F.local,
-                    (void*)F.local_rhs, (void*)F.io, (void*)F.fmask, (void*)F.con_idx, (void*)F.con_val})
+                    (void*)F.local_rhs, (void*)F.io, (void*)F.fmask, (void*)F.con_idx, (void*)F.con_val,
+                    (void*)F.dmask, (void*)F.face_id})
         dfree(p);
     F = pfem2gpu_handle::Fem{};
 }
@@ -1547,11 +1550,18 @@ static int fem_pattern_build(pfem2gpu_handle* h)
 static int fem_pattern(pfem2gpu_handle* h)
 {
     if (h->fem.nnz >= 0) return PFEM2GPU_OK;
-    uint16_t* keep = h->fem.fmask;  // the boundary ids survive a failed build
-    h->fem.fmask = nullptr;
+    auto& F = h->fem;  // the boundary ids survive a failed build
+    uint16_t* keep = F.fmask;
+    uint8_t* keep_d = F.dmask;
+    int32_t* keep_f = F.face_id;
+    F.fmask = nullptr;
+    F.dmask = nullptr;
+    F.face_id = nullptr;
     const int rc = fem_pattern_build(h);
-    if (rc != PFEM2GPU_OK) free_fem(h->fem);
-    h->fem.fmask = keep;
+    if (rc != PFEM2GPU_OK) free_fem(F);
+    F.fmask = keep;
+    F.dmask = keep_d;
+    F.face_id = keep_f;
     return rc;
 }
 
@@ -1649,13 +1659,18 @@ int pfem2gpu_fem_set_boundary(pfem2gpu_handle* h, const int32_t* face_ids, int32
     if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "no mesh");
     auto& F = h->fem;
     dfree(F.fmask);
+    dfree(F.dmask);
+    dfree(F.face_id);
     F.fmask = nullptr;
+    F.dmask = nullptr;
+    F.face_id = nullptr;
     if (!face_ids) return PFEM2GPU_OK;
     if ((n_velocity_dirichlet > 0 && !velocity_dirichlet) || (n_pressure_dirichlet > 0 && !pressure_dirichlet) ||
         n_velocity_dirichlet < 0 || n_pressure_dirichlet < 0)
         return fail(h, PFEM2GPU_ERR_ARG, "bad Dirichlet id list");
     const int nf = 2 * h->dim;
     std::vector<uint16_t> mask(h->nC, 0);
+    std::vector<uint8_t> dmask(h->nC, 0);
     auto in = [](int32_t id, int32_t n, const int32_t* ids) {
         for (int32_t k = 0; k < n; ++k)
             if (ids[k] == id) return true;
@@ -1666,11 +1681,75 @@ int pfem2gpu_fem_set_boundary(pfem2gpu_handle* h, const int32_t* face_ids, int32
             const int32_t id = face_ids[(size_t)c * nf + f];
             if (id < 0) continue;  // interior face
             if (!in(id, n_velocity_dirichlet, velocity_dirichlet)) mask[c] |= (uint16_t)(1u << f);
+            else dmask[c] |= (uint8_t)(1u << f);
             if (!in(id, n_pressure_dirichlet, pressure_dirichlet)) mask[c] |= (uint16_t)(1u << (8 + f));
         }
     CK(dalloc(&F.fmask, (size_t)h->nC));
+    CK(dalloc(&F.dmask, (size_t)h->nC));
+    CK(dalloc(&F.face_id, (size_t)h->nC * nf));
     CK(cudaMemcpyAsync(F.fmask, mask.data(), (size_t)h->nC * sizeof(uint16_t), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(F.dmask, dmask.data(), (size_t)h->nC, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(F.face_id, face_ids, (size_t)h->nC * nf * 4, cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_fem_velocity_bc(pfem2gpu_handle* h, double rho, double dt, const double* P, int32_t n_ids,
+                             const int32_t* ids, const double* velocities, int32_t* rows, double* values,
+                             int64_t capacity, int64_t* n)
+{
+    if (!h || !n || !P || n_ids < 0 || (n_ids > 0 && (!ids || !velocities))) return PFEM2GPU_ERR_ARG;
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "no mesh");
+    auto& F = h->fem;
+    if (!F.dmask) return fail(h, PFEM2GPU_ERR_STATE, "no boundary ids (pfem2gpu_fem_set_boundary)");
+    int rc = fem_pattern(h);
+    if (rc) return rc;
+    const int dim = h->dim, NV = 1 << dim;
+    const size_t nd = h->nD, nloc = (size_t)h->nC * NV;
+    Scratch sc;
+    double *dP = nullptr, *loc = nullptr, *vel = nullptr, *val = nullptr;
+    int32_t *lid = nullptr, *dids = nullptr, *flag = nullptr;
+    CK(sc.get(&dP, nd));
+    CK(sc.get(&loc, nloc * (dim + 1)));
+    CK(sc.get(&lid, nloc));
+    CK(sc.get(&dids, std::max<int32_t>(n_ids, 1)));
+    CK(sc.get(&vel, (size_t)std::max<int32_t>(n_ids, 1) * dim));
+    CK(sc.get(&val, nd * dim));
+    CK(sc.get(&flag, nd));
+    CK(cudaMemcpyAsync(dP, P, nd * 8, cudaMemcpyHostToDevice, h->stream));
+    if (n_ids > 0) {
+        CK(cudaMemcpyAsync(dids, ids, (size_t)n_ids * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(vel, velocities, (size_t)n_ids * dim * 8, cudaMemcpyHostToDevice, h->stream));
+    }
+    FemArgs f{};
+    f.nC = h->nC;
+    f.nD = h->nD;
+    f.cellX = h->cellX;
+    f.cd = h->cd;
+    f.d2c_off = h->d2c_off;
+    f.d2c_ent = h->d2c_ent;
+    run(h, "fem_velocity_bc", [&] {
+        return launch_fem_velocity_bc(dim, f, F.dmask, F.face_id, dP, loc, lid, n_ids, dids, vel, dt / rho, val, flag,
+                                      h->stream);
+    });
+    std::vector<int32_t> hf(nd);
+    std::vector<double> hv(nd * dim);
+    CK(cudaMemcpyAsync(hf.data(), flag, nd * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(hv.data(), val, nd * dim * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if ((rc = check_async(h))) return rc;
+    int64_t m = 0;
+    for (size_t r = 0; r < nd; ++r) m += hf[r] ? 1 : 0;
+    *n = m;
+    if (!rows && !values) return PFEM2GPU_OK;
+    if (capacity < m || !rows || !values) return fail(h, PFEM2GPU_ERR_ARG, "output arrays too small");
+    int64_t k = 0;
+    for (size_t r = 0; r < nd; ++r)
+        if (hf[r]) {
+            rows[k] = (int32_t)r;
+            for (int d = 0; d < dim; ++d) values[(size_t)d * m + k] = hv[(size_t)d * nd + r];
+            ++k;
+        }
     return PFEM2GPU_OK;
 }
 

@@ -573,6 +573,92 @@ __global__ void __launch_bounds__(256) k_fem_constrain(int nD, long long nnz, in
     }
 }
 
+// velocity_prediction_bc (src/pfem2fem.cpp:150-245), per (cell, vertex i):
+// over the cell's velocity-Dirichlet boundary faces (ascending) and their
+// points, the pressure gradient at the point, sum_j grad N_j p_j (j
+// ascending), times N_i, and N_i itself (the weight); and the boundary id of
+// the last such face containing vertex i (-1: none), for the Dirichlet
+// velocity the reference's map keeps.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_fem_bc_local(FemArgs f, const uint8_t* __restrict__ dmask,
+                                                      const int32_t* __restrict__ face_id, const double* __restrict__ P,
+                                                      double* __restrict__ out, int32_t* __restrict__ last_id)
+{
+    constexpr int NV = 1 << DIM;
+    const long long total = (long long)f.nC * NV;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long c = t / NV;
+        const int i = (int)(t % NV);
+        const unsigned faces = dmask[c];
+        double acc[DIM + 1];
+#pragma unroll
+        for (int k = 0; k <= DIM; ++k) acc[k] = 0.0;
+        int lid = -1;
+        if (faces) {
+            double X[NV * DIM];
+#pragma unroll
+            for (int k = 0; k < NV * DIM; ++k) X[k] = f.cellX[(size_t)c * NV * DIM + k];
+            double p[NV];
+#pragma unroll
+            for (int j = 0; j < NV; ++j) p[j] = P[f.cd[(size_t)c * NV + j]];
+            for (int fc = 0; fc < 2 * DIM; ++fc) {
+                if (!((faces >> fc) & 1u)) continue;
+                if ((((i >> (fc >> 1)) & 1) == (fc & 1))) lid = face_id[(size_t)c * 2 * DIM + fc];
+                for (int qf = 0; qf < (1 << (DIM - 1)); ++qf) {
+                    FaceQuad<DIM> F;
+                    face_point<DIM>(X, fc, qf, F);
+                    double g[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) g[d] = 0.0;
+#pragma unroll
+                    for (int j = 0; j < NV; ++j)
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) g[d] = g[d] + F.g[j][d] * p[j];
+                    const double sv = F.N[i];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) acc[d] = acc[d] + sv * g[d];
+                    acc[DIM] = acc[DIM] + sv;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k <= DIM; ++k) out[(size_t)t * (DIM + 1) + k] = acc[k];
+        last_id[t] = lid;
+    }
+}
+
+// Per DoF: the cells' values summed in ascending cell order, then, on a DoF
+// of a Dirichlet face, value_k = grad_k * (dt / rho) / weight + the Dirichlet
+// velocity of the last face's id (flag 1), else flag 0.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_fem_bc_dof(FemArgs f, const double* __restrict__ in,
+                                                    const int32_t* __restrict__ last_id, int n_ids,
+                                                    const int32_t* __restrict__ ids, const double* __restrict__ id_vel,
+                                                    double coeff, double* __restrict__ value, int32_t* __restrict__ flag)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < f.nD; r += (long long)gridDim.x * blockDim.x) {
+        double acc[DIM + 1];
+#pragma unroll
+        for (int k = 0; k <= DIM; ++k) acc[k] = 0.0;
+        int lid = -1;
+        for (int k = f.d2c_off[r]; k < f.d2c_off[r + 1]; ++k) {
+            const size_t t = (size_t)f.d2c_ent[k];
+#pragma unroll
+            for (int q = 0; q <= DIM; ++q) acc[q] = acc[q] + in[t * (DIM + 1) + q];
+            if (last_id[t] >= 0) lid = last_id[t];
+        }
+        int slot = -1;
+        for (int k = 0; k < n_ids; ++k)
+            if (ids[k] == lid) slot = k;
+        flag[r] = lid >= 0 ? 1 : 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+            value[(size_t)d * f.nD + r] =
+                lid >= 0 ? acc[d] * coeff / acc[DIM] + (slot >= 0 ? id_vel[(size_t)slot * DIM + d] : 0.0) : 0.0;
+    }
+}
+
 int fem_grid(const void* k, int threads) { return occupancy_grid(k, threads); }
 
 }  // namespace
@@ -583,6 +669,24 @@ int launch_fem_constrain(int nD, long long nnz, int nm, int ns, const int32_t* r
     k_fem_constrain<<<fem_grid((const void*)k_fem_constrain, 256), 256, 0, s>>>(nD, nnz, nm, ns, row_ptr, cols, con_idx,
                                                                                   n_con, g, A, rhs);
     return 1;
+}
+
+int launch_fem_velocity_bc(int dim, const FemArgs& f, const uint8_t* dmask, const int32_t* face_id, const double* P,
+                           double* local, int32_t* last_id, int n_ids, const int32_t* ids, const double* id_vel,
+                           double coeff, double* value, int32_t* flag, cudaStream_t s)
+{
+    if (dim == 2) {
+        k_fem_bc_local<2><<<fem_grid((const void*)k_fem_bc_local<2>, 128), 128, 0, s>>>(f, dmask, face_id, P, local,
+                                                                                       last_id);
+        k_fem_bc_dof<2><<<fem_grid((const void*)k_fem_bc_dof<2>, 256), 256, 0, s>>>(f, local, last_id, n_ids, ids,
+                                                                                   id_vel, coeff, value, flag);
+    } else {
+        k_fem_bc_local<3><<<fem_grid((const void*)k_fem_bc_local<3>, 128), 128, 0, s>>>(f, dmask, face_id, P, local,
+                                                                                       last_id);
+        k_fem_bc_dof<3><<<fem_grid((const void*)k_fem_bc_dof<3>, 256), 256, 0, s>>>(f, local, last_id, n_ids, ids,
+                                                                                   id_vel, coeff, value, flag);
+    }
+    return 2;
 }
 
 int launch_fem_contrib(int dim, const FemArgs& f, bool fill, uint32_t* count, cudaStream_t s)

@@ -75,6 +75,9 @@ int launch_d2c_build(long long nE, int nD, const int32_t* cd, const uint32_t* of
 int launch_fem_pattern(int dim, const FemArgs& f, bool fill, uint32_t* count, unsigned* err, cudaStream_t s);
 int launch_fem_assemble(int dim, int sys, const FemArgs& f, cudaStream_t s);
 int launch_fem_contrib(int dim, const FemArgs& f, bool fill, uint32_t* count, cudaStream_t s);
+int launch_fem_velocity_bc(int dim, const FemArgs& f, const uint8_t* dmask, const int32_t* face_id, const double* P,
+                           double* local, int32_t* last_id, int n_ids, const int32_t* ids, const double* id_vel,
+                           double coeff, double* value, int32_t* flag, cudaStream_t s);
 int launch_fem_constrain(int nD, long long nnz, int nm, int ns, const int32_t* row_ptr, const int32_t* cols,
                          const int32_t* con_idx, int n_con, const double* g, double* A, double* rhs, cudaStream_t s);
 

@@ -249,6 +249,24 @@ class ParticleHandler:
                                               *[_ptr(a) for a in keep], _ptr(A), _ptr(rhs)))
         return A[:, : n.value], rhs
 
+    def fem_velocity_bc(self, rho, dt, P, velocity_bc):
+        """velocity_prediction_bc: (rows, values (dim, n)) of the prediction's
+        Dirichlet rows; velocity_bc maps a Dirichlet boundary id to its
+        velocity vector."""
+        P = _host(P, np.float64)
+        ids = np.asarray(sorted(velocity_bc), np.int32)
+        vel = np.ascontiguousarray([velocity_bc[i] for i in ids], np.float64).reshape(len(ids), self.dim)
+        n = C.c_int64()
+        args = (_ptr(ids) if len(ids) else None, _ptr(vel) if len(ids) else None)
+        self._ck(self.L.pfem2gpu_fem_velocity_bc(self.h, float(rho), float(dt), _ptr(P), len(ids), *args, None,
+                                                 None, 0, C.byref(n)))
+        rows = np.zeros(max(n.value, 1), np.int32)
+        vals = np.zeros((self.dim, max(n.value, 1)))
+        self._ck(self.L.pfem2gpu_fem_velocity_bc(self.h, float(rho), float(dt), _ptr(P), len(ids), *args, _ptr(rows),
+                                                 _ptr(vals), n.value, C.byref(n)))
+        k = n.value
+        return rows[:k], np.ascontiguousarray(vals.ravel()[: self.dim * k].reshape(self.dim, k))
+
     def fem_constrain(self, system, A, rhs, rows, values):
         """Dirichlet rows (pfem2gpu_fem_constrain) on host copies of an
         assembled system: returns the constrained (A, rhs).  values: one row

@@ -217,3 +217,49 @@ def test_fem_dirichlet_rows_match_oracle_and_hold(which):
             x = spl.spsolve(S.tocsc(), rc[q])
             assert np.allclose(x[rows], vals[q], rtol=1e-10, atol=1e-10)
     g.close()
+
+
+VELOCITY_BC = {  # Dirichlet velocity per boundary id (inflow moves, walls and obstacle still)
+    "channel": {0: (1.0, 0.0), 2: (0.0, 0.0), 3: (0.0, 0.0)},
+    "cylinder": {0: (1.5, 0.0), 2: (0.0, 0.0), 3: (0.0, 0.0), 4: (0.0, 0.0)},
+    "box": {0: (1.0, 0.0, 0.0), 2: (0.0,) * 3, 3: (0.0,) * 3, 4: (0.0,) * 3, 5: (0.0,) * 3},
+    "cube": {0: (0.5, 0.0, 0.0), 1: (0.0,) * 3, 2: (0.0,) * 3, 3: (0.0,) * 3},
+}
+
+
+@pytest.mark.parametrize("which", ["channel", "cylinder", "box", "cube"])
+def test_fem_velocity_bc_matches_oracle_and_linear_pressure(which):
+    """velocity_prediction_bc (src/pfem2fem.cpp:150-245) on the device equals
+    the oracle's rows and values bit for bit; with p = x the face-averaged
+    gradient is (1, 0, 0), so every value is dt / rho e_x plus the Dirichlet
+    velocity of the DoF's last Dirichlet face."""
+    m = _mesh(which)
+    g = _handler(m)
+    fid = M.boundary_face_ids(m)
+    vd, pd = BOUNDARY[which]
+    bc = VELOCITY_BC[which]
+    g.fem_set_boundary(fid, vd, pd)
+    rng = np.random.default_rng(7)
+    P = rng.standard_normal(m.n_dofs)
+    rows, vals = g.fem_velocity_bc(RHO, DT, P, bc)
+    ro, vo = O.fem_velocity_bc(m, fid, vd, bc, RHO, DT, P)
+    assert np.array_equal(rows, ro) and vals.tobytes() == vo.tobytes()
+    rows, vals = g.fem_velocity_bc(RHO, DT, m.vertices[:, 0].copy(), bc)
+    _, vo = O.fem_velocity_bc(m, fid, vd, bc, RHO, DT, m.vertices[:, 0].copy())
+    shift = vals.copy()
+    shift[0] -= DT / RHO
+    allowed = np.array([bc[k] for k in sorted(bc)]).T  # (dim, ids)
+    for k in range(len(rows)):
+        assert any(np.allclose(shift[:, k], allowed[:, j], atol=1e-11) for j in range(allowed.shape[1]))
+    # the whole prediction step: assemble, Dirichlet rows, solve; the rows hold their values
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+
+    rp, cols = g.fem_pattern()
+    U, U2, _ = _fields(m, 8)
+    A, r = g.fem_assemble(O.FEM_PREDICTION, RHO, MU, DT, U=U, U2=U2)
+    A, r = g.fem_constrain(O.FEM_PREDICTION, A, r, rows, vals)
+    for d in range(m.dim):
+        x = spl.spsolve(sp.csr_matrix((A[d], cols, rp), shape=(m.n_dofs,) * 2).tocsc(), r[d])
+        assert np.allclose(x[rows], vals[d], rtol=1e-10, atol=1e-10)
+    g.close()
