@@ -322,6 +322,29 @@ public:
                                     rhs),
               h_);
     }
+    // velocity_prediction_bc (:150-245): the prediction's Dirichlet rows and
+    // their values (values[d * rows.size() + k]) from the pressure P, for the
+    // Dirichlet velocities of the listed boundary ids.
+    void velocity_prediction_bc(double time_step, const double* P, const std::vector<int32_t>& ids,
+                                const std::vector<double>& id_velocities, std::vector<int32_t>& rows,
+                                std::vector<double>& values)
+    {
+        int64_t n = 0;
+        check(pfem2gpu_fem_velocity_bc(h_, rho_, time_step, P, (int32_t)ids.size(), ids.data(), id_velocities.data(),
+                                       nullptr, nullptr, 0, &n),
+              h_);
+        rows.resize((size_t)n);
+        values.resize((size_t)n * dim);
+        check(pfem2gpu_fem_velocity_bc(h_, rho_, time_step, P, (int32_t)ids.size(), ids.data(), id_velocities.data(),
+                                       rows.data(), values.data(), n, &n),
+              h_);
+    }
+    // The constraints' effect on an assembled system (Dirichlet rows).
+    void apply_dirichlet(int system, const std::vector<int32_t>& rows, const std::vector<double>& values, double* A,
+                         double* rhs)
+    {
+        check(pfem2gpu_fem_constrain(h_, system, (int32_t)rows.size(), rows.data(), values.data(), A, rhs), h_);
+    }
     int64_t nnz() const { return nnz_; }
 
 private:

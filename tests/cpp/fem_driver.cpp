@@ -4,7 +4,9 @@
 // n_vel, n_p; double rho, mu, dt; vertices (f64), cell_vertices, cell_dofs,
 // face_ids (i32, n_cells x 2 dim), velocity ids (i32), pressure ids (i32),
 // U, U2 (f64, dim x n_dofs), P (f64).  Output: int64 nnz, row_ptr, cols
-// (i32), then for prediction, pressure, correction: A then rhs (f64).
+// (i32), then for prediction, pressure, correction: A then rhs (f64); then
+// the prediction's Dirichlet rows (int64 n, rows, values) and the constrained
+// prediction A and rhs.
 #include <cstdio>
 #include <vector>
 
@@ -55,6 +57,21 @@ static int run(const std::vector<int64_t>& hd, const std::vector<double>& coef, 
     fwrite(rhs.data(), 8, nD, out);
     fem.assemble_velocity_correction(coef[2], U.data(), P.data(), A.data(), rhs.data());
     fwrite(A.data(), 8, nnz, out);
+    fwrite(rhs.data(), 8, dim * nD, out);
+    // the prediction's boundary values (every velocity-Dirichlet id moves with
+    // velocity (1, 0, 0)) and the constrained prediction system
+    std::vector<double> idv(vid.size() * dim, 0.0);
+    for (size_t k = 0; k < vid.size(); ++k) idv[k * dim] = 1.0;
+    std::vector<int32_t> rows;
+    std::vector<double> vals;
+    fem.velocity_prediction_bc(coef[2], P.data(), vid, idv, rows, vals);
+    fem.assemble_velocity_prediction(coef[2], U.data(), U2.data(), A.data(), rhs.data());
+    fem.apply_dirichlet(PFEM2GPU_FEM_PREDICTION, rows, vals, A.data(), rhs.data());
+    const int64_t nr = (int64_t)rows.size();
+    fwrite(&nr, 8, 1, out);
+    fwrite(rows.data(), 4, rows.size(), out);
+    fwrite(vals.data(), 8, vals.size(), out);
+    fwrite(A.data(), 8, dim * nnz, out);
     fwrite(rhs.data(), 8, dim * nD, out);
     return 0;
 }

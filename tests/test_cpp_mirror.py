@@ -177,3 +177,19 @@ def test_cpp_fem_systems_match_oracle(tmp_path, which):
         o += 8 * ns * m.n_dofs
         Ao, ro = O.fem_assemble(m, system, rho, mu, dt, pattern=(orp, ocols), face_mask=mask, **kw)
         assert A.tobytes() == Ao.tobytes() and rhs.tobytes() == ro.tobytes(), system
+        if system == O.FEM_PREDICTION:
+            Apred, rpred = Ao, ro
+    nr = int(np.frombuffer(raw[o:o + 8], np.int64)[0])
+    o += 8
+    rows = np.frombuffer(raw[o:o + 4 * nr], np.int32)
+    o += 4 * nr
+    vals = np.frombuffer(raw[o:o + 8 * m.dim * nr], np.float64).reshape(m.dim, nr)
+    o += 8 * m.dim * nr
+    bc = {i: (1.0,) + (0.0,) * (m.dim - 1) for i in vd}
+    ro_, vo_ = O.fem_velocity_bc(m, fid, vd, bc, rho, dt, P)
+    assert np.array_equal(rows, ro_) and vals.tobytes() == vo_.tobytes()
+    A = np.frombuffer(raw[o:o + 8 * m.dim * nnz], np.float64).reshape(m.dim, nnz)
+    o += 8 * m.dim * nnz
+    rhs = np.frombuffer(raw[o:o + 8 * m.dim * m.n_dofs], np.float64).reshape(m.dim, m.n_dofs)
+    Ac, rc = O.fem_constrain(orp, ocols, Apred, rpred, rows, vals)
+    assert A.tobytes() == Ac.tobytes() and rhs.tobytes() == rc.tobytes()
