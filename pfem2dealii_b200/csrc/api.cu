@@ -91,6 +91,9 @@ struct pfem2gpu_handle {
         uint16_t* fmask = nullptr;  // per cell: faces with prediction / pressure face terms
         uint8_t* dmask = nullptr;    // per cell: boundary faces in the velocity Dirichlet set
         int32_t* face_id = nullptr;  // per cell and face: boundary id, -1 interior
+        double *bc_P = nullptr, *bc_loc = nullptr, *bc_val = nullptr, *bc_vel = nullptr;  // velocity_bc buffers
+        int32_t *bc_lid = nullptr, *bc_flag = nullptr, *bc_ids = nullptr;
+        int32_t bc_ncap = 0;                // ids the bc_ids / bc_vel buffers hold
         int32_t* con_idx = nullptr;  // per DoF: index among the constrained rows, or -1
         double* con_val = nullptr;
         size_t con_val_n = 0;
@@ -276,7 +279,8 @@ void free_fem(pfem2gpu_handle::Fem& F)
 {
     for (void* p : {(void*)F.row_ptr, (void*)F.cols, (void*)F.con_off, (void*)F.con, (void*)F.local,
                     (void*)F.local_rhs, (void*)F.io, (void*)F.fmask, (void*)F.con_idx, (void*)F.con_val,
-                    (void*)F.dmask, (void*)F.face_id})
+                    (void*)F.dmask, (void*)F.face_id, (void*)F.bc_P, (void*)F.bc_loc, (void*)F.bc_val,
+                    (void*)F.bc_vel, (void*)F.bc_lid, (void*)F.bc_flag, (void*)F.bc_ids})
         dfree(p);
     F = pfem2gpu_handle::Fem{};
 }
@@ -1706,16 +1710,31 @@ int pfem2gpu_fem_velocity_bc(pfem2gpu_handle* h, double rho, double dt, const do
     if (rc) return rc;
     const int dim = h->dim, NV = 1 << dim;
     const size_t nd = h->nD, nloc = (size_t)h->nC * NV;
-    Scratch sc;
-    double *dP = nullptr, *loc = nullptr, *vel = nullptr, *val = nullptr;
-    int32_t *lid = nullptr, *dids = nullptr, *flag = nullptr;
-    CK(sc.get(&dP, nd));
-    CK(sc.get(&loc, nloc * (dim + 1)));
-    CK(sc.get(&lid, nloc));
-    CK(sc.get(&dids, std::max<int32_t>(n_ids, 1)));
-    CK(sc.get(&vel, (size_t)std::max<int32_t>(n_ids, 1) * dim));
-    CK(sc.get(&val, nd * dim));
-    CK(sc.get(&flag, nd));
+    // buffers kept with the mesh (the call comes once per time step)
+    if (!F.bc_P || !F.bc_loc || !F.bc_lid || !F.bc_val || !F.bc_flag) {
+        for (void** q : {(void**)&F.bc_P, (void**)&F.bc_loc, (void**)&F.bc_lid, (void**)&F.bc_val, (void**)&F.bc_flag}) {
+            dfree(*q);
+            *q = nullptr;
+        }
+        CK(dalloc(&F.bc_P, nd));
+        CK(dalloc(&F.bc_loc, nloc * (dim + 1)));
+        CK(dalloc(&F.bc_lid, nloc));
+        CK(dalloc(&F.bc_val, nd * dim));
+        CK(dalloc(&F.bc_flag, nd));
+    }
+    if (n_ids > F.bc_ncap || !F.bc_ids) {
+        dfree(F.bc_ids);
+        dfree(F.bc_vel);
+        F.bc_ids = nullptr;
+        F.bc_vel = nullptr;
+        F.bc_ncap = 0;
+        const int32_t cap = std::max<int32_t>(n_ids, 16);
+        CK(dalloc(&F.bc_ids, (size_t)cap));
+        CK(dalloc(&F.bc_vel, (size_t)cap * dim));
+        F.bc_ncap = cap;
+    }
+    double *dP = F.bc_P, *loc = F.bc_loc, *vel = F.bc_vel, *val = F.bc_val;
+    int32_t *lid = F.bc_lid, *dids = F.bc_ids, *flag = F.bc_flag;
     CK(cudaMemcpyAsync(dP, P, nd * 8, cudaMemcpyHostToDevice, h->stream));
     if (n_ids > 0) {
         CK(cudaMemcpyAsync(dids, ids, (size_t)n_ids * 4, cudaMemcpyHostToDevice, h->stream));
