@@ -788,7 +788,10 @@ __device__ __forceinline__ void write_cell_fast(const StepArgs& a, WrWarp<DIM, R
     reset_cell(a, c, lane);
 }
 
-template <int DIM, typename Real>
+// BULK: stage each chunk's old slots by bulk copies (meshes whose chunks of
+// CHC cells usually fit the stage); else by plain loads (a kernel without the
+// bulk-copy code, faster where the chunks are too large to stage anyway).
+template <int DIM, typename Real, bool BULK>
 __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
 {
     pdl_entry();
@@ -803,7 +806,7 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
     const int apply = a.apply_counts, maxpp = a.pp.maxpp;
     unsigned long long removed = 0;
     uint32_t err = 0;
-    if (lane == 0) {
+    if (BULK && lane == 0) {
         mbar_init(&w.bar, 1);
         mbar_fence_init();
     }
@@ -833,9 +836,23 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
         // the chunk's old slot range [S, E), staged by bulk copies of whole
         // 16-byte pieces [SA, EA) (the capacity is a multiple of 4 slots)
         const uint32_t S = __shfl_sync(0xffffffffu, csl, 0), E = __shfl_sync(0xffffffffu, csl, ncell);
-        const uint32_t SA = S & ~3u, EA = (E + 3u) & ~3u;
+        const uint32_t SA = BULK ? (S & ~3u) : S, EA = BULK ? ((E + 3u) & ~3u) : E;
         bool staged = stage_ok && EA - SA <= (uint32_t)UCAP;
-        if (staged && EA > SA) {
+        if constexpr (!BULK) {
+            if (staged) {
+                for (uint32_t j = lane; j < E - S; j += 32) {
+                    const uint32_t i = S + j;
+                    w.key[j] = a.key[i];
+                    w.id[j] = a.S0.id[i];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        w.xi[d][j] = ldr<Real>(a.T.xi[d], i);
+                        w.v[d][j] = ldr<Real>(a.T.v[d], i);
+                        if constexpr (WrCfg<DIM, Real>::HX) w.x[d][j] = ldr<double>(a.T.x[d], i);
+                    }
+                }
+            }
+        } else if (staged && EA > SA) {
             const uint32_t nb = EA - SA;
             if (lane == 0) {
                 fence_proxy_async();  // the previous chunk's reads of the stage come first

@@ -75,8 +75,13 @@ template <int DIM>
 static int write32_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = WR_WARPS * (int)sizeof(WrWarp<DIM, float>);
-    static const int grid = smem_grid32(k_write<DIM, float>, WR_WARPS * 32, smem);
-    return launch_pdl(k_write<DIM, float>, grid, WR_WARPS * 32, smem, s, a);
+    // bulk-copy staging where a chunk of cells at the seeding density fits the stage
+    if (WrCfg<DIM, float>::CHC * a.pp.npart <= WrCfg<DIM, float>::UCAP) {
+        static const int grid = smem_grid32(k_write<DIM, float, true>, WR_WARPS * 32, smem);
+        return launch_pdl(k_write<DIM, float, true>, grid, WR_WARPS * 32, smem, s, a);
+    }
+    static const int grid = smem_grid32(k_write<DIM, float, false>, WR_WARPS * 32, smem);
+    return launch_pdl(k_write<DIM, float, false>, grid, WR_WARPS * 32, smem, s, a);
     return 1;
 }
 

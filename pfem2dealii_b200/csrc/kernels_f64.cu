@@ -141,8 +141,13 @@ template <int DIM>
 static int write_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = WR_WARPS * (int)sizeof(WrWarp<DIM, double>);
-    static const int grid = smem_grid(k_write<DIM, double>, WR_WARPS * 32, smem);
-    return launch_pdl(k_write<DIM, double>, grid, WR_WARPS * 32, smem, s, a);
+    // bulk-copy staging where a chunk of cells at the seeding density fits the stage
+    if (WrCfg<DIM, double>::CHC * a.pp.npart <= WrCfg<DIM, double>::UCAP) {
+        static const int grid = smem_grid(k_write<DIM, double, true>, WR_WARPS * 32, smem);
+        return launch_pdl(k_write<DIM, double, true>, grid, WR_WARPS * 32, smem, s, a);
+    }
+    static const int grid = smem_grid(k_write<DIM, double, false>, WR_WARPS * 32, smem);
+    return launch_pdl(k_write<DIM, double, false>, grid, WR_WARPS * 32, smem, s, a);
     return 1;
 }
 

@@ -214,11 +214,13 @@ def test_vector_order_oracle_agrees_on_counts():
         assert o.stats()[k] == g.stats()[k]
 
 
-@pytest.mark.parametrize("which", ["channel", "duct", "cylinder"])
+@pytest.mark.parametrize("which", ["channel", "duct", "cylinder", "cube"])
 def test_fp32_error_against_fp64_oracle(which):
+    # the cube seeds 64 particles per cell: its write pass stages by plain loads
     c = {"channel": lambda: cases.channel(),
          "duct": lambda: cases.duct(32, 8, 8, dt=0.02),
-         "cylinder": lambda: cases.cylinder(24, 12, 60, dt=2e-3)}[which]()
+         "cylinder": lambda: cases.cylinder(24, 12, 60, dt=2e-3),
+         "cube": lambda: cases.cube(6, q=(4, 4, 4), dt=0.05)}[which]()
     o, g = make(c, precision="fp32")
     o.seed(c.V)
     g.seed_particles(c.V)
@@ -244,14 +246,15 @@ def test_vtu_output(tmp_path):
     assert (tmp_path / "particles-03.pvtu").exists()
 
 
+@pytest.mark.parametrize("which", ["duct", "cube"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_step_device_graph_replay(precision):
+def test_step_device_graph_replay(precision, which):
     """pfem2gpu_step_device (eager first call, captured second, replayed
     afterwards) gives the oracle's particles, bit-exact in FP64; a new output
     pointer re-captures; the result matches the separate host calls."""
     import torch
 
-    c = cases.duct(32, 8, 8, dt=0.05)
+    c = cases.duct(32, 8, 8, dt=0.05) if which == "duct" else cases.cube(6, q=(4, 4, 4), dt=0.05)
     o, g = make(c, precision)
     _, h = make(c, precision)
     o.seed(c.V)
