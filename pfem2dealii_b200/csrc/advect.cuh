@@ -736,10 +736,9 @@ __global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
 // Queued FP32 particles: FP64 relocation of sub-step s (x = F(xi) + u dt_p,
 // own cell first, then the vertex-patch search), then the remaining
 // sub-steps in FP32 (relocating in FP64 again whenever needed).
-template <int DIM, bool AFF = false>
-__global__ void __launch_bounds__(128) k_cross32(StepArgs a)
+template <int DIM, bool AFF>
+__device__ __forceinline__ void cross32(const StepArgs& a)
 {
-    pdl_entry();
     const uint32_t nq = *a.nxq < a.capacity ? *a.nxq : a.capacity;
     const MeshDev& m = a.mesh;
     AdvCounters k;
@@ -785,6 +784,23 @@ __global__ void __launch_bounds__(128) k_cross32(StepArgs a)
         else k.lost++;
     }
     flush_counters(a, k);
+}
+
+template <int DIM, bool AFF = false>
+__global__ void __launch_bounds__(128) k_cross32(StepArgs a)
+{
+    pdl_entry();
+    cross32<DIM, AFF>(a);
+}
+
+// The same for 2D meshes with non-affine cells (many crossers, each a chain
+// of dependent loads): 6 blocks per SM (80 registers, a few spills); more
+// blocks cost the 3D forms about 10 %.
+template <int DIM>
+__global__ void __launch_bounds__(128, 6) k_cross32_occ(StepArgs a)
+{
+    pdl_entry();
+    cross32<DIM, false>(a);
 }
 
 }  // namespace pfem2

@@ -55,7 +55,10 @@ template <int DIM>
 static int cross32_t(const StepArgs& a, cudaStream_t s)
 {
     if (a.mesh.all_affine) return launch_pdl(k_cross32<DIM, true>, PFEM2_GRID((k_cross32<DIM, true>), 128), 128, 0, s, a);
-    return launch_pdl(k_cross32<DIM, false>, PFEM2_GRID((k_cross32<DIM, false>), 128), 128, 0, s, a);
+    if constexpr (DIM == 2)
+        return launch_pdl(k_cross32_occ<DIM>, PFEM2_GRID((k_cross32_occ<DIM>), 128), 128, 0, s, a);
+    else
+        return launch_pdl(k_cross32<DIM, false>, PFEM2_GRID((k_cross32<DIM, false>), 128), 128, 0, s, a);
 }
 
 int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s)
