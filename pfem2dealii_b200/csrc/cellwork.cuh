@@ -623,11 +623,11 @@ __device__ __forceinline__ void write_cell_simple(const StepArgs& a, WrWarp<DIM,
     reset_cell(a, c, lane);
 }
 
-// Fast path of one cell (at most 64 old slots + arrivals and 64 output
+// Fast path of one cell (at most 96 old slots + arrivals and 96 output
 // slots), R rounds of the warp: virtual slots u = 32 r + lane, u < L the
 // cell's old slots (a stayer where its key is c), L <= u < L + na the
-// arrivals.  R = 1 when L + na <= 32, so one-round cells issue no second
-// round.
+// arrivals.  R = ceil((L + na) / 32), so a cell issues only the rounds it
+// fills.
 template <int DIM, typename Real, int R>
 __device__ __forceinline__ void write_cell_fast(const StepArgs& a, WrWarp<DIM, Real>& w, uint32_t c, uint32_t s0,
                                                 uint32_t L, uint32_t na, uint32_t h, uint32_t off, uint32_t ub,
@@ -706,19 +706,24 @@ __device__ __forceinline__ void write_cell_fast(const StepArgs& a, WrWarp<DIM, R
     // order: stayers (slot order), then arrivals by key
     const unsigned ltm = (1u << lane) - 1u;
     uint32_t seq[R];
-    seq[0] = is_stay[0] ? (uint32_t)__popc(stm[0] & ltm) : ns + (uint32_t)lane - L;
-    if constexpr (R == 2)
-        seq[R - 1] = is_stay[R - 1] ? (uint32_t)(__popc(stm[0]) + __popc(stm[R - 1] & ltm))
-                                    : ns + 32u + (uint32_t)lane - L;
+    uint32_t before = 0;  // stayers in the earlier rounds
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        seq[r] = is_stay[r] ? before + (uint32_t)__popc(stm[r] & ltm) : ns + 32u * r + (uint32_t)lane - L;
+        before += (uint32_t)__popc(stm[r]);
+    }
     if (na > 1) {
         uint32_t ar[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) ar[r] = 0u;
         for (uint32_t t = 0; t < na; ++t) {
             const uint32_t u2 = L + t;
-            const uint32_t k0 = __shfl_sync(0xffffffffu, key[0], (int)(u2 & 31u));
-            const uint32_t k1 = R == 2 ? __shfl_sync(0xffffffffu, key[R - 1], (int)(u2 & 31u)) : 0u;
-            const uint32_t kl = (u2 >> 5) ? k1 : k0;
+            uint32_t kl = 0u;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t kr = __shfl_sync(0xffffffffu, key[r], (int)(u2 & 31u));
+                if ((u2 >> 5) == (uint32_t)r) kl = kr;
+            }
 #pragma unroll
             for (int r = 0; r < R; ++r) ar[r] += (kl < key[r]) ? 1u : 0u;
         }
@@ -900,8 +905,8 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
                 __syncwarp();
                 continue;
             }
-            // Cells beyond 64 particles take the general path.
-            if (!(L + na <= 64 && ub <= 64)) {
+            // Cells beyond 96 particles take the general path.
+            if (!(L + na <= 96 && ub <= 96)) {
                 const uint2 gr = write_cell_general<DIM, Real>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0,
                                                                lane);
                 removed += gr.x;
@@ -911,7 +916,10 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
                 __syncwarp();
                 continue;
             }
-            if (L + na > 32)
+            if (L + na > 64)
+                write_cell_fast<DIM, Real, 3>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0, SA, staged, lane,
+                                              removed, err);
+            else if (L + na > 32)
                 write_cell_fast<DIM, Real, 2>(a, w, c, s0, L, na, h, off, ub, nseed_expect, sb, id0, SA, staged, lane,
                                               removed, err);
             else
