@@ -20,7 +20,7 @@ constexpr int MAX_CAND = 64;   // cells around one vertex tried by the relocatio
 constexpr int REG_CAND = 12;   // FP32 form on affine meshes: candidates kept in registers
 constexpr int NPE_MAX = 256;   // extended cell parts (q0+1)(q1+1)(q2+1)
 constexpr int OCCW_MAX = 4;    // 64-bit part-occupancy words per cell
-constexpr int ARRCAP = 16;     // arrival slots per cell before the overflow list
+constexpr int ARRCAP = 32;     // arrival slots per cell before the overflow list
 constexpr int CELL_WARPS = 4;  // warps per block of the warp-per-cell helper kernels
 constexpr int KEY_CACHE = 128; // (part, key) pairs cached per warp on the general path
 constexpr int ADV_CH = 768;    // particles per staged chunk of the FP32 advect pass

@@ -100,6 +100,17 @@ def test_fp64_perturbed_cube_many_particles_per_cell():
     run_fp64(c, 6)
 
 
+def test_fp64_many_arrivals_and_cells_beyond_64_particles():
+    """64 particles per cell and a time step that carries particles across
+    much of a cell: more than 32 arrivals into a cell (the overflow list
+    beyond the per-cell arrival slots) and cells of more than 64 old slots
+    plus arrivals (the write pass's three-round and general paths), with
+    removals."""
+    c = cases.channel(32, 8, q=(8, 8), maxpp=5, dt=0.1)
+    o, g = run_fp64(c, 8)
+    assert g.stats()["removed"] > 0
+
+
 @pytest.mark.parametrize("q,maxpp", [((6, 6), 1), ((7, 7), 0)])
 def test_fp64_cells_of_33_to_64_particles(q, maxpp):
     """36 or 49 particles per cell: the write pass's two-round path (more
