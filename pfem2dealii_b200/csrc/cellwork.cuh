@@ -319,7 +319,8 @@ __device__ __forceinline__ void partial_pairs32(float (*tr)[TRW], bool active, c
 template <int DIM, typename Real>
 struct WrCfg {
     static constexpr bool HX = std::is_same<Real, double>::value;
-    static constexpr int CHC = WR_CHC;   // cells per chunk
+    static constexpr int CHC = WR_CHC;   // cells per chunk on affine meshes
+    static constexpr int CHC_UNEVEN = 2; // on other meshes (cells differ more in work)
     static constexpr int UCAP = 128;     // staged particles per chunk
 };
 
@@ -796,11 +797,11 @@ __device__ __forceinline__ void write_cell_fast(const StepArgs& a, WrWarp<DIM, R
 // BULK: stage each chunk's old slots by bulk copies (meshes whose chunks of
 // CHC cells usually fit the stage); else by plain loads (a kernel without the
 // bulk-copy code, faster where the chunks are too large to stage anyway).
-template <int DIM, typename Real, bool BULK>
+template <int DIM, typename Real, bool BULK, int CHC>
 __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
 {
     pdl_entry();
-    constexpr int CHC = WrCfg<DIM, Real>::CHC, UCAP = WrCfg<DIM, Real>::UCAP;
+    constexpr int UCAP = WrCfg<DIM, Real>::UCAP;
     extern __shared__ __align__(16) unsigned char wr_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     WrWarp<DIM, Real>& w = reinterpret_cast<WrWarp<DIM, Real>*>(wr_raw)[warp];

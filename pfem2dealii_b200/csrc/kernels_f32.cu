@@ -74,18 +74,27 @@ int launch_cross(int dim, int prec, const StepArgs& a, cudaStream_t s)
     return dim == 2 ? cross32_t<2>(a, s) : cross32_t<3>(a, s);
 }
 
-template <int DIM>
-static int write32_t(const StepArgs& a, cudaStream_t s)
+template <int DIM, int CHC>
+static int write32_c(const StepArgs& a, cudaStream_t s)
 {
     const int smem = WR_WARPS * (int)sizeof(WrWarp<DIM, float>);
     // bulk-copy staging where a chunk of cells at the seeding density fits the stage
-    if (WrCfg<DIM, float>::CHC * a.pp.npart <= WrCfg<DIM, float>::UCAP) {
-        static const int grid = smem_grid32(k_write<DIM, float, true>, WR_WARPS * 32, smem);
-        return launch_pdl(k_write<DIM, float, true>, grid, WR_WARPS * 32, smem, s, a);
+    if (CHC * a.pp.npart <= WrCfg<DIM, float>::UCAP) {
+        static const int grid = smem_grid32(k_write<DIM, float, true, CHC>, WR_WARPS * 32, smem);
+        return launch_pdl(k_write<DIM, float, true, CHC>, grid, WR_WARPS * 32, smem, s, a);
     }
-    static const int grid = smem_grid32(k_write<DIM, float, false>, WR_WARPS * 32, smem);
-    return launch_pdl(k_write<DIM, float, false>, grid, WR_WARPS * 32, smem, s, a);
-    return 1;
+    static const int grid = smem_grid32(k_write<DIM, float, false, CHC>, WR_WARPS * 32, smem);
+    return launch_pdl(k_write<DIM, float, false, CHC>, grid, WR_WARPS * 32, smem, s, a);
+}
+
+// Chunks of 4 cells on affine meshes; of 2 on the others (graded and
+// unstructured meshes, whose cells differ most in particles and arrivals:
+// smaller chunks spread the busiest cells over more warps).
+template <int DIM>
+static int write32_t(const StepArgs& a, cudaStream_t s)
+{
+    if (a.mesh.all_affine) return write32_c<DIM, WrCfg<DIM, float>::CHC>(a, s);
+    return write32_c<DIM, WrCfg<DIM, float>::CHC_UNEVEN>(a, s);
 }
 
 int launch_write(int dim, int prec, const StepArgs& a, cudaStream_t s)

@@ -137,18 +137,27 @@ int launch64_cross(int dim, const StepArgs& a, cudaStream_t s)
     return 1;
 }
 
-template <int DIM>
-static int write_t(const StepArgs& a, cudaStream_t s)
+template <int DIM, int CHC>
+static int write_c(const StepArgs& a, cudaStream_t s)
 {
     const int smem = WR_WARPS * (int)sizeof(WrWarp<DIM, double>);
     // bulk-copy staging where a chunk of cells at the seeding density fits the stage
-    if (WrCfg<DIM, double>::CHC * a.pp.npart <= WrCfg<DIM, double>::UCAP) {
-        static const int grid = smem_grid(k_write<DIM, double, true>, WR_WARPS * 32, smem);
-        return launch_pdl(k_write<DIM, double, true>, grid, WR_WARPS * 32, smem, s, a);
+    if (CHC * a.pp.npart <= WrCfg<DIM, double>::UCAP) {
+        static const int grid = smem_grid(k_write<DIM, double, true, CHC>, WR_WARPS * 32, smem);
+        return launch_pdl(k_write<DIM, double, true, CHC>, grid, WR_WARPS * 32, smem, s, a);
     }
-    static const int grid = smem_grid(k_write<DIM, double, false>, WR_WARPS * 32, smem);
-    return launch_pdl(k_write<DIM, double, false>, grid, WR_WARPS * 32, smem, s, a);
-    return 1;
+    static const int grid = smem_grid(k_write<DIM, double, false, CHC>, WR_WARPS * 32, smem);
+    return launch_pdl(k_write<DIM, double, false, CHC>, grid, WR_WARPS * 32, smem, s, a);
+}
+
+// Chunks of 4 cells on affine meshes; of 2 on the others (graded and
+// unstructured meshes, whose cells differ most in particles and arrivals:
+// smaller chunks spread the busiest cells over more warps).
+template <int DIM>
+static int write_t(const StepArgs& a, cudaStream_t s)
+{
+    if (a.mesh.all_affine) return write_c<DIM, WrCfg<DIM, double>::CHC>(a, s);
+    return write_c<DIM, WrCfg<DIM, double>::CHC_UNEVEN>(a, s);
 }
 
 int launch64_write(int dim, const StepArgs& a, cudaStream_t s)
