@@ -177,6 +177,13 @@ int pfem2gpu_seed(pfem2gpu_handle* h, const double* V);
 /* correct_particle_velocity (:112-139): v += sum N_i (V - Vold)_i; applied
  * fused with the next move, or before any call that reads particles. */
 int pfem2gpu_correct(pfem2gpu_handle* h, const double* V, const double* Vold);
+/* correct_particle_velocity with Vold = the handle's last projection
+ * (pfem2gpu_project / pfem2gpu_step_device), which stays on the device: the
+ * reference's data flow, where fem_step copies the projected velocity into
+ * the old solution (src/pfem2fem.cpp:523-524) before it solves for the new
+ * one (src/pfem2solver.cpp:162-165), so only V crosses the boundary.
+ * PFEM2GPU_ERR_STATE before the first projection. */
+int pfem2gpu_correct_from_projection(pfem2gpu_handle* h, const double* V);
 /* move_particles (:142-171): sub-steps + relocation + count correction.
  * V == NULL reuses the velocity of the preceding seed/correct/move call. */
 int pfem2gpu_move(pfem2gpu_handle* h, const double* V);
@@ -188,8 +195,12 @@ int pfem2gpu_seed_device(pfem2gpu_handle* h, const double* dV);
 int pfem2gpu_correct_device(pfem2gpu_handle* h, const double* dV, const double* dVold);
 int pfem2gpu_move_device(pfem2gpu_handle* h, const double* dV);
 int pfem2gpu_project_device(pfem2gpu_handle* h, double* dV_out);
+int pfem2gpu_correct_from_projection_device(pfem2gpu_handle* h, const double* dV);
 /* One whole time step (correct + move + project) on device vectors, replayed
- * as one CUDA graph after the first calls with the same pointers. */
+ * as one CUDA graph after the first calls with the same pointers.  dVold NULL:
+ * Vold = the handle's last projection, as pfem2gpu_correct_from_projection
+ * (PFEM2GPU_ERR_STATE before the first projection); the step's projection
+ * becomes the handle's last projection either way. */
 int pfem2gpu_step_device(pfem2gpu_handle* h, const double* dV, const double* dVold, double* dV_out);
 
 /* Particle access for output_particle_solution (:218-317) and begin()/end():
@@ -289,7 +300,10 @@ int pfem2gpu_window_particles(pfem2gpu_handle* h, int32_t* cell, double* xi, dou
  *
  * The work memory is one static device array of
  * PFEM2GPU_NOALLOC_SCRATCH_BYTES (64 MiB) per device, part of this library's
- * image: it exists on each device where the call has run.  The call needs
+ * image.  With CUDA's lazy module loading (the default since CUDA 12.2) it is
+ * reserved on a device when the call first runs there; with
+ * CUDA_MODULE_LOADING=EAGER every context that loads the library reserves it
+ * at once.  It stays reserved until the process exits.  The call needs
  *   256 + 4*n_dofs + 4*(n_dofs+1) + 4*ceil(n_dofs/2048)
  *       + 4*n_cells*2^dim + 32*n_cells*2^dim          bytes
  * (each term rounded up to 256), about 290 B per cell in 3D and 115 B per
@@ -304,16 +318,17 @@ int pfem2gpu_window_particles(pfem2gpu_handle* h, int32_t* cell, double* xi, dou
  * get NaN (empty_dof_policy 0, the reference's 0/0) or keep their value on
  * entry (policy 1).  Nothing else needs any value on entry: the call zeroes
  * the counters it uses itself.  *n_empty_dofs (if not NULL) gets the count of
- * such DoFs.  Unsorted or out-of-range cells or DoFs: PFEM2GPU_ERR_ARG.
+ * such DoFs.  Unsorted or out-of-range cells or DoFs: PFEM2GPU_ERR_ARG,
+ * with V_out left as it was on entry.
  *
  * The call runs on `stream` (a cudaStream_t; NULL = the default stream) and
  * returns after its work there has finished.  Calls on one device share the
  * one scratch array, so two calls in flight at once would race on it; the
  * library prevents that with a per-device lock held until the call's work
  * has finished, so concurrent callers wait for each other.  A stream that is
- * being captured into a CUDA graph is refused (PFEM2GPU_ERR_STATE).  The
- * first call on a device looks up the scratch array's address
- * (cudaGetSymbolAddress) with that device current.
+ * being captured into a CUDA graph is refused (PFEM2GPU_ERR_STATE).  Every
+ * call looks up the scratch array's address (cudaGetSymbolAddress) with its
+ * device current, so it follows the context that is current.
  * The sums are those of the FP64 form: V_out equals pfem2gpu_project of an
  * FP64 handle that holds the same particles in the same order, bit for bit.
  */

@@ -2,8 +2,10 @@
 // mesh DoFs that allocates no device memory.
 //
 // The work memory is one file-scope __device__ array (na_scratch), whose
-// address is taken with cudaGetSymbolAddress once per device, with that device
-// current, under a per-device lock.  A call validates its sizes against the
+// address is taken with cudaGetSymbolAddress on every call, with the call's
+// device current, under a per-device lock: the address belongs to the context
+// that is current, and a cached one would go stale after cudaDeviceReset or
+// under another context on the same device.  A call validates its sizes against the
 // array first and returns PFEM2GPU_ERR_SCRATCH when the mesh does not fit.
 // Nothing in the array needs to hold any value on entry: the call zeroes the
 // counters it accumulates into (the status block and the per-DoF entry
@@ -205,10 +207,13 @@ __device__ __forceinline__ int64_t lower_bound(const int32_t* a, int64_t n, int3
 
 // Warp per cell: the cell's particle range by binary search in the sorted
 // cell array, then the FP64 form's per-cell sums over it, in order.
+// Skipped, like the gather, when k_na_count flagged bad input.
 template <int DIM>
-__global__ void __launch_bounds__(CELL_WARPS * 32) k_na_partials(StepArgs a, PartState S, int64_t np)
+__global__ void __launch_bounds__(CELL_WARPS * 32) k_na_partials(StepArgs a, PartState S, int64_t np,
+                                                                 const DevStats* st)
 {
     __shared__ __align__(16) double tr_s[CELL_WARPS][32][TRW];
+    if (*(volatile const unsigned int*)&st->error_flags) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int32_t* pc = reinterpret_cast<const int32_t*>(S.cell);
     for (int c = blockIdx.x * CELL_WARPS + warp; c < a.mesh.nC; c += gridDim.x * CELL_WARPS) {
@@ -220,12 +225,14 @@ __global__ void __launch_bounds__(CELL_WARPS * 32) k_na_partials(StepArgs a, Par
 }
 
 // V_d = sum num_d / sum den over the DoF's entries in ascending order; 0/0
-// gives NaN, or the value on entry under empty_dof_policy 1.
+// gives NaN, or the value on entry under empty_dof_policy 1.  Bad input
+// flagged by k_na_count leaves V untouched.
 template <int DIM>
 __global__ void k_na_gather(int nD, const int32_t* off, const int32_t* ent, const double* P, int keep_empty,
                             double* V, DevStats* st)
 {
     constexpr int NV = 1 << DIM, PW = Dims<DIM>::PW;
+    if (*(volatile const unsigned int*)&st->error_flags) return;
     unsigned long long empty = 0;
     const int stride = gridDim.x * blockDim.x;
     const int nloop = (nD + stride - 1) / stride * stride;
@@ -254,7 +261,6 @@ __global__ void k_na_gather(int nD, const int32_t* off, const int32_t* ent, cons
 }
 
 std::mutex na_mutex[NA_MAX_DEVICES];
-void* na_base[NA_MAX_DEVICES];
 
 int grid_for(int64_t n, int threads)
 {
@@ -282,6 +288,8 @@ extern "C" int pfem2gpu_project_noalloc(int dim, int32_t n_cells, int32_t n_dofs
     if (L.total > NA_BYTES) return PFEM2GPU_ERR_SCRATCH;
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // an error left pending by earlier work of this host thread is not this call's
+    (void)cudaGetLastError();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return PFEM2GPU_ERR_NODEVICE;
     if (dev < 0 || dev >= NA_MAX_DEVICES) return PFEM2GPU_ERR_ARG;
@@ -290,12 +298,9 @@ extern "C" int pfem2gpu_project_noalloc(int dim, int32_t n_cells, int32_t n_dofs
     if (cap != cudaStreamCaptureStatusNone) return PFEM2GPU_ERR_STATE;  // the call synchronises its stream
 
     std::lock_guard<std::mutex> lock(na_mutex[dev]);
-    if (!na_base[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, na_scratch) != cudaSuccess || !p) return PFEM2GPU_ERR_CUDA;
-        na_base[dev] = p;
-    }
-    unsigned char* base = static_cast<unsigned char*>(na_base[dev]);
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, na_scratch) != cudaSuccess || !p) return PFEM2GPU_ERR_CUDA;
+    unsigned char* base = static_cast<unsigned char*>(p);
     DevStats* st = reinterpret_cast<DevStats*>(base + L.stats);
     int32_t* cnt = reinterpret_cast<int32_t*>(base + L.cnt);
     int32_t* off = reinterpret_cast<int32_t*>(base + L.off);
@@ -304,8 +309,14 @@ extern "C" int pfem2gpu_project_noalloc(int dim, int32_t n_cells, int32_t n_dofs
     double* partials = reinterpret_cast<double*>(base + L.partials);
     const int64_t nE = (int64_t)n_cells * NV;
     const int ntiles = (int)((n_dofs + NA_TILE - 1) / NA_TILE);
+    // once work is queued, every return waits for it, so that the lock covers
+    // the work that uses the shared array
+    auto fail_after_enqueue = [&](int code) {
+        cudaStreamSynchronize(s);
+        return code;
+    };
 
-    if (cudaMemsetAsync(base, 0, L.off, s) != cudaSuccess) return PFEM2GPU_ERR_CUDA;  // status block + counts
+    if (cudaMemsetAsync(base, 0, L.off, s) != cudaSuccess) return fail_after_enqueue(PFEM2GPU_ERR_CUDA);
     const int64_t ncount = nE > n_particles ? nE : n_particles;
     k_na_count<<<grid_for(ncount, NA_THREADS), NA_THREADS, 0, s>>>(n_cells, NV, n_dofs, d_cell_dofs, n_particles,
                                                                     d_cell, cnt, st);
@@ -326,17 +337,18 @@ extern "C" int pfem2gpu_project_noalloc(int dim, int32_t n_cells, int32_t n_dofs
     }
     const int cgrid = grid_for((int64_t)n_cells, CELL_WARPS);
     if (dim == 2) {
-        k_na_partials<2><<<cgrid, CELL_WARPS * 32, 0, s>>>(a, S, n_particles);
+        k_na_partials<2><<<cgrid, CELL_WARPS * 32, 0, s>>>(a, S, n_particles, st);
         k_na_gather<2><<<grid_for(n_dofs, 256), 256, 0, s>>>(n_dofs, off, ent, partials, empty_dof_policy, d_V_out,
                                                               st);
     } else {
-        k_na_partials<3><<<cgrid, CELL_WARPS * 32, 0, s>>>(a, S, n_particles);
+        k_na_partials<3><<<cgrid, CELL_WARPS * 32, 0, s>>>(a, S, n_particles, st);
         k_na_gather<3><<<grid_for(n_dofs, 256), 256, 0, s>>>(n_dofs, off, ent, partials, empty_dof_policy, d_V_out,
                                                               st);
     }
-    if (cudaGetLastError() != cudaSuccess) return PFEM2GPU_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return fail_after_enqueue(PFEM2GPU_ERR_CUDA);
     DevStats h{};
-    if (cudaMemcpyAsync(&h, st, sizeof(DevStats), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PFEM2GPU_ERR_CUDA;
+    if (cudaMemcpyAsync(&h, st, sizeof(DevStats), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return fail_after_enqueue(PFEM2GPU_ERR_CUDA);
     if (cudaStreamSynchronize(s) != cudaSuccess) return PFEM2GPU_ERR_CUDA;
     if (h.error_flags) return PFEM2GPU_ERR_ARG;
     if (n_empty_dofs) *n_empty_dofs = (int64_t)h.nan_dofs;

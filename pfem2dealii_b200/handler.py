@@ -92,7 +92,17 @@ def project_noalloc(cell_dofs, cell, xi, v, out, empty_dof_policy=0, stream=None
     int32, cell (n,) int32 ascending, xi and v (dim, n) float64, out
     (dim, n_dofs) float64.  Allocates no device memory; returns the number of
     DoFs no particle reaches."""
+    import torch
+
     dim, n_dofs = out.shape
+    n = cell.shape[0]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    for name, t, dtype, shape in (("cell_dofs", cell_dofs, torch.int32, (cell_dofs.shape[0], 1 << dim)),
+                                  ("cell", cell, torch.int32, (n,)), ("xi", xi, torch.float64, (dim, n)),
+                                  ("v", v, torch.float64, (dim, n)), ("out", out, torch.float64, (dim, n_dofs))):
+        if t.dtype != dtype or tuple(t.shape) != shape or not t.is_contiguous() or t.device != dev:
+            raise ValueError(f"project_noalloc: {name} must be a contiguous {dtype} tensor of shape {shape} "
+                             f"on {dev}, got {t.dtype} {tuple(t.shape)} on {t.device}")
     n_empty = C.c_int64(0)
     _lib.check(_lib.load().pfem2gpu_project_noalloc(
         dim, cell_dofs.shape[0], n_dofs, _ptr(cell_dofs), cell.shape[0], _ptr(cell), _ptr(xi), _ptr(v),
@@ -159,6 +169,13 @@ class ParticleHandler:
         Vold = _host(Vold, np.float64)
         self._ck(self.L.pfem2gpu_correct(self.h, _ptr(V), _ptr(Vold)))
 
+    def correct_particle_velocity_from_projection(self, V):
+        """correct_particle_velocity with Vold = the last projection, kept on
+        the device (the reference's data flow: fem_step copies the projected
+        velocity into the old solution, src/pfem2fem.cpp:523-524)."""
+        V = _host(V, np.float64)
+        self._ck(self.L.pfem2gpu_correct_from_projection(self.h, _ptr(V)))
+
     def move_particles(self, V=None):
         V = None if V is None else _host(V, np.float64)
         self._ck(self.L.pfem2gpu_move(self.h, _ptr(V)))
@@ -187,8 +204,19 @@ class ParticleHandler:
     def project_particle_fields_device(self, dout):
         self._ck(self.L.pfem2gpu_project_device(self.h, _ptr(dout)))
 
+    def correct_particle_velocity_from_projection_device(self, dV):
+        self._ck(self.L.pfem2gpu_correct_from_projection_device(self.h, _ptr(dV)))
+
+    def step_solver(self, V):
+        """One time step with the solver's data flow: correct with Vold = the
+        last projection, move, project (host vectors)."""
+        self.correct_particle_velocity_from_projection(V)
+        self.move_particles(None)
+        return self.project_particle_fields()
+
     def step_device(self, dV, dVold, dout):
-        """correct + move + project on device vectors as one CUDA graph."""
+        """correct + move + project on device vectors as one CUDA graph
+        (dVold None: the last projection)."""
         self._ck(self.L.pfem2gpu_step_device(self.h, _ptr(dV), _ptr(dVold), _ptr(dout)))
 
     # -- differentiated window (no counterpart in the reference) -------------

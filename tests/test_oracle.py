@@ -7,6 +7,7 @@ partition of unity in the projection, the seeding pattern, the count cap
 inverse/forward map round trips.
 """
 import io
+import os
 
 import numpy as np
 import pytest
@@ -216,13 +217,13 @@ def test_unv_round_trip():
     assert np.array_equal(r.cells, m.cells)
 
 
-def test_reference_turek_mesh_reads_if_present():
-    import os
+MESH3 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "Mesh3.tgz")
 
-    p = "/root/reference/cases/TurekBenchmark/Mesh3.tgz"
-    if not os.path.exists(p):
-        pytest.skip("reference tree not mounted")
-    m = M.read_unv(p)
+
+def test_reference_turek_mesh_reads():
+    """The reference's Turek benchmark mesh (cases/TurekBenchmark/Mesh3.tgz,
+    committed as a fixture)."""
+    m = M.read_unv(MESH3)
     assert m.n_cells == 60450 and m.n_verts == 61075
     assert np.allclose(m.vertices.min(0), [0, 0]) and np.allclose(m.vertices.max(0), [2.2, 0.41])
 
@@ -320,12 +321,7 @@ def test_native_unv_reader_errors(tmp_path):
     assert b"2D" in L.pfem2gpu_read_unv_error()
 
 
-def test_native_unv_reader_reference_mesh_if_present():
-    import os
-
-    p = "/root/reference/cases/TurekBenchmark/Mesh3.tgz"
-    if not os.path.exists(p):
-        pytest.skip("reference tree not mounted")
-    a = M.read_unv(p)
-    b = M.read_unv_native(p)
+def test_native_unv_reader_reference_mesh():
+    a = M.read_unv(MESH3)
+    b = M.read_unv_native(MESH3)
     assert np.array_equal(a.vertices, b.vertices) and np.array_equal(a.cells, b.cells)
