@@ -102,6 +102,8 @@ def load():
         "pfem2gpu_move_device": [P, dptr],
         "pfem2gpu_project_device": [P, dptr],
         "pfem2gpu_step_device": [P, dptr, dptr, dptr],
+        "pfem2gpu_correct_from_projection": [P, dptr],
+        "pfem2gpu_correct_from_projection_device": [P, dptr],
         "pfem2gpu_get_particles": [P, dptr, dptr, dptr, dptr, dptr, i64, C.POINTER(i64)],
         "pfem2gpu_set_particles": [P, i64, dptr, dptr, dptr, dptr, dptr, u32],
         "pfem2gpu_write_vtu": [P, C.c_char_p],

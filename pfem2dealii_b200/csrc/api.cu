@@ -66,6 +66,7 @@ struct pfem2gpu_handle {
     DevStats* stats = nullptr;
     DevStats* stats_h = nullptr;
     bool has_particles = false, pending_correct = false, partials_valid = false;
+    bool has_projection = false;  // Vout holds the last projection of this mesh
     // accounting
     uint64_t launches = 0;
     bool profiling = false;
@@ -386,7 +387,8 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
 }
 
 // Nodal velocity staging: host or device component-major V (and Vold) ->
-// padded per-DoF V (and V - Vold) in the form's precision.
+// padded per-DoF V (and V - Vold) in the form's precision.  Vold is on the
+// device when `device` is set or when it is the handle's last projection.
 int stage_v(pfem2gpu_handle* h, const double* V, const double* Vold, bool device)
 {
     const size_t bytes = (size_t)h->dim * h->nD * sizeof(double);
@@ -395,7 +397,7 @@ int stage_v(pfem2gpu_handle* h, const double* V, const double* Vold, bool device
     if (!device) {
         CK(cudaMemcpyAsync(h->Vstage, V, bytes, cudaMemcpyHostToDevice, h->stream));
         v = h->Vstage;
-        if (Vold) {
+        if (Vold && Vold != h->Vout) {
             CK(cudaMemcpyAsync(h->Vstage2, Vold, bytes, cudaMemcpyHostToDevice, h->stream));
             vo = h->Vstage2;
         }
@@ -1028,6 +1030,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     free_win_mesh(h->win);
     free_fem(h->fem);
     h->has_mesh = false;
+    h->has_projection = false;
     h->nC = (int)n_cells;
     h->nV = (int)n_verts;
     h->nD = (int)n_dofs;
@@ -1136,6 +1139,23 @@ int pfem2gpu_correct_device(pfem2gpu_handle* h, const double* dV, const double* 
     return correct_impl(h, dV, dVold, true);
 }
 
+// Vold = the handle's last projection, which stays on the device.
+static int correct_from_projection(pfem2gpu_handle* h, const double* V, bool device)
+{
+    if (!h || !V) return PFEM2GPU_ERR_ARG;
+    if (!h->has_projection) return fail(h, PFEM2GPU_ERR_STATE, "correct from projection before any projection");
+    return correct_impl(h, V, h->Vout, device);
+}
+
+int pfem2gpu_correct_from_projection(pfem2gpu_handle* h, const double* V)
+{
+    return correct_from_projection(h, V, false);
+}
+int pfem2gpu_correct_from_projection_device(pfem2gpu_handle* h, const double* dV)
+{
+    return correct_from_projection(h, dV, true);
+}
+
 static int move_impl(pfem2gpu_handle* h, const double* V, bool device)
 {
     if (!h) return PFEM2GPU_ERR_ARG;
@@ -1165,6 +1185,7 @@ static int project_impl(pfem2gpu_handle* h, double* out, bool device)
     CK(cudaMemsetAsync(&h->stats->nan_dofs, 0, sizeof(unsigned long long), h->stream));
     run(h, "gather", [&] { return launch_gather(h->dim, h->prec, a, h->prm.empty_dof_policy == 1, h->stream); });
     if ((rc = check_async(h))) return rc;
+    h->has_projection = true;
     const size_t bytes = (size_t)h->dim * h->nD * sizeof(double);
     if (device) {
         if (out != h->Vout) CK(cudaMemcpyAsync(out, h->Vout, bytes, cudaMemcpyDeviceToDevice, h->stream));
@@ -1180,8 +1201,12 @@ int pfem2gpu_project_device(pfem2gpu_handle* h, double* dV_out) { return project
 
 int pfem2gpu_step_device(pfem2gpu_handle* h, const double* dV, const double* dVold, double* dV_out)
 {
-    if (!h || !dV || !dVold || !dV_out) return PFEM2GPU_ERR_ARG;
+    if (!h || !dV || !dV_out) return PFEM2GPU_ERR_ARG;
     if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "step before seed");
+    if (!dVold) {  // the reference's data flow: Vold = the last projection
+        if (!h->has_projection) return fail(h, PFEM2GPU_ERR_STATE, "step from projection before any projection");
+        dVold = h->Vout;
+    }
     int rc = apply_pending_correction(h);
     if (rc) return rc;
     rc = graphed(h, h->step_graph[h->parity], dV, dVold, dV_out, [&]() -> int {
@@ -1192,10 +1217,12 @@ int pfem2gpu_step_device(pfem2gpu_handle* h, const double* dV, const double* dVo
         if ((r = enqueue_move(h, 1, 1))) return r;
         StepArgs a = args(h);
         a.Vout = dV_out;
+        a.Vout2 = dV_out != h->Vout ? h->Vout : nullptr;  // the handle keeps its last projection
         run(h, "gather", [&] { return launch_gather(h->dim, h->prec, a, h->prm.empty_dof_policy == 1, h->stream); });
         return PFEM2GPU_OK;
     });
     if (rc) return rc;
+    h->has_projection = true;
     h->vaos_valid = true;
     h->pending_correct = false;
     swap_state(h);

@@ -1047,6 +1047,7 @@ __global__ void k_gather(StepArgs a, int keep_empty)
             double r = num[d] / den;
             if (den == 0.0 && keep_empty) r = a.Vkeep[(size_t)d * a.mesh.nD + dof];
             a.Vout[(size_t)d * a.mesh.nD + dof] = r;
+            if (a.Vout2) a.Vout2[(size_t)d * a.mesh.nD + dof] = r;
         }
     }
     nan_dofs = warp_sum_u64(nan_dofs);

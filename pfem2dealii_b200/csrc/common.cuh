@@ -125,6 +125,7 @@ struct StepArgs {
     uint4* gscr;               // write pass, general path: per-particle scratch in the cell's output range
     void* partials;                // nC x PW projection partial sums
     double* Vout;                  // nD x DIM component-major projected velocity
+    double* Vout2;                 // a second copy of it (the handle's last projection), or null
     const double* Vkeep;           // empty_dof_policy 1: value kept where no particle contributes
     DevStats* stats;
     uint32_t capacity;

@@ -80,6 +80,44 @@ def test_fp64_channel_config_bit_exact():
     assert st["lost"] > 0 and st["seeded"] > 0 and st["searched"] > 0 and st["near_face"] > 0
 
 
+def test_fp64_solver_data_flow_bit_exact():
+    """The reference's data flow (src/pfem2solver.cpp:162-165 with fem_step
+    copying the projection into the old solution, src/pfem2fem.cpp:523-524):
+    every step corrects with Vold = the previous projection.  The host path
+    (pfem2gpu_correct_from_projection, only V uploaded) and the device step
+    (pfem2gpu_step_device with dVold NULL) both equal the oracle fed its own
+    previous projection, bit for bit."""
+    import torch
+
+    c = cases.channel(32, 8, dt=0.02)
+    o, g = make(c)
+    _, gd = make(c)
+    o.seed(c.V)
+    g.seed_particles(c.V)
+    gd.seed_particles(c.V)
+    Vo = o.project()
+    Vg = g.project_particle_fields()
+    dV = torch.from_numpy(np.ascontiguousarray(c.V)).cuda()
+    dout = torch.empty_like(dV)
+    gd.project_particle_fields_device(dout)
+    assert_v_close(Vo, Vg, V_RTOL_FP64)
+    for s in range(12):
+        Vo = o.step(c.V, Vo)
+        Vg = g.step_solver(c.V)
+        gd.step_device(dV, None, dout)
+        assert_same_particles(o.particles(), g.particles())
+        assert_v_close(Vo, Vg, V_RTOL_FP64)
+        assert np.array_equal(Vg, dout.cpu().numpy())
+    assert_same_particles(o.particles(), gd.particles())
+    # before any projection there is no previous one to correct from
+    _, g2 = make(c)
+    g2.seed_particles(c.V)
+    with pytest.raises(Exception):
+        g2.correct_particle_velocity_from_projection(c.V)
+    for h in (g, gd, g2):
+        h.close()
+
+
 def test_fp64_duct_bit_exact():
     c = cases.duct(32, 8, 8, dt=0.05)
     o, g = run_fp64(c, 12)
