@@ -1,0 +1,3 @@
+// Stand-in: see dealii_stub.h.
+#pragma once
+#include "../../dealii_stub.h"

@@ -1,0 +1,65 @@
+"""The reference-side drop-in: pfem2dealii_b200/dealii/pfem2particlehandler_b200.cpp
+implements the reference's own pfem2ParticleHandler<dim> (its header
+src/pfem2particlehandler.h unchanged) over the C ABI.  g++ compiles it
+against the reference's unchanged headers (pfem2particlehandler.h,
+pfem2solver.h, pfem2fem.h, pfem2parameterhandler.h, pfem2particle.h) with
+minimal stand-ins for the deal.II and Trilinos types they name
+(tests/dealii_stub); every public method of the class is defined for dim 2
+and 3, and every C-ABI function it calls is exported by libpfem2gpu.so.
+
+The reference's headers are read from $PFEM2DEALII_SRC (the reference's
+src/ directory); without it the test is skipped."""
+import os
+import subprocess
+
+import pytest
+
+from pfem2dealii_b200 import _lib, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ADAPTER = os.path.join(ROOT, "pfem2dealii_b200", "dealii", "pfem2particlehandler_b200.cpp")
+REF_SRC = os.environ.get("PFEM2DEALII_SRC", "/root/reference/src")
+
+PUBLIC = ["pfem2ParticleHandler({fe})", "~pfem2ParticleHandler()", "clear_particles()", "remove_particle(",
+          "insert_particle(", "begin()", "end()", "initialize_maps()", "getPfem2Solver() const",
+          "setPfem2Solver(pfem2Solver<{d}>*)", "seed_particles()", "correct_particle_velocity()",
+          "move_particles()", "project_particle_fields()", "output_particle_solution(int)"]
+
+
+@pytest.fixture(scope="module")
+def adapter_object(tmp_path_factory):
+    if not os.path.exists(os.path.join(REF_SRC, "pfem2particlehandler.h")):
+        pytest.skip("the reference's src/ headers are not available (set PFEM2DEALII_SRC)")
+    d = tmp_path_factory.mktemp("adapter")
+    outs = []
+    for k, defs in enumerate(([], ["-DPFEM2_B200_FP32", "-DPFEM2_B200_UPLOAD_OLD_SOLUTION"])):
+        out = str(d / f"adapter{k}.o")
+        cmd = ["g++", "-std=c++17", "-Wall", "-Wextra", "-Wno-ignored-qualifiers", "-Werror", *defs, "-c", ADAPTER,
+               "-I", os.path.join(ROOT, "tests", "dealii_stub"), "-I", REF_SRC, "-I", os.path.join(ROOT, "include"),
+               "-o", out]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr[-4000:]
+        outs.append(out)
+    return outs[0]  # the default build: FP64 form, old solution from the last projection
+
+
+def symbols(path, *flags):
+    return subprocess.run(["nm", *flags, path], capture_output=True, text=True, check=True).stdout.splitlines()
+
+
+def test_adapter_defines_the_reference_class(adapter_object):
+    defined = [l.split(" ", 2)[-1] for l in symbols(adapter_object, "-C") if " W " in l or " T " in l]
+    for d in (2, 3):
+        for m in PUBLIC:
+            sig = f"pfem2ParticleHandler<{d}>::" + m.format(d=d, fe=f"dealii::FE_Q<{d}, {d}> const*")
+            assert any(s.startswith(sig) for s in defined), sig
+
+
+def test_adapter_calls_only_exported_abi_functions(adapter_object):
+    build.build()
+    need = {l.split()[-1] for l in symbols(adapter_object) if l.strip().startswith("U pfem2gpu_")}
+    assert {"pfem2gpu_create", "pfem2gpu_set_mesh", "pfem2gpu_seed", "pfem2gpu_correct_from_projection",
+            "pfem2gpu_move", "pfem2gpu_project"} <= need
+    exported = {l.split()[-1] for l in symbols(_lib.LIB_PATH, "-D", "--defined-only")}
+    assert need <= exported, need - exported
+    assert need <= set(_lib.declared_symbols())
