@@ -29,7 +29,12 @@ ERRORS = {
     8: "mesh larger than the static scratch of pfem2gpu_project_noalloc",
 }
 ERR_ARG = 1
+ERR_CUDA = 2
 ERR_STATE = 3
+ERR_CAPACITY = 4
+ERR_NOMEM = 5
+ERR_NODEVICE = 6
+ERR_DEVICE = 7
 ERR_SCRATCH = 8
 
 

@@ -316,16 +316,46 @@ struct AdvStage {
 
 __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
 
-// Thread 0: bulk-copy particles [chunk*CH, chunk*CH + cnt) of S0 into stage st.
+// FP32 form: the velocity records (V and V - Vold) of the consecutive cells
+// [cfirst, cfirst + ncell) that one chunk's particles lie in (they are
+// sorted by cell), staged with the chunk.  ncell = 0: not staged.
+template <int DIM>
+struct AdvRecStage {
+    static constexpr int MAXC = AdvRec<DIM>::MAXC, F4 = Dims<DIM>::REC4;
+    float4 v[MAXC][F4];
+    float4 dv[MAXC][F4];
+    uint32_t cfirst, ncell;
+};
+
+// Thread 0: bulk-copy particles [chunk*CH, chunk*CH + cnt) of S0 into stage
+// st, and (rs not null) the records of their cells into rs: the cells from
+// the chunk's first cell to the next chunk's first cell, as the seed and
+// write passes recorded them (a range that is out of order or too long is
+// not staged; the particles then read their records from global memory).
 template <int DIM, typename Real, int CH>
 __device__ __forceinline__ void stage_chunk(const StepArgs& a, AdvStage<DIM, Real, CH>& st, uint64_t* bar,
-                                            uint32_t chunk, uint32_t n)
+                                            uint32_t chunk, uint32_t n, AdvRecStage<DIM>* rs = nullptr)
 {
     constexpr bool HX = std::is_same<Real, double>::value;
     const uint32_t base = chunk * CH;
     const uint32_t cnt = n - base < (uint32_t)CH ? n - base : (uint32_t)CH;
     const uint32_t b4 = round16(cnt * 4u), br = round16(cnt * (uint32_t)sizeof(Real));
-    mbar_expect_tx(bar, b4 + (2 + (HX ? 1 : 0)) * DIM * br);
+    uint32_t cf = 0, nrec = 0;
+    if (rs) {
+        const uint32_t nC = (uint32_t)a.mesh.nC;
+        cf = a.chunk_first[chunk];
+        const uint32_t cl = base + CH < n ? a.chunk_first[chunk + 1] : nC - 1;
+        if (cf <= cl && cl < nC && cl - cf < (uint32_t)AdvRecStage<DIM>::MAXC) nrec = cl - cf + 1;
+        rs->cfirst = cf;
+        rs->ncell = nrec;
+    }
+    constexpr uint32_t RB = Dims<DIM>::REC4 * 16u;  // bytes of one cell's record
+    const uint32_t recb = nrec * RB * (a.do_correct ? 2u : 1u);
+    mbar_expect_tx(bar, b4 + (2 + (HX ? 1 : 0)) * DIM * br + recb);
+    if (nrec) {
+        bulk_g2s(rs->v, a.vrec32 + (size_t)cf * Dims<DIM>::REC4 * 4, nrec * RB, bar);
+        if (a.do_correct) bulk_g2s(rs->dv, a.dvrec32 + (size_t)cf * Dims<DIM>::REC4 * 4, nrec * RB, bar);
+    }
     bulk_g2s(st.cell, a.S0.cell + base, b4, bar);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
@@ -342,7 +372,8 @@ __device__ __forceinline__ void stage_chunk(const StepArgs& a, AdvStage<DIM, Rea
 // that drew cheap chunks take more; a block holds tickets for the chunk it
 // processes and the one being staged.
 template <int DIM, typename Real, int CH, typename F>
-__device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Real, CH>* st, uint64_t* bar, F&& f)
+__device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Real, CH>* st, uint64_t* bar, F&& f,
+                                            AdvRecStage<DIM>* rs = nullptr)
 {
     __shared__ uint32_t tk[2];
     const uint32_t n = (uint32_t)a.stats->n_slots;
@@ -357,7 +388,7 @@ __device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Rea
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
             tk[b] = atomicAdd(&a.stats->adv_next, 1u);
-            if (tk[b] < nchunks) stage_chunk<DIM, Real, CH>(a, st[b], &bar[b], tk[b], n);
+            if (tk[b] < nchunks) stage_chunk<DIM, Real, CH>(a, st[b], &bar[b], tk[b], n, rs ? rs + b : nullptr);
         }
     }
     __syncthreads();
@@ -375,14 +406,14 @@ __device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Rea
         const uint32_t base = chunk * CH;
         const uint32_t cnt = n - base < (uint32_t)CH ? n - base : (uint32_t)CH;
 #pragma unroll 1
-        for (uint32_t t = threadIdx.x; t < (uint32_t)CH; t += blockDim.x) f(st[sidx], t, base + t, t < cnt);
+        for (uint32_t t = threadIdx.x; t < (uint32_t)CH; t += blockDim.x) f(st[sidx], sidx, t, base + t, t < cnt);
         __syncthreads();
         if (threadIdx.x == 0) {
             const uint32_t nxt = atomicAdd(&a.stats->adv_next, 1u);
             tk[sidx] = nxt;
             if (nxt < nchunks) {
                 fence_proxy_async();
-                stage_chunk<DIM, Real, CH>(a, st[sidx], &bar[sidx], nxt, n);
+                stage_chunk<DIM, Real, CH>(a, st[sidx], &bar[sidx], nxt, n, rs ? rs + sidx : nullptr);
             }
         }
         __syncthreads();
@@ -458,8 +489,8 @@ __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
     auto* st = reinterpret_cast<AdvStage<DIM, double, ADV64_CH>*>(adv_raw);
     const MeshDev& m = a.mesh;
     AdvCounters k;
-    staged_loop<DIM, double, ADV64_CH>(a, st, bar, [&](AdvStage<DIM, double, ADV64_CH>& sg, uint32_t t, uint32_t i,
-                                                       bool in) {
+    staged_loop<DIM, double, ADV64_CH>(a, st, bar, [&](AdvStage<DIM, double, ADV64_CH>& sg, int, uint32_t t,
+                                                       uint32_t i, bool in) {
         const uint32_t c = in ? sg.cell[t] : HOLE;
         const bool act = c != HOLE && in;
         bool want = false, counted = false;
@@ -602,6 +633,27 @@ __device__ __forceinline__ void load_rec32(const float* __restrict__ rec, uint32
     r.affine = buf[(1 << DIM) * DIM] != 0.0f;
 }
 
+// The same record from a shared-memory stage.
+template <int DIM>
+__device__ __forceinline__ void load_rec32_s(const float4* p, Rec32<DIM>& r)
+{
+    constexpr int F4 = Dims<DIM>::REC4;
+    float buf[F4 * 4];
+#pragma unroll
+    for (int k = 0; k < F4; ++k) {
+        const float4 t = p[k];
+        buf[4 * k] = t.x;
+        buf[4 * k + 1] = t.y;
+        buf[4 * k + 2] = t.z;
+        buf[4 * k + 3] = t.w;
+    }
+#pragma unroll
+    for (int k = 0; k < (1 << DIM); ++k)
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) r.b[k][d] = buf[k * DIM + d];
+    r.affine = buf[(1 << DIM) * DIM] != 0.0f;
+}
+
 // f(xi) = sum_k b_k prod_{d in k} xi_d, nested: 3 (2D) / 7 (3D) FMAs per component.
 template <int DIM>
 __device__ __forceinline__ void eval_poly(const float (*b)[DIM], const float* xi, float* f)
@@ -644,10 +696,8 @@ __device__ __noinline__ F3<DIM> newton32(const float* __restrict__ geo, uint32_t
 // affine, so the Newton branch (an out-of-line call whose saved registers
 // would spill in the hot loop) is left out.
 template <int DIM, bool AFF = false>
-__device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi)
+__device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi, const Rec32<DIM>& r)
 {
-    Rec32<DIM> r;
-    load_rec32<DIM>(a.vrec32, c, r);
     const float dtp = (float)a.pp.dtp;
     int s = s0;
     for (; s < a.pp.S; ++s) {
@@ -678,6 +728,14 @@ __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0,
     return s;
 }
 
+template <int DIM, bool AFF = false>
+__device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi)
+{
+    Rec32<DIM> r;
+    load_rec32<DIM>(a.vrec32, c, r);
+    return substeps32<DIM, AFF>(a, c, s0, xi, r);
+}
+
 template <int DIM, bool AFF>
 __global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
 {
@@ -685,9 +743,11 @@ __global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
     extern __shared__ __align__(128) unsigned char adv_raw[];
     __shared__ uint64_t bar[2];
     auto* st = reinterpret_cast<AdvStage<DIM, float, ADV_CH>*>(adv_raw);
+    auto* rs = reinterpret_cast<AdvRecStage<DIM>*>(adv_raw + 2 * sizeof(AdvStage<DIM, float, ADV_CH>));
     const MeshDev& m = a.mesh;
     AdvCounters k;
-    staged_loop<DIM, float, ADV_CH>(a, st, bar, [&](AdvStage<DIM, float, ADV_CH>& sg, uint32_t t, uint32_t i, bool in) {
+    staged_loop<DIM, float, ADV_CH>(a, st, bar, [&](AdvStage<DIM, float, ADV_CH>& sg, int sidx, uint32_t t, uint32_t i,
+                                                    bool in) {
         const uint32_t c = in ? sg.cell[t] : HOLE;
         const bool act = c != HOLE && in;
         bool want = false, counted = false;
@@ -703,15 +763,23 @@ __global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
             const bool alive = c < (uint32_t)m.nC;
             if (!alive) k.err |= ERR_BAD_CELL;
             if (alive) {
+                // the cell's records: staged with the chunk, or from global memory
+                const AdvRecStage<DIM>& rsg = rs[sidx];
+                const uint32_t lc = c - rsg.cfirst;
+                const bool srec = a.chunk_first && lc < rsg.ncell;
                 if (a.do_correct) {  // v += sum N_i (V - Vold)_i, src/pfem2particlehandler.cpp:126-138
                     Rec32<DIM> dr;
-                    load_rec32<DIM>(a.dvrec32, c, dr);
+                    if (srec) load_rec32_s<DIM>(rsg.dv[lc], dr);
+                    else load_rec32<DIM>(a.dvrec32, c, dr);
                     float dv[DIM];
                     eval_poly<DIM>(dr.b, xi, dv);
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) v[d] += dv[d];
                 }
-                s = substeps32<DIM, AFF>(a, c, 0, xi);
+                Rec32<DIM> r;
+                if (srec) load_rec32_s<DIM>(rsg.v[lc], r);
+                else load_rec32<DIM>(a.vrec32, c, r);
+                s = substeps32<DIM, AFF>(a, c, 0, xi, r);
                 want = s < a.pp.S;
             }
 #pragma unroll
@@ -729,7 +797,7 @@ __global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
         }
         defer(a, want, i, s);
         count_cells(a, counted, c, pe);
-    });
+    }, a.chunk_first ? rs : nullptr);
     flush_counters(a, k);
 }
 

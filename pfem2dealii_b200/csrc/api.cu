@@ -33,6 +33,7 @@ struct pfem2gpu_handle {
     bool all_affine = false;
     // velocities
     double *Vstage = nullptr, *Vstage2 = nullptr, *Vout = nullptr;
+    double* Vin = nullptr;  // host V of the current call, uploaded before its check (see stage_v)
     void *Vc = nullptr, *dVc = nullptr;
     bool vaos_valid = false;
     // particles
@@ -46,6 +47,7 @@ struct pfem2gpu_handle {
     uint32_t *carr = nullptr, *carrs = nullptr, *ccount = nullptr;
     unsigned long long *cocc = nullptr, *cub = nullptr, *coff = nullptr, *tiles64 = nullptr;
     uint4* gscr = nullptr;
+    uint32_t* chunk_first = nullptr;  // FP32 form: first cell of each advect chunk of the current layout
     float *jinv32 = nullptr, *vrec32 = nullptr, *dvrec32 = nullptr;
     bool launch_failed = false;
     // CUDA graphs of the per-step sequences (one per buffer parity and
@@ -238,6 +240,7 @@ StepArgs args(pfem2gpu_handle* h)
     a.cocc = h->cocc;
     a.cub = h->cub;
     a.coff = h->coff;
+    a.chunk_first = h->chunk_first;
     a.gscr = h->gscr;
     a.partials = h->partials;
     a.Vout = h->Vout;
@@ -335,17 +338,39 @@ cudaError_t alloc_state(pfem2gpu_handle* h, PartState& s, uint32_t cap, bool wit
     return e;
 }
 
-// Particle arrays sized for `need` particles (grown by 1.5x, S0 kept).
-int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
+// The particle slots params.capacity allows (0: no limit), in whole
+// 16-byte chunks of 4-byte slots.
+uint64_t capacity_limit(const pfem2gpu_handle* h)
 {
-    if (need <= h->cap && h->S0.cell) return PFEM2GPU_OK;
-    uint64_t cap = std::max<uint64_t>(need, (uint64_t)h->cap * 3 / 2);
+    return h->prm.capacity > 0 ? ((uint64_t)h->prm.capacity + 3) & ~3ull : 0x7FFFFFF0ull;
+}
+
+// Particle arrays sized for `need` particles (grown by 1.5x, S0 kept), up to
+// `want` when that is more, never beyond params.capacity: a `need` above it
+// is PFEM2GPU_ERR_CAPACITY before any allocation.
+int ensure_capacity(pfem2gpu_handle* h, uint64_t need, uint64_t want = 0)
+{
+    const uint64_t limit = capacity_limit(h);
+    if (need > limit)
+        return fail(h, PFEM2GPU_ERR_CAPACITY, "particle capacity " + std::to_string(limit) + " below the " +
+                                                  std::to_string(need) + " particles needed");
+    if (need <= h->cap && h->S0.cell && want <= h->cap) return PFEM2GPU_OK;
+    if (h->cap >= limit && h->S0.cell) return PFEM2GPU_OK;  // at the limit: need fits already
+    uint64_t cap = std::max<uint64_t>(std::max(need, want), (uint64_t)h->cap * 3 / 2);
     cap = (std::max<uint64_t>(cap, 1024) + 3) & ~3ull;  // whole 16-byte chunks for the bulk copies
-    if (cap > 0x7FFFFFF0ull) return fail(h, PFEM2GPU_ERR_CAPACITY, "particle capacity beyond 2^31");
+    cap = std::min(cap, limit);
     PartState n0{}, n1{}, nt{};
     CK(alloc_state(h, n0, (uint32_t)cap, true));
     CK(alloc_state(h, n1, (uint32_t)cap, true));
     CK(alloc_state(h, nt, (uint32_t)cap, false));
+    uint32_t* cf_new = nullptr;
+    const size_t ncf = (cap + ADV_CH - 1) / ADV_CH + 1;
+    if (h->prec == PFEM2GPU_FP32) {
+        CK(dalloc(&cf_new, ncf));
+        if (h->chunk_first)
+            CK(cudaMemcpyAsync(cf_new, h->chunk_first, ((size_t)h->cap + ADV_CH - 1) / ADV_CH * 4 + 4,
+                               cudaMemcpyDeviceToDevice, h->stream));
+    }
     if (h->S0.cell && h->has_particles) {
         const size_t n = h->cap, es = esize(h);
         CK(cudaMemcpyAsync(n0.cell, h->S0.cell, n * 4, cudaMemcpyDeviceToDevice, h->stream));
@@ -357,9 +382,12 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
         }
         CK(cudaStreamSynchronize(h->stream));
     }
+    CK(cudaStreamSynchronize(h->stream));
     free_state(h->S0);
     free_state(h->S1);
     free_state(h->T);
+    dfree(h->chunk_first);
+    h->chunk_first = cf_new;
     dfree(h->key);
     dfree(h->next);
     dfree(h->xtmp);
@@ -386,24 +414,39 @@ int ensure_capacity(pfem2gpu_handle* h, uint64_t need)
     return PFEM2GPU_OK;
 }
 
+// A host nodal velocity (the FEM solution) must be finite everywhere.
+// Device vectors are not inspected.  Vold is not checked either: it may be a
+// projection, which is NaN where no particle reaches (the reference's 0/0).
+bool all_finite(const double* V, size_t n)
+{
+    const uint64_t* b = reinterpret_cast<const uint64_t*>(V);
+    uint64_t bad = 0;
+    for (size_t i = 0; i < n; ++i) bad |= (uint64_t)((b[i] & 0x7FF0000000000000ull) == 0x7FF0000000000000ull);
+    return bad == 0;
+}
+
 // Nodal velocity staging: host or device component-major V (and Vold) ->
 // padded per-DoF V (and V - Vold) in the form's precision.  Vold is on the
 // device when `device` is set or when it is the handle's last projection.
+// A host V is uploaded into a buffer of its own and checked while the copy
+// is in flight; a non-finite value returns PFEM2GPU_ERR_ARG before any
+// kernel runs, so the staged velocity and the particles stay as they were.
 int stage_v(pfem2gpu_handle* h, const double* V, const double* Vold, bool device)
 {
     const size_t bytes = (size_t)h->dim * h->nD * sizeof(double);
     const double* v = V;
     const double* vo = Vold;
     if (!device) {
-        CK(cudaMemcpyAsync(h->Vstage, V, bytes, cudaMemcpyHostToDevice, h->stream));
-        v = h->Vstage;
+        CK(cudaMemcpyAsync(h->Vin, V, bytes, cudaMemcpyHostToDevice, h->stream));
+        v = h->Vin;
         if (Vold && Vold != h->Vout) {
             CK(cudaMemcpyAsync(h->Vstage2, Vold, bytes, cudaMemcpyHostToDevice, h->stream));
             vo = h->Vstage2;
         }
+        if (!all_finite(V, (size_t)h->dim * h->nD)) return fail(h, PFEM2GPU_ERR_ARG, "non-finite nodal velocity");
     }
-    // device vectors: the staging kernel also writes the kept copy of V
-    double* vcopy = device && V != h->Vstage ? h->Vstage : nullptr;
+    // the staging kernel also writes the kept copy of V
+    double* vcopy = v != h->Vstage ? h->Vstage : nullptr;
     if (h->prec == PFEM2GPU_FP64) {
         run(h, "stage_velocity", [&] {
             return launch_cell_v(h->dim, h->prec, v, vo, h->cd, h->nC, h->nD, h->Vc, Vold ? h->dVc : nullptr, vcopy,
@@ -552,7 +595,8 @@ int sync_stats(pfem2gpu_handle* h)
 int maybe_grow(pfem2gpu_handle* h)
 {
     const uint64_t n = h->stats_h->n_slots;
-    if (n + (uint64_t)h->nC * h->pp.npart / 2 > h->cap) return ensure_capacity(h, n + (uint64_t)h->nC * h->pp.npart);
+    if (n + (uint64_t)h->nC * h->pp.npart / 2 > h->cap && h->cap < capacity_limit(h))
+        return ensure_capacity(h, n, n + (uint64_t)h->nC * h->pp.npart);
     return PFEM2GPU_OK;
 }
 
@@ -897,12 +941,13 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (void* p : {(void*)h->cv, (void*)h->cd, (void*)h->v2c_off, (void*)h->v2c_cells, (void*)h->d2c_off,
                     (void*)h->d2c_ent, (void*)h->verts, (void*)h->cellX, (void*)h->aff, (void*)h->v2c_dirs,
-                    (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, h->Vc, h->dVc,
+                    (void*)h->geo32, (void*)h->Vstage, (void*)h->Vstage2, (void*)h->Vout, (void*)h->Vin, h->Vc, h->dVc,
                     (void*)h->key, (void*)h->next, (void*)h->xtmp, (void*)h->head, (void*)h->cs0, (void*)h->cs1,
                     (void*)h->carr, (void*)h->carrs, (void*)h->ccount, (void*)h->cocc, (void*)h->cub, (void*)h->coff,
                     (void*)h->tiles64, (void*)h->gscr, (void*)h->jinv32, (void*)h->xq, (void*)h->nxq,
                     (void*)h->vrec32, (void*)h->dvrec32, h->partials, (void*)h->stats, (void*)h->twisted})
         dfree(p);
+    dfree(h->chunk_first);
     free_state(h->S0);
     free_state(h->S1);
     free_state(h->T);
@@ -1020,7 +1065,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     for (void** p : {(void**)&h->cv, (void**)&h->cd, (void**)&h->v2c_off, (void**)&h->v2c_cells, (void**)&h->d2c_off,
                      (void**)&h->d2c_ent, (void**)&h->verts, (void**)&h->cellX, (void**)&h->aff,
                      (void**)&h->v2c_dirs, (void**)&h->geo32, (void**)&h->Vstage, (void**)&h->Vstage2,
-                     (void**)&h->Vout, (void**)&h->Vc, (void**)&h->dVc, (void**)&h->head, (void**)&h->cs0,
+                     (void**)&h->Vout, (void**)&h->Vin, (void**)&h->Vc, (void**)&h->dVc, (void**)&h->head, (void**)&h->cs0,
                      (void**)&h->cs1, (void**)&h->carr, (void**)&h->carrs, (void**)&h->ccount, (void**)&h->cocc,
                      (void**)&h->cub, (void**)&h->coff, (void**)&h->tiles64, (void**)&h->jinv32, (void**)&h->vrec32,
                      (void**)&h->dvrec32, (void**)&h->partials, (void**)&h->twisted}) {
@@ -1047,6 +1092,7 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     CK(dalloc(&h->geo32, nc * GS));
     CK(dalloc(&h->Vstage, nd * dim));
     CK(dalloc(&h->Vstage2, nd * dim));
+    CK(dalloc(&h->Vin, nd * dim));
     CK(dalloc(&h->Vout, nd * dim));
     const size_t vcn = h->prec == PFEM2GPU_FP64 ? nc * NV * VS : 1;
     CK(cudaMalloc(&h->Vc, vcn * esize(h)));
@@ -1099,15 +1145,23 @@ int pfem2gpu_set_mesh(pfem2gpu_handle* h, int64_t n_cells, int64_t n_verts, int6
     return check_async(h);
 }
 
+// Seeding checks its host V before it allocates anything (stage_v checks the
+// V of the other calls while it is uploaded).
+static int host_velocity_ok(pfem2gpu_handle* h, const double* V, bool device)
+{
+    if (device || all_finite(V, (size_t)h->dim * h->nD)) return PFEM2GPU_OK;
+    return fail(h, PFEM2GPU_ERR_ARG, "non-finite nodal velocity");
+}
+
 static int seed_impl(pfem2gpu_handle* h, const double* V, bool device)
 {
     if (!h || !V) return PFEM2GPU_ERR_ARG;
     if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "seed before set_mesh");
     if (h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "seed called twice");
     const uint64_t n = (uint64_t)h->nC * h->pp.npart;
-    const uint64_t want = h->prm.capacity > 0 ? (uint64_t)h->prm.capacity : 2 * n;
-    int rc = ensure_capacity(h, std::max(want, n));
+    int rc = host_velocity_ok(h, V, device);
     if (rc) return rc;
+    if ((rc = ensure_capacity(h, n, h->prm.capacity > 0 ? (uint64_t)h->prm.capacity : 2 * n))) return rc;
     if ((rc = stage_v(h, V, nullptr, device))) return rc;
     StepArgs a = args(h);
     run(h, "seed", [&] { return launch_seed(h->dim, h->prec, a, h->cs0, h->stream); });
@@ -1303,7 +1357,14 @@ int pfem2gpu_set_particles(pfem2gpu_handle* h, int64_t n, const uint32_t* id, co
     if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "set_particles before set_mesh");
     for (int64_t i = 0; i < n; ++i)
         if (cell[i] < 0 || cell[i] >= h->nC) return fail(h, PFEM2GPU_ERR_ARG, "bad particle cell");
-    int rc = ensure_capacity(h, std::max<uint64_t>((uint64_t)n + (uint64_t)h->nC * h->pp.npart, h->cap));
+    // reference coordinates inside the unit cell (GeometryInfo::is_inside_unit_cell, the test every
+    // particle of the reference passed), finite velocities and positions
+    for (int64_t i = 0; i < n * h->dim; ++i) {
+        if (!(xi[i] >= 0.0 && xi[i] <= 1.0)) return fail(h, PFEM2GPU_ERR_ARG, "particle reference coordinate outside [0, 1]");
+        if (!std::isfinite(v[i])) return fail(h, PFEM2GPU_ERR_ARG, "non-finite particle velocity");
+        if (x && h->prec == PFEM2GPU_FP64 && !std::isfinite(x[i])) return fail(h, PFEM2GPU_ERR_ARG, "non-finite particle position");
+    }
+    int rc = ensure_capacity(h, (uint64_t)n, std::max<uint64_t>((uint64_t)n + (uint64_t)h->nC * h->pp.npart, h->cap));
     if (rc) return rc;
     CK(cudaStreamSynchronize(h->stream));
     const int dim = h->dim;

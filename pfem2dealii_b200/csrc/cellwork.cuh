@@ -117,6 +117,7 @@ __global__ void k_seed(StepArgs a, uint32_t* cell_start)
         Real xi[DIM], v[DIM];
         new_particle<DIM, Real>(a, a.S0, t, c, idx, id0 + t + 1, xi, v);
         if (k == 0) cell_start[c] = t;
+        if (a.chunk_first && t % ADV_CH == 0) a.chunk_first[t / ADV_CH] = c;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) cell_start[a.mesh.nC] = total;
 }
@@ -897,7 +898,13 @@ __global__ void __launch_bounds__(WR_WARPS * 32) k_write(StepArgs a)
             const unsigned long long ofw = __shfl_sync(0xffffffffu, h_off, jc);
             const uint32_t ub = (uint32_t)ubw, nseed_expect = (uint32_t)(ubw >> 32);
             const uint32_t off = (uint32_t)ofw, sb = (uint32_t)(ofw >> 32);
-            if (lane == 0) a.cs_new[c] = off;
+            if (lane == 0) {
+                a.cs_new[c] = off;
+                // the advect chunks that start in this cell's new range
+                if (a.chunk_first)
+                    for (uint32_t k = (off + ADV_CH - 1) / ADV_CH; (uint64_t)k * ADV_CH < (uint64_t)off + ub; ++k)
+                        a.chunk_first[k] = c;
+            }
             const uint32_t occ = __shfl_sync(0xffffffffu, h_occ, jc);
             // count - occupied parts <= max: no part above max + 1 particles
             const bool no_removal = !apply || (maxpp >= 0 && ub - nseed_expect <= occ + (uint32_t)maxpp);

@@ -23,7 +23,13 @@ constexpr int OCCW_MAX = 4;    // 64-bit part-occupancy words per cell
 constexpr int ARRCAP = 32;     // arrival slots per cell before the overflow list
 constexpr int CELL_WARPS = 4;  // warps per block of the warp-per-cell helper kernels
 constexpr int KEY_CACHE = 128; // (part, key) pairs cached per warp on the general path
-constexpr int ADV_CH = 768;    // particles per staged chunk of the FP32 advect pass
+constexpr int ADV_CH = 512;    // particles per staged chunk of the FP32 advect pass
+// cells whose velocity records an FP32 advect chunk stages with its particles
+// (a chunk spans about ADV_CH / particles-per-cell + 1 cells; beyond this
+// many, the chunk's particles read their records from global memory)
+template <int DIM> struct AdvRec {
+    static constexpr int MAXC = DIM == 3 ? 32 : 48;
+};
 constexpr int WR_WARPS = 4;    // write pass: warps per block
 constexpr int WR_CHC = 4;      // write pass: cells per warp chunk
 
@@ -118,6 +124,8 @@ struct StepArgs {
     unsigned long long* cocc;  // nC x occw: parts occupied after the move
     unsigned long long* cub;   // nC: new particles << 32 | slots needed
     unsigned long long* coff;  // nC + 1: exclusive scan of cub
+    uint32_t* chunk_first;     // per ADV_CH-slot chunk of the layout the step writes: the cell its first slot
+                               // belongs to (the seed and write passes fill it; null: not kept)
     const uint32_t* cs_old;    // nC + 1: cell ranges of S0
     uint32_t* cs_new;          // nC + 1: cell ranges of S1
     uint2* xq;                 // particles (index, sub-step) queued for FP64 relocation

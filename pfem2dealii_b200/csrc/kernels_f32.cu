@@ -40,7 +40,7 @@ static int smem_grid32(K kernel, int threads, int smem)
 template <int DIM>
 static int advect32_t(const StepArgs& a, cudaStream_t s)
 {
-    const int smem = 2 * (int)sizeof(AdvStage<DIM, float, ADV_CH>);
+    const int smem = 2 * (int)(sizeof(AdvStage<DIM, float, ADV_CH>) + sizeof(AdvRecStage<DIM>));
     if (a.mesh.all_affine) {
         static const int grid = smem_grid32(k_advect32<DIM, true>, 256, smem);
         return launch_pdl(k_advect32<DIM, true>, grid, 256, smem, s, a);

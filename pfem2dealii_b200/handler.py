@@ -5,9 +5,13 @@ reference; the solver-owned inputs (parameters, mesh, the FEM velocity
 vectors) are passed in explicitly instead of being fetched from a
 pfem2Solver.  Velocity vectors are component-major arrays of shape
 (dim, n_dofs), host numpy arrays or (for the *_device calls) CUDA tensors.
+The *_device calls run on the handle's own CUDA stream and are ordered
+against torch's current stream on both sides, so their tensors can be
+produced and consumed by torch operations without further synchronisation.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import dataclasses
 import json
@@ -124,6 +128,29 @@ class ParticleHandler:
         _lib.check(self.L.pfem2gpu_create(dim, prec, C.byref(params.to_c(dim)), C.byref(h)))
         self.h = h
         self.mesh = None
+        self._hs = None
+
+    @contextlib.contextmanager
+    def _torch_ordered(self):
+        """Order a device call against torch's current stream: the handle's
+        stream first waits for the work torch has queued (the tensors the
+        call reads may still be being written), and torch's stream then waits
+        for the call's work (the tensors it writes, and the reuse of freed
+        tensor memory), so the *_device calls compose with torch operations
+        like any torch operation."""
+        import torch
+
+        if self._hs is None:
+            self._hs = torch.cuda.ExternalStream(self.stream_handle())
+            self._ev = (torch.cuda.Event(), torch.cuda.Event())
+        cur = torch.cuda.current_stream()
+        self._ev[0].record(cur)
+        self._hs.wait_event(self._ev[0])
+        try:
+            yield
+        finally:
+            self._ev[1].record(self._hs)
+            cur.wait_event(self._ev[1])
 
     def close(self):
         if getattr(self, "h", None):
@@ -193,19 +220,24 @@ class ParticleHandler:
 
     # device-resident variants (torch CUDA tensors, float64, shape (dim, n_dofs))
     def seed_particles_device(self, dV):
-        self._ck(self.L.pfem2gpu_seed_device(self.h, _ptr(dV)))
+        with self._torch_ordered():
+            self._ck(self.L.pfem2gpu_seed_device(self.h, _ptr(dV)))
 
     def correct_particle_velocity_device(self, dV, dVold):
-        self._ck(self.L.pfem2gpu_correct_device(self.h, _ptr(dV), _ptr(dVold)))
+        with self._torch_ordered():
+            self._ck(self.L.pfem2gpu_correct_device(self.h, _ptr(dV), _ptr(dVold)))
 
     def move_particles_device(self, dV=None):
-        self._ck(self.L.pfem2gpu_move_device(self.h, _ptr(dV)))
+        with self._torch_ordered():
+            self._ck(self.L.pfem2gpu_move_device(self.h, _ptr(dV)))
 
     def project_particle_fields_device(self, dout):
-        self._ck(self.L.pfem2gpu_project_device(self.h, _ptr(dout)))
+        with self._torch_ordered():
+            self._ck(self.L.pfem2gpu_project_device(self.h, _ptr(dout)))
 
     def correct_particle_velocity_from_projection_device(self, dV):
-        self._ck(self.L.pfem2gpu_correct_from_projection_device(self.h, _ptr(dV)))
+        with self._torch_ordered():
+            self._ck(self.L.pfem2gpu_correct_from_projection_device(self.h, _ptr(dV)))
 
     def step_solver(self, V):
         """One time step with the solver's data flow: correct with Vold = the
@@ -217,7 +249,8 @@ class ParticleHandler:
     def step_device(self, dV, dVold, dout):
         """correct + move + project on device vectors as one CUDA graph
         (dVold None: the last projection)."""
-        self._ck(self.L.pfem2gpu_step_device(self.h, _ptr(dV), _ptr(dVold), _ptr(dout)))
+        with self._torch_ordered():
+            self._ck(self.L.pfem2gpu_step_device(self.h, _ptr(dV), _ptr(dVold), _ptr(dout)))
 
     # -- differentiated window (no counterpart in the reference) -------------
     def window_forward_device(self, steps, checkpoint_every, dV, dVold=None, dv0=None, dU=None):
@@ -229,14 +262,16 @@ class ParticleHandler:
             import torch
 
             dU = torch.empty_like(dV)
-        self._ck(self.L.pfem2gpu_window_forward_device(self.h, int(steps), int(checkpoint_every), _ptr(dV),
-                                                       _ptr(dVold), _ptr(dv0), _ptr(dU)))
+        with self._torch_ordered():
+            self._ck(self.L.pfem2gpu_window_forward_device(self.h, int(steps), int(checkpoint_every), _ptr(dV),
+                                                           _ptr(dVold), _ptr(dv0), _ptr(dU)))
         return dU
 
     def window_backward_device(self, dgU, dg_v0=None, dg_V=None, dg_Vold=None):
         """Adjoint of the last window forward for dJ/dU = dgU (CUDA tensors)."""
-        self._ck(self.L.pfem2gpu_window_backward_device(self.h, _ptr(dgU), _ptr(dg_v0), _ptr(dg_V),
-                                                        _ptr(dg_Vold)))
+        with self._torch_ordered():
+            self._ck(self.L.pfem2gpu_window_backward_device(self.h, _ptr(dgU), _ptr(dg_v0), _ptr(dg_V),
+                                                            _ptr(dg_Vold)))
 
     # -- the solver step's Q1 systems (src/pfem2fem.cpp:247-510, volume terms) ----
     FEM_PREDICTION, FEM_PRESSURE, FEM_CORRECTION = 0, 1, 2
@@ -377,7 +412,8 @@ class ParticleHandler:
         if dout is None:
             dout = torch.empty(max(6 * n, 1), dtype=torch.float32, device="cuda")
         got = C.c_int64()
-        self._ck(self.L.pfem2gpu_pack_output_device(self.h, _ptr(dout), dout.numel() // 6, C.byref(got)))
+        with self._torch_ordered():
+            self._ck(self.L.pfem2gpu_pack_output_device(self.h, _ptr(dout), dout.numel() // 6, C.byref(got)))
         return dout, got.value
 
     def output_particle_solution(self, timestep_number: int, directory: str = "."):

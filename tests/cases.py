@@ -4,6 +4,7 @@ property tests), built identically for the oracle and the GPU handler."""
 from __future__ import annotations
 
 import dataclasses
+import os
 
 import numpy as np
 
@@ -41,6 +42,39 @@ def cylinder(n_t=96, n_r=48, n_x=480, q=(4, 4), maxpp=2, S=3, dt=5e-4, old_scale
     m = M.turek_channel(n_t, n_r, n_x)
     V = M.field_at_dofs(m, M.cylinder_inflow(1.5))
     return Case("cylinder", m, V, old_scale * V, q, maxpp, S, dt)
+
+
+MESH3 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "Mesh3.tgz")
+
+
+def turek_mesh3(q=(4, 4), maxpp=2, S=3, dt=5e-4, old_scale=0.9):
+    """The reference's Turek benchmark mesh (cases/TurekBenchmark/Mesh3.tgz:
+    60,450 quads around a cylinder of radius 0.05 at (0.2, 0.2) in the
+    2.2 x 0.41 channel) with the parabolic inflow of Umax 1.5
+    (cases/TurekBenchmark/TurekBenchmark.cc:6-9), zero on the walls and the
+    cylinder."""
+    m = M.read_unv_native(MESH3)
+    V = M.field_at_dofs(m, M.cylinder_inflow(1.5))
+    return Case("turek_mesh3", m, V, old_scale * V, q, maxpp, S, dt)
+
+
+def noisy_start(case, sigma=0.01, seed=0):
+    """The case's seeded particles (FP64 form) with N(0, sigma) added to each
+    velocity component, drawn in id order: the initial particle velocities
+    of the Turek configuration.  Returns (particles, next_id) for
+    ParticleHandler.set_particles."""
+    from pfem2dealii_b200.handler import ParticleHandler
+
+    g = ParticleHandler(case.mesh.dim, params(case), "fp64")
+    g.initialize_maps(case.mesh)
+    g.seed_particles(case.V)
+    P = g.particles()
+    nid = g.stats()["next_id"]
+    g.close()
+    order = np.argsort(P["id"])
+    P["v"] = P["v"].copy()
+    P["v"][order] += np.random.default_rng(seed).normal(0.0, sigma, size=P["v"].shape)
+    return P, nid
 
 
 def cube(n=80, q=(4, 4, 4), maxpp=2, S=3, dt=1e-3, amplitude=0.1, seed=0, old_scale=0.9):

@@ -84,3 +84,59 @@ def test_fp32_vs_fp64_forms_full_duct():
     assert len(common) > 0.99 * len(P64["id"])
     xerr = np.linalg.norm(P64["x"][ia] - P32["x"][ib]) / np.linalg.norm(P64["x"][ia])
     assert xerr <= 1e-6, xerr
+
+
+def solver_flow_projection(case, precision, steps, start=None):
+    """`steps` time steps with the solver's data flow (V fixed, Vold = the
+    previous projection) as device steps; returns the last projection."""
+    import torch
+
+    g = ParticleHandler(case.mesh.dim, cases.params(case), precision)
+    g.initialize_maps(case.mesh)
+    g.seed_particles(case.V)
+    if start is not None:
+        g.set_particles(*start)
+    dV = torch.from_numpy(np.ascontiguousarray(case.V)).cuda()
+    out = torch.empty_like(dV)
+    g.project_particle_fields_device(out)
+    for _ in range(steps):
+        g.step_device(dV, None, out)
+    V = out.cpu().numpy()
+    st = g.stats()
+    g.close()
+    return V, st
+
+
+def rel_l2(a, b):
+    m = np.isfinite(a) & np.isfinite(b)
+    return np.linalg.norm((a - b)[m]) / np.linalg.norm(a[m])
+
+
+FORM_TOL = 1e-4  # relative L2 of the projected velocity, FP32 form against FP64 form
+
+
+def test_fp32_vs_fp64_config2_turek_mesh3_200_steps():
+    """Configuration 2 at full size: the reference's Turek mesh (60,450
+    quads, 16 ppc, 967,200 particles), initial velocities = inflow + N(0,
+    0.01), 200 steps at dt 5e-4 with 3 sub-steps.  The FP32 form's final
+    projected velocity is within 1e-4 relative L2 of the FP64 form's."""
+    case = cases.turek_mesh3()
+    start = cases.noisy_start(case)
+    V64, s64 = solver_flow_projection(case, "fp64", 200, start)
+    V32, s32 = solver_flow_projection(case, "fp32", 200, start)
+    assert s64["error_flags"] == 0 and s32["error_flags"] == 0
+    err = rel_l2(V64, V32)
+    assert err <= FORM_TOL, err
+    assert abs(s64["n_particles"] - s32["n_particles"]) < 1e-4 * s64["n_particles"]
+
+
+def test_fp32_vs_fp64_config3_duct_100_steps():
+    """Configuration 3 at full size: the 3.5 M-particle duct, 100 steps at
+    dt 2e-3 with the solver's data flow; FP32 within 1e-4 relative L2 of
+    FP64."""
+    case = cases.duct()
+    V64, s64 = solver_flow_projection(case, "fp64", 100)
+    V32, s32 = solver_flow_projection(case, "fp32", 100)
+    err = rel_l2(V64, V32)
+    assert err <= FORM_TOL, err
+    assert s64["error_flags"] == 0 and s32["error_flags"] == 0

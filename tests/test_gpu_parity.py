@@ -85,8 +85,10 @@ def test_fp64_solver_data_flow_bit_exact():
     copying the projection into the old solution, src/pfem2fem.cpp:523-524):
     every step corrects with Vold = the previous projection.  The host path
     (pfem2gpu_correct_from_projection, only V uploaded) and the device step
-    (pfem2gpu_step_device with dVold NULL) both equal the oracle fed its own
-    previous projection, bit for bit."""
+    (pfem2gpu_step_device with dVold NULL) both equal the oracle given the
+    same Vold (the GPU's previous projection, which it keeps on the device),
+    bit for bit; the projections agree to 1e-12 as everywhere (their
+    summation orders differ), and the two GPU paths agree bit for bit."""
     import torch
 
     c = cases.channel(32, 8, dt=0.02)
@@ -102,7 +104,7 @@ def test_fp64_solver_data_flow_bit_exact():
     gd.project_particle_fields_device(dout)
     assert_v_close(Vo, Vg, V_RTOL_FP64)
     for s in range(12):
-        Vo = o.step(c.V, Vo)
+        Vo = o.step(c.V, Vg)
         Vg = g.step_solver(c.V)
         gd.step_device(dV, None, dout)
         assert_same_particles(o.particles(), g.particles())
