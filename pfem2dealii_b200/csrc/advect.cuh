@@ -327,25 +327,45 @@ struct AdvRecStage {
     uint32_t cfirst, ncell;
 };
 
+// A chunk ticket and, for the record stage, the chunk's first and last
+// cells: the cells from the chunk's first cell to the next chunk's first
+// cell, as the seed and write passes recorded them.  Thread 0 draws tickets
+// ahead and issues these loads early, so their latency passes while the
+// block works on earlier chunks.
+struct ChunkTicket {
+    uint32_t tk, cf, cl;
+};
+
+template <int CH>
+__device__ __forceinline__ void ticket_cells(const StepArgs& a, uint32_t n, ChunkTicket& t, bool recs)
+{
+    const uint32_t nchunks = (n + CH - 1) / CH;
+    t.cf = 1u;
+    t.cl = 0u;  // no range unless loaded
+    if (recs && t.tk < nchunks) {
+        t.cf = a.chunk_first[t.tk];
+        t.cl = t.tk + 1 < nchunks ? a.chunk_first[t.tk + 1] : (uint32_t)a.mesh.nC - 1;
+    }
+}
+
 // Thread 0: bulk-copy particles [chunk*CH, chunk*CH + cnt) of S0 into stage
-// st, and (rs not null) the records of their cells into rs: the cells from
-// the chunk's first cell to the next chunk's first cell, as the seed and
-// write passes recorded them (a range that is out of order or too long is
-// not staged; the particles then read their records from global memory).
+// st, and (rs not null) the records of the chunk's cells [t.cf, t.cl] into
+// rs (a range that is out of order or too long is not staged; the particles
+// then read their records from global memory).
 template <int DIM, typename Real, int CH>
 __device__ __forceinline__ void stage_chunk(const StepArgs& a, AdvStage<DIM, Real, CH>& st, uint64_t* bar,
-                                            uint32_t chunk, uint32_t n, AdvRecStage<DIM>* rs = nullptr)
+                                            const ChunkTicket& t, uint32_t n, AdvRecStage<DIM>* rs = nullptr)
 {
     constexpr bool HX = std::is_same<Real, double>::value;
+    const uint32_t chunk = t.tk;
     const uint32_t base = chunk * CH;
     const uint32_t cnt = n - base < (uint32_t)CH ? n - base : (uint32_t)CH;
     const uint32_t b4 = round16(cnt * 4u), br = round16(cnt * (uint32_t)sizeof(Real));
     uint32_t cf = 0, nrec = 0;
     if (rs) {
         const uint32_t nC = (uint32_t)a.mesh.nC;
-        cf = a.chunk_first[chunk];
-        const uint32_t cl = base + CH < n ? a.chunk_first[chunk + 1] : nC - 1;
-        if (cf <= cl && cl < nC && cl - cf < (uint32_t)AdvRecStage<DIM>::MAXC) nrec = cl - cf + 1;
+        cf = t.cf;
+        if (t.cf <= t.cl && t.cl < nC && t.cl - t.cf < (uint32_t)AdvRecStage<DIM>::MAXC) nrec = t.cl - t.cf + 1;
         rs->cfirst = cf;
         rs->ncell = nrec;
     }
@@ -365,12 +385,16 @@ __device__ __forceinline__ void stage_chunk(const StepArgs& a, AdvStage<DIM, Rea
     }
 }
 
-// The chunk loop shared by both forms: double-buffered staging, f(stage, t,
-// i, active) per particle slot (every lane of every warp calls it, so warp
-// collectives are allowed inside).  Chunks are handed out one at a time from
-// a counter (stats->adv_next, reset when the step is finalised), so blocks
-// that drew cheap chunks take more; a block holds tickets for the chunk it
-// processes and the one being staged.
+// The chunk loop shared by both forms: double-buffered staging, f(stage,
+// buffer, t, i, active) per particle slot (every lane of every warp calls it,
+// so warp collectives are allowed inside).  Chunks are handed out one at a
+// time from a counter (stats->adv_next, reset when the step is finalised), so
+// blocks that drew cheap chunks take more.  A block holds the chunks it works
+// on and stages, and thread 0 keeps one more ticket in hand: it loads that
+// chunk's cell range and draws the ticket after it while the block works, so
+// restaging a buffer waits on no memory.  One barrier per chunk: the reads of
+// a buffer end there, and a ticket written after it is read only after the
+// next chunk's barrier.
 template <int DIM, typename Real, int CH, typename F>
 __device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Real, CH>* st, uint64_t* bar, F&& f,
                                             AdvRecStage<DIM>* rs = nullptr)
@@ -378,6 +402,8 @@ __device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Rea
     __shared__ uint32_t tk[2];
     const uint32_t n = (uint32_t)a.stats->n_slots;
     const uint32_t nchunks = (n + CH - 1) / CH;
+    const bool recs = rs != nullptr;
+    ChunkTicket hand{0u, 1u, 0u};  // thread 0: the next chunk to stage
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -387,9 +413,12 @@ __device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Rea
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
-            tk[b] = atomicAdd(&a.stats->adv_next, 1u);
-            if (tk[b] < nchunks) stage_chunk<DIM, Real, CH>(a, st[b], &bar[b], tk[b], n, rs ? rs + b : nullptr);
+            ChunkTicket t{atomicAdd(&a.stats->adv_next, 1u), 1u, 0u};
+            ticket_cells<CH>(a, n, t, recs);
+            tk[b] = t.tk;
+            if (t.tk < nchunks) stage_chunk<DIM, Real, CH>(a, st[b], &bar[b], t, n, recs ? rs + b : nullptr);
         }
+        hand.tk = atomicAdd(&a.stats->adv_next, 1u);
     }
     __syncthreads();
     for (uint32_t it = 0;; ++it) {
@@ -403,20 +432,24 @@ __device__ __forceinline__ void staged_loop(const StepArgs& a, AdvStage<DIM, Rea
             if (tk[sidx ^ 1] < nchunks) mbar_wait(&bar[sidx ^ 1], ((it + 1) >> 1) & 1u);
             return;
         }
+        uint32_t after = 0;
+        if (threadIdx.x == 0) {  // loads and a ticket in flight while the block works
+            ticket_cells<CH>(a, n, hand, recs);
+            after = hand.tk < nchunks ? atomicAdd(&a.stats->adv_next, 1u) : 0xffffffffu;
+        }
         const uint32_t base = chunk * CH;
         const uint32_t cnt = n - base < (uint32_t)CH ? n - base : (uint32_t)CH;
 #pragma unroll 1
         for (uint32_t t = threadIdx.x; t < (uint32_t)CH; t += blockDim.x) f(st[sidx], sidx, t, base + t, t < cnt);
         __syncthreads();
         if (threadIdx.x == 0) {
-            const uint32_t nxt = atomicAdd(&a.stats->adv_next, 1u);
-            tk[sidx] = nxt;
-            if (nxt < nchunks) {
+            tk[sidx] = hand.tk;
+            if (hand.tk < nchunks) {
                 fence_proxy_async();
-                stage_chunk<DIM, Real, CH>(a, st[sidx], &bar[sidx], nxt, n, rs ? rs + sidx : nullptr);
+                stage_chunk<DIM, Real, CH>(a, st[sidx], &bar[sidx], hand, n, recs ? rs + sidx : nullptr);
             }
+            hand.tk = after;
         }
-        __syncthreads();
     }
 }
 
