@@ -51,7 +51,18 @@ typedef struct pfem2gpu_params {
     uint32_t removal_seed;                /* over-full parts keep the smallest key(id); 0: key = id */
     int32_t empty_dof_policy;             /* 0: reference (0/0 = NaN at DoFs no particle reaches); 1: keep input V */
     int64_t capacity;                     /* particle capacity (0: 2 x cells x parts) */
+    int32_t integrator;                   /* PFEM2GPU_EULER (the reference's sub-steps) or PFEM2GPU_RK2 */
 } pfem2gpu_params;
+
+/* Sub-step integrators.  Euler is the reference's move_particles
+ * (src/pfem2particlehandler.cpp:151-163): x += h u(xi).  RK2 has no
+ * counterpart in the reference: the midpoint rule in the particle's own cell,
+ * x += h u(xi_mid) with xi_mid = xi + (h/2) J(xi)^-1 u(xi) and u the cell's Q1
+ * field (extrapolated where xi_mid lies outside the unit cell; a
+ * non-positive Jacobian determinant falls back to u(xi)); second order.  The
+ * differentiated window supports Euler only (PFEM2GPU_ERR_ARG with RK2). */
+#define PFEM2GPU_EULER 0
+#define PFEM2GPU_RK2 1
 
 typedef struct pfem2gpu_stats {
     int64_t n_particles;

@@ -17,6 +17,8 @@ _SO = os.path.join(_HERE, "_build", "liboracle.so")
 
 ORDER_ID = 0
 ORDER_VECTOR = 1
+EULER = 0  # sub-step integrators (orc_params.integrator)
+RK2 = 1
 
 
 class Params(C.Structure):
@@ -28,6 +30,7 @@ class Params(C.Structure):
         ("removal_order", C.c_int32),
         ("removal_seed", C.c_uint32),
         ("n_threads", C.c_int32),
+        ("integrator", C.c_int32),
     ]
 
 
@@ -111,7 +114,7 @@ class Oracle:
     """FP64 restatement of pfem2ParticleHandler (src/pfem2particlehandler.h:17-71)."""
 
     def __init__(self, mesh, q, max_per_part, substeps, dt, removal_order=ORDER_ID, removal_seed=0,
-                 n_threads=1):
+                 n_threads=1, integrator=EULER):
         self.L = lib()
         self.dim = mesh.dim
         p = Params()
@@ -123,6 +126,7 @@ class Oracle:
         p.removal_order = removal_order
         p.removal_seed = removal_seed
         p.n_threads = n_threads
+        p.integrator = integrator
         self.h = self.L.orc_create(self.dim, C.byref(p))
         if not self.h:
             raise ValueError("orc_create failed")

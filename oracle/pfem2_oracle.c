@@ -695,6 +695,30 @@ typedef struct {
     reloc_counts rc;
 } move_task;
 
+/* The transport velocity of one sub-step from reference coordinates xi of
+ * cell c.  Euler (the reference, move_particles :151-159): u(xi).  RK2, an
+ * opt-in with no counterpart in the reference: the midpoint rule in the
+ * particle's own cell, u(xi_mid) with xi_mid = xi + (h/2) J(xi)^-1 u(xi) and
+ * u the cell's Q1 field (extrapolated where xi_mid lies outside the unit
+ * cell).  xi_mid is the midpoint's exact reference position on affine cells
+ * and within O(h^2) of it on others, so the scheme is second order.  A
+ * non-positive Jacobian determinant falls back to u(xi). */
+static void transport_velocity(const orc_handle* h, int64_t c, const double* xi, const double* V, double* u)
+{
+    interp(h, c, xi, V, u);
+    if (h->prm.integrator != ORC_RK2) return;
+    const int dim = h->dim;
+    double Xc[MAXV * 3], J[3][3], Ji[3][3], dl[3], xm[3];
+    cell_coords(h, c, Xc);
+    jacobian(dim, Xc, xi, J);
+    const double det = invert(dim, J, Ji);
+    if (!(det > 0.0)) return;
+    matvec(dim, Ji, u, dl);
+    const double half = h->dtp * 0.5;
+    for (int d = 0; d < dim; ++d) xm[d] = xi[d] + half * dl[d];
+    interp(h, c, xm, V, u);
+}
+
 static void move_range(move_task* t)
 {
     orc_handle* h = t->h;
@@ -705,7 +729,7 @@ static void move_range(move_task* t)
         for (int s = 0; s < h->S; ++s) {
             /* move_particles :151-163 */
             double u[3], step[3];
-            interp(h, q->cell, q->xi, t->V, u);
+            transport_velocity(h, q->cell, q->xi, t->V, u);
             for (int d = 0; d < dim; ++d) {
                 q->vext[d] = u[d];
                 step[d] = u[d] * h->dtp;
@@ -1139,6 +1163,7 @@ static int window_forward(const orc_handle* h, int K, const double* V, const dou
 int orc_window_forward(orc_handle* h, int K, const double* V, const double* Vold, const double* v0,
                        int empty_policy, double* U)
 {
+    if (h->prm.integrator != ORC_EULER) return -2; /* the window differentiates Euler sub-steps */
     if (!h->X || K < 0) return -1;
     const int64_t n = h->n;
     orc_particle* fin = (orc_particle*)malloc(sizeof(orc_particle) * (n ? n : 1));
@@ -1156,6 +1181,7 @@ int orc_window_forward(orc_handle* h, int K, const double* V, const double* Vold
 int orc_window_particles(orc_handle* h, int K, const double* V, const double* Vold, const double* v0, int32_t* cell,
                          double* x, double* xi, double* v)
 {
+    if (h->prm.integrator != ORC_EULER) return -2; /* the window differentiates Euler sub-steps */
     if (!h->X || K < 0) return -1;
     const int dim = h->dim;
     for (int64_t p = 0; p < h->n; ++p) {
@@ -1179,6 +1205,7 @@ int orc_window_particles(orc_handle* h, int K, const double* V, const double* Vo
 int orc_window_adjoint(orc_handle* h, int K, const double* V, const double* Vold, const double* v0,
                        int empty_policy, const double* gU, double* U, double* g_v0, double* g_V, double* g_Vold)
 {
+    if (h->prm.integrator != ORC_EULER) return -2; /* the window differentiates Euler sub-steps */
     if (!h->X || K < 0) return -1;
     const int dim = h->dim, nv = h->nv, S = h->S;
     const int64_t n = h->n, nD = h->nD;

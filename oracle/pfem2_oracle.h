@@ -39,7 +39,13 @@ typedef struct orc_params {
     int32_t removal_order;        /* ORC_ORDER_* */
     uint32_t removal_seed;        /* key(id) = seed ? mix32(id ^ seed) : id */
     int32_t n_threads;            /* >1: parallel particle loops (baseline timing) */
+    int32_t integrator;           /* ORC_EULER (the reference) or ORC_RK2 (opt-in, see orc_move) */
 } orc_params;
+
+enum {
+    ORC_EULER = 0, /* x += h u(xi): move_particles, src/pfem2particlehandler.cpp:151-163 */
+    ORC_RK2 = 1    /* midpoint rule in the particle's own cell; no reference counterpart */
+};
 
 typedef struct orc_stats {
     int64_t n_particles;

@@ -53,6 +53,7 @@ class Params(C.Structure):
         ("removal_seed", C.c_uint32),
         ("empty_dof_policy", C.c_int32),
         ("capacity", C.c_int64),
+        ("integrator", C.c_int32),
     ]
 
 

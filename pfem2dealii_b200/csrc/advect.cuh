@@ -479,9 +479,32 @@ __device__ __forceinline__ void velocity64(const double* __restrict__ Vc, uint32
         for (int d = 0; d < DIM; ++d) u[d] = u[d] + N[iv] * __ldg(p + iv * VS + d);
 }
 
+// The transport velocity of a sub-step from xi in cell c (vertices X).
+// Euler (move_particles :151-159): u(xi).  RK2 (PFEM2GPU_RK2, no reference
+// counterpart): u(xi_mid), xi_mid = xi + (h/2) J(xi)^-1 u(xi), the cell's Q1
+// field extrapolated where xi_mid leaves the unit cell; a non-positive
+// Jacobian determinant keeps u(xi).  The oracle's transport_velocity does the
+// same operations in the same order.
+template <int DIM, bool RK>
+__device__ __forceinline__ void transport64(const StepArgs& a, const double (*X)[DIM], uint32_t c, const double* xi,
+                                            double* u)
+{
+    velocity64<DIM>((const double*)a.Vc, c, xi, u);
+    if constexpr (!RK) return;
+    double J[DIM][DIM], Ji[DIM][DIM], dl[DIM], xm[DIM];
+    jac64<DIM>(X, xi, J);
+    const double det = invert64<DIM>(J, Ji);
+    if (!(det > 0.0)) return;
+    matvec64<DIM>(Ji, u, dl);
+    const double half = a.pp.dtp * 0.5;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) xm[d] = xi[d] + half * dl[d];
+    velocity64<DIM>((const double*)a.Vc, c, xm, u);
+}
+
 // Sub-steps s0.. of one FP64 particle starting in cell c; returns the
 // sub-step at which it leaves its cell (S if it never does).
-template <int DIM>
+template <int DIM, bool RK>
 __device__ __forceinline__ int substeps64(const StepArgs& a, uint32_t c, int s0, double* x, double* xi, double* u,
                                           AdvCounters& k)
 {
@@ -491,7 +514,7 @@ __device__ __forceinline__ int substeps64(const StepArgs& a, uint32_t c, int s0,
     load_cell64<DIM>(m.cellX, c, X);
     int s = s0;
     for (; s < a.pp.S; ++s) {
-        velocity64<DIM>((const double*)a.Vc, c, xi, u);
+        transport64<DIM, RK>(a, X, c, xi, u);
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
             const double st = u[d] * a.pp.dtp;
@@ -513,7 +536,7 @@ __device__ __forceinline__ int substeps64(const StepArgs& a, uint32_t c, int s0,
 
 constexpr int ADV64_CH = 512;
 
-template <int DIM>
+template <int DIM, bool RK>
 __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
 {
     pdl_entry();
@@ -546,7 +569,7 @@ __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) v[d] = v[d] + corr[d];
                 }
-                s = substeps64<DIM>(a, c, 0, x, xi, u, k);
+                s = substeps64<DIM, RK>(a, c, 0, x, xi, u, k);
                 want = s < a.pp.S;
             }
 #pragma unroll
@@ -571,7 +594,7 @@ __global__ void __launch_bounds__(256) k_advect64(StepArgs a)
 
 // Deferred FP64 particles: the search of sub-step s (:438-491), then the
 // remaining sub-steps (searching again whenever needed).
-template <int DIM>
+template <int DIM, bool RK>
 __global__ void __launch_bounds__(128) k_search64(StepArgs a)
 {
     pdl_entry();
@@ -593,7 +616,13 @@ __global__ void __launch_bounds__(128) k_search64(StepArgs a)
         bool alive = true;
         while (true) {
             // velocity_ext of sub-step s, recomputed from the start-of-sub-step state
-            velocity64<DIM>((const double*)a.Vc, c, xi, u);
+            if constexpr (RK) {
+                double X[1 << DIM][DIM];
+                load_cell64<DIM>(m.cellX, c, X);
+                transport64<DIM, RK>(a, X, c, xi, u);
+            } else {
+                velocity64<DIM>((const double*)a.Vc, c, xi, u);
+            }
             Vec<DIM> xo, ve, xp;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
@@ -613,7 +642,7 @@ __global__ void __launch_bounds__(128) k_search64(StepArgs a)
             c = so.cell;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) xi[d] = so.xi[d];
-            s = substeps64<DIM>(a, c, s + 1, x, xi, u, k);
+            s = substeps64<DIM, RK>(a, c, s + 1, x, xi, u, k);
             if (s >= a.pp.S) break;
         }
 #pragma unroll
@@ -724,11 +753,33 @@ __device__ __noinline__ F3<DIM> newton32(const float* __restrict__ geo, uint32_t
     return out;
 }
 
+// RK2 midpoint of a non-affine cell in the FP32 form: xi + (h/2) J(xi)^-1 u
+// with the cell's FP32 geometry, out of line (by value); xi itself when the
+// Jacobian determinant is not positive.
+template <int DIM>
+__device__ __noinline__ F3<DIM> midpoint32(const float* __restrict__ geo, uint32_t c, F3<DIM> xi, F3<DIM> u, float hh)
+{
+    Geo32<DIM> g;
+    load_geo32<DIM>(geo, c, g);
+    float J[DIM][DIM], Ji[DIM][DIM];
+    jac32<DIM>(g, xi.v, J);
+    F3<DIM> out = xi;
+    if (!(invert32<DIM>(J, Ji) > 0.0f)) return out;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        float s = 0.0f;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) s += Ji[k][d] * u.v[d];
+        out.v[k] = xi.v[k] + hh * s;
+    }
+    return out;
+}
+
 // FP32 sub-steps s0.. in cell c; returns the sub-step that leaves the cell
 // (S if none).  xi is advanced in place.  AFF: every cell of the mesh is
 // affine, so the Newton branch (an out-of-line call whose saved registers
 // would spill in the hot loop) is left out.
-template <int DIM, bool AFF = false>
+template <int DIM, bool AFF = false, bool RK = false>
 __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi, const Rec32<DIM>& r)
 {
     const float dtp = (float)a.pp.dtp;
@@ -736,6 +787,24 @@ __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0,
     for (; s < a.pp.S; ++s) {
         float w[DIM], dl[DIM], y[DIM];
         eval_poly<DIM>(r.b, xi, w);
+        if constexpr (RK) {  // the midpoint rule: w (or u) at xi + (h/2) J^-1 u
+            float xm[DIM];
+            if (AFF || r.affine) {
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) xm[d] = xi[d] + (0.5f * dtp) * w[d];
+            } else {
+                F3<DIM> x0, u0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    x0.v[d] = xi[d];
+                    u0.v[d] = w[d];
+                }
+                const F3<DIM> mid = midpoint32<DIM>(a.mesh.geo32, c, x0, u0, 0.5f * dtp);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) xm[d] = mid.v[d];
+            }
+            eval_poly<DIM>(r.b, xm, w);
+        }
         bool ok = true;
         if (AFF || r.affine) {
 #pragma unroll
@@ -761,15 +830,15 @@ __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0,
     return s;
 }
 
-template <int DIM, bool AFF = false>
+template <int DIM, bool AFF = false, bool RK = false>
 __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi)
 {
     Rec32<DIM> r;
     load_rec32<DIM>(a.vrec32, c, r);
-    return substeps32<DIM, AFF>(a, c, s0, xi, r);
+    return substeps32<DIM, AFF, RK>(a, c, s0, xi, r);
 }
 
-template <int DIM, bool AFF>
+template <int DIM, bool AFF, bool RK = false>
 __global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
 {
     pdl_entry();
@@ -812,7 +881,7 @@ __global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
                 Rec32<DIM> r;
                 if (srec) load_rec32_s<DIM>(rsg.v[lc], r);
                 else load_rec32<DIM>(a.vrec32, c, r);
-                s = substeps32<DIM, AFF>(a, c, 0, xi, r);
+                s = substeps32<DIM, AFF, RK>(a, c, 0, xi, r);
                 want = s < a.pp.S;
             }
 #pragma unroll
@@ -837,7 +906,7 @@ __global__ void __launch_bounds__(256, AFF ? 4 : 3) k_advect32(StepArgs a)
 // Queued FP32 particles: FP64 relocation of sub-step s (x = F(xi) + u dt_p,
 // own cell first, then the vertex-patch search), then the remaining
 // sub-steps in FP32 (relocating in FP64 again whenever needed).
-template <int DIM, bool AFF>
+template <int DIM, bool AFF, bool RK>
 __device__ __forceinline__ void cross32(const StepArgs& a)
 {
     const uint32_t nq = *a.nxq < a.capacity ? *a.nxq : a.capacity;
@@ -858,6 +927,17 @@ __device__ __forceinline__ void cross32(const StepArgs& a)
 #pragma unroll
             for (int d = 0; d < DIM; ++d) xo.v[d] = (double)xi[d];
             velocity_from_dofs<DIM>(m.cd, a.Vd, m.nD, c, xo.v, ue.v);
+            if constexpr (RK) {  // the midpoint rule in FP64 (transport64's operations)
+                double X[1 << DIM][DIM], J[DIM][DIM], Ji[DIM][DIM], dl[DIM], xm[DIM];
+                load_cell64<DIM>(m.cellX, c, X);
+                jac64<DIM>(X, xo.v, J);
+                if (invert64<DIM>(J, Ji) > 0.0) {
+                    matvec64<DIM>(Ji, ue.v, dl);
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) xm[d] = xo.v[d] + (a.pp.dtp * 0.5) * dl[d];
+                    velocity_from_dofs<DIM>(m.cd, a.Vd, m.nD, c, xm, ue.v);
+                }
+            }
             k.fallback++;
             const uint32_t c0 = c;
             const SearchOut so = fallback64<DIM, AFF>(m, c, xo, ue, a.pp.dtp);
@@ -875,7 +955,7 @@ __device__ __forceinline__ void cross32(const StepArgs& a)
                 const float t = (float)so.xi[d];
                 xi[d] = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
             }
-            s = substeps32<DIM, AFF>(a, c, s + 1, xi);
+            s = substeps32<DIM, AFF, RK>(a, c, s + 1, xi);
             if (s >= a.pp.S) break;
         }
 #pragma unroll
@@ -887,21 +967,21 @@ __device__ __forceinline__ void cross32(const StepArgs& a)
     flush_counters(a, k);
 }
 
-template <int DIM, bool AFF = false>
+template <int DIM, bool AFF = false, bool RK = false>
 __global__ void __launch_bounds__(128) k_cross32(StepArgs a)
 {
     pdl_entry();
-    cross32<DIM, AFF>(a);
+    cross32<DIM, AFF, RK>(a);
 }
 
 // The same for 2D meshes with non-affine cells (many crossers, each a chain
 // of dependent loads): 6 blocks per SM (80 registers, a few spills); more
 // blocks cost the 3D forms about 10 %.
-template <int DIM>
+template <int DIM, bool RK = false>
 __global__ void __launch_bounds__(128, 6) k_cross32_occ(StepArgs a)
 {
     pdl_entry();
-    cross32<DIM, false>(a);
+    cross32<DIM, false, RK>(a);
 }
 
 }  // namespace pfem2

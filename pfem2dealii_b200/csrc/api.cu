@@ -731,6 +731,7 @@ int window_forward_impl(pfem2gpu_handle* h, int K, int C, const double* V, const
                         double* U_out, bool host)
 {
     if (!h || !V || K < 0 || C < 1) return PFEM2GPU_ERR_ARG;
+    if (h->pp.rk2) return fail(h, PFEM2GPU_ERR_ARG, "the differentiated window supports Euler sub-steps only");
     if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "window before seed");
     if ((int64_t)C * h->pp.S > 100000) return fail(h, PFEM2GPU_ERR_ARG, "checkpoint_every x sub-steps too large");
     int rc = apply_pending_correction(h);
@@ -891,6 +892,7 @@ int pfem2gpu_create(int dim, int precision, const pfem2gpu_params* prm, pfem2gpu
     }
     if (npe > NPE_MAX) return PFEM2GPU_ERR_ARG;
     if (!(std::isfinite(prm->time_step)) || prm->particle_integration_steps < 0) return PFEM2GPU_ERR_ARG;
+    if (prm->integrator != PFEM2GPU_EULER && prm->integrator != PFEM2GPU_RK2) return PFEM2GPU_ERR_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -912,6 +914,7 @@ int pfem2gpu_create(int dim, int precision, const pfem2gpu_params* prm, pfem2gpu
     pp.S = prm->particle_integration_steps == 0 ? 1 : prm->particle_integration_steps;  // :34-36
     pp.dtp = prm->time_step / (double)pp.S;                                               // :38
     pp.seed = prm->removal_seed;
+    pp.rk2 = prm->integrator == PFEM2GPU_RK2 ? 1 : 0;
     pp.occw = (npe + 63) / 64;
     for (int w = 0; w < OCCW_MAX; ++w) pp.realmask[w] = 0;
     for (int e = 0; e < npe; ++e) {  // extended-part digits, x-major, base q_d + 1

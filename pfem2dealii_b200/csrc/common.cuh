@@ -85,6 +85,7 @@ struct PartParams {
     int maxpp;     // maximum particles per cell part (max+1 survive)
     int S;         // sub-steps
     double dtp;    // dt / S
+    int rk2;       // sub-steps by the midpoint rule (PFEM2GPU_RK2) instead of Euler
     double h[3];   // 1.0 / q
     uint32_t seed; // removal key seed
     unsigned long long realmask[OCCW_MAX];  // real parts among the extended parts, 64 per word

@@ -37,41 +37,45 @@ static int smem_grid32(K kernel, int threads, int smem)
     return sms * (per > 0 ? per : 1);
 }
 
-template <int DIM>
+// RK: the midpoint sub-step (params.integrator = PFEM2GPU_RK2), compiled as
+// its own kernels so that the Euler ones carry no trace of it.
+template <int DIM, bool RK>
 static int advect32_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = 2 * (int)(sizeof(AdvStage<DIM, float, ADV_CH>) + sizeof(AdvRecStage<DIM>));
     if (a.mesh.all_affine) {
-        static const int grid = smem_grid32(k_advect32<DIM, true>, 256, smem);
-        return launch_pdl(k_advect32<DIM, true>, grid, 256, smem, s, a);
+        static const int grid = smem_grid32(k_advect32<DIM, true, RK>, 256, smem);
+        return launch_pdl(k_advect32<DIM, true, RK>, grid, 256, smem, s, a);
     } else {
-        static const int grid = smem_grid32(k_advect32<DIM, false>, 256, smem);
-        return launch_pdl(k_advect32<DIM, false>, grid, 256, smem, s, a);
+        static const int grid = smem_grid32(k_advect32<DIM, false, RK>, 256, smem);
+        return launch_pdl(k_advect32<DIM, false, RK>, grid, 256, smem, s, a);
     }
-    return 1;
 }
 
-template <int DIM>
+template <int DIM, bool RK>
 static int cross32_t(const StepArgs& a, cudaStream_t s)
 {
-    if (a.mesh.all_affine) return launch_pdl(k_cross32<DIM, true>, PFEM2_GRID((k_cross32<DIM, true>), 128), 128, 0, s, a);
+    if (a.mesh.all_affine)
+        return launch_pdl(k_cross32<DIM, true, RK>, PFEM2_GRID((k_cross32<DIM, true, RK>), 128), 128, 0, s, a);
     if constexpr (DIM == 2)
-        return launch_pdl(k_cross32_occ<DIM>, PFEM2_GRID((k_cross32_occ<DIM>), 128), 128, 0, s, a);
+        return launch_pdl(k_cross32_occ<DIM, RK>, PFEM2_GRID((k_cross32_occ<DIM, RK>), 128), 128, 0, s, a);
     else
-        return launch_pdl(k_cross32<DIM, false>, PFEM2_GRID((k_cross32<DIM, false>), 128), 128, 0, s, a);
+        return launch_pdl(k_cross32<DIM, false, RK>, PFEM2_GRID((k_cross32<DIM, false, RK>), 128), 128, 0, s, a);
 }
 
 int launch_advect(int dim, int prec, const StepArgs& a, cudaStream_t s)
 {
     if (prec == 0) return launch64_advect(dim, a, s);
-    return dim == 2 ? advect32_t<2>(a, s) : advect32_t<3>(a, s);
+    if (a.pp.rk2) return dim == 2 ? advect32_t<2, true>(a, s) : advect32_t<3, true>(a, s);
+    return dim == 2 ? advect32_t<2, false>(a, s) : advect32_t<3, false>(a, s);
 }
 
 // The queued face crossers of the advect pass (relocation in FP64).
 int launch_cross(int dim, int prec, const StepArgs& a, cudaStream_t s)
 {
     if (prec == 0) return launch64_cross(dim, a, s);
-    return dim == 2 ? cross32_t<2>(a, s) : cross32_t<3>(a, s);
+    if (a.pp.rk2) return dim == 2 ? cross32_t<2, true>(a, s) : cross32_t<3, true>(a, s);
+    return dim == 2 ? cross32_t<2, false>(a, s) : cross32_t<3, false>(a, s);
 }
 
 template <int DIM, int CHC>

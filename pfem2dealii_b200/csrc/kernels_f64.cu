@@ -116,25 +116,32 @@ static int smem_grid(K kernel, int threads, int smem)
     return sms * (per > 0 ? per : 1);
 }
 
-template <int DIM>
+// RK: the midpoint sub-step (params.integrator = PFEM2GPU_RK2), compiled as
+// its own kernels so that the Euler ones carry no trace of it.
+template <int DIM, bool RK>
 static int advect_t(const StepArgs& a, cudaStream_t s)
 {
     const int smem = 2 * (int)sizeof(AdvStage<DIM, double, ADV64_CH>);
-    static const int grid = smem_grid(k_advect64<DIM>, 256, smem);
-    return launch_pdl(k_advect64<DIM>, grid, 256, smem, s, a);
-    return 1;
+    static const int grid = smem_grid(k_advect64<DIM, RK>, 256, smem);
+    return launch_pdl(k_advect64<DIM, RK>, grid, 256, smem, s, a);
+}
+
+template <int DIM, bool RK>
+static int search_t(const StepArgs& a, cudaStream_t s)
+{
+    return launch_pdl(k_search64<DIM, RK>, PFEM2_GRID((k_search64<DIM, RK>), 128), 128, 0, s, a);
 }
 
 int launch64_advect(int dim, const StepArgs& a, cudaStream_t s)
 {
-    return dim == 2 ? advect_t<2>(a, s) : advect_t<3>(a, s);
+    if (a.pp.rk2) return dim == 2 ? advect_t<2, true>(a, s) : advect_t<3, true>(a, s);
+    return dim == 2 ? advect_t<2, false>(a, s) : advect_t<3, false>(a, s);
 }
 
 int launch64_cross(int dim, const StepArgs& a, cudaStream_t s)
 {
-    if (dim == 2) return launch_pdl(k_search64<2>, PFEM2_GRID(k_search64<2>, 128), 128, 0, s, a);
-    return launch_pdl(k_search64<3>, PFEM2_GRID(k_search64<3>, 128), 128, 0, s, a);
-    return 1;
+    if (a.pp.rk2) return dim == 2 ? search_t<2, true>(a, s) : search_t<3, true>(a, s);
+    return dim == 2 ? search_t<2, false>(a, s) : search_t<3, false>(a, s);
 }
 
 template <int DIM, int CHC>

@@ -16,6 +16,7 @@
 # compiles unchanged.  PFEM2_B200_FP32=ON selects the FP32 form.
 option(PFEM2_WITH_B200 "pfem2ParticleHandler on one B200 (libpfem2gpu.so)" OFF)
 option(PFEM2_B200_FP32 "with PFEM2_WITH_B200: the FP32 form instead of the FP64 form" OFF)
+option(PFEM2_B200_RK2 "with PFEM2_WITH_B200: midpoint (RK2) sub-steps instead of the reference's Euler" OFF)
 get_filename_component(PFEM2_B200_ROOT "${CMAKE_CURRENT_LIST_DIR}/../.." ABSOLUTE)
 
 function(pfem2_b200_sources var)
@@ -33,6 +34,9 @@ function(pfem2_b200_link target)
     target_link_libraries(${target} PUBLIC "${PFEM2_B200_ROOT}/pfem2dealii_b200/_build/libpfem2gpu.so")
     if(PFEM2_B200_FP32)
       target_compile_definitions(${target} PRIVATE PFEM2_B200_FP32)
+    endif()
+    if(PFEM2_B200_RK2)
+      target_compile_definitions(${target} PRIVATE PFEM2_B200_RK2)
     endif()
   endif()
 endfunction()

@@ -37,7 +37,8 @@
 // solution every step instead.
 //
 // Form: the FP64 form (the reference's arithmetic) unless PFEM2_B200_FP32
-// is defined.  Errors of the C ABI throw std::runtime_error with the
+// is defined.  Sub-steps: Euler (the reference's) unless PFEM2_B200_RK2 is
+// defined (the midpoint rule, which the reference does not have).  Errors of the C ABI throw std::runtime_error with the
 // library's message; the reference throws deal.II exceptions.
 #include "pfem2particlehandler.h"
 
@@ -173,6 +174,9 @@ DeviceState<dim>& device_for(pfem2ParticleHandler<dim>* self, pfem2Solver<dim>* 
         p.max_particles_per_cell_part = (int32_t)max_per_part;
         p.particle_integration_steps = (int32_t)steps;
         p.time_step = solver->getParameterHandler().getTimeStep();
+#ifdef PFEM2_B200_RK2
+        p.integrator = PFEM2GPU_RK2;
+#endif
         check(pfem2gpu_create(dim, kPrecision, &p, &s.h), nullptr, "create");
     }
     if (!s.has_mesh) {

@@ -34,6 +34,7 @@ class ParticleParams:
     removal_seed: int = 0
     empty_dof_policy: int = 0
     capacity: int = 0
+    integrator: int = 0  # 0 Euler (the reference), 1 RK2 midpoint (opt-in)
 
     def to_c(self, dim):
         p = _lib.Params()
@@ -46,6 +47,7 @@ class ParticleParams:
         p.removal_seed = int(self.removal_seed)
         p.empty_dof_policy = int(self.empty_dof_policy)
         p.capacity = int(self.capacity)
+        p.integrator = int(self.integrator)
         return p
 
 

@@ -32,7 +32,7 @@ def adapter_object(tmp_path_factory):
         pytest.skip("the reference's src/ headers are not available (set PFEM2DEALII_SRC)")
     d = tmp_path_factory.mktemp("adapter")
     outs = []
-    for k, defs in enumerate(([], ["-DPFEM2_B200_FP32", "-DPFEM2_B200_UPLOAD_OLD_SOLUTION"])):
+    for k, defs in enumerate(([], ["-DPFEM2_B200_FP32", "-DPFEM2_B200_UPLOAD_OLD_SOLUTION", "-DPFEM2_B200_RK2"])):
         out = str(d / f"adapter{k}.o")
         cmd = ["g++", "-std=c++17", "-Wall", "-Wextra", "-Wno-ignored-qualifiers", "-Werror", *defs, "-c", ADAPTER,
                "-I", os.path.join(ROOT, "tests", "dealii_stub"), "-I", REF_SRC, "-I", os.path.join(ROOT, "include"),

@@ -422,3 +422,53 @@ def test_device_vertex_maps_collapsed_cell():
     assert np.array_equal(off, o2) and np.array_equal(cl, c2) and dirs.tobytes() == d2.tobytes()
     assert off[4] - off[3] == 2
     g.close()
+
+
+# The opt-in RK2 sub-step (PFEM2GPU_RK2; the reference has Euler only): the
+# FP64 form equals the oracle's RK2 bit for bit, on affine and non-affine
+# meshes; the FP32 form stays within the FP32 tolerances of the oracle.
+RK2 = {"oracle_kw": {"integrator": 1}, "integrator": 1}
+
+
+@pytest.mark.parametrize("which", ["channel", "cylinder", "cube"])
+def test_fp64_rk2_bit_exact(which):
+    c = {"channel": lambda: cases.channel(32, 8, dt=0.02),
+         "cylinder": lambda: cases.cylinder(16, 8, 40, dt=0.01),
+         "cube": lambda: cases.cube(5, q=(3, 3, 3), dt=0.1)}[which]()
+    o, g = run_fp64(c, 10, **RK2)
+    assert g.stats()["searched"] > 0
+
+
+@pytest.mark.parametrize("which", ["channel", "cylinder", "duct"])
+def test_fp32_rk2_error_against_fp64_oracle(which):
+    c = {"channel": lambda: cases.channel(),
+         "cylinder": lambda: cases.cylinder(24, 12, 60, dt=2e-3),
+         "duct": lambda: cases.duct(32, 8, 8, dt=0.02)}[which]()
+    o, g = make(c, precision="fp32", **RK2)
+    o.seed(c.V)
+    g.seed_particles(c.V)
+    for _ in range(20):
+        Vo = o.step(c.V, c.Vold)
+        Vg = g.step(c.V, c.Vold)
+    assert rel_l2(Vo, Vg) <= V_RTOL_FP32
+    a, b = by_id(o.particles()), by_id(g.particles())
+    common, ia, ib = np.intersect1d(a["id"], b["id"], return_indices=True)
+    assert len(common) >= 0.99 * len(a["id"])
+    assert rel_l2(a["x"][ia], b["x"][ib]) <= X_RTOL_FP32
+
+
+def test_rk2_differs_from_euler_and_window_refuses_it():
+    import torch
+
+    c = cases.channel(16, 4, dt=0.05)
+    out = {}
+    for integ in (0, 1):
+        _, g = make(c, integrator=integ)
+        g.seed_particles(c.V)
+        out[integ] = g.step(c.V, c.Vold)
+        if integ == 1:
+            dV = torch.from_numpy(np.ascontiguousarray(c.V)).cuda()
+            with pytest.raises(Exception):
+                g.window_forward_device(2, 1, dV)
+        g.close()
+    assert not np.array_equal(out[0], out[1], equal_nan=True)

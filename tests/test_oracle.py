@@ -325,3 +325,56 @@ def test_native_unv_reader_reference_mesh():
     a = M.read_unv(MESH3)
     b = M.read_unv_native(MESH3)
     assert np.array_equal(a.vertices, b.vertices) and np.array_equal(a.cells, b.cells)
+
+
+def _rotation_error(integrator, S, T=0.4):
+    """Largest position error after time T of particles in the solid-body
+    rotation u = (-(y - 1/2), x - 1/2) on an 8x8 unit square, taken as one
+    time step of S sub-steps.  The Q1 field reproduces the linear velocity
+    exactly, so the error is the integrator's alone."""
+    from oracle.oracle import Oracle
+
+    m = M.hyper_rectangle((0.0, 0.0), (1.0, 1.0), (8, 8))
+    xy = m.dof_coordinates()
+    V = np.ascontiguousarray(np.stack([-(xy[:, 1] - 0.5), xy[:, 0] - 0.5]))
+    o = Oracle(m, (4, 4), 100, S, T, integrator=integrator)
+    o.seed(V)
+    P0 = o.particles()
+    x0 = {int(i): x for i, x in zip(P0["id"], P0["x"])}
+    o.move(V)
+    P = o.particles()
+    c, s = np.cos(T), np.sin(T)
+    err = 0.0
+    for i, x in zip(P["id"], P["x"]):
+        if int(i) not in x0:
+            continue  # seeded by count correction
+        r = x0[int(i)] - 0.5
+        if np.hypot(*r) > 0.3:
+            continue  # may leave the square
+        ex = np.array([c * r[0] - s * r[1], s * r[0] + c * r[1]]) + 0.5
+        err = max(err, float(np.max(np.abs(x - ex))))
+    return err
+
+
+def test_rk2_substeps_are_second_order():
+    """The opt-in RK2 sub-step (midpoint rule in the particle's own cell; the
+    reference has Euler only): halving the sub-step divides the error by 4,
+    against 2 for Euler, the reference's integrator."""
+    from oracle.oracle import EULER, RK2
+
+    e = {k: [_rotation_error(k, S) for S in (8, 16, 32)] for k in (EULER, RK2)}
+    for a, b in zip(e[EULER], e[EULER][1:]):
+        assert 1.8 < a / b < 2.2, e[EULER]
+    for a, b in zip(e[RK2], e[RK2][1:]):
+        assert 3.6 < a / b < 4.4, e[RK2]
+    assert e[RK2][-1] < 1e-2 * e[EULER][-1]
+
+
+def test_window_refuses_rk2():
+    from oracle.oracle import RK2, Oracle
+
+    c = cases.channel(8, 4)
+    o = Oracle(c.mesh, c.q, c.max_per_part, c.substeps, c.dt, integrator=RK2)
+    o.seed(c.V)
+    with pytest.raises(Exception):
+        o.window_forward(2, c.V)
