@@ -235,6 +235,58 @@ int pfem2gpu_write_vtu(pfem2gpu_handle* h, const char* path);
  * d_out from another stream or the host. */
 int pfem2gpu_pack_output_device(pfem2gpu_handle* h, float* d_out, int64_t capacity, int64_t* n);
 
+/* ---------------------------------------------------------------------------
+ * Cell-range partitions: one handle per GPU, each holding the whole mesh and
+ * the whole nodal velocity and owning the particles of cells
+ * [cell_begin, cell_end).  The reference distributes cells over MPI ranks and
+ * sends the particles found in another rank's cells after each relocation
+ * (send_recv_particles, src/pfem2particlehandler.cpp:480-502,507-618), and
+ * sums the projection over the ghost cells of each DoF
+ * (project_particle_fields, :202-205 compress(add)).  A partitioned move is
+ * host-driven in three phases; the caller routes the outboxes to the owners
+ * of their cells and scans the seed counts over the partitions in cell order:
+ *
+ *   begin(h, V, &n_out)            correct + sub-steps + relocation
+ *   outbox(h, ..., &n)             particles that ended in foreign cells
+ *   inbox(h, m, ..., &n_seeds)     particles that ended in this handle's cells
+ *   end(h, first_id, next_id)      count correction, new layout, partials
+ *
+ * first_id = the ids handed out before this move + the seeds of all lower
+ * partitions; next_id = the ids handed out before + every partition's seeds.
+ * With those, every cell's particles, their order and their ids are those of
+ * one unpartitioned handle, so the FP64 form is bit-identical to it.  The
+ * projection then needs the partial sums of the cells that share a DoF with
+ * this handle's cells (get/set_partials) before pfem2gpu_project; DoFs none of
+ * whose cells are this handle's or were set are NaN (no particles).
+ * pfem2gpu_move, pfem2gpu_move_device and pfem2gpu_step_device return
+ * PFEM2GPU_ERR_STATE on a partitioned handle.
+ * ------------------------------------------------------------------------- */
+/* Own cells [cell_begin, cell_end) of the mesh; after set_mesh, before seed or
+ * set_particles.  seed then seeds the own cells only, with the ids of an
+ * unpartitioned seed (next_id afterwards = n_cells x particles per cell). */
+int pfem2gpu_set_partition(pfem2gpu_handle* h, int64_t cell_begin, int64_t cell_end);
+/* Phase 1: velocity correction (if pending), sub-steps and relocation; *n_out
+ * gets the number of particles that ended in other partitions' cells.
+ * V == NULL reuses the staged velocity. */
+int pfem2gpu_move_exchange_begin(pfem2gpu_handle* h, const double* V, int64_t* n_out);
+/* Phase 2a: those particles (arrays of >= capacity entries; x, xi, v row-major
+ * n x dim; x may be NULL in the FP32 form); they leave this handle. */
+int pfem2gpu_move_outbox(pfem2gpu_handle* h, uint32_t* id, int32_t* cell, double* x, double* xi, double* v,
+                         int64_t capacity, int64_t* n);
+/* Phase 2b: the particles other partitions sent to this handle's cells (all
+ * of them, in any order); *n_seeds gets the number of particles the count
+ * correction will add in this handle's cells.  PFEM2GPU_ERR_ARG if a cell is
+ * foreign, PFEM2GPU_ERR_CAPACITY beyond the particle capacity. */
+int pfem2gpu_move_inbox(pfem2gpu_handle* h, int64_t n, const uint32_t* id, const int32_t* cell, const double* x,
+                        const double* xi, const double* v, int64_t* n_seeds);
+/* Phase 3: count correction, sorted layout and projection partials; the new
+ * particles get ids first_id + 1 ...; the handle's next id becomes next_id. */
+int pfem2gpu_move_exchange_end(pfem2gpu_handle* h, uint32_t first_id, uint32_t next_id);
+/* Projection partial sums of n cells (out/in: n x 32 doubles in 3D, n x 16 in
+ * 2D, the per-vertex sum N v and sum N of the cell); valid after a move. */
+int pfem2gpu_get_partials(pfem2gpu_handle* h, int64_t n, const int32_t* cells, double* out);
+int pfem2gpu_set_partials(pfem2gpu_handle* h, int64_t n, const int32_t* cells, const double* in);
+
 int pfem2gpu_get_stats(pfem2gpu_handle* h, pfem2gpu_stats* out);
 int pfem2gpu_reset_stats(pfem2gpu_handle* h);
 int pfem2gpu_synchronize(pfem2gpu_handle* h);

@@ -112,6 +112,13 @@ def load():
         "pfem2gpu_correct_from_projection_device": [P, dptr],
         "pfem2gpu_get_particles": [P, dptr, dptr, dptr, dptr, dptr, i64, C.POINTER(i64)],
         "pfem2gpu_set_particles": [P, i64, dptr, dptr, dptr, dptr, dptr, u32],
+        "pfem2gpu_set_partition": [P, i64, i64],
+        "pfem2gpu_move_exchange_begin": [P, dptr, C.POINTER(i64)],
+        "pfem2gpu_move_outbox": [P, dptr, dptr, dptr, dptr, dptr, i64, C.POINTER(i64)],
+        "pfem2gpu_move_inbox": [P, i64, dptr, dptr, dptr, dptr, dptr, C.POINTER(i64)],
+        "pfem2gpu_move_exchange_end": [P, u32, u32],
+        "pfem2gpu_get_partials": [P, i64, dptr, dptr],
+        "pfem2gpu_set_partials": [P, i64, dptr, dptr],
         "pfem2gpu_write_vtu": [P, C.c_char_p],
         "pfem2gpu_pack_output_device": [P, dptr, i64, C.POINTER(i64)],
         "pfem2gpu_get_stats": [P, C.POINTER(Stats)],

@@ -69,6 +69,15 @@ struct pfem2gpu_handle {
     DevStats* stats_h = nullptr;
     bool has_particles = false, pending_correct = false, partials_valid = false;
     bool has_projection = false;  // Vout holds the last projection of this mesh
+    // cell-range partition (pfem2gpu_set_partition): the handle owns cells
+    // [pbeg, pend); pend < 0 is the whole mesh.  A partitioned move runs in
+    // phases (move_phase 1: outbox ready, 2: inbox entered and slots scanned).
+    int64_t pbeg = 0, pend = -1;
+    int move_phase = 0;
+    uint32_t *ob_i = nullptr, *ob_c = nullptr, *ob_n = nullptr;
+    uint32_t ob_cap = 0, ob_count = 0;
+    void* xbuf = nullptr;  // staging of exchanged particles and partial sums
+    size_t xbuf_bytes = 0;
     // accounting
     uint64_t launches = 0;
     bool profiling = false;
@@ -247,6 +256,8 @@ StepArgs args(pfem2gpu_handle* h)
     a.Vkeep = h->Vstage;
     a.stats = h->stats;
     a.capacity = h->cap;
+    a.cbeg = (int)h->pbeg;
+    a.cend = h->pend < 0 ? h->nC : (int)h->pend;
     return a;
 }
 
@@ -595,8 +606,8 @@ int sync_stats(pfem2gpu_handle* h)
 int maybe_grow(pfem2gpu_handle* h)
 {
     const uint64_t n = h->stats_h->n_slots;
-    if (n + (uint64_t)h->nC * h->pp.npart / 2 > h->cap && h->cap < capacity_limit(h))
-        return ensure_capacity(h, n, n + (uint64_t)h->nC * h->pp.npart);
+    const uint64_t own = (uint64_t)((h->pend < 0 ? h->nC : h->pend) - h->pbeg) * h->pp.npart;
+    if (n + own / 2 > h->cap && h->cap < capacity_limit(h)) return ensure_capacity(h, n, n + own);
     return PFEM2GPU_OK;
 }
 
@@ -727,11 +738,15 @@ WinArgs winargs(pfem2gpu_handle* h)
     return w;
 }
 
+// Does the handle own only part of the mesh's cells (pfem2gpu_set_partition)?
+static bool split(const pfem2gpu_handle* h) { return h->pend >= 0 && (h->pbeg > 0 || h->pend < h->nC); }
+
 int window_forward_impl(pfem2gpu_handle* h, int K, int C, const double* V, const double* Vold, const double* v0,
                         double* U_out, bool host)
 {
     if (!h || !V || K < 0 || C < 1) return PFEM2GPU_ERR_ARG;
     if (h->pp.rk2) return fail(h, PFEM2GPU_ERR_ARG, "the differentiated window supports Euler sub-steps only");
+    if (h->move_phase || split(h)) return fail(h, PFEM2GPU_ERR_STATE, "the differentiated window needs an unpartitioned handle");
     if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "window before seed");
     if ((int64_t)C * h->pp.S > 100000) return fail(h, PFEM2GPU_ERR_ARG, "checkpoint_every x sub-steps too large");
     int rc = apply_pending_correction(h);
@@ -951,6 +966,7 @@ int pfem2gpu_destroy(pfem2gpu_handle* h)
                     (void*)h->vrec32, (void*)h->dvrec32, h->partials, (void*)h->stats, (void*)h->twisted})
         dfree(p);
     dfree(h->chunk_first);
+    for (void* p : {(void*)h->ob_i, (void*)h->ob_c, (void*)h->ob_n, h->xbuf}) dfree(p);
     free_state(h->S0);
     free_state(h->S1);
     free_state(h->T);
@@ -1159,16 +1175,19 @@ static int host_velocity_ok(pfem2gpu_handle* h, const double* V, bool device)
 static int seed_impl(pfem2gpu_handle* h, const double* V, bool device)
 {
     if (!h || !V) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase) return fail(h, PFEM2GPU_ERR_STATE, "inside a partitioned move");
     if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "seed before set_mesh");
     if (h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "seed called twice");
-    const uint64_t n = (uint64_t)h->nC * h->pp.npart;
+    // a partitioned handle seeds its own cells; ids count every cell's parts
+    const int64_t own = (h->pend < 0 ? h->nC : h->pend) - h->pbeg;
+    const uint64_t n = (uint64_t)own * h->pp.npart, n_all = (uint64_t)h->nC * h->pp.npart;
     int rc = host_velocity_ok(h, V, device);
     if (rc) return rc;
     if ((rc = ensure_capacity(h, n, h->prm.capacity > 0 ? (uint64_t)h->prm.capacity : 2 * n))) return rc;
     if ((rc = stage_v(h, V, nullptr, device))) return rc;
     StepArgs a = args(h);
     run(h, "seed", [&] { return launch_seed(h->dim, h->prec, a, h->cs0, h->stream); });
-    run(h, "finalize", [&] { return launch_set_state(h->stats, (long long)n, -1, (long long)n, h->stream); });
+    run(h, "finalize", [&] { return launch_set_state(h->stats, (long long)n, -1, (long long)n_all, h->stream); });
     h->has_particles = true;
     h->partials_valid = false;
     h->pending_correct = false;
@@ -1181,6 +1200,7 @@ int pfem2gpu_seed_device(pfem2gpu_handle* h, const double* dV) { return seed_imp
 static int correct_impl(pfem2gpu_handle* h, const double* V, const double* Vold, bool device)
 {
     if (!h || !V || !Vold) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase) return fail(h, PFEM2GPU_ERR_STATE, "inside a partitioned move");
     if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "correct before seed");
     int rc = apply_pending_correction(h);
     if (rc) return rc;
@@ -1216,7 +1236,9 @@ int pfem2gpu_correct_from_projection_device(pfem2gpu_handle* h, const double* dV
 static int move_impl(pfem2gpu_handle* h, const double* V, bool device)
 {
     if (!h) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase) return fail(h, PFEM2GPU_ERR_STATE, "inside a partitioned move");
     if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "move before seed");
+    if (split(h)) return fail(h, PFEM2GPU_ERR_STATE, "a partitioned handle moves with pfem2gpu_move_exchange_*");
     if (V) {
         // keep a staged correction: only V is re-staged
         int rc = stage_v(h, V, nullptr, device);
@@ -1231,6 +1253,7 @@ int pfem2gpu_move_device(pfem2gpu_handle* h, const double* dV) { return move_imp
 static int project_impl(pfem2gpu_handle* h, double* out, bool device)
 {
     if (!h || !out) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase) return fail(h, PFEM2GPU_ERR_STATE, "inside a partitioned move");
     if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "project before seed");
     int rc = apply_pending_correction(h);
     if (rc) return rc;
@@ -1259,7 +1282,9 @@ int pfem2gpu_project_device(pfem2gpu_handle* h, double* dV_out) { return project
 int pfem2gpu_step_device(pfem2gpu_handle* h, const double* dV, const double* dVold, double* dV_out)
 {
     if (!h || !dV || !dV_out) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase) return fail(h, PFEM2GPU_ERR_STATE, "inside a partitioned move");
     if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "step before seed");
+    if (split(h)) return fail(h, PFEM2GPU_ERR_STATE, "a partitioned handle moves with pfem2gpu_move_exchange_*");
     if (!dVold) {  // the reference's data flow: Vold = the last projection
         if (!h->has_projection) return fail(h, PFEM2GPU_ERR_STATE, "step from projection before any projection");
         dVold = h->Vout;
@@ -1290,6 +1315,7 @@ int pfem2gpu_get_particles(pfem2gpu_handle* h, uint32_t* id, int32_t* cell, doub
                            int64_t capacity, int64_t* n)
 {
     if (!h || !n) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase) return fail(h, PFEM2GPU_ERR_STATE, "inside a partitioned move");
     *n = 0;
     if (!h->has_particles) return PFEM2GPU_OK;
     int rc = apply_pending_correction(h);
@@ -1357,9 +1383,11 @@ int pfem2gpu_set_particles(pfem2gpu_handle* h, int64_t n, const uint32_t* id, co
 {
     if (!h || n < 0 || (n > 0 && (!id || !cell || !xi || !v))) return PFEM2GPU_ERR_ARG;
     if (h->prec == PFEM2GPU_FP64 && n > 0 && !x) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase) return fail(h, PFEM2GPU_ERR_STATE, "inside a partitioned move");
     if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "set_particles before set_mesh");
+    const int64_t cb = h->pbeg, ce = h->pend < 0 ? h->nC : h->pend;
     for (int64_t i = 0; i < n; ++i)
-        if (cell[i] < 0 || cell[i] >= h->nC) return fail(h, PFEM2GPU_ERR_ARG, "bad particle cell");
+        if (cell[i] < cb || cell[i] >= ce) return fail(h, PFEM2GPU_ERR_ARG, "particle cell outside the handle's cells");
     // reference coordinates inside the unit cell (GeometryInfo::is_inside_unit_cell, the test every
     // particle of the reference passed), finite velocities and positions
     for (int64_t i = 0; i < n * h->dim; ++i) {
@@ -1401,6 +1429,223 @@ int pfem2gpu_set_particles(pfem2gpu_handle* h, int64_t n, const uint32_t* id, co
     h->pending_correct = false;
     if ((rc = write_and_swap(h, a, 0))) return rc;
     return sync_stats(h);
+}
+
+// ---------------------------------------------------------------------------
+// Cell-range partitions (shard.cuh): one handle per GPU, each owning a
+// contiguous range of cells of the same mesh.
+// ---------------------------------------------------------------------------
+
+int pfem2gpu_set_partition(pfem2gpu_handle* h, int64_t cell_begin, int64_t cell_end)
+{
+    if (!h) return PFEM2GPU_ERR_ARG;
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "set_partition before set_mesh");
+    if (h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "set_partition after particles exist");
+    if (cell_begin < 0 || cell_begin > cell_end || cell_end > h->nC) return fail(h, PFEM2GPU_ERR_ARG, "bad cell range");
+    h->pbeg = cell_begin;
+    h->pend = cell_end;
+    h->gen++;
+    return PFEM2GPU_OK;
+}
+
+// Device staging of `bytes` for an exchange.
+static int xbuf_reserve(pfem2gpu_handle* h, size_t bytes)
+{
+    if (bytes <= h->xbuf_bytes) return PFEM2GPU_OK;
+    CK(cudaStreamSynchronize(h->stream));
+    dfree(h->xbuf);
+    h->xbuf = nullptr;
+    h->xbuf_bytes = 0;
+    CK(cudaMalloc(&h->xbuf, bytes));
+    h->xbuf_bytes = bytes;
+    return PFEM2GPU_OK;
+}
+
+// Offsets of id, cell, x, xi, v for n particles in the staging buffer.
+struct XLayout {
+    size_t id, cell, x, xi, v, total;
+};
+static XLayout xlayout(int dim, size_t n)
+{
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    XLayout L;
+    L.id = 0;
+    L.cell = al(4 * n);
+    L.x = L.cell + al(4 * n);
+    L.xi = L.x + al(8 * n * dim);
+    L.v = L.xi + al(8 * n * dim);
+    L.total = L.v + al(8 * n * dim) + 256;
+    return L;
+}
+
+int pfem2gpu_move_exchange_begin(pfem2gpu_handle* h, const double* V, int64_t* n_out)
+{
+    if (!h || !n_out) return PFEM2GPU_ERR_ARG;
+    if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "move before seed");
+    if (h->move_phase != 0) return fail(h, PFEM2GPU_ERR_STATE, "a partitioned move is in progress");
+    int rc;
+    if (V && (rc = stage_v(h, V, nullptr, false))) return rc;
+    if (!h->vaos_valid) return fail(h, PFEM2GPU_ERR_STATE, "move without a velocity");
+    if (h->ob_cap < h->cap) {
+        CK(cudaStreamSynchronize(h->stream));
+        for (void* p : {(void*)h->ob_i, (void*)h->ob_c}) dfree(p);
+        h->ob_i = h->ob_c = nullptr;
+        h->ob_cap = 0;
+        CK(dalloc(&h->ob_i, h->cap));
+        CK(dalloc(&h->ob_c, h->cap));
+        h->ob_cap = h->cap;
+    }
+    if (!h->ob_n) CK(dalloc(&h->ob_n, 1));
+    StepArgs a = args(h);
+    a.do_correct = h->pending_correct ? 1 : 0;
+    h->pending_correct = false;
+    h->partials_valid = false;
+    CK(cudaMemsetAsync(h->ob_n, 0, sizeof(uint32_t), h->stream));
+    run(h, "advect", [&] { return launch_advect(h->dim, h->prec, a, h->stream); });
+    run(h, "cross", [&] { return launch_cross(h->dim, h->prec, a, h->stream); });
+    run(h, "outbox", [&] { return launch_outbox(h->prec, a, h->ob_i, h->ob_c, h->ob_n, h->ob_cap, h->stream); });
+    if ((rc = check_async(h))) return rc;
+    uint32_t n = 0;
+    CK(cudaMemcpyAsync(&n, h->ob_n, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    if ((rc = sync_stats(h))) return rc;  // also the current slot count, for the inbox
+    h->ob_count = n < h->ob_cap ? n : h->ob_cap;
+    h->move_phase = 1;
+    *n_out = h->ob_count;
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_move_outbox(pfem2gpu_handle* h, uint32_t* id, int32_t* cell, double* x, double* xi, double* v,
+                         int64_t capacity, int64_t* n)
+{
+    if (!h || !n) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase != 1) return fail(h, PFEM2GPU_ERR_STATE, "outbox outside a partitioned move");
+    const size_t m = h->ob_count, dim = (size_t)h->dim;
+    *n = (int64_t)m;
+    if (capacity < (int64_t)m) return fail(h, PFEM2GPU_ERR_ARG, "outbox arrays too small");
+    if (m == 0) return PFEM2GPU_OK;
+    if (!id || !cell || !xi || !v || (h->prec == PFEM2GPU_FP64 && !x)) return PFEM2GPU_ERR_ARG;
+    const XLayout L = xlayout(h->dim, m);
+    int rc = xbuf_reserve(h, L.total);
+    if (rc) return rc;
+    char* b = static_cast<char*>(h->xbuf);
+    StepArgs a = args(h);
+    run(h, "outbox_pack", [&] {
+        return launch_outbox_pack(h->dim, h->prec, a, h->ob_i, h->ob_c, (uint32_t)m, (uint32_t*)(b + L.id),
+                                  (int32_t*)(b + L.cell), (double*)(b + L.x), (double*)(b + L.xi), (double*)(b + L.v),
+                                  h->stream);
+    });
+    if ((rc = check_async(h))) return rc;
+    CK(cudaMemcpyAsync(id, b + L.id, 4 * m, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(cell, b + L.cell, 4 * m, cudaMemcpyDeviceToHost, h->stream));
+    if (h->prec == PFEM2GPU_FP64) CK(cudaMemcpyAsync(x, b + L.x, 8 * m * dim, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(xi, b + L.xi, 8 * m * dim, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(v, b + L.v, 8 * m * dim, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_move_inbox(pfem2gpu_handle* h, int64_t n, const uint32_t* id, const int32_t* cell, const double* x,
+                        const double* xi, const double* v, int64_t* n_seeds)
+{
+    if (!h || !n_seeds || n < 0 || (n > 0 && (!id || !cell || !xi || !v))) return PFEM2GPU_ERR_ARG;
+    if (h->prec == PFEM2GPU_FP64 && n > 0 && !x) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase != 1) return fail(h, PFEM2GPU_ERR_STATE, "inbox outside a partitioned move");
+    const int64_t cb = h->pbeg, ce = h->pend < 0 ? h->nC : h->pend;
+    for (int64_t i = 0; i < n; ++i)
+        if (cell[i] < cb || cell[i] >= ce) return fail(h, PFEM2GPU_ERR_ARG, "inbox particle outside the handle's cells");
+    for (int64_t i = 0; i < n * h->dim; ++i)
+        if (!(xi[i] >= 0.0 && xi[i] <= 1.0) || !std::isfinite(v[i]))
+            return fail(h, PFEM2GPU_ERR_ARG, "inbox particle with a bad reference coordinate or velocity");
+    const uint64_t base = h->stats_h->n_slots;  // read when the move began
+    if (base + (uint64_t)n > h->cap) return fail(h, PFEM2GPU_ERR_CAPACITY, "inbox beyond the particle capacity");
+    StepArgs a = args(h);
+    int rc;
+    if (n > 0) {
+        const size_t m = (size_t)n, dim = (size_t)h->dim;
+        const XLayout L = xlayout(h->dim, m);
+        if ((rc = xbuf_reserve(h, L.total))) return rc;
+        char* b = static_cast<char*>(h->xbuf);
+        CK(cudaMemcpyAsync(b + L.id, id, 4 * m, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(b + L.cell, cell, 4 * m, cudaMemcpyHostToDevice, h->stream));
+        if (h->prec == PFEM2GPU_FP64)
+            CK(cudaMemcpyAsync(b + L.x, x, 8 * m * dim, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(b + L.xi, xi, 8 * m * dim, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(b + L.v, v, 8 * m * dim, cudaMemcpyHostToDevice, h->stream));
+        run(h, "inbox", [&] {
+            return launch_inbox(h->dim, h->prec, a, (uint32_t)m, (uint32_t)base, (const uint32_t*)(b + L.id),
+                                (const int32_t*)(b + L.cell), (const double*)(b + L.x), (const double*)(b + L.xi),
+                                (const double*)(b + L.v), h->stream);
+        });
+    }
+    run(h, "slots_scan", [&] { return launch_slots_scan(a, h->tiles64, h->stream); });
+    if ((rc = check_async(h))) return rc;
+    unsigned long long po = 0;
+    CK(cudaMemcpyAsync(&po, h->coff + h->nC, sizeof(po), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *n_seeds = (int64_t)(po >> 32);
+    h->move_phase = 2;
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_move_exchange_end(pfem2gpu_handle* h, uint32_t first_id, uint32_t next_id)
+{
+    if (!h) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase != 2) return fail(h, PFEM2GPU_ERR_STATE, "exchange_end before the inbox");
+    StepArgs a = args(h);
+    a.count_step = 1;
+    a.reset_nan = 0;
+    run(h, "finalize", [&] { return launch_set_state(h->stats, -1, first_id, 0, h->stream); });
+    run(h, "write", [&] { return launch_write(h->dim, h->prec, a, h->stream); });
+    swap_state(h);
+    run(h, "finalize", [&] { return launch_set_state(h->stats, -1, next_id, 0, h->stream); });
+    h->move_phase = 0;
+    int rc = check_async(h);
+    if (rc || (rc = sync_stats(h))) return rc;
+    return maybe_grow(h);
+}
+
+static int partials_io(pfem2gpu_handle* h, int64_t n, const int32_t* cells, double* out, const double* in)
+{
+    if (!h || n < 0 || (n > 0 && !cells)) return PFEM2GPU_ERR_ARG;
+    if (!h->has_mesh) return fail(h, PFEM2GPU_ERR_STATE, "partials before set_mesh");
+    for (int64_t i = 0; i < n; ++i)
+        if (cells[i] < 0 || cells[i] >= h->nC) return fail(h, PFEM2GPU_ERR_ARG, "bad cell");
+    if (!h->has_particles) return fail(h, PFEM2GPU_ERR_STATE, "partials before seed");
+    if (h->move_phase != 0) return fail(h, PFEM2GPU_ERR_STATE, "partials inside a partitioned move");
+    int rc = apply_pending_correction(h);
+    if (rc) return rc;
+    if (!h->partials_valid) {
+        StepArgs a = args(h);
+        run(h, "partials", [&] { return launch_partials(h->dim, h->prec, a, h->cs0, h->stream); });
+        h->partials_valid = true;
+    }
+    if (n == 0) return check_async(h);
+    const int pw = h->dim == 3 ? 32 : 16;
+    const size_t cb = ((size_t)4 * n + 255) & ~(size_t)255, vb = (size_t)8 * n * pw;
+    if ((rc = xbuf_reserve(h, cb + vb))) return rc;
+    char* b = static_cast<char*>(h->xbuf);
+    CK(cudaMemcpyAsync(b, cells, 4 * n, cudaMemcpyHostToDevice, h->stream));
+    if (in) CK(cudaMemcpyAsync(b + cb, in, vb, cudaMemcpyHostToDevice, h->stream));
+    run(h, "partials_io", [&] {
+        return launch_partials_io(h->prec, h->partials, pw, (uint32_t)n, (const int32_t*)b, (double*)(b + cb),
+                                  in ? 0 : 1, h->stream);
+    });
+    if ((rc = check_async(h))) return rc;
+    if (out) CK(cudaMemcpyAsync(out, b + cb, vb, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PFEM2GPU_OK;
+}
+
+int pfem2gpu_get_partials(pfem2gpu_handle* h, int64_t n, const int32_t* cells, double* out)
+{
+    if (!out && n > 0) return PFEM2GPU_ERR_ARG;
+    return partials_io(h, n, cells, out, nullptr);
+}
+
+int pfem2gpu_set_partials(pfem2gpu_handle* h, int64_t n, const int32_t* cells, const double* in)
+{
+    if (!in && n > 0) return PFEM2GPU_ERR_ARG;
+    return partials_io(h, n, cells, nullptr, in);
 }
 
 int pfem2gpu_get_stats(pfem2gpu_handle* h, pfem2gpu_stats* out)
@@ -1506,6 +1751,7 @@ int pfem2gpu_launch_count(pfem2gpu_handle* h, uint64_t* count)
 int pfem2gpu_pack_output_device(pfem2gpu_handle* h, float* d_out, int64_t capacity, int64_t* n)
 {
     if (!h || !n || (capacity > 0 && !d_out)) return PFEM2GPU_ERR_ARG;
+    if (h->move_phase) return fail(h, PFEM2GPU_ERR_STATE, "inside a partitioned move");
     return pack_output(h, d_out, capacity, n);
 }
 

@@ -103,14 +103,18 @@ __device__ __forceinline__ void part_digits(int k, const PartParams& pp, int* id
     }
 }
 
-// seed_particles (:43-109): nC x npart particles, cell-major, parts x-major.
+// seed_particles (:43-109): npart particles per owned cell, cell-major, parts
+// x-major; ids by the global (cell, part) index, so a partitioned run hands
+// out the ids of an unpartitioned one.  Cells outside [cbeg, cend) get empty
+// ranges.
 template <int DIM, typename Real>
 __global__ void k_seed(StepArgs a, uint32_t* cell_start)
 {
-    const uint32_t total = (uint32_t)a.mesh.nC * a.pp.npart;
-    const uint32_t id0 = a.stats->next_id;
+    const uint32_t cb = (uint32_t)a.cbeg, ce = (uint32_t)a.cend;
+    const uint32_t total = (ce - cb) * a.pp.npart;
+    const uint32_t id0 = a.stats->next_id + cb * a.pp.npart;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const uint32_t c = t / a.pp.npart;
+        const uint32_t c = cb + t / a.pp.npart;
         const int k = (int)(t % a.pp.npart);
         int idx[3];
         part_digits<DIM>(k, a.pp, idx);
@@ -119,6 +123,8 @@ __global__ void k_seed(StepArgs a, uint32_t* cell_start)
         if (k == 0) cell_start[c] = t;
         if (a.chunk_first && t % ADV_CH == 0) a.chunk_first[t / ADV_CH] = c;
     }
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < (uint32_t)a.mesh.nC; c += gridDim.x * blockDim.x)
+        if (c < cb || c >= ce) cell_start[c] = c < cb ? 0u : total;
     if (blockIdx.x == 0 && threadIdx.x == 0) cell_start[a.mesh.nC] = total;
 }
 

@@ -138,6 +138,7 @@ struct StepArgs {
     const double* Vkeep;           // empty_dof_policy 1: value kept where no particle contributes
     DevStats* stats;
     uint32_t capacity;
+    int cbeg, cend;     // the cells this handle owns (the whole mesh unless partitioned)
 };
 
 // Differentiated window (window.cuh): device arrays of one window.

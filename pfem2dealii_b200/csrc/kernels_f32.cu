@@ -4,6 +4,7 @@
 #include "advect.cuh"
 #include "cellwork.cuh"
 #include "launch.h"
+#include "shard.cuh"
 
 namespace pfem2 {
 
@@ -14,6 +15,13 @@ int launch64_write(int dim, const StepArgs& a, cudaStream_t s);
 int launch64_partials(int dim, const StepArgs& a, const uint32_t* cs, cudaStream_t s);
 int launch64_correct(int dim, const StepArgs& a, cudaStream_t s);
 int launch64_gather(int dim, const StepArgs& a, int keep, cudaStream_t s);
+int launch64_outbox(const StepArgs& a, uint32_t* out_i, uint32_t* out_c, uint32_t* n_out, uint32_t cap, cudaStream_t s);
+int launch64_outbox_pack(int dim, const StepArgs& a, const uint32_t* out_i, const uint32_t* out_c, uint32_t n,
+                         uint32_t* id, int32_t* cell, double* x, double* xi, double* v, cudaStream_t s);
+int launch64_inbox(int dim, const StepArgs& a, uint32_t n, uint32_t base, const uint32_t* id, const int32_t* cell,
+                   const double* x, const double* xi, const double* v, cudaStream_t s);
+int launch64_partials_io(void* partials, int pw, uint32_t n, const int32_t* cells, double* buf, int to_buf,
+                         cudaStream_t s);
 
 #define PFEM2_GRID(kern, thr) occupancy_grid((const void*)(kern), (thr))
 #define CELL_THREADS (CELL_WARPS * 32)
@@ -146,6 +154,46 @@ int launch_positions32(int dim, const StepArgs& a, double* xout, cudaStream_t s)
 {
     if (dim == 2) k_positions32<2><<<PFEM2_GRID(k_positions32<2>, 256), 256, 0, s>>>(a, xout);
     else k_positions32<3><<<PFEM2_GRID(k_positions32<3>, 256), 256, 0, s>>>(a, xout);
+    return 1;
+}
+
+static int grid_n(size_t n, int threads)
+{
+    const size_t g = (n + threads - 1) / threads;
+    return (int)(g < 1 ? 1 : g > 148 * 32 ? 148 * 32 : g);
+}
+
+int launch_outbox(int prec, const StepArgs& a, uint32_t* out_i, uint32_t* out_c, uint32_t* n_out, uint32_t cap,
+                  cudaStream_t s)
+{
+    if (prec == 0) return launch64_outbox(a, out_i, out_c, n_out, cap, s);
+    k_outbox<float><<<grid_n((size_t)a.mesh.nC, 256), 256, 0, s>>>(a, out_i, out_c, n_out, cap);
+    return 1;
+}
+
+int launch_outbox_pack(int dim, int prec, const StepArgs& a, const uint32_t* out_i, const uint32_t* out_c, uint32_t n,
+                       uint32_t* id, int32_t* cell, double* x, double* xi, double* v, cudaStream_t s)
+{
+    if (prec == 0) return launch64_outbox_pack(dim, a, out_i, out_c, n, id, cell, x, xi, v, s);
+    if (dim == 2) k_outbox_pack<2, float><<<grid_n(n, 256), 256, 0, s>>>(a, out_i, out_c, n, id, cell, x, xi, v);
+    else k_outbox_pack<3, float><<<grid_n(n, 256), 256, 0, s>>>(a, out_i, out_c, n, id, cell, x, xi, v);
+    return 1;
+}
+
+int launch_inbox(int dim, int prec, const StepArgs& a, uint32_t n, uint32_t base, const uint32_t* id,
+                 const int32_t* cell, const double* x, const double* xi, const double* v, cudaStream_t s)
+{
+    if (prec == 0) return launch64_inbox(dim, a, n, base, id, cell, x, xi, v, s);
+    if (dim == 2) k_inbox<2, float><<<grid_n(n, 256), 256, 0, s>>>(a, n, base, id, cell, x, xi, v);
+    else k_inbox<3, float><<<grid_n(n, 256), 256, 0, s>>>(a, n, base, id, cell, x, xi, v);
+    return 1;
+}
+
+int launch_partials_io(int prec, void* partials, int pw, uint32_t n, const int32_t* cells, double* buf, int to_buf,
+                       cudaStream_t s)
+{
+    if (prec == 0) return launch64_partials_io(partials, pw, n, cells, buf, to_buf, s);
+    k_partials_io<float><<<grid_n((size_t)n * pw, 256), 256, 0, s>>>(partials, pw, n, cells, buf, to_buf);
     return 1;
 }
 

@@ -5,6 +5,7 @@
 #include "advect.cuh"
 #include "cellwork.cuh"
 #include "launch.h"
+#include "shard.cuh"
 
 namespace pfem2 {
 
@@ -352,6 +353,41 @@ int launch_v2c_build(int dim, int nC, int nV, const double* verts, const int32_t
         k_v2c_finish<3><<<PFEM2_GRID(k_v2c_finish<3>, 128), 128, 0, s>>>(nV, verts, cv, off, cells, dirs);
     }
     return 2;
+}
+
+static int grid_n64(size_t n, int threads)
+{
+    const size_t g = (n + threads - 1) / threads;
+    return (int)(g < 1 ? 1 : g > 148 * 32 ? 148 * 32 : g);
+}
+
+int launch64_outbox(const StepArgs& a, uint32_t* out_i, uint32_t* out_c, uint32_t* n_out, uint32_t cap, cudaStream_t s)
+{
+    k_outbox<double><<<grid_n64((size_t)a.mesh.nC, 256), 256, 0, s>>>(a, out_i, out_c, n_out, cap);
+    return 1;
+}
+
+int launch64_outbox_pack(int dim, const StepArgs& a, const uint32_t* out_i, const uint32_t* out_c, uint32_t n,
+                         uint32_t* id, int32_t* cell, double* x, double* xi, double* v, cudaStream_t s)
+{
+    if (dim == 2) k_outbox_pack<2, double><<<grid_n64(n, 256), 256, 0, s>>>(a, out_i, out_c, n, id, cell, x, xi, v);
+    else k_outbox_pack<3, double><<<grid_n64(n, 256), 256, 0, s>>>(a, out_i, out_c, n, id, cell, x, xi, v);
+    return 1;
+}
+
+int launch64_inbox(int dim, const StepArgs& a, uint32_t n, uint32_t base, const uint32_t* id, const int32_t* cell,
+                   const double* x, const double* xi, const double* v, cudaStream_t s)
+{
+    if (dim == 2) k_inbox<2, double><<<grid_n64(n, 256), 256, 0, s>>>(a, n, base, id, cell, x, xi, v);
+    else k_inbox<3, double><<<grid_n64(n, 256), 256, 0, s>>>(a, n, base, id, cell, x, xi, v);
+    return 1;
+}
+
+int launch64_partials_io(void* partials, int pw, uint32_t n, const int32_t* cells, double* buf, int to_buf,
+                         cudaStream_t s)
+{
+    k_partials_io<double><<<grid_n64((size_t)n * pw, 256), 256, 0, s>>>(partials, pw, n, cells, buf, to_buf);
+    return 1;
 }
 
 }  // namespace pfem2

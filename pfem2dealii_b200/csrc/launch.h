@@ -60,6 +60,15 @@ int launch_partials(int dim, int prec, const StepArgs& a, const uint32_t* cell_s
 int launch_correct(int dim, int prec, const StepArgs& a, cudaStream_t s);
 int launch_gather(int dim, int prec, const StepArgs& a, int keep_empty, cudaStream_t s);
 int launch_positions32(int dim, const StepArgs& a, double* xout, cudaStream_t s);
+// shard.cuh: the exchange of a partitioned move, and partial sums to and from doubles
+int launch_outbox(int prec, const StepArgs& a, uint32_t* out_i, uint32_t* out_c, uint32_t* n_out, uint32_t cap,
+                  cudaStream_t s);
+int launch_outbox_pack(int dim, int prec, const StepArgs& a, const uint32_t* out_i, const uint32_t* out_c, uint32_t n,
+                       uint32_t* id, int32_t* cell, double* x, double* xi, double* v, cudaStream_t s);
+int launch_inbox(int dim, int prec, const StepArgs& a, uint32_t n, uint32_t base, const uint32_t* id,
+                 const int32_t* cell, const double* x, const double* xi, const double* v, cudaStream_t s);
+int launch_partials_io(int prec, void* partials, int pw, uint32_t n, const int32_t* cells, double* buf, int to_buf,
+                       cudaStream_t s);
 int launch_pack_output(int dim, int prec, const StepArgs& a, const uint32_t* slot, uint32_t n, float* out,
                        cudaStream_t s);
 

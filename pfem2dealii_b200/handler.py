@@ -403,6 +403,54 @@ class ParticleHandler:
                 _host(P["xi"], np.float64), _host(P["v"], np.float64)]
         self._ck(self.L.pfem2gpu_set_particles(self.h, n, *[_ptr(a) for a in arrs], next_id))
 
+    # -- cell-range partitions (pfem2dealii_b200.shard) -----------------------
+    def set_partition(self, cell_begin: int, cell_end: int):
+        """Own the particles of cells [cell_begin, cell_end) only."""
+        self._ck(self.L.pfem2gpu_set_partition(self.h, int(cell_begin), int(cell_end)))
+
+    def move_exchange_begin(self, V=None) -> int:
+        """Phase 1 of a partitioned move; returns the outbox size."""
+        V = None if V is None else _host(V, np.float64)
+        n = C.c_int64()
+        self._ck(self.L.pfem2gpu_move_exchange_begin(self.h, _ptr(V), C.byref(n)))
+        return n.value
+
+    def move_outbox(self, n: int):
+        """The n particles that ended the move in foreign cells (dict of
+        id, cell, x, xi, v)."""
+        P = {"id": np.zeros(n, np.uint32), "cell": np.zeros(n, np.int32), "x": np.zeros((n, self.dim)),
+             "xi": np.zeros((n, self.dim)), "v": np.zeros((n, self.dim))}
+        got = C.c_int64()
+        self._ck(self.L.pfem2gpu_move_outbox(self.h, *[_ptr(P[k]) for k in ("id", "cell", "x", "xi", "v")], n,
+                                             C.byref(got)))
+        return P
+
+    def move_inbox(self, P) -> int:
+        """The particles sent to this handle's cells; returns the number of
+        particles count correction will add."""
+        arrs = [_host(P["id"], np.uint32), _host(P["cell"], np.int32), _host(P["x"], np.float64),
+                _host(P["xi"], np.float64), _host(P["v"], np.float64)]
+        ns = C.c_int64()
+        self._ck(self.L.pfem2gpu_move_inbox(self.h, len(arrs[0]), *[_ptr(a) for a in arrs], C.byref(ns)))
+        return ns.value
+
+    def move_exchange_end(self, first_id: int, next_id: int):
+        self._ck(self.L.pfem2gpu_move_exchange_end(self.h, int(first_id), int(next_id)))
+
+    def get_partials(self, cells):
+        """Projection partial sums of the listed cells, (n, 2^dim x 4)."""
+        cells = _host(cells, np.int32)
+        out = np.zeros((len(cells), 4 << self.dim))
+        self._ck(self.L.pfem2gpu_get_partials(self.h, len(cells), _ptr(cells), _ptr(out)))
+        return out
+
+    def set_partials(self, cells, values):
+        cells = _host(cells, np.int32)
+        values = _host(values, np.float64)
+        if values.shape != (len(cells), 4 << self.dim):
+            raise ValueError(f"set_partials: values must have shape ({len(cells)}, {4 << self.dim})")
+        self._ck(self.L.pfem2gpu_set_partials(self.h, len(cells), _ptr(cells), _ptr(values)))
+
     def pack_output_device(self, dout=None):
         """Float32 positions and velocities of the particles packed on the
         device (a CUDA tensor of 6 n floats: n x 3 positions, then n x 3
