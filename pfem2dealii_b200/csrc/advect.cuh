@@ -203,34 +203,153 @@ __device__ __noinline__ SearchOut search64(const MeshDev m, uint32_t c, Vec<DIM>
     return out;
 }
 
+// L1 prefetch of a cell's rows that the FP64 relocation reads (vertex
+// coordinates, affine inverse, vertex and DoF ids), issued as soon as the
+// cell is known so that the dependent steps after it find them on chip.
+__device__ __forceinline__ void prefetch_l1(const void* p)
+{
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+template <int DIM>
+__device__ __forceinline__ void prefetch_cell64(const MeshDev& m, uint32_t c)
+{
+    constexpr int NV = 1 << DIM, AFF = Dims<DIM>::AFF;
+    const double* X = m.cellX + (size_t)c * NV * DIM;
+    prefetch_l1(X);
+    prefetch_l1(X + NV * DIM - 1);
+    if (DIM == 3) prefetch_l1(X + NV * DIM / 2);
+    prefetch_l1(m.aff + (size_t)c * AFF);
+    prefetch_l1(m.aff + (size_t)c * AFF + AFF - 1);
+    prefetch_l1(m.cv + (size_t)c * NV);
+    prefetch_l1(m.cd + (size_t)c * NV);
+}
+
 // Full FP64 relocation of an FP32-form particle: rebuild x = F(xi) + u dt_p in
-// FP64, inverse map in the own cell, then the vertex-patch search (LIN: the
-// affine inverse, see search64).
+// FP64, inverse map in the own cell, then the vertex-patch search of search64
+// (LIN: the affine inverse) with two changes of arithmetic that keep its
+// choices: the closest vertex maximises (u . p_v) / |p_v| (p_v = vertex -
+// previous position) as one product with a reciprocal square root, which
+// orders the vertices as the angle cos = (u/|u|) . (p_v/|p_v|) does (a
+// positive factor per particle), and the candidates are ordered by their
+// centre directions' dot products with the unnormalised vertex->particle
+// vector.  Results differ from search64's only where two products tie to
+// the last bits.  The vertex ids of the cell are loaded with its coordinates
+// and the vertices' cell ranges are prefetched while the angles are
+// computed.  A vertex with more than REG_CAND cells takes search64 itself.
 template <int DIM, bool LIN = false>
 __device__ __noinline__ SearchOut fallback64(const MeshDev m, uint32_t c, Vec<DIM> xo, Vec<DIM> ue, double dtp)
 {
-    constexpr int AFF = Dims<DIM>::AFF;
-    double X[1 << DIM][DIM], x[DIM], xin[DIM];
+    constexpr int NV = 1 << DIM, AFF = Dims<DIM>::AFF;
+    int32_t vids[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) vids[v] = __ldg(m.cv + (size_t)c * NV + v);
+    double X[NV][DIM], x[DIM], xin[DIM];
     load_cell64<DIM>(m.cellX, c, X);
     fwd64<DIM>(X, xo.v, x);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) x[d] = x[d] + ue.v[d] * dtp;
     const int st = LIN ? inverse_affine64<DIM>(m.aff + (size_t)c * AFF, x, xin)
                        : inverse_map64<DIM>(X, m.aff + (size_t)c * AFF, x, xin);
+    SearchOut out;
+    out.cell = c;
+    out.flags = 0;
+    out.map_failures = st ? 1u : 0u;
     if (st == 0 && inside_unit<DIM>(xin)) {
-        SearchOut out;
-        out.cell = c;
         out.flags = SRCH_FOUND | (near_face64<DIM>(xin) ? SRCH_NEAR : 0u);
-        out.map_failures = 0;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) out.xi[d] = xin[d];
         return out;
     }
-    Vec<DIM> xp;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) xp.v[d] = x[d];
-    SearchOut out = search64<DIM, LIN>(m, c, xo, ue, xp);
-    out.map_failures += st ? 1u : 0u;
+    for (int v = 0; v < NV; ++v) prefetch_l1(m.v2c_off + vids[v]);
+    int cvx = 0;
+    {
+        double old[DIM];
+        fwd64<DIM>(X, xo.v, old);
+        double best = 0.0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            double ptv[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) ptv[d] = X[v][d] - old[d];
+            double dot = ue.v[0] * ptv[0];
+#pragma unroll
+            for (int d = 1; d < DIM; ++d) dot = dot + ue.v[d] * ptv[d];
+            const double ang = dot * rsqrt(norm2_64<DIM>(ptv));
+            if (v == 0) best = ang;
+            else if (ang > best) {
+                best = ang;
+                cvx = v;
+            }
+        }
+    }
+    int32_t vid = vids[0];
+#pragma unroll
+    for (int v = 1; v < NV; ++v) vid = cvx == v ? vids[v] : vid;
+    double vtp[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) vtp[d] = x[d] - X[cvx][d];
+    const int32_t b = __ldg(m.v2c_off + vid);
+    const int n = __ldg(m.v2c_off + vid + 1) - b;
+    if (n > REG_CAND) {
+        Vec<DIM> xp;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xp.v[d] = x[d];
+        SearchOut o2 = search64<DIM, LIN>(m, c, xo, ue, xp);
+        o2.map_failures += out.map_failures;
+        return o2;
+    }
+    double dk[REG_CAND];
+    uint32_t ck[REG_CAND];
+#pragma unroll
+    for (int k = 0; k < REG_CAND; ++k) {
+        dk[k] = 0.0;
+        ck[k] = c;
+        if (k < n) {
+            const double* cd = m.v2c_dirs + (size_t)(b + k) * DIM;
+            double sdot = __ldg(cd) * vtp[0];
+#pragma unroll
+            for (int d = 1; d < DIM; ++d) sdot = sdot + __ldg(cd + d) * vtp[d];
+            dk[k] = sdot;
+            ck[k] = (uint32_t)__ldg(m.v2c_cells + b + k);
+        }
+    }
+    uint32_t tried = 0;
+    for (int t = 0; t < n; ++t) {
+        int bi = -1;
+        double bv = 0.0;
+        uint32_t cand = c;
+#pragma unroll
+        for (int k = 0; k < REG_CAND; ++k) {
+            const bool open = k < n && !((tried >> k) & 1u);
+            if (open && (bi < 0 || dk[k] > bv)) {
+                bi = k;
+                bv = dk[k];
+                cand = ck[k];
+            }
+        }
+        tried |= 1u << bi;
+        if (cand == c) continue;
+        double xc[DIM];
+        int sc;
+        if constexpr (LIN) {
+            sc = inverse_affine64<DIM>(m.aff + (size_t)cand * AFF, x, xc);
+        } else {
+            load_cell64<DIM>(m.cellX, cand, X);
+            sc = inverse_map64<DIM>(X, m.aff + (size_t)cand * AFF, x, xc);
+        }
+        if (sc) {
+            out.map_failures++;
+            continue;
+        }
+        if (inside_unit<DIM>(xc)) {
+            out.cell = cand;
+            out.flags |= SRCH_FOUND | (near_face64<DIM>(xc) ? SRCH_NEAR : 0u);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) out.xi[d] = xc[d];
+            return out;
+        }
+    }
     return out;
 }
 
@@ -923,6 +1042,7 @@ __device__ __forceinline__ void cross32(const StepArgs& a)
         for (int d = 0; d < DIM; ++d) xi[d] = ((const float*)a.T.xi[d])[i];
         bool alive = true;
         while (true) {
+            prefetch_cell64<DIM>(m, c);
             Vec<DIM> xo, ue;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) xo.v[d] = (double)xi[d];

@@ -1019,26 +1019,37 @@ __device__ __forceinline__ void load4(const double* p, double* q)
 // DoF gather: V_d = sum num_d / sum den over the cells sharing the DoF, in
 // ascending cell order, FP64 sums and division (0/0 -> NaN as the reference,
 // or the kept input value under empty_dof_policy 1).  Up to 8 cell entries
-// are fetched before any is summed.
+// are fetched before any is summed; a thread's first DoF's entries (mesh
+// data) are fetched before the kernel waits for the write pass.
 template <int DIM, typename PReal>
 __global__ void k_gather(StepArgs a, int keep_empty)
 {
-    pdl_entry();
     constexpr int NV = 1 << DIM, PW = Dims<DIM>::PW;
-    const PReal* P = reinterpret_cast<const PReal*>(a.partials);
-    unsigned long long nan_dofs = 0;
     const int stride = gridDim.x * blockDim.x;
     const int nloop = (a.mesh.nD + stride - 1) / stride * stride;
-    for (int dof = blockIdx.x * blockDim.x + threadIdx.x; dof < nloop; dof += stride) {
+    const int dof0 = blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t b0 = 0, e0 = 0, ent0[8];
+    if (dof0 < a.mesh.nD) {
+        b0 = __ldg(a.mesh.d2c_off + dof0);
+        e0 = __ldg(a.mesh.d2c_off + dof0 + 1);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) ent0[j] = b0 + j < e0 ? __ldg(a.mesh.d2c_ent + b0 + j) : -1;
+    pdl_entry();
+    const PReal* P = reinterpret_cast<const PReal*>(a.partials);
+    unsigned long long nan_dofs = 0;
+    for (int dof = dof0; dof < nloop; dof += stride) {
         if (dof >= a.mesh.nD) continue;
         double num[DIM], den = 0.0;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) num[d] = 0.0;
-        const int32_t b = __ldg(a.mesh.d2c_off + dof), e = __ldg(a.mesh.d2c_off + dof + 1);
+        const bool first = dof == dof0;
+        const int32_t b = first ? b0 : __ldg(a.mesh.d2c_off + dof), e = first ? e0 : __ldg(a.mesh.d2c_off + dof + 1);
         for (int32_t k0 = b; k0 < e; k0 += 8) {
             int32_t ent[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) ent[j] = k0 + j < e ? __ldg(a.mesh.d2c_ent + k0 + j) : -1;
+            for (int j = 0; j < 8; ++j)
+                ent[j] = first && k0 == b ? ent0[j] : k0 + j < e ? __ldg(a.mesh.d2c_ent + k0 + j) : -1;
             PReal q[8][4];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
