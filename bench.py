@@ -66,8 +66,8 @@ STEP_BYTES = {"fp32": 5 * (4 + 24) + 8, "fp64": 5 * (4 + 48) + 8}
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one write-pass
 # launch on this workload, from an ncu capture taken apart from the timed
 # run (a profiler cannot run inside it); the line names it as such.
-TRAFFIC_WRITE = 202.1e6
-TRAFFIC_SRC = "ncu dram bytes of one k_write launch, separate capture"
+TRAFFIC_WRITE = 203.3e6
+TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_write launch (time step 4), separate capture"
 
 
 def reduce_over_ranks(ms, particle_steps, world, device):
