@@ -101,6 +101,7 @@ int launch_fill_u32(uint32_t* p, uint32_t n, uint32_t v, cudaStream_t s);
 int launch_set_state(DevStats* st, long long n, long long next_id, long long add_id, cudaStream_t s);
 int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const int32_t* cd, int nC, int nD, void* Vc,
                   void* dVc, double* Vcopy, cudaStream_t s);
+int launch_nonfinite(const double* v, size_t n, unsigned* flag, cudaStream_t s);
 int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
                       const float* jinv32, int nC, int nD, float* vrec, float* dvrec, double* Vcopy,
                       cudaStream_t s);

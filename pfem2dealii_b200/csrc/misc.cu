@@ -361,6 +361,30 @@ int launch_cell_v(int dim, int prec, const double* V, const double* Vold, const 
     return 1;
 }
 
+// Non-finite entries of an uploaded host vector (16-byte aligned, n doubles):
+// any sets *flag, a mapped host word the caller cleared.  One pass over the
+// vector in HBM replaces a host scan of it.
+__global__ void k_nonfinite(const double* __restrict__ v, size_t n, unsigned* flag)
+{
+    bool bad = false;
+    const size_t stride = (size_t)gridDim.x * blockDim.x, t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const double2* v2 = reinterpret_cast<const double2*>(v);
+    for (size_t i = t0; i < n / 2; i += stride) {
+        const double2 q = v2[i];
+        bad = bad || !isfinite(q.x) || !isfinite(q.y);
+    }
+    if (t0 == 0 && (n & 1)) bad = bad || !isfinite(v[n - 1]);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) *reinterpret_cast<volatile unsigned*>(flag) = 1u;
+}
+
+int launch_nonfinite(const double* v, size_t n, unsigned* flag, cudaStream_t s)
+{
+    const size_t g = (n / 2 + 255) / 256;
+    const int grid = g < 1 ? 1 : (g > 148 * 8 ? 148 * 8 : (int)g);
+    k_nonfinite<<<grid, 256, 0, s>>>(v, n, flag);
+    return 1;
+}
+
 int launch_cell_rec32(int dim, const double* V, const double* Vold, const int32_t* cd, const double* aff,
                       const float* jinv32, int nC, int nD, float* vrec, float* dvrec, double* Vcopy, cudaStream_t s)
 {
