@@ -154,6 +154,83 @@ public:
     void correct_particle_velocity(const double* V, const double* Vold) { check(pfem2gpu_correct(h_, V, Vold), h_); }
     void move_particles(const double* V) { check(pfem2gpu_move(h_, V), h_); }
     void project_particle_fields(double* V_out) { check(pfem2gpu_project(h_, V_out), h_); }
+    // correct_particle_velocity with Vold = the last projection, kept on the
+    // device (fem_step copies the projection into the old solution,
+    // src/pfem2fem.cpp:523-524): only V crosses the boundary.
+    void correct_particle_velocity_from_projection(const double* V)
+    {
+        check(pfem2gpu_correct_from_projection(h_, V), h_);
+    }
+
+    // Cell-range partitions: this handle owns the particles of cells
+    // [cell_begin, cell_end) of the mesh (the reference's distribution of the
+    // cells over MPI ranks); a move runs in three phases around the caller's
+    // exchange, the reference's send_recv_particles
+    // (src/pfem2particlehandler.cpp:480-502,507-618), and the projection
+    // needs the partial sums of the cells that share a DoF with this handle's
+    // cells (:202-205).  See include/pfem2gpu.h for the ids to pass.
+    struct Exchange {
+        std::vector<uint32_t> id;
+        std::vector<int32_t> cell;
+        std::vector<double> x, xi, v;  // n x dim, row-major
+        size_t size() const { return id.size(); }
+        void resize(size_t n)
+        {
+            id.resize(n);
+            cell.resize(n);
+            x.resize(n * dim);
+            xi.resize(n * dim);
+            v.resize(n * dim);
+        }
+    };
+    void set_partition(int64_t cell_begin, int64_t cell_end)
+    {
+        initialize_maps();
+        check(pfem2gpu_set_partition(h_, cell_begin, cell_end), h_);
+    }
+    // Phases 1 and 2a: correction, sub-steps and relocation; returns the
+    // particles that ended in other partitions' cells (they leave this
+    // handle).  V null: the staged velocity.
+    Exchange move_exchange_begin(const double* V)
+    {
+        int64_t n = 0, got = 0;
+        check(pfem2gpu_move_exchange_begin(h_, V, &n), h_);
+        Exchange out;
+        out.resize((size_t)n);
+        check(pfem2gpu_move_outbox(h_, out.id.data(), out.cell.data(), out.x.data(), out.xi.data(), out.v.data(), n,
+                                   &got),
+              h_);
+        return out;
+    }
+    // Phase 2b: the particles other partitions sent to this handle's cells;
+    // returns the number of particles count correction will add here.
+    int64_t move_inbox(const Exchange& in)
+    {
+        int64_t seeds = 0;
+        check(pfem2gpu_move_inbox(h_, (int64_t)in.size(), in.id.data(), in.cell.data(), in.x.data(), in.xi.data(),
+                                  in.v.data(), &seeds),
+              h_);
+        return seeds;
+    }
+    // Phase 3: count correction and the new layout; new particles get ids
+    // first_id + 1, ..., the handle's next id becomes next_id.
+    void move_exchange_end(uint32_t first_id, uint32_t next_id)
+    {
+        check(pfem2gpu_move_exchange_end(h_, first_id, next_id), h_);
+    }
+    // Projection partial sums of cells, (4 << dim) doubles per cell.
+    std::vector<double> get_partials(const std::vector<int32_t>& cells)
+    {
+        std::vector<double> out(cells.size() * (4u << dim));
+        check(pfem2gpu_get_partials(h_, (int64_t)cells.size(), cells.data(), out.data()), h_);
+        return out;
+    }
+    void set_partials(const std::vector<int32_t>& cells, const std::vector<double>& values)
+    {
+        if (values.size() != cells.size() * (4u << dim))
+            throw Error(PFEM2GPU_ERR_ARG, "pfem2gpu: set_partials needs (4 << dim) values per cell");
+        check(pfem2gpu_set_partials(h_, (int64_t)cells.size(), cells.data(), values.data()), h_);
+    }
 
     // output_particle_solution (:218-317) for one rank: particles-NN.000.vtu + particles-NN.pvtu.
     void output_particle_solution(int timestep_number, const std::string& directory = ".")
