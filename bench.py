@@ -154,7 +154,7 @@ class Case:
         self.name, self.mesh, self.V, self.prm, self.noise, self.text = name, mesh, V, prm, noise, text
 
 
-def build_case(name="duct"):
+def build_case(name="duct", cube_n=80):
     from pfem2dealii_b200 import mesh as M
     from pfem2dealii_b200.handler import ParticleParams
 
@@ -166,11 +166,11 @@ def build_case(name="duct"):
         return Case(name, m, V, prm, 0.01, f"2D Turek channel, Mesh3.unv ({m.n_cells} Q1 quads), 16 ppc, "
                                            "max 2/part, 3 sub-steps, dt 5e-4, Umax 1.5, N(0,0.01) noise")
     if name == "cube":
-        m = M.perturbed_cube(80, amplitude=0.1, seed=0)
+        m = M.perturbed_cube(cube_n, amplitude=0.1, seed=0)
         V = M.field_at_dofs(m, M.taylor_green_3d())
         prm = ParticleParams(particles_per_cell=(4, 4, 4), max_particles_per_cell_part=2,
                              particle_integration_steps=3, time_step=1e-3)
-        return Case(name, m, V, prm, 0.0, "3D cube [0,2pi]^3 80^3 hexes perturbed +-0.1h, 64 ppc, "
+        return Case(name, m, V, prm, 0.0, f"3D cube [0,2pi]^3 {cube_n}^3 hexes perturbed +-0.1h, 64 ppc, "
                                           "max 2/part, 3 sub-steps, dt 1e-3, Taylor-Green u")
     m = M.hyper_rectangle((0.0, 0.0, 0.0), (8.0, 1.0, 1.0), (128, 32, 32), "duct")
     V = M.field_at_dofs(m, M.duct_profile(1.0))
@@ -532,6 +532,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-extra", action="store_true", help="headline workload only (no cfg2/cfg4/cfg5 reports)")
+    ap.add_argument("--cube-n", type=int, default=80,
+                    help="cells per edge of the cube workload (smaller for profiler captures; 80 = config 5)")
     ap.add_argument("--workload", choices=["duct", "cube", "turek"], default="duct",
                     help="with --only/--adjoint-only: duct (the headline), cube (32.8 M particles) or turek "
                          "(Mesh3.unv, 0.97 M particles)")
@@ -564,7 +566,7 @@ def main():
         torch.cuda.set_device(0)
     from pfem2dealii_b200.handler import ParticleHandler as H
 
-    case = build_case(args.workload if (args.only or args.adjoint_only or args.fem_only) else "duct")
+    case = build_case(args.workload if (args.only or args.adjoint_only or args.fem_only) else "duct", args.cube_n)
     noisy = noisy_particles(case, H) if case.noise else None
     if args.adjoint_only:
         rep = adjoint_report(H, case, torch, K=10 if case.name == "cube" else 20, start_particles=noisy)
