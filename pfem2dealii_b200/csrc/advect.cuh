@@ -872,6 +872,70 @@ __device__ __noinline__ F3<DIM> newton32(const float* __restrict__ geo, uint32_t
     return out;
 }
 
+// Euler sub-steps s0.. of a particle in a non-affine cell (FP32 form), out of
+// line: the cell's FP32 geometry is loaded and its inverse Jacobian at the
+// particle's start taken once, and every sub-step solves
+// x(xi + d) - x(xi) = u dt_p by the chord iteration with that inverse (a
+// particle moves a few hundredths of the cell per sub-step, so the
+// iteration still contracts by the cell's twist times that distance).  The
+// sub-step that leaves the cell, or whose solve does not settle, is returned
+// (S if none) with xi where it stopped; the caller relocates it in FP64.
+template <int DIM>
+struct SubOut {
+    float xi[DIM];
+    int s;
+};
+
+template <int DIM>
+__device__ __noinline__ SubOut<DIM> twisted_substeps32(const float* __restrict__ geo, uint32_t c, int s0, int S,
+                                                       float dtp, const Rec32<DIM> r, F3<DIM> x0)
+{
+    Geo32<DIM> g;
+    load_geo32<DIM>(geo, c, g);
+    SubOut<DIM> out;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) out.xi[d] = x0.v[d];
+    out.s = s0;
+    float J[DIM][DIM], Ji[DIM][DIM];
+    jac32<DIM>(g, out.xi, J);
+    if (!(invert32<DIM>(J, Ji) > 0.0f)) return out;
+    for (; out.s < S; ++out.s) {
+        float w[DIM], dx[DIM], dl[DIM], y[DIM];
+        eval_poly<DIM>(r.b, out.xi, w);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) dx[d] = w[d] * dtp;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            float t = 0.0f;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) t += Ji[k][d] * dx[d];
+            dl[k] = t;
+        }
+        bool ok = g.affine;
+        for (int it = 0; it < 8 && !ok; ++it) {
+            float q[DIM];
+            delta32<DIM>(g, out.xi, dl, q);
+            float mx = 0.0f;
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) {
+                float t = 0.0f;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) t += Ji[k][d] * (q[d] - dx[d]);
+                dl[k] -= t;
+                mx = fmaxf(mx, fabsf(t));
+            }
+            ok = mx <= 2e-7f;
+        }
+        if (!ok) break;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) y[d] = out.xi[d] + dl[d];
+        if (!inside_unit<DIM>(y)) break;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) out.xi[d] = y[d];
+    }
+    return out;
+}
+
 // RK2 midpoint of a non-affine cell in the FP32 form: xi + (h/2) J(xi)^-1 u
 // with the cell's FP32 geometry, out of line (by value); xi itself when the
 // Jacobian determinant is not positive.
@@ -902,6 +966,17 @@ template <int DIM, bool AFF = false, bool RK = false>
 __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0, float* xi, const Rec32<DIM>& r)
 {
     const float dtp = (float)a.pp.dtp;
+    if constexpr (!AFF && !RK) {
+        if (!r.affine) {
+            F3<DIM> x0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) x0.v[d] = xi[d];
+            const SubOut<DIM> o = twisted_substeps32<DIM>(a.mesh.geo32, c, s0, a.pp.S, dtp, r, x0);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) xi[d] = o.xi[d];
+            return o.s;
+        }
+    }
     int s = s0;
     for (; s < a.pp.S; ++s) {
         float w[DIM], dl[DIM], y[DIM];
