@@ -240,7 +240,7 @@ __device__ __forceinline__ void store_rec(float* r, const float* w, float flag)
 constexpr int REC_TILE = 128;
 
 template <int DIM>
-__global__ void __launch_bounds__(REC_TILE) k_cell_rec32(const double* __restrict__ V, const double* __restrict__ Vold,
+__global__ void __launch_bounds__(REC_TILE, 4) k_cell_rec32(const double* __restrict__ V, const double* __restrict__ Vold,
                                                          const int32_t* __restrict__ cd, const double* __restrict__ aff,
                                                          const float* __restrict__ jinv32, int nC, int nD,
                                                          float* __restrict__ vrec, float* __restrict__ dvrec,
