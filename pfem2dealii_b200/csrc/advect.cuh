@@ -872,6 +872,37 @@ __device__ __noinline__ F3<DIM> newton32(const float* __restrict__ geo, uint32_t
     return out;
 }
 
+// A sub-step that moves a particle by less than 2^-46 (1.4e-14) of its
+// cell in every reference direction is taken as no motion.  The FP64 form,
+// like the reference, advances the physical position, and at |x| / h of
+// 10^2..10^3 cells its rounding leaves x unchanged for such a step: a
+// particle that the flow drives into a no-slip wall stops about 1e-14 of a
+// cell from it and stays in its cell.  The FP32 form's reference coordinate
+// would instead keep shrinking into subnormal floats, where the increment
+// keeps only a few bits and can come out with the wrong sign; the particle
+// then lands outside its cell, and the FP64 relocation finds it just beyond
+// the wall and drops it while the FP64 form holds it at rest.  Such particles
+// carry large velocities (the correction pulls them towards the wall's zero
+// velocity step after step while they no longer move), so dropping one moves
+// the projection at the wall's DoFs by up to 1e-1.  Affine cells need no
+// pin: towards a xi = 0 wall their increment is a product of the coordinate
+// itself (the face's velocity terms are exact zeros), which rounds towards
+// the face but never past it, and towards a xi = 1 wall the spacing of FP32
+// numbers below 1 (6e-8) stops the particle long before subnormals.
+constexpr float XI_PIN = 1.4210855e-14f;
+
+template <int DIM>
+__device__ __forceinline__ void pin32(float* dl)
+{
+    float m = 0.0f;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) m = fmaxf(m, fabsf(dl[d]));
+    if (m < XI_PIN) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) dl[d] = 0.0f;
+    }
+}
+
 // Euler sub-steps s0.. of a particle in a non-affine cell (FP32 form), out of
 // line: the cell's FP32 geometry is loaded and its inverse Jacobian at the
 // particle's start taken once, and every sub-step solves
@@ -927,6 +958,7 @@ __device__ __noinline__ SubOut<DIM> twisted_substeps32(const float* __restrict__
             ok = mx <= 2e-7f;
         }
         if (!ok) break;
+        pin32<DIM>(dl);
 #pragma unroll
         for (int d = 0; d < DIM; ++d) y[d] = out.xi[d] + dl[d];
         if (!inside_unit<DIM>(y)) break;
@@ -1015,6 +1047,7 @@ __device__ __forceinline__ int substeps32(const StepArgs& a, uint32_t c, int s0,
 #pragma unroll
             for (int d = 0; d < DIM; ++d) dl[d] = res.v[d];
         }
+        if (!(AFF || r.affine)) pin32<DIM>(dl);
 #pragma unroll
         for (int d = 0; d < DIM; ++d) y[d] = xi[d] + dl[d];
         if (!(ok && inside_unit<DIM>(y))) break;

@@ -283,12 +283,19 @@ template <int DIM, typename Real>
 __device__ __forceinline__ int ext_part(const Real* xi, const PartParams& pp)
 {
     if constexpr (sizeof(Real) == 4) {
-        // FP32 form: (int)(xi * q) in FP32
+        // FP32 form: (int)(xi * q) in FP32, at most q - 1.  A stored FP32
+        // xi_d of exactly 1 stands for every inside point within 3e-8 of the
+        // upper face, where the FP64 form (and the reference) has xi_d < 1
+        // and so part q - 1; only an xi_d of exactly 1 in FP64 reaches the
+        // extra part q.  Particles pile up there at no-slip walls that the
+        // flow runs into (the stagnation side of an obstacle): without the
+        // cap they fall out of part q - 1 in the FP32 form, which then seeds
+        // and removes differently from the FP64 form.
         int e = 0;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
             int k = (int)(xi[d] * (float)pp.q[d]);
-            k = k < 0 ? 0 : (k > pp.q[d] ? pp.q[d] : k);
+            k = k < 0 ? 0 : (k > pp.q[d] - 1 ? pp.q[d] - 1 : k);
             e = e * (pp.q[d] + 1) + k;
         }
         return e;
