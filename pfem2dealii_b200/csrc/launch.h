@@ -91,8 +91,8 @@ int launch_fem_constrain(int nD, long long nnz, int nm, int ns, const int32_t* r
                          const int32_t* con_idx, int n_con, const double* g, double* A, double* rhs, cudaStream_t s);
 
 // misc.cu
-constexpr int SCAN_TILE = 1024;       // cells per tile of the slot-offset scan
-constexpr int SCAN_MAX_TILES = 8192;  // tile sums the scan buffer holds
+constexpr int SCAN_TILE = 512;        // cells per tile of the slot-offset scan
+constexpr int SCAN_MAX_TILES = 16384; // tile sums the scan buffer holds
 // Slots per cell (count + new particles) into cub, their exclusive scan into
 // coff (coff[nC] = totals); two kernels.
 int launch_slots_scan(const StepArgs& a, unsigned long long* tiles, cudaStream_t s);

@@ -10,7 +10,7 @@ namespace pfem2 {
 
 namespace {
 
-constexpr int SB = 1024;             // scan block: one cell per thread
+constexpr int SB = 512;              // scan block: one cell per thread
 constexpr int SI = SCAN_TILE / SB;   // rows of SB cells per tile
 constexpr int STILE = SCAN_TILE;     // cells per tile
 
@@ -246,16 +246,22 @@ __global__ void __launch_bounds__(REC_TILE, 4) k_cell_rec32(const double* __rest
                                                          float* __restrict__ vrec, float* __restrict__ dvrec,
                                                          double* __restrict__ Vcopy, size_t ncopy)
 {
-    pdl_entry();
-    copy_v(V, Vcopy, ncopy);
     constexpr int NV = 1 << DIM, F = Dims<DIM>::REC4 * 4, F4 = Dims<DIM>::REC4, AFF = Dims<DIM>::AFF;
     __shared__ __align__(16) float rec_s[2][REC_TILE * F];
+    // the first tile's cell DoFs are mesh data, which no kernel of the step
+    // writes: loaded before the wait on the previous kernel, so only the
+    // velocity loads remain after it (the copy of V goes last)
+    const int cf = blockIdx.x * REC_TILE + threadIdx.x;
+    int dof0[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) dof0[k] = cf < nC ? __ldg(cd + (size_t)cf * NV + k) : 0;
+    pdl_entry();
     for (int c0 = blockIdx.x * REC_TILE; c0 < nC; c0 += gridDim.x * REC_TILE) {
         const int c = c0 + threadIdx.x;
         if (c < nC) {
             int dof[NV];
 #pragma unroll
-            for (int k = 0; k < NV; ++k) dof[k] = __ldg(cd + (size_t)c * NV + k);
+            for (int k = 0; k < NV; ++k) dof[k] = c == cf ? dof0[k] : __ldg(cd + (size_t)c * NV + k);
             double f[NV][DIM], g[NV][DIM];
 #pragma unroll
             for (int k = 0; k < NV; ++k)
@@ -310,6 +316,7 @@ __global__ void __launch_bounds__(REC_TILE, 4) k_cell_rec32(const double* __rest
         }
         __syncthreads();
     }
+    copy_v(V, Vcopy, ncopy);
 }
 
 int grid_for(const void* k, int threads) { return occupancy_grid(k, threads); }
