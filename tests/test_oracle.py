@@ -3,7 +3,8 @@
 The reference ships no tests or golden data, so the oracle is pinned by
 mathematics: Q1 reproduction, exact Euler transport on affine cells,
 partition of unity in the projection, the seeding pattern, the count cap
-(max+1 survivors per part, src/pfem2particlehandler.cpp:372) and
+(max+1 survivors per part, src/pfem2particlehandler.cpp:372), the
+relocation's search confined to the cells around the closest vertex, and
 inverse/forward map round trips.
 """
 import io
@@ -114,6 +115,41 @@ def test_uniform_flow_is_exact_on_affine_cells(dim):
     xq = np.einsum("pi,pid->pd", np.array([shape_values(dim, z) for z in P1["xi"]]), X)
     assert np.allclose(xq, P1["x"], atol=1e-13)
     assert np.all((P1["xi"] >= 0) & (P1["xi"] <= 1))
+
+
+@pytest.mark.parametrize("shift, survivors", [(0.7, "neighbour"), (1.7, "none")])
+def test_relocation_searches_only_the_closest_vertex_patch(shift, survivors):
+    """One particle per cell at its centre, a uniform flow along x moving each
+    by `shift` cells in one sub-step.  0.7 cells: every particle leaves its
+    cell through the face ahead and is found in the next cell, which holds
+    the vertices of that face (src/pfem2particlehandler.cpp:413-503 with
+    src/pfem2particle.cpp:186-211); the last column leaves the mesh.  1.7
+    cells: the particle lands two cells ahead, outside the cells around the
+    closest vertex of its old cell, and is deleted although it is inside
+    the mesh: the reference searches no further."""
+    nx, ny, h = 8, 2, 0.5
+    m = M.hyper_rectangle((0.0, 0.0), (nx * h, ny * h), (nx, ny))
+    u = shift * h / 0.1
+    V = np.repeat(np.array([u, 0.0])[:, None], m.n_dofs, axis=1)
+    o = Oracle(m, (1, 1), 100, 1, 0.1)
+    o.seed(V)
+    P0 = o.particles()
+    o.move(V)
+    P1 = o.particles()
+    st = o.stats()
+    if survivors == "neighbour":
+        assert st["lost"] == ny
+        assert len(P1["id"]) == (nx - 1) * ny
+        for i, c in zip(P1["id"], P1["cell"]):
+            c0 = P0["cell"][P0["id"] == i][0]
+            x0 = m.vertices[m.cells[c0]].mean(0)
+            xc = m.vertices[m.cells[c]]
+            assert np.all(xc.min(0) <= x0 + [shift * h, 0.0]) and np.all(x0 + [shift * h, 0.0] <= xc.max(0))
+            assert np.isclose(xc.min(0)[0] - x0[0], 0.5 * h)  # the next cell along x
+        assert np.allclose(P1["xi"][:, 0], 0.2, atol=1e-12)
+    else:
+        assert len(P1["id"]) == 0
+        assert st["lost"] == nx * ny
 
 
 def test_projection_partition_of_unity():
