@@ -357,6 +357,47 @@ def test_native_unv_reader_errors(tmp_path):
     assert b"2D" in L.pfem2gpu_read_unv_error()
 
 
+MESH2 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "Mesh2.tgz")
+
+
+def test_native_unv_reader_reference_mesh2():
+    """The mesh the reference's own Turek case reads (cases/TurekBenchmark/
+    Mesh2.tgz, its input_data.prm: `Mesh file name = Mesh2.unv`), committed
+    as a fixture: both readers agree and give the 2.2 x 0.41 channel."""
+    a = M.read_unv(MESH2)
+    b = M.read_unv_native(MESH2)
+    assert np.array_equal(a.vertices, b.vertices) and np.array_equal(a.cells, b.cells)
+    assert a.n_cells == 19700 and a.n_verts == 20060
+    assert np.allclose(a.vertices.min(0), [0, 0]) and np.allclose(a.vertices.max(0), [2.2, 0.41])
+
+
+def test_uniform_flow_on_the_reference_turek_case():
+    """Mesh2 with the particle settings of the reference's Turek case
+    (input_data.prm: 2 x 2 particles per cell, at most 5 per part, 3
+    integration steps, time step 0.001) in a uniform field u = (1, -0.2):
+    every particle carries u, so each projected DoF is u up to rounding
+    (partition of unity), and every particle that stays in the mesh moves by
+    exactly u dt in the FP64 position, whatever the cell's shape."""
+    m = M.read_unv_native(MESH2)
+    u = np.array([1.0, -0.2])
+    V = np.repeat(u[:, None], m.n_dofs, axis=1)
+    o = Oracle(m, (2, 2), 5, 3, 1e-3)
+    o.seed(V)
+    Vold = o.project()
+    for _ in range(3):
+        P0 = o.particles()
+        Vold = o.step(V, Vold)
+        P1 = o.particles()
+        common, i0, i1 = np.intersect1d(P0["id"], P1["id"], return_indices=True)
+        assert len(common) > 0.99 * len(P0["id"])
+        assert np.allclose(P1["x"][i1] - P0["x"][i0], u * 1e-3, rtol=0, atol=1e-15)
+        assert np.all((P1["xi"] >= 0) & (P1["xi"] <= 1))
+        assert np.allclose(P1["v"], u, rtol=0, atol=1e-15)
+        f = np.isfinite(Vold[0])
+        assert f.mean() > 0.99
+        assert np.allclose(Vold[:, f], u[:, None], rtol=0, atol=1e-14)
+
+
 def test_native_unv_reader_reference_mesh():
     a = M.read_unv(MESH3)
     b = M.read_unv_native(MESH3)
