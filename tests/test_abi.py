@@ -2,6 +2,7 @@
 header declares, rejects bad arguments, and reports a missing device with
 an error code instead of crashing."""
 import ctypes as C
+import os
 import subprocess
 
 import pytest
@@ -73,3 +74,20 @@ end
     p = read_prm(text)
     assert p.particles_per_cell == (3, 2, 4)
     assert p.max_particles_per_cell_part == 5 and p.particle_integration_steps == 3 and p.time_step == 0.005
+
+
+@pytest.mark.parametrize("case, q, maxpp, S, dt", [
+    ("TurekBenchmark", (2, 2, 2), 5, 3, 0.001),
+    ("PoiseuilleFlow3D", (2, 2, 2), 5, 3, 0.005),
+    ("nacaAirfoil", (2, 2, 2), 5, 3, 0.001),
+])
+def test_read_prm_reference_cases(case, q, maxpp, S, dt):
+    """The reference's own case files (cases/*/input_data.prm, committed as
+    fixtures): the particle keys and the time step as its parameter handler
+    reads them (src/pfem2parameterhandler.cpp:64-72,131-137); a missing z count is 2, its
+    default, and a 2D handle uses the first two."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "prm", case + ".prm")
+    p = read_prm(path)
+    assert p.particles_per_cell == q
+    assert p.max_particles_per_cell_part == maxpp and p.particle_integration_steps == S and p.time_step == dt
+
