@@ -145,12 +145,14 @@ def test_fp32_vs_fp64_config3_duct_100_steps():
 def test_fp32_vs_fp64_config2_every_step():
     """Configuration 2 with both forms side by side: the FP32 form's
     projected velocity after each of 200 steps against the FP64 form's.
-    Most steps differ by about 1e-6; a few differ by up to a few 1e-4, where
-    particles on the cylinder's upstream stagnation streamline pass on
-    different sides of the cylinder in the two forms (the split of two
-    trajectories that start 1e-7 apart grows without bound there) and reach
-    the few wall DoFs first.  Measured on a B200: median 1.2e-6, 6 of 210
-    steps above 1e-4, maximum 2.7e-4."""
+    Most steps differ by about 1e-6; a few differ by up to a few 1e-4 at
+    the DoFs on the cylinder's upstream wall.  The fixed inflow field drives
+    particles head-on into the cylinder, they pile up in the wall cells, the
+    count correction removes most of them, and the survivors carry
+    velocities far from the field's (the correction keeps pulling them while
+    they no longer move); the forms keep different survivors there now and
+    then.  Measured on a B200: median 1.2e-6, 6 of 210 steps above 1e-4,
+    maximum 2.7e-4."""
     import torch
 
     case = cases.turek_mesh3()
