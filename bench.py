@@ -27,7 +27,9 @@ Line keys beyond the base contract:
            the step of the maximum, steps above 1e-4)
   cfg4     the differentiated window (K = 20, checkpoints every 5) on the
            same case: forward/backward time of both forms and the gradient
-           along the inflow amplitude against FP64 central differences
+           along the inflow amplitude against FP64 central differences (64
+           probe DoFs off the no-slip walls, drawn from the FP64 window and
+           used by both forms)
   cfg5     the perturbed 80^3 cube (32.8 M particles): both forms, their
            difference, and the K = 10 window's backward/forward ratio
 Longer per-kernel, output, mesh-setup and FEM-assembly figures go to stderr
